@@ -1,0 +1,236 @@
+/* C ABI of the B200 simulation core.
+ *
+ * Every NeuronGPU_* entry point has the name, signature, argument meaning,
+ * return convention and error behaviour of the reference's C interface
+ * (golosio/NeuronGPU src/neurongpu_C.h; the line of each reference
+ * declaration is given beside it), so the reference's ctypes layer
+ * (pythonlib/neurongpu.py) or C++ programs linking -lneurongpu bind to this
+ * library unchanged. Errors: each call clears the error state; on failure the
+ * code is 2 (library error), 1 (allocation failure) or 255 (other), the
+ * message is kept for NeuronGPU_GetErrorMessage, and the process exits with
+ * that code unless NeuronGPU_SetOnException(1) was called. Arrays returned by
+ * Get* calls are allocated by the library and owned by the caller.
+ *
+ * The NGB200_* entry points at the end have no counterpart in the reference:
+ * they expose device counters and run-time controls of this build.
+ */
+#ifndef NEURONGPU_B200_C_H
+#define NEURONGPU_B200_C_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+char *NeuronGPU_GetErrorMessage();                          /* neurongpu_C.h:22 */
+unsigned char NeuronGPU_GetErrorCode();                     /* neurongpu_C.h:24 */
+void NeuronGPU_SetOnException(int on_exception);            /* neurongpu_C.h:26 */
+int NeuronGPU_SetRandomSeed(unsigned long long seed);       /* neurongpu_C.h:28 */
+int NeuronGPU_SetTimeResolution(float time_res);            /* neurongpu_C.h:30 */
+float NeuronGPU_GetTimeResolution();                        /* neurongpu_C.h:32 */
+int NeuronGPU_SetMaxSpikeBufferSize(int max_size);          /* neurongpu_C.h:34 */
+int NeuronGPU_GetMaxSpikeBufferSize();                      /* neurongpu_C.h:36 */
+int NeuronGPU_SetSimTime(float sim_time);                   /* neurongpu_C.h:38 */
+int NeuronGPU_SetVerbosityLevel(int verbosity_level);       /* neurongpu_C.h:40 */
+int NeuronGPU_Create(char *model_name, int n_neuron, int n_port);   /* :42 */
+int NeuronGPU_CreatePoissonGenerator(int n_node, float rate);       /* :44 */
+int NeuronGPU_CreateRecord(char *file_name, char *var_name_arr[],
+                           int *i_node_arr, int *port_arr, int n_node); /* :46 */
+int NeuronGPU_GetRecordDataRows(int i_record);              /* neurongpu_C.h:50 */
+int NeuronGPU_GetRecordDataColumns(int i_record);           /* neurongpu_C.h:52 */
+float **NeuronGPU_GetRecordData(int i_record);              /* neurongpu_C.h:54 */
+int NeuronGPU_SetNeuronScalParam(int i_node, int n_neuron, char *param_name,
+                                 float val);                /* neurongpu_C.h:56 */
+int NeuronGPU_SetNeuronArrayParam(int i_node, int n_neuron, char *param_name,
+                                  float *param, int array_size);    /* :59 */
+int NeuronGPU_SetNeuronPtScalParam(int *i_node, int n_neuron,
+                                   char *param_name, float val);    /* :63 */
+int NeuronGPU_SetNeuronPtArrayParam(int *i_node, int n_neuron,
+                                    char *param_name, float *param,
+                                    int array_size);                /* :66 */
+int NeuronGPU_IsNeuronScalParam(int i_node, char *param_name);      /* :70 */
+int NeuronGPU_IsNeuronPortParam(int i_node, char *param_name);      /* :72 */
+int NeuronGPU_IsNeuronArrayParam(int i_node, char *param_name);     /* :74 */
+int NeuronGPU_SetNeuronIntVar(int i_node, int n_neuron, char *var_name,
+                              int val);                     /* neurongpu_C.h:77 */
+int NeuronGPU_SetNeuronScalVar(int i_node, int n_neuron, char *var_name,
+                               float val);                  /* neurongpu_C.h:80 */
+int NeuronGPU_SetNeuronArrayVar(int i_node, int n_neuron, char *var_name,
+                                float *var, int array_size);        /* :83 */
+int NeuronGPU_SetNeuronPtIntVar(int *i_node, int n_neuron, char *var_name,
+                                int val);                   /* neurongpu_C.h:87 */
+int NeuronGPU_SetNeuronPtScalVar(int *i_node, int n_neuron, char *var_name,
+                                 float val);                /* neurongpu_C.h:90 */
+int NeuronGPU_SetNeuronPtArrayVar(int *i_node, int n_neuron, char *var_name,
+                                  float *var, int array_size);      /* :93 */
+int NeuronGPU_IsNeuronIntVar(int i_node, char *var_name);           /* :97 */
+int NeuronGPU_IsNeuronScalVar(int i_node, char *var_name);          /* :99 */
+int NeuronGPU_IsNeuronPortVar(int i_node, char *var_name);          /* :101 */
+int NeuronGPU_IsNeuronArrayVar(int i_node, char *var_name);         /* :103 */
+int NeuronGPU_GetNeuronParamSize(int i_node, char *param_name);     /* :105 */
+int NeuronGPU_GetNeuronVarSize(int i_node, char *var_name);         /* :107 */
+float *NeuronGPU_GetNeuronParam(int i_node, int n_neuron,
+                                char *param_name);          /* neurongpu_C.h:109 */
+float *NeuronGPU_GetNeuronPtParam(int *i_node, int n_neuron,
+                                  char *param_name);        /* neurongpu_C.h:112 */
+float *NeuronGPU_GetArrayParam(int i_node, char *param_name);       /* :115 */
+int *NeuronGPU_GetNeuronIntVar(int i_node, int n_neuron,
+                               char *param_name);           /* neurongpu_C.h:117 */
+int *NeuronGPU_GetNeuronPtIntVar(int *i_node, int n_neuron,
+                                 char *param_name);         /* neurongpu_C.h:120 */
+float *NeuronGPU_GetNeuronVar(int i_node, int n_neuron,
+                              char *param_name);            /* neurongpu_C.h:123 */
+float *NeuronGPU_GetNeuronPtVar(int *i_node, int n_neuron,
+                                char *param_name);          /* neurongpu_C.h:126 */
+float *NeuronGPU_GetArrayVar(int i_node, char *var_name);           /* :129 */
+int NeuronGPU_Calibrate();                                  /* neurongpu_C.h:131 */
+int NeuronGPU_Simulate();                                   /* neurongpu_C.h:133 */
+int NeuronGPU_StartSimulation();                            /* neurongpu_C.h:135 */
+int NeuronGPU_SimulationStep();                             /* neurongpu_C.h:137 */
+int NeuronGPU_EndSimulation();                              /* neurongpu_C.h:139 */
+int NeuronGPU_ConnectMpiInit(int argc, char *argv[]);       /* neurongpu_C.h:141 */
+int NeuronGPU_MpiId();                                      /* neurongpu_C.h:143 */
+int NeuronGPU_MpiNp();                                      /* neurongpu_C.h:145 */
+int NeuronGPU_ProcMaster();                                 /* neurongpu_C.h:147 */
+int NeuronGPU_MpiFinalize();                                /* neurongpu_C.h:149 */
+unsigned int *NeuronGPU_RandomInt(size_t n);                /* neurongpu_C.h:151 */
+float *NeuronGPU_RandomUniform(size_t n);                   /* neurongpu_C.h:153 */
+float *NeuronGPU_RandomNormal(size_t n, float mean, float stddev);  /* :155 */
+float *NeuronGPU_RandomNormalClipped(size_t n, float mean, float stddev,
+                                     float vmin, float vmax,
+                                     float vstep);          /* neurongpu_C.h:157 */
+int NeuronGPU_Connect(int i_source_node, int i_target_node,
+                      unsigned char port, unsigned char syn_group,
+                      float weight, float delay);           /* neurongpu_C.h:160 */
+int NeuronGPU_ConnSpecInit();                               /* neurongpu_C.h:164 */
+int NeuronGPU_SetConnSpecParam(char *param_name, int value);        /* :166 */
+int NeuronGPU_ConnSpecIsParam(char *param_name);            /* neurongpu_C.h:168 */
+int NeuronGPU_SynSpecInit();                                /* neurongpu_C.h:170 */
+int NeuronGPU_SetSynSpecIntParam(char *param_name, int value);      /* :172 */
+int NeuronGPU_SetSynSpecFloatParam(char *param_name, float value);  /* :174 */
+int NeuronGPU_SetSynSpecFloatPtParam(char *param_name,
+                                     float *array_pt);      /* neurongpu_C.h:176 */
+int NeuronGPU_SynSpecIsIntParam(char *param_name);          /* neurongpu_C.h:178 */
+int NeuronGPU_SynSpecIsFloatParam(char *param_name);        /* neurongpu_C.h:180 */
+int NeuronGPU_SynSpecIsFloatPtParam(char *param_name);      /* neurongpu_C.h:182 */
+int NeuronGPU_ConnectSeqSeq(int i_source, int n_source, int i_target,
+                            int n_target);                  /* neurongpu_C.h:184 */
+int NeuronGPU_ConnectSeqGroup(int i_source, int n_source, int *i_target,
+                              int n_target);                /* neurongpu_C.h:187 */
+int NeuronGPU_ConnectGroupSeq(int *i_source, int n_source, int i_target,
+                              int n_target);                /* neurongpu_C.h:190 */
+int NeuronGPU_ConnectGroupGroup(int *i_source, int n_source, int *i_target,
+                                int n_target);              /* neurongpu_C.h:193 */
+int NeuronGPU_RemoteConnectSeqSeq(int i_source_host, int i_source,
+                                  int n_source, int i_target_host,
+                                  int i_target, int n_target);      /* :196 */
+int NeuronGPU_RemoteConnectSeqGroup(int i_source_host, int i_source,
+                                    int n_source, int i_target_host,
+                                    int *i_target, int n_target);   /* :200 */
+int NeuronGPU_RemoteConnectGroupSeq(int i_source_host, int *i_source,
+                                    int n_source, int i_target_host,
+                                    int i_target, int n_target);    /* :204 */
+int NeuronGPU_RemoteConnectGroupGroup(int i_source_host, int *i_source,
+                                      int n_source, int i_target_host,
+                                      int *i_target, int n_target); /* :208 */
+char **NeuronGPU_GetIntVarNames(int i_node);                /* neurongpu_C.h:212 */
+char **NeuronGPU_GetScalVarNames(int i_node);               /* neurongpu_C.h:214 */
+int NeuronGPU_GetNIntVar(int i_node);                       /* neurongpu_C.h:216 */
+int NeuronGPU_GetNScalVar(int i_node);                      /* neurongpu_C.h:218 */
+char **NeuronGPU_GetPortVarNames(int i_node);               /* neurongpu_C.h:220 */
+int NeuronGPU_GetNPortVar(int i_node);                      /* neurongpu_C.h:222 */
+char **NeuronGPU_GetScalParamNames(int i_node);             /* neurongpu_C.h:224 */
+int NeuronGPU_GetNScalParam(int i_node);                    /* neurongpu_C.h:226 */
+char **NeuronGPU_GetPortParamNames(int i_node);             /* neurongpu_C.h:228 */
+int NeuronGPU_GetNGroupParam(int i_node);                   /* neurongpu_C.h:230 */
+char **NeuronGPU_GetGroupParamNames(int i_node);            /* neurongpu_C.h:232 */
+int NeuronGPU_GetNPortParam(int i_node);                    /* neurongpu_C.h:234 */
+char **NeuronGPU_GetArrayParamNames(int i_node);            /* neurongpu_C.h:236 */
+int NeuronGPU_GetNArrayParam(int i_node);                   /* neurongpu_C.h:238 */
+char **NeuronGPU_GetArrayVarNames(int i_node);              /* neurongpu_C.h:240 */
+int NeuronGPU_GetNArrayVar(int i_node);                     /* neurongpu_C.h:242 */
+int *NeuronGPU_GetSeqSeqConnections(int i_source, int n_source, int i_target,
+                                    int n_target, int syn_group,
+                                    int *n_conn);           /* neurongpu_C.h:244 */
+int *NeuronGPU_GetSeqGroupConnections(int i_source, int n_source,
+                                      int *i_target, int n_target,
+                                      int syn_group, int *n_conn);  /* :247 */
+int *NeuronGPU_GetGroupSeqConnections(int *i_source, int n_source,
+                                      int i_target, int n_target,
+                                      int syn_group, int *n_conn);  /* :251 */
+int *NeuronGPU_GetGroupGroupConnections(int *i_source, int n_source,
+                                        int *i_target, int n_target,
+                                        int syn_group, int *n_conn); /* :255 */
+int NeuronGPU_GetConnectionStatus(int i_source, int i_group, int i_conn,
+                                  int *i_target, unsigned char *port,
+                                  unsigned char *syn_group, float *delay,
+                                  float *weight);           /* neurongpu_C.h:258 */
+int NeuronGPU_CreateSynGroup(char *model_name);             /* neurongpu_C.h:263 */
+int NeuronGPU_GetSynGroupNParam(int i_syn_group);           /* neurongpu_C.h:265 */
+char **NeuronGPU_GetSynGroupParamNames(int i_syn_group);    /* neurongpu_C.h:267 */
+int NeuronGPU_IsSynGroupParam(int i_syn_group, char *param_name);   /* :269 */
+int NeuronGPU_GetSynGroupParamIdx(int i_syn_group, char *param_name); /* :271 */
+float NeuronGPU_GetSynGroupParam(int i_syn_group, char *param_name);  /* :273 */
+int NeuronGPU_SetSynGroupParam(int i_syn_group, char *param_name,
+                               float val);                  /* neurongpu_C.h:275 */
+int NeuronGPU_ActivateSpikeCount(int i_node, int n_node);   /* neurongpu_C.h:277 */
+int NeuronGPU_ActivateRecSpikeTimes(int i_node, int n_node,
+                                    int max_n_rec_spike_times);     /* :279 */
+int NeuronGPU_GetNRecSpikeTimes(int i_node);                /* neurongpu_C.h:282 */
+float *NeuronGPU_GetRecSpikeTimes(int i_node);              /* neurongpu_C.h:284 */
+int NeuronGPU_PushSpikesToNodes(int n_spikes, int *node_id);        /* :286 */
+int NeuronGPU_GetExtNeuronInputSpikes(int *n_spikes, int **node, int **port,
+                                      float **spike_height,
+                                      int include_zeros);   /* neurongpu_C.h:288 */
+int NeuronGPU_SetNeuronGroupParam(int i_node, int n_node, char *param_name,
+                                  float val);               /* neurongpu_C.h:292 */
+int NeuronGPU_IsNeuronGroupParam(int i_node, char *param_name);     /* :295 */
+float NeuronGPU_GetNeuronGroupParam(int i_node, char *param_name);  /* :297 */
+int NeuronGPU_GetNFloatParam();                             /* neurongpu_C.h:299 */
+char **NeuronGPU_GetFloatParamNames();                      /* neurongpu_C.h:301 */
+int NeuronGPU_IsFloatParam(char *param_name);               /* neurongpu_C.h:303 */
+int NeuronGPU_GetFloatParamIdx(char *param_name);           /* neurongpu_C.h:305 */
+float NeuronGPU_GetFloatParam(char *param_name);            /* neurongpu_C.h:307 */
+int NeuronGPU_SetFloatParam(char *param_name, float val);   /* neurongpu_C.h:309 */
+int NeuronGPU_GetNIntParam();                               /* neurongpu_C.h:311 */
+char **NeuronGPU_GetIntParamNames();                        /* neurongpu_C.h:313 */
+int NeuronGPU_IsIntParam(char *param_name);                 /* neurongpu_C.h:315 */
+int NeuronGPU_GetIntParamIdx(char *param_name);             /* neurongpu_C.h:317 */
+int NeuronGPU_GetIntParam(char *param_name);                /* neurongpu_C.h:319 */
+int NeuronGPU_SetIntParam(char *param_name, int val);       /* neurongpu_C.h:321 */
+int NeuronGPU_RemoteCreate(int i_host, char *model_name, int n_neuron,
+                           int n_port);                     /* neurongpu_C.h:323 */
+
+/* ---- extensions of this build (no counterpart in the reference) ---- */
+
+/* Destroys the simulation instance and frees its device memory, so one
+ * process can build and run several independent networks in sequence. */
+int NGB200_Reset();
+/* RK5 right-hand-side evaluations performed so far (all RK5 groups). */
+unsigned long long NGB200_StageEvaluations();
+/* Synaptic events (spike x synapse) delivered so far. */
+unsigned long long NGB200_DeliveredEvents();
+/* Spikes emitted so far (all nodes). */
+unsigned long long NGB200_TotalSpikes();
+/* Host wall time of the last NeuronGPU_Simulate call, in seconds. */
+double NGB200_LastSimulateSeconds();
+/* Steps per captured CUDA graph (default 100); 0 launches without graphs. */
+int NGB200_SetGraphChunk(int n_steps);
+/* Total number of nodes and of connections. */
+long long NGB200_NNodes();
+long long NGB200_NConnections();
+/* Device time (CUDA events on the simulation stream) of the step loop of the
+ * last NeuronGPU_Simulate call, in ms. */
+double NGB200_LastSimulateDeviceMs();
+/* Per-kernel-class timing: on != 0 records CUDA events around every kernel
+ * class of every step (resets the totals). Classes: 0 node updates,
+ * 1 spike delivery, 2 STDP post rule, 3 recording and step bookkeeping. */
+int NGB200_SetKernelTiming(int on);
+int NGB200_GetKernelTiming(int kind, double *total_ms, long long *launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,1659 @@
+// NeuronGPU host driver: node groups, parameters, calibration and the
+// simulation loop. Connection handling lives in ngpu_connect.cpp.
+//
+// Reference behaviour followed here (paths within golosio/NeuronGPU):
+//   node creation and group table      src/neurongpu.cu:201-243, src/neuron_models.cu:44-149
+//   calibration                        src/neurongpu.cu:277-333
+//   Simulate / StartSimulation / Step  src/neurongpu.cu:340-605
+//   parameter and variable access      src/base_neuron.cu:175-1266
+//   multimeter records                 src/multimeter.cu:23-140
+#include "ngpu_core.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+#include <algorithm>
+#include <chrono>
+#include <cstdlib>
+
+#include "ngpu_rng.h"
+
+namespace ngpu {
+
+static const char *kFloatParamNames[] = {"time_resolution",
+                                         "max_spike_num_fact",
+                                         "max_spike_per_host_fact"};
+static const char *kIntParamNames[] = {"rnd_seed", "verbosity_level",
+                                       "max_spike_buffer_size",
+                                       "remote_spike_height_flag"};
+
+// ---------------------------------------------------------------------------
+// NodeGroup name lookup
+// ---------------------------------------------------------------------------
+static int find_name(const std::vector<std::string> &v, const std::string &n) {
+  for (size_t i = 0; i < v.size(); i++)
+    if (v[i] == n) return (int)i;
+  return -1;
+}
+int NodeGroup::ScalVarIdx(const std::string &n) const { return find_name(mi->scal_var, n); }
+int NodeGroup::PortVarIdx(const std::string &n) const { return find_name(mi->port_var, n); }
+int NodeGroup::ScalParamIdx(const std::string &n) const { return find_name(mi->scal_param, n); }
+int NodeGroup::PortParamIdx(const std::string &n) const { return find_name(mi->port_param, n); }
+int NodeGroup::GroupParamIdx(const std::string &n) const { return find_name(mi->group_param, n); }
+int NodeGroup::IntVarIdx(const std::string &n) const { return find_name(int_var_names, n); }
+int NodeGroup::ArrayParamIdx(const std::string &n) const { return find_name(mi->array_param, n); }
+
+// ---------------------------------------------------------------------------
+// construction
+// ---------------------------------------------------------------------------
+NeuronGPU::NeuronGPU() {
+  memset(&syn_table_, 0, sizeof(syn_table_));
+}
+
+NeuronGPU::~NeuronGPU() {
+  for (auto &r : records_) {
+    if (r.fp) fclose(r.fp);
+  }
+  try {
+    FreeDevice();
+  } catch (...) {
+  }
+  for (NodeGroup *g : groups_) delete g;
+}
+
+void NeuronGPU::FreeDevice() {
+  InvalidateGraphs();
+  auto F = [](void *p) { if (p) cudaFree(p); };
+  for (NodeGroup *g : groups_) {
+    F(g->d_var); F(g->d_param); F(g->d_h); F(g->d_dx);
+    F(g->d_spike_count); F(g->d_rec_times); F(g->d_n_rec);
+    F(g->d_sg_off); F(g->d_sg_step); F(g->d_sg_next); F(g->d_sg_height);
+    F(g->d_blk_evals);
+    g->d_var = g->d_param = g->d_h = g->d_dx = nullptr;
+  }
+  F(d_ctx_); F(d_acc_); F(d_ring_src_); F(d_ring_h_); F(d_ring_cnt_);
+  F(d_last_spike_T_); F(d_last_rev_T_); F(d_last_post_T_); F(d_last_spike_h_);
+  F(d_grp_off_); F(d_e_slot_); F(d_e_w_); F(d_e_syn_); F(d_e_stamp_);
+  F(d_e_post_); F(d_rev_off_); F(d_rev_edge_); F(d_delays_);
+  F(d_dc_off_); F(d_dc_gen_); F(d_dc_port_); F(d_dc_w_); F(d_dc_delay_);
+  F(d_dc_stream_); F(d_gen_rate_); F(d_gen_origin_); F(d_gen_start_);
+  F(d_gen_stop_); F(d_gen_lambda_); F(d_gen_explam_); F(d_blk_events_);
+  F(d_rec_cols_); F(d_rec_buf_);
+  for (cudaEvent_t e : kev_) cudaEventDestroy(e);
+  kev_.clear();
+  if (ev_start_) cudaEventDestroy(ev_start_);
+  if (ev_stop_) cudaEventDestroy(ev_stop_);
+  ev_start_ = ev_stop_ = nullptr;
+  d_ctx_ = nullptr;
+  if (stream_) {
+    cudaStreamDestroy(stream_);
+    stream_ = nullptr;
+  }
+}
+
+void NeuronGPU::CheckUncalibrated(const std::string &msg) {
+  if (calibrate_flag_) throw ngpu_exception(msg);
+}
+
+// ---------------------------------------------------------------------------
+// kernel parameters (src/neurongpu.cu:59-85, 1643-1818)
+// ---------------------------------------------------------------------------
+int NeuronGPU::SetRandomSeed(unsigned long long seed) {
+  rnd_seed_ = seed;
+  kernel_seed_ = seed + 12345ULL;
+  rng_calls_ = 0;
+  return 0;
+}
+
+int NeuronGPU::SetTimeResolution(float t) {
+  CheckUncalibrated("Time resolution cannot be changed after calibration");
+  if (!(t > 0.0f)) throw ngpu_exception("Time resolution must be > 0");
+  time_resolution_ = t;
+  return 0;
+}
+
+std::vector<std::string> NeuronGPU::GetFloatParamNames() {
+  return std::vector<std::string>(kFloatParamNames, kFloatParamNames + 3);
+}
+std::vector<std::string> NeuronGPU::GetIntParamNames() {
+  return std::vector<std::string>(kIntParamNames, kIntParamNames + 4);
+}
+bool NeuronGPU::IsFloatParam(const std::string &n) {
+  return find_name(GetFloatParamNames(), n) >= 0;
+}
+bool NeuronGPU::IsIntParam(const std::string &n) {
+  return find_name(GetIntParamNames(), n) >= 0;
+}
+int NeuronGPU::GetFloatParamIdx(const std::string &n) {
+  int i = find_name(GetFloatParamNames(), n);
+  if (i < 0) throw ngpu_exception(std::string("Unrecognized kernel float parameter ") + n);
+  return i;
+}
+int NeuronGPU::GetIntParamIdx(const std::string &n) {
+  int i = find_name(GetIntParamNames(), n);
+  if (i < 0) throw ngpu_exception(std::string("Unrecognized kernel int parameter ") + n);
+  return i;
+}
+float NeuronGPU::GetFloatParam(const std::string &n) {
+  switch (GetFloatParamIdx(n)) {
+    case 0: return time_resolution_;
+    case 1: return max_spike_num_fact_;
+    default: return max_spike_per_host_fact_;
+  }
+}
+int NeuronGPU::GetIntParam(const std::string &n) {
+  switch (GetIntParamIdx(n)) {
+    case 0: return (int)rnd_seed_;
+    case 1: return verbosity_level_;
+    case 2: return max_spike_buffer_size_;
+    default: return remote_spike_height_flag_;
+  }
+}
+int NeuronGPU::SetFloatParam(const std::string &n, float v) {
+  switch (GetFloatParamIdx(n)) {
+    case 0: return SetTimeResolution(v);
+    case 1: max_spike_num_fact_ = v; return 0;
+    default: max_spike_per_host_fact_ = v; return 0;
+  }
+}
+int NeuronGPU::SetIntParam(const std::string &n, int v) {
+  switch (GetIntParamIdx(n)) {
+    case 0: return SetRandomSeed((unsigned long long)v);
+    case 1: verbosity_level_ = v; return 0;
+    case 2: max_spike_buffer_size_ = v; return 0;
+    default:
+      if (v != 0 && v != 1)
+        throw ngpu_exception("Admissible values of remote_spike_height_flag are only 0 or 1");
+      remote_spike_height_flag_ = v;
+      return 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// node creation
+// ---------------------------------------------------------------------------
+int NeuronGPU::Create(const std::string &model, int n_node, int n_port) {
+  CheckUncalibrated("Nodes cannot be created after calibration");
+  if (n_node <= 0) throw ngpu_exception("Number of nodes must be greater than zero.");
+  if (n_port < 0) throw ngpu_exception("Number of ports must be >= zero.");
+  int m = FindModel(model);
+  if (m < 0) throw ngpu_exception(std::string("Unknown neuron model name: ") + model);
+  const ModelInfo &mi = ModelCatalogue()[m];
+  if (mi.fixed_n_port >= 0) n_port = mi.fixed_n_port;
+  if (n_port > 128) throw ngpu_exception("Maximum number of ports 128 exceeded");
+  if (mi.kind == MK_RK5 && n_port > 20)
+    throw ngpu_exception("RK5 models support at most 20 receptor ports");
+  if ((long long)node_group_map_.size() + n_node > 0x7FFFFFFFLL)
+    throw ngpu_exception("Maximum number of nodes exceeded");
+  if (cudaSuccess != cudaFree(0)) throw ngpu_exception("CUDA device not available");
+  if (!stream_) NGPU_CUDA(cudaStreamCreate(&stream_));
+
+  NodeGroup *g = new NodeGroup;
+  g->model = m;
+  g->mi = &mi;
+  g->i_node_0 = (int)node_group_map_.size();
+  g->n_node = n_node;
+  g->n_port = n_port;
+  g->n_pad = (n_node + 127) / 128 * 128;
+  g->nvar = (int)(mi.scal_var.size() + mi.port_var.size() * n_port);
+  g->nparam = (int)(mi.scal_param.size() + mi.port_param.size() * n_port);
+  if (g->nparam > NGPU_MAX_PARAM || g->nvar > NGPU_MAX_VAR) {
+    delete g;
+    throw ngpu_exception("Too many ports for this model");
+  }
+  g->group_param = mi.group_param_def;
+  try {
+    if (g->nvar > 0)
+      NGPU_CUDA(cudaMalloc(&g->d_var, sizeof(float) * (size_t)g->nvar * g->n_pad));
+    if (g->nparam > 0)
+      NGPU_CUDA(cudaMalloc(&g->d_param, sizeof(float) * (size_t)g->nparam * g->n_pad));
+    if (mi.kind == MK_RK5) {
+      NGPU_CUDA(cudaMalloc(&g->d_h, sizeof(float) * g->n_pad));
+      NGPU_CUDA(cudaMalloc(&g->d_dx, sizeof(float) * g->n_pad));
+    }
+  } catch (...) {
+    delete g;
+    throw;
+  }
+  // defaults
+  const int NSV = g->NSV(), NPV = g->NPV(), NSP = g->NSP(), NPP = g->NPP();
+  for (int j = 0; j < NSV; j++)
+    LaunchFillFloat(g->d_var + (size_t)j * g->n_pad, g->n_pad, mi.scal_var_def[j], stream_);
+  for (int p = 0; p < n_port; p++)
+    for (int k = 0; k < NPV; k++)
+      LaunchFillFloat(g->d_var + (size_t)(NSV + p * NPV + k) * g->n_pad, g->n_pad,
+                      mi.port_var_def[k], stream_);
+  g->p_uniform.assign(g->nparam, 1);
+  g->p_uval.assign(g->nparam, 0.0f);
+  for (int j = 0; j < NSP; j++) g->p_uval[j] = mi.scal_param_def[j];
+  for (int p = 0; p < n_port; p++)
+    for (int k = 0; k < NPP; k++) g->p_uval[NSP + p * NPP + k] = mi.port_param_def[k];
+  for (int j = 0; j < g->nparam; j++)
+    LaunchFillFloat(g->d_param + (size_t)j * g->n_pad, g->n_pad, g->p_uval[j], stream_);
+  if (mi.kind == MK_RK5) {
+    float h0 = g->group_param[1] * 0.1f;
+    LaunchFillFloat(g->d_h, g->n_pad, h0, stream_);
+    LaunchFillFloat(g->d_dx, g->n_pad, 0.0f, stream_);
+  }
+  if (mi.kind == MK_SPIKE_GENERATOR) {
+    g->sg_times.assign(n_node, std::vector<float>());
+    g->sg_heights.assign(n_node, std::vector<float>());
+  }
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  groups_.push_back(g);
+  node_group_map_.insert(node_group_map_.end(), n_node, (int)groups_.size() - 1);
+  host_csr_valid_ = false;
+  return g->i_node_0;
+}
+
+int NeuronGPU::CreatePoissonGenerator(int n_node, float rate) {
+  CheckUncalibrated("Poisson generator cannot be created after calibration");
+  for (NodeGroup *g : groups_)
+    if (g->mi->kind == MK_POISSON_NODES)
+      throw ngpu_exception("Number of poisson generators cannot be modified.");
+  if (n_node <= 0) throw ngpu_exception("Number of nodes must be greater than zero.");
+  static ModelInfo pn;
+  if (pn.name.empty()) {
+    pn.name = "";
+    pn.kind = MK_POISSON_NODES;
+    pn.rk5_model = -1;
+    pn.fixed_n_port = 0;
+    pn.in_var = -1; pn.in_step = 0; pn.w_param = false; pn.w_param_idx = -1;
+    pn.refr_param = -1; pn.den_delay_param = -1;
+  }
+  if (!stream_) NGPU_CUDA(cudaStreamCreate(&stream_));
+  NodeGroup *g = new NodeGroup;
+  g->model = -1;
+  g->mi = &pn;
+  g->i_node_0 = (int)node_group_map_.size();
+  g->n_node = n_node;
+  g->n_port = 0;
+  g->n_pad = (n_node + 127) / 128 * 128;
+  // lambda as the reference computes it (src/neurongpu.cu:260)
+  g->poisson_lambda = (float)(rate * time_resolution_ / 1000.0);
+  groups_.push_back(g);
+  node_group_map_.insert(node_group_map_.end(), n_node, (int)groups_.size() - 1);
+  host_csr_valid_ = false;
+  return g->i_node_0;
+}
+
+// ---------------------------------------------------------------------------
+// group lookup
+// ---------------------------------------------------------------------------
+NodeGroup *NeuronGPU::GroupOf(int i_node, int n, int &i_local) {
+  if (i_node < 0 || n <= 0 || (long long)i_node + n > (long long)node_group_map_.size())
+    throw ngpu_exception("Unrecognized node in getting node sequence offset");
+  int ig = node_group_map_[i_node];
+  if (node_group_map_[i_node + n - 1] != ig)
+    throw ngpu_exception("Nodes belong to different node groups in setting parameter");
+  i_local = i_node - groups_[ig]->i_node_0;
+  return groups_[ig];
+}
+
+NodeGroup *NeuronGPU::GroupOfList(const int *nodes, int n, std::vector<int> &local) {
+  if (n <= 0) throw ngpu_exception("Number of nodes must be greater than zero");
+  int in0 = nodes[0];
+  if (in0 < 0 || in0 >= (int)node_group_map_.size())
+    throw ngpu_exception("Unrecognized node in setting parameter");
+  int ig = node_group_map_[in0];
+  NodeGroup *g = groups_[ig];
+  local.resize(n);
+  for (int k = 0; k < n; k++) {
+    int in = nodes[k];
+    if (in < 0 || in >= (int)node_group_map_.size())
+      throw ngpu_exception("Unrecognized node in setting parameter");
+    if (node_group_map_[in] != ig)
+      throw ngpu_exception("Nodes belong to different node groups in setting parameter");
+    local[k] = in - g->i_node_0;
+  }
+  return g;
+}
+
+// ---------------------------------------------------------------------------
+// parameter columns
+// ---------------------------------------------------------------------------
+void NeuronGPU::SetParamColumn(NodeGroup *g, int col, int i0, int n,
+                               const int *nodes, float val, const float *vals,
+                               int stride) {
+  float *base = g->d_param + (size_t)col * g->n_pad;
+  bool whole = (nodes == nullptr && i0 == 0 && n == g->n_node);
+  if (vals == nullptr) {
+    if (whole) {
+      g->p_uniform[col] = 1;
+      g->p_uval[col] = val;
+    } else if (!(g->p_uniform[col] && g->p_uval[col] == val)) {
+      g->p_uniform[col] = 0;
+    }
+  } else {
+    g->p_uniform[col] = 0;
+  }
+  if (nodes == nullptr && vals == nullptr) {
+    LaunchFillFloat(base + i0, n, val, stream_);
+  } else if (nodes == nullptr) {
+    std::vector<float> tmp(n);
+    for (int k = 0; k < n; k++) tmp[k] = vals[(size_t)k * stride];
+    NGPU_CUDA(cudaMemcpyAsync(base + i0, tmp.data(), sizeof(float) * n,
+                              cudaMemcpyHostToDevice, stream_));
+    NGPU_CUDA(cudaStreamSynchronize(stream_));
+  } else {
+    int *d_idx = nullptr;
+    float *d_vals = nullptr;
+    NGPU_CUDA(cudaMalloc(&d_idx, sizeof(int) * n));
+    NGPU_CUDA(cudaMemcpyAsync(d_idx, nodes, sizeof(int) * n, cudaMemcpyHostToDevice, stream_));
+    if (vals) {
+      std::vector<float> tmp(n);
+      for (int k = 0; k < n; k++) tmp[k] = vals[(size_t)k * stride];
+      NGPU_CUDA(cudaMalloc(&d_vals, sizeof(float) * n));
+      NGPU_CUDA(cudaMemcpyAsync(d_vals, tmp.data(), sizeof(float) * n,
+                                cudaMemcpyHostToDevice, stream_));
+    }
+    LaunchScatterFloat(base, d_idx, n, val, d_vals, 1, stream_);
+    NGPU_CUDA(cudaStreamSynchronize(stream_));
+    cudaFree(d_idx);
+    if (d_vals) cudaFree(d_vals);
+  }
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  InvalidateGraphs();
+}
+
+void NeuronGPU::GetParamColumn(NodeGroup *g, float *col_base, int i0, int n,
+                               const int *nodes, float *out, int stride) {
+  (void)g;
+  std::vector<float> tmp(n);
+  if (nodes == nullptr) {
+    NGPU_CUDA(cudaMemcpyAsync(tmp.data(), col_base + i0, sizeof(float) * n,
+                              cudaMemcpyDeviceToHost, stream_));
+  } else {
+    int *d_idx = nullptr;
+    float *d_out = nullptr;
+    NGPU_CUDA(cudaMalloc(&d_idx, sizeof(int) * n));
+    NGPU_CUDA(cudaMalloc(&d_out, sizeof(float) * n));
+    NGPU_CUDA(cudaMemcpyAsync(d_idx, nodes, sizeof(int) * n, cudaMemcpyHostToDevice, stream_));
+    LaunchGatherFloat(col_base, d_idx, n, d_out, 1, stream_);
+    NGPU_CUDA(cudaMemcpyAsync(tmp.data(), d_out, sizeof(float) * n,
+                              cudaMemcpyDeviceToHost, stream_));
+    NGPU_CUDA(cudaStreamSynchronize(stream_));
+    cudaFree(d_idx);
+    cudaFree(d_out);
+  }
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  for (int k = 0; k < n; k++) out[(size_t)k * stride] = tmp[k];
+}
+
+static void check_local(NodeGroup *g, const std::vector<int> &loc) {
+  for (int v : loc)
+    if (v < 0 || v >= g->n_node) throw ngpu_exception("Neuron index out of range");
+}
+
+int NeuronGPU::SetNeuronParam(int i_node, int n, const std::string &name, float val) {
+  int il;
+  NodeGroup *g = GroupOf(i_node, n, il);
+  if (g->mi->kind == MK_POISSON_NODES)
+    throw ngpu_exception(std::string("Unrecognized scalar parameter ") + name);
+  int j = g->ScalParamIdx(name);
+  if (j < 0) throw ngpu_exception(std::string("Unrecognized scalar parameter ") + name);
+  SetParamColumn(g, j, il, n, nullptr, val, nullptr, 1);
+  return 0;
+}
+
+int NeuronGPU::SetNeuronParam(const int *nodes, int n, const std::string &name, float val) {
+  std::vector<int> loc;
+  NodeGroup *g = GroupOfList(nodes, n, loc);
+  int j = g->ScalParamIdx(name);
+  if (j < 0) throw ngpu_exception(std::string("Unrecognized scalar parameter ") + name);
+  SetParamColumn(g, j, 0, n, loc.data(), val, nullptr, 1);
+  return 0;
+}
+
+int NeuronGPU::SetNeuronParam(int i_node, int n, const std::string &name,
+                              const float *arr, int size) {
+  int il;
+  NodeGroup *g = GroupOf(i_node, n, il);
+  int k = g->PortParamIdx(name);
+  if (k >= 0) {
+    if (size != g->n_port)
+      throw ngpu_exception("Parameter array size must be equal to the number of ports.");
+    for (int p = 0; p < g->n_port; p++)
+      SetParamColumn(g, g->NSP() + p * g->NPP() + k, il, n, nullptr, arr[p], nullptr, 1);
+    return 0;
+  }
+  if (g->ArrayParamIdx(name) >= 0) {
+    if (g->mi->kind != MK_SPIKE_GENERATOR)
+      throw ngpu_exception(std::string("Unrecognized array parameter ") + name);
+    CheckUncalibrated("Spike generator array parameters must be set before calibration");
+    for (int i = il; i < il + n; i++) {
+      if (name == "spike_times") g->sg_times[i].assign(arr, arr + size);
+      else g->sg_heights[i].assign(arr, arr + size);
+    }
+    return 0;
+  }
+  throw ngpu_exception(std::string("Unrecognized array parameter ") + name);
+}
+
+int NeuronGPU::SetNeuronParam(const int *nodes, int n, const std::string &name,
+                              const float *arr, int size) {
+  std::vector<int> loc;
+  NodeGroup *g = GroupOfList(nodes, n, loc);
+  int k = g->PortParamIdx(name);
+  if (k >= 0) {
+    if (size != g->n_port)
+      throw ngpu_exception("Parameter array size must be equal to the number of ports.");
+    for (int p = 0; p < g->n_port; p++)
+      SetParamColumn(g, g->NSP() + p * g->NPP() + k, 0, n, loc.data(), arr[p], nullptr, 1);
+    return 0;
+  }
+  if (g->ArrayParamIdx(name) >= 0 && g->mi->kind == MK_SPIKE_GENERATOR) {
+    CheckUncalibrated("Spike generator array parameters must be set before calibration");
+    for (int i : loc) {
+      if (name == "spike_times") g->sg_times[i].assign(arr, arr + size);
+      else g->sg_heights[i].assign(arr, arr + size);
+    }
+    return 0;
+  }
+  throw ngpu_exception(std::string("Unrecognized array parameter ") + name);
+}
+
+int NeuronGPU::IsNeuronScalParam(int i_node, const std::string &n) {
+  int il; NodeGroup *g = GroupOf(i_node, 1, il);
+  return g->ScalParamIdx(n) >= 0;
+}
+int NeuronGPU::IsNeuronPortParam(int i_node, const std::string &n) {
+  int il; NodeGroup *g = GroupOf(i_node, 1, il);
+  return g->PortParamIdx(n) >= 0;
+}
+int NeuronGPU::IsNeuronArrayParam(int i_node, const std::string &n) {
+  int il; NodeGroup *g = GroupOf(i_node, 1, il);
+  return g->ArrayParamIdx(n) >= 0;
+}
+int NeuronGPU::IsNeuronGroupParam(int i_node, const std::string &n) {
+  int il; NodeGroup *g = GroupOf(i_node, 1, il);
+  return g->GroupParamIdx(n) >= 0 || (g->mi->kind == MK_RK5 && n == "rk5_eps");
+}
+int NeuronGPU::IsNeuronIntVar(int i_node, const std::string &n) {
+  int il; NodeGroup *g = GroupOf(i_node, 1, il);
+  return g->IntVarIdx(n) >= 0;
+}
+int NeuronGPU::IsNeuronScalVar(int i_node, const std::string &n) {
+  int il; NodeGroup *g = GroupOf(i_node, 1, il);
+  return g->ScalVarIdx(n) >= 0;
+}
+int NeuronGPU::IsNeuronPortVar(int i_node, const std::string &n) {
+  int il; NodeGroup *g = GroupOf(i_node, 1, il);
+  return g->PortVarIdx(n) >= 0;
+}
+int NeuronGPU::IsNeuronArrayVar(int i_node, const std::string &n) {
+  int il; GroupOf(i_node, 1, il);
+  (void)n;
+  return 0;
+}
+
+int NeuronGPU::GetNeuronParamSize(int i_node, const std::string &n) {
+  int il; NodeGroup *g = GroupOf(i_node, 1, il);
+  if (g->ArrayParamIdx(n) >= 0) {
+    return (int)(n == "spike_times" ? g->sg_times[il].size() : g->sg_heights[il].size());
+  }
+  if (g->ScalParamIdx(n) >= 0) return 1;
+  if (g->PortParamIdx(n) >= 0) return g->n_port;
+  throw ngpu_exception(std::string("Unrecognized parameter ") + n);
+}
+
+int NeuronGPU::GetNeuronVarSize(int i_node, const std::string &n) {
+  int il; NodeGroup *g = GroupOf(i_node, 1, il);
+  if (g->ScalVarIdx(n) >= 0 || g->IntVarIdx(n) >= 0) return 1;
+  if (g->PortVarIdx(n) >= 0) return g->n_port;
+  throw ngpu_exception(std::string("Unrecognized variable ") + n);
+}
+
+// Returned arrays are malloc'd and owned by the caller, as in
+// src/base_neuron.cu:446-471.
+float *NeuronGPU::GetNeuronParam(int i_node, int n, const std::string &name) {
+  int il; NodeGroup *g = GroupOf(i_node, n, il);
+  int j = g->ScalParamIdx(name);
+  if (j >= 0) {
+    float *out = (float *)malloc(sizeof(float) * n);
+    GetParamColumn(g, g->d_param + (size_t)j * g->n_pad, il, n, nullptr, out, 1);
+    return out;
+  }
+  int k = g->PortParamIdx(name);
+  if (k >= 0) {
+    float *out = (float *)malloc(sizeof(float) * (size_t)n * g->n_port);
+    for (int p = 0; p < g->n_port; p++)
+      GetParamColumn(g, g->d_param + (size_t)(g->NSP() + p * g->NPP() + k) * g->n_pad,
+                     il, n, nullptr, out + p, g->n_port);
+    return out;
+  }
+  if (g->ArrayParamIdx(name) >= 0) {
+    if (n != 1) throw ngpu_exception("Cannot get array parameters for more than one node at a time");
+    return GetArrayParam(i_node, name);
+  }
+  throw ngpu_exception(std::string("Unrecognized parameter ") + name);
+}
+
+float *NeuronGPU::GetNeuronParam(const int *nodes, int n, const std::string &name) {
+  std::vector<int> loc;
+  NodeGroup *g = GroupOfList(nodes, n, loc);
+  int j = g->ScalParamIdx(name);
+  if (j >= 0) {
+    float *out = (float *)malloc(sizeof(float) * n);
+    GetParamColumn(g, g->d_param + (size_t)j * g->n_pad, 0, n, loc.data(), out, 1);
+    return out;
+  }
+  int k = g->PortParamIdx(name);
+  if (k >= 0) {
+    float *out = (float *)malloc(sizeof(float) * (size_t)n * g->n_port);
+    for (int p = 0; p < g->n_port; p++)
+      GetParamColumn(g, g->d_param + (size_t)(g->NSP() + p * g->NPP() + k) * g->n_pad,
+                     0, n, loc.data(), out + p, g->n_port);
+    return out;
+  }
+  if (g->ArrayParamIdx(name) >= 0) {
+    if (n != 1) throw ngpu_exception("Cannot get array parameters for more than one node at a time");
+    return GetArrayParam(nodes[0], name);
+  }
+  throw ngpu_exception(std::string("Unrecognized parameter ") + name);
+}
+
+float *NeuronGPU::GetArrayParam(int i_node, const std::string &name) {
+  int il; NodeGroup *g = GroupOf(i_node, 1, il);
+  if (g->ArrayParamIdx(name) < 0 || g->mi->kind != MK_SPIKE_GENERATOR)
+    throw ngpu_exception(std::string("Unrecognized parameter ") + name);
+  std::vector<float> &v = (name == "spike_times") ? g->sg_times[il] : g->sg_heights[il];
+  float *out = (float *)malloc(sizeof(float) * (v.size() > 0 ? v.size() : 1));
+  for (size_t k = 0; k < v.size(); k++) out[k] = v[k];
+  return out;
+}
+
+int NeuronGPU::SetNeuronIntVar(int i_node, int n, const std::string &name, int val) {
+  int il; NodeGroup *g = GroupOf(i_node, n, il);
+  int j = g->IntVarIdx(name);
+  if (j < 0) throw ngpu_exception(std::string("Unrecognized integer variable ") + name);
+  int *base = (g->int_var_names[j] == "spike_count") ? g->d_spike_count : g->d_n_rec;
+  LaunchFillInt(base + il, n, val, stream_);
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  return 0;
+}
+
+int NeuronGPU::SetNeuronIntVar(const int *nodes, int n, const std::string &name, int val) {
+  std::vector<int> loc;
+  NodeGroup *g = GroupOfList(nodes, n, loc);
+  int j = g->IntVarIdx(name);
+  if (j < 0) throw ngpu_exception(std::string("Unrecognized integer variable ") + name);
+  int *base = (g->int_var_names[j] == "spike_count") ? g->d_spike_count : g->d_n_rec;
+  for (int v : loc) NGPU_CUDA(cudaMemcpy(base + v, &val, sizeof(int), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int NeuronGPU::SetNeuronVar(int i_node, int n, const std::string &name, float val) {
+  FlushInput();
+  int il; NodeGroup *g = GroupOf(i_node, n, il);
+  int j = g->ScalVarIdx(name);
+  if (j < 0) throw ngpu_exception(std::string("Unrecognized scalar variable ") + name);
+  LaunchFillFloat(g->d_var + (size_t)j * g->n_pad + il, n, val, stream_);
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  return 0;
+}
+
+int NeuronGPU::SetNeuronVar(const int *nodes, int n, const std::string &name, float val) {
+  FlushInput();
+  std::vector<int> loc;
+  NodeGroup *g = GroupOfList(nodes, n, loc);
+  int j = g->ScalVarIdx(name);
+  if (j < 0) throw ngpu_exception(std::string("Unrecognized scalar variable ") + name);
+  int *d_idx;
+  NGPU_CUDA(cudaMalloc(&d_idx, sizeof(int) * n));
+  NGPU_CUDA(cudaMemcpy(d_idx, loc.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  LaunchScatterFloat(g->d_var + (size_t)j * g->n_pad, d_idx, n, val, nullptr, 1, stream_);
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  cudaFree(d_idx);
+  return 0;
+}
+
+int NeuronGPU::SetNeuronVar(int i_node, int n, const std::string &name,
+                            const float *arr, int size) {
+  FlushInput();
+  int il; NodeGroup *g = GroupOf(i_node, n, il);
+  int k = g->PortVarIdx(name);
+  if (k < 0) throw ngpu_exception(std::string("Unrecognized port variable ") + name);
+  if (size != g->n_port)
+    throw ngpu_exception("Variable array size must be equal to the number of ports.");
+  for (int p = 0; p < g->n_port; p++)
+    LaunchFillFloat(g->d_var + (size_t)(g->NSV() + p * g->NPV() + k) * g->n_pad + il, n,
+                    arr[p], stream_);
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  return 0;
+}
+
+int NeuronGPU::SetNeuronVar(const int *nodes, int n, const std::string &name,
+                            const float *arr, int size) {
+  FlushInput();
+  std::vector<int> loc;
+  NodeGroup *g = GroupOfList(nodes, n, loc);
+  int k = g->PortVarIdx(name);
+  if (k < 0) throw ngpu_exception(std::string("Unrecognized port variable ") + name);
+  if (size != g->n_port)
+    throw ngpu_exception("Variable array size must be equal to the number of ports.");
+  int *d_idx;
+  NGPU_CUDA(cudaMalloc(&d_idx, sizeof(int) * n));
+  NGPU_CUDA(cudaMemcpy(d_idx, loc.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  for (int p = 0; p < g->n_port; p++)
+    LaunchScatterFloat(g->d_var + (size_t)(g->NSV() + p * g->NPV() + k) * g->n_pad, d_idx,
+                       n, arr[p], nullptr, 1, stream_);
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  cudaFree(d_idx);
+  return 0;
+}
+
+int *NeuronGPU::GetNeuronIntVar(int i_node, int n, const std::string &name) {
+  int il; NodeGroup *g = GroupOf(i_node, n, il);
+  int j = g->IntVarIdx(name);
+  if (j < 0) throw ngpu_exception(std::string("Unrecognized integer variable ") + name);
+  int *base = (g->int_var_names[j] == "spike_count") ? g->d_spike_count : g->d_n_rec;
+  int *out = (int *)malloc(sizeof(int) * n);
+  NGPU_CUDA(cudaMemcpy(out, base + il, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  return out;
+}
+
+int *NeuronGPU::GetNeuronIntVar(const int *nodes, int n, const std::string &name) {
+  std::vector<int> loc;
+  NodeGroup *g = GroupOfList(nodes, n, loc);
+  int j = g->IntVarIdx(name);
+  if (j < 0) throw ngpu_exception(std::string("Unrecognized variable ") + name);
+  int *base = (g->int_var_names[j] == "spike_count") ? g->d_spike_count : g->d_n_rec;
+  int *out = (int *)malloc(sizeof(int) * n);
+  for (int k = 0; k < n; k++)
+    NGPU_CUDA(cudaMemcpy(out + k, base + loc[k], sizeof(int), cudaMemcpyDeviceToHost));
+  return out;
+}
+
+float *NeuronGPU::GetNeuronVar(int i_node, int n, const std::string &name) {
+  FlushInput();
+  int il; NodeGroup *g = GroupOf(i_node, n, il);
+  int j = g->ScalVarIdx(name);
+  if (j >= 0) {
+    float *out = (float *)malloc(sizeof(float) * n);
+    GetParamColumn(g, g->d_var + (size_t)j * g->n_pad, il, n, nullptr, out, 1);
+    return out;
+  }
+  int k = g->PortVarIdx(name);
+  if (k >= 0) {
+    float *out = (float *)malloc(sizeof(float) * (size_t)n * g->n_port);
+    for (int p = 0; p < g->n_port; p++)
+      GetParamColumn(g, g->d_var + (size_t)(g->NSV() + p * g->NPV() + k) * g->n_pad,
+                     il, n, nullptr, out + p, g->n_port);
+    return out;
+  }
+  throw ngpu_exception(std::string("Unrecognized variable ") + name);
+}
+
+float *NeuronGPU::GetNeuronVar(const int *nodes, int n, const std::string &name) {
+  FlushInput();
+  std::vector<int> loc;
+  NodeGroup *g = GroupOfList(nodes, n, loc);
+  int j = g->ScalVarIdx(name);
+  if (j >= 0) {
+    float *out = (float *)malloc(sizeof(float) * n);
+    GetParamColumn(g, g->d_var + (size_t)j * g->n_pad, 0, n, loc.data(), out, 1);
+    return out;
+  }
+  int k = g->PortVarIdx(name);
+  if (k >= 0) {
+    float *out = (float *)malloc(sizeof(float) * (size_t)n * g->n_port);
+    for (int p = 0; p < g->n_port; p++)
+      GetParamColumn(g, g->d_var + (size_t)(g->NSV() + p * g->NPV() + k) * g->n_pad,
+                     0, n, loc.data(), out + p, g->n_port);
+    return out;
+  }
+  throw ngpu_exception(std::string("Unrecognized variable ") + name);
+}
+
+float *NeuronGPU::GetArrayVar(int i_node, const std::string &name) {
+  int il; GroupOf(i_node, 1, il);
+  throw ngpu_exception(std::string("Unrecognized array variable ") + name);
+}
+
+int NeuronGPU::SetNeuronGroupParam(int i_node, int n, const std::string &name, float val) {
+  int il; NodeGroup *g = GroupOf(i_node, n, il);
+  if (il != 0 || n != g->n_node)
+    throw ngpu_exception("Group parameters must be set for all the nodes of a group");
+  if (g->mi->kind == MK_RK5 && name == "rk5_eps") {
+    if (!(val > 0.0f)) throw ngpu_exception("rk5_eps must be > 0");
+    g->rk5_eps = val;
+    InvalidateGraphs();
+    return 0;
+  }
+  int j = g->GroupParamIdx(name);
+  if (j < 0) throw ngpu_exception(std::string("Unrecognized group parameter ") + name);
+  g->group_param[j] = val;
+  InvalidateGraphs();
+  return 0;
+}
+
+float NeuronGPU::GetNeuronGroupParam(int i_node, const std::string &name) {
+  int il; NodeGroup *g = GroupOf(i_node, 1, il);
+  if (g->mi->kind == MK_RK5 && name == "rk5_eps") return g->rk5_eps;
+  int j = g->GroupParamIdx(name);
+  if (j < 0) throw ngpu_exception(std::string("Unrecognized group parameter ") + name);
+  return g->group_param[j];
+}
+
+std::vector<std::string> NeuronGPU::GetIntVarNames(int i_node) {
+  int il; return GroupOf(i_node, 1, il)->int_var_names;
+}
+std::vector<std::string> NeuronGPU::GetScalVarNames(int i_node) {
+  int il; return GroupOf(i_node, 1, il)->mi->scal_var;
+}
+std::vector<std::string> NeuronGPU::GetPortVarNames(int i_node) {
+  int il; return GroupOf(i_node, 1, il)->mi->port_var;
+}
+std::vector<std::string> NeuronGPU::GetScalParamNames(int i_node) {
+  int il; return GroupOf(i_node, 1, il)->mi->scal_param;
+}
+std::vector<std::string> NeuronGPU::GetPortParamNames(int i_node) {
+  int il; return GroupOf(i_node, 1, il)->mi->port_param;
+}
+std::vector<std::string> NeuronGPU::GetGroupParamNames(int i_node) {
+  int il; return GroupOf(i_node, 1, il)->mi->group_param;
+}
+std::vector<std::string> NeuronGPU::GetArrayParamNames(int i_node) {
+  int il; return GroupOf(i_node, 1, il)->mi->array_param;
+}
+std::vector<std::string> NeuronGPU::GetArrayVarNames(int i_node) {
+  int il; GroupOf(i_node, 1, il);
+  return std::vector<std::string>();
+}
+
+// ---------------------------------------------------------------------------
+// recording
+// ---------------------------------------------------------------------------
+int NeuronGPU::CreateRecord(const std::string &file, const std::vector<std::string> &vars,
+                            const int *nodes, const int *ports, int n) {
+  if (calibrate_flag_ && !first_simulation_flag_)
+    throw ngpu_exception("Records cannot be created after the simulation started");
+  Record r;
+  r.file_name = file;
+  r.var_names = vars;
+  for (int k = 0; k < n; k++) {
+    int il;
+    NodeGroup *g = GroupOf(nodes[k], 1, il);
+    int port = ports ? ports[k] : 0;
+    if (vars[k] != "spike") {
+      if (g->ScalVarIdx(vars[k]) < 0 && g->PortVarIdx(vars[k]) < 0 &&
+          g->ScalParamIdx(vars[k]) < 0 && g->PortParamIdx(vars[k]) < 0)
+        throw ngpu_exception(std::string("Unrecognized variable ") + vars[k]);
+      if ((g->PortVarIdx(vars[k]) >= 0 || g->PortParamIdx(vars[k]) >= 0) &&
+          (port < 0 || port >= g->n_port))
+        throw ngpu_exception("Port index out of range in record");
+    }
+    r.nodes.push_back(nodes[k]);
+    r.ports.push_back(port);
+  }
+  records_.push_back(r);
+  return (int)records_.size() - 1;
+}
+
+std::vector<std::vector<float>> *NeuronGPU::GetRecordData(int i_record) {
+  if (i_record < 0 || i_record >= (int)records_.size())
+    throw ngpu_exception("Record does not exist.");
+  FlushRecords();
+  return &records_[i_record].data;
+}
+
+int NeuronGPU::ActivateSpikeCount(int i_node, int n) {
+  CheckUncalibrated("Spike count must be activated before calibration");
+  int il; NodeGroup *g = GroupOf(i_node, n, il);
+  if (il != 0 || n != g->n_node)
+    throw ngpu_exception("Spike count must be activated for all and only the nodes of the same group");
+  if (g->IntVarIdx("spike_count") >= 0) throw ngpu_exception("Spike count already activated");
+  g->int_var_names.push_back("spike_count");
+  NGPU_CUDA(cudaMalloc(&g->d_spike_count, sizeof(int) * g->n_pad));
+  NGPU_CUDA(cudaMemset(g->d_spike_count, 0, sizeof(int) * g->n_pad));
+  return 0;
+}
+
+int NeuronGPU::ActivateRecSpikeTimes(int i_node, int n, int max_n) {
+  CheckUncalibrated("Spike time recording must be activated before calibration");
+  int il; NodeGroup *g = GroupOf(i_node, n, il);
+  if (il != 0 || n != g->n_node)
+    throw ngpu_exception("Spike count must be activated for all and only the nodes of the same group");
+  if (max_n <= 0) throw ngpu_exception("Maximum number of recorded spike times must be greater than 0");
+  if (g->IntVarIdx("n_rec_spike_times") >= 0)
+    throw ngpu_exception("Spike times recording already activated");
+  g->int_var_names.push_back("n_rec_spike_times");
+  g->max_rec = max_n;
+  NGPU_CUDA(cudaMalloc(&g->d_n_rec, sizeof(int) * g->n_pad));
+  NGPU_CUDA(cudaMemset(g->d_n_rec, 0, sizeof(int) * g->n_pad));
+  NGPU_CUDA(cudaMalloc(&g->d_rec_times, sizeof(float) * (size_t)g->n_pad * max_n));
+  return 0;
+}
+
+int NeuronGPU::GetNRecSpikeTimes(int i_node) {
+  int il; NodeGroup *g = GroupOf(i_node, 1, il);
+  if (g->d_n_rec == nullptr) throw ngpu_exception("Spike times recording was not activated");
+  int v = 0;
+  NGPU_CUDA(cudaMemcpy(&v, g->d_n_rec + il, sizeof(int), cudaMemcpyDeviceToHost));
+  return v;
+}
+
+std::vector<float> NeuronGPU::GetRecSpikeTimes(int i_node) {
+  int il; NodeGroup *g = GroupOf(i_node, 1, il);
+  int n = GetNRecSpikeTimes(i_node);
+  std::vector<float> v(n);
+  if (n > 0)
+    NGPU_CUDA(cudaMemcpy(v.data(), g->d_rec_times + (size_t)il * g->max_rec,
+                         sizeof(float) * n, cudaMemcpyDeviceToHost));
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// argument builders
+// ---------------------------------------------------------------------------
+GroupArgs NeuronGPU::MakeGroupArgs(NodeGroup *g) {
+  GroupArgs a;
+  memset(&a, 0, sizeof(a));
+  a.n = g->n_node;
+  a.n_pad = g->n_pad;
+  a.i_node_0 = g->i_node_0;
+  a.nvar = g->nvar;
+  a.nparam = g->nparam;
+  a.var = g->d_var;
+  a.param = g->d_param;
+  a.h = g->d_h;
+  a.dx = g->d_dx;
+  for (int j = 0; j < g->nparam; j++) {
+    bool per_neuron = !g->p_uniform[j] || j == g->mi->refr_param;
+    if (per_neuron) a.pmask[j >> 5] |= (1u << (j & 31));
+    a.puni[j] = g->p_uval[j];
+  }
+  if (g->mi->kind == MK_RK5) {
+    a.h_min = g->group_param[0] * time_resolution_;
+    a.eps = g->rk5_eps;
+  }
+  a.dt = time_resolution_;
+  a.den_delay_col = g->mi->den_delay_param;
+  a.blk_evals = g->d_blk_evals;
+  a.sg_off = g->d_sg_off;
+  a.sg_step = g->d_sg_step;
+  a.sg_height = g->d_sg_height;
+  a.sg_next = g->d_sg_next;
+  return a;
+}
+
+InputArgs NeuronGPU::MakeInputArgs(NodeGroup *g) {
+  InputArgs in;
+  memset(&in, 0, sizeof(in));
+  const ModelInfo *mi = g->mi;
+  in.acc = d_acc_;
+  in.acc_base = g->acc_base;
+  in.np = g->n_port;
+  if (mi->kind == MK_RK5) {
+    in.in_var = mi->in_var - (mi->port_var.empty() ? 0 : 0);
+  }
+  in.in_var = mi->in_var;
+  in.in_step = mi->in_step;
+  in.w_param = mi->w_param ? 1 : 0;
+  in.w_col = mi->w_param ? (int)mi->scal_param.size() + mi->w_param_idx : 0;
+  in.w_col_step = (int)mi->port_param.size();
+  for (int q = 0; q < 4; q++) {
+    if (mi->w_const.empty()) in.w_const[q] = 1.0f;
+    else in.w_const[q] = mi->w_const[q < (int)mi->w_const.size() ? q : mi->w_const.size() - 1];
+  }
+  if (g->has_dc) {
+    in.dc_off = g->d_dc_off;
+    in.dc_gen = d_dc_gen_;
+    in.dc_port = d_dc_port_;
+    in.dc_weight = d_dc_w_;
+    in.dc_delay = d_dc_delay_;
+    in.dc_stream = d_dc_stream_;
+    in.gen_rate = d_gen_rate_;
+    in.gen_origin = d_gen_origin_;
+    in.gen_start = d_gen_start_;
+    in.gen_stop = d_gen_stop_;
+    in.gen_lambda = d_gen_lambda_;
+    in.gen_explam = d_gen_explam_;
+  }
+  in.seed = kernel_seed_;
+  return in;
+}
+
+PushArgs NeuronGPU::MakePushArgs(NodeGroup *g) {
+  PushArgs pa;
+  memset(&pa, 0, sizeof(pa));
+  pa.ring_src = d_ring_src_;
+  pa.ring_h = d_ring_h_;
+  pa.ring_cnt = d_ring_cnt_;
+  pa.ring_R = ring_R_;
+  pa.ring_C = ring_C_;
+  pa.last_spike_T = d_last_spike_T_;
+  pa.last_spike_h = d_last_spike_h_;
+  pa.last_rev_T = d_last_rev_T_;
+  pa.spike_count = g->d_spike_count;
+  pa.rec_times = g->d_rec_times;
+  pa.n_rec = g->d_n_rec;
+  pa.max_rec = g->max_rec;
+  return pa;
+}
+
+DeliverArgs NeuronGPU::MakeDeliverArgs() {
+  DeliverArgs d;
+  memset(&d, 0, sizeof(d));
+  d.grp_off = d_grp_off_;
+  d.e_slot = d_e_slot_;
+  d.e_w = d_e_w_;
+  d.e_syn = plastic_ ? d_e_syn_ : nullptr;
+  d.e_stamp = d_e_stamp_;
+  d.e_post = d_e_post_;
+  d.acc = d_acc_;
+  d.ring_src = d_ring_src_;
+  d.ring_h = d_ring_h_;
+  d.ring_cnt = d_ring_cnt_;
+  d.ring_R = ring_R_;
+  d.ring_C = ring_C_;
+  d.nd = (int)delays_.size();
+  d.delays = d_delays_;
+  d.last_rev_T = d_last_rev_T_;
+  d.last_post_T = d_last_post_T_;
+  d.rev_off = d_rev_off_;
+  d.rev_edge = d_rev_edge_;
+  d.dt = time_resolution_;
+  d.blk_events = d_blk_events_;
+  return d;
+}
+
+// ---------------------------------------------------------------------------
+// calibration (src/neurongpu.cu:277-333)
+// ---------------------------------------------------------------------------
+int NeuronGPU::Calibrate() {
+  CheckUncalibrated("Calibration can be made only once");
+  if (groups_.empty()) throw ngpu_exception("No nodes were created");
+  if (!stream_) NGPU_CUDA(cudaStreamCreate(&stream_));
+  if (verbosity_level_ >= 1) printf("Calibrating ...\n");
+  neural_time_ = t_min_;
+  BuildHostCSR();
+  BuildDevice();
+  calibrate_flag_ = true;
+  return 0;
+}
+
+// per-group calibration: defaults of derived parameters (g0, I0, iaf
+// propagators), initial step sizes and spike generator tables
+static void calibrate_group(NodeGroup *g, float dt, cudaStream_t s) {
+  const ModelInfo *mi = g->mi;
+  if (mi->kind == MK_RK5) {
+    GroupArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = g->n_node; a.n_pad = g->n_pad; a.param = g->d_param;
+    LaunchCalibrateRk5(mi->rk5_model, a, g->n_port, s);
+    float h0 = g->group_param[1] * dt;
+    LaunchFillFloat(g->d_h, g->n_pad, h0, s);
+    LaunchFillFloat(g->d_dx, g->n_pad, 0.0f, s);
+    NGPU_CUDA(cudaStreamSynchronize(s));
+    // derived parameters: uniform iff their inputs are uniform
+    auto derive = [&](int out_col, std::vector<int> in_cols) {
+      bool uni = true;
+      for (int c : in_cols) uni = uni && g->p_uniform[c];
+      g->p_uniform[out_col] = uni ? 1 : 0;
+      if (uni) {
+        float v;
+        NGPU_CUDA(cudaMemcpy(&v, g->d_param + (size_t)out_col * g->n_pad, sizeof(float),
+                             cudaMemcpyDeviceToHost));
+        g->p_uval[out_col] = v;
+      }
+    };
+    const int NSP = g->NSP(), NPP = g->NPP();
+    g->p_uniform[mi->refr_param] = 1;
+    g->p_uval[mi->refr_param] = 0.0f;
+    for (int q = 0; q < g->n_port; q++) {
+      int b = NSP + q * NPP;
+      switch (mi->rk5_model) {
+        case RK5_AEIF_COND_BETA:
+        case RK5_IZHIKEVICH_COND_BETA: derive(b + 3, {b + 1, b + 2}); break;
+        case RK5_AEIF_COND_ALPHA: derive(b + 2, {b + 1}); break;
+        case RK5_AEIF_PSC_ALPHA: derive(b + 1, {b + 0}); break;
+        default: break;
+      }
+    }
+  } else if (mi->kind == MK_IAF_PSC_EXP) {
+    GroupArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = g->n_node; a.n_pad = g->n_pad; a.param = g->d_param;
+    LaunchCalibrateIaf(a, dt, s);
+    NGPU_CUDA(cudaStreamSynchronize(s));
+    bool uni = g->p_uniform[0] && g->p_uniform[1] && g->p_uniform[6] && g->p_uniform[7];
+    for (int c = 10; c <= 15; c++) {
+      g->p_uniform[c] = uni ? 1 : 0;
+      if (uni) {
+        float v;
+        NGPU_CUDA(cudaMemcpy(&v, g->d_param + (size_t)c * g->n_pad, sizeof(float),
+                             cudaMemcpyDeviceToHost));
+        g->p_uval[c] = v;
+      }
+    }
+  } else if (mi->kind == MK_SPIKE_GENERATOR) {
+    // spike times -> step indices (src/spike_generator.cu:214-257)
+    std::vector<int> off(g->n_node + 1, 0), step;
+    std::vector<float> height;
+    for (int i = 0; i < g->n_node; i++) {
+      std::vector<float> &tv = g->sg_times[i];
+      std::vector<float> &hv = g->sg_heights[i];
+      if (!tv.empty() && !hv.empty() && hv.size() != tv.size())
+        throw ngpu_exception("spike time array and spike height array must have the same size in spike generator");
+      int prev = -0x7fffffff;
+      for (size_t k = 0; k < tv.size(); k++) {
+        int si = (int)round((tv[k] - 0.0f) / dt);
+        if (k > 0 && si <= prev)
+          throw ngpu_exception("Spike times must be ordered, and the difference between\nconsecutive spikes must be >= the time resolution");
+        prev = si;
+        step.push_back(si);
+        height.push_back(hv.empty() ? 1.0f : hv[k]);
+      }
+      off[i + 1] = (int)step.size();
+    }
+    NGPU_CUDA(cudaMalloc(&g->d_sg_off, sizeof(int) * (g->n_node + 1)));
+    NGPU_CUDA(cudaMalloc(&g->d_sg_next, sizeof(int) * (g->n_node + 1)));
+    NGPU_CUDA(cudaMalloc(&g->d_sg_step, sizeof(int) * (step.size() + 1)));
+    NGPU_CUDA(cudaMalloc(&g->d_sg_height, sizeof(float) * (height.size() + 1)));
+    NGPU_CUDA(cudaMemcpy(g->d_sg_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
+    NGPU_CUDA(cudaMemcpy(g->d_sg_next, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
+    if (!step.empty()) {
+      NGPU_CUDA(cudaMemcpy(g->d_sg_step, step.data(), sizeof(int) * step.size(), cudaMemcpyHostToDevice));
+      NGPU_CUDA(cudaMemcpy(g->d_sg_height, height.data(), sizeof(float) * height.size(), cudaMemcpyHostToDevice));
+    }
+  }
+}
+
+void NeuronGPU::BuildDevice() {
+  const long long N = (long long)node_group_map_.size();
+  const int nd = (int)delays_.size();
+  // accumulator slots
+  n_acc_ = 0;
+  for (NodeGroup *g : groups_) {
+    g->acc_base = n_acc_;
+    n_acc_ += (long long)g->n_port * g->n_pad;
+  }
+  if (n_acc_ > 0xFFFFFFFFLL) throw ngpu_exception("Too many (node, port) input slots");
+  NGPU_CUDA(cudaMalloc(&d_acc_, sizeof(long long) * (n_acc_ > 0 ? n_acc_ : 1)));
+  NGPU_CUDA(cudaMemset(d_acc_, 0, sizeof(long long) * (n_acc_ > 0 ? n_acc_ : 1)));
+  // check ports of every edge and build the slot array
+  const uint64_t E = e_src_.size();
+  std::vector<uint32_t> slot(E);
+  std::vector<float> w(E);
+  std::vector<uint8_t> syn;
+  std::vector<uint32_t> post;
+  plastic_ = false;
+  for (uint64_t k = 0; k < E; k++) {
+    if (e_syn_[h_order_[k]] > 0) { plastic_ = true; break; }
+  }
+  if (plastic_) { syn.resize(E); post.resize(E); }
+  long long bad_port = -1;
+  bool bad_syn = false;
+#pragma omp parallel for schedule(static) if (E > 1000000)
+  for (long long k = 0; k < (long long)E; k++) {
+    uint64_t o = h_order_[k];
+    int t = e_tgt_[o];
+    NodeGroup *g = groups_[node_group_map_[t]];
+    int port = e_port_[o];
+    if (port >= g->n_port) {
+      bad_port = k;
+      continue;
+    }
+    slot[k] = (uint32_t)(g->acc_base + (long long)port * g->n_pad + (t - g->i_node_0));
+    w[k] = e_w_[o];
+    if (plastic_) {
+      syn[k] = e_syn_[o];
+      post[k] = (uint32_t)t;
+      if (syn[k] > (int)syn_groups_.size()) bad_syn = true;
+    }
+  }
+  if (bad_port >= 0) {
+    uint64_t o = h_order_[bad_port];
+    throw ngpu_exception("Port index " + std::to_string((int)e_port_[o]) +
+                         " out of range for target node " + std::to_string(e_tgt_[o]));
+  }
+  if (bad_syn) throw ngpu_exception("Unrecognized synapse group");
+  NGPU_CUDA(cudaMalloc(&d_grp_off_, sizeof(unsigned long long) * h_grp_off_.size()));
+  NGPU_CUDA(cudaMemcpy(d_grp_off_, h_grp_off_.data(), sizeof(unsigned long long) * h_grp_off_.size(),
+                       cudaMemcpyHostToDevice));
+  NGPU_CUDA(cudaMalloc(&d_e_slot_, sizeof(unsigned) * (E > 0 ? E : 1)));
+  NGPU_CUDA(cudaMalloc(&d_e_w_, sizeof(float) * (E > 0 ? E : 1)));
+  if (E > 0) {
+    NGPU_CUDA(cudaMemcpy(d_e_slot_, slot.data(), sizeof(unsigned) * E, cudaMemcpyHostToDevice));
+    NGPU_CUDA(cudaMemcpy(d_e_w_, w.data(), sizeof(float) * E, cudaMemcpyHostToDevice));
+  }
+  std::vector<uint32_t>().swap(slot);
+  std::vector<int> dl(delays_.begin(), delays_.end());
+  NGPU_CUDA(cudaMalloc(&d_delays_, sizeof(int) * (nd > 0 ? nd : 1)));
+  if (nd > 0) NGPU_CUDA(cudaMemcpy(d_delays_, dl.data(), sizeof(int) * nd, cudaMemcpyHostToDevice));
+  if (nd > NGPU_MAX_DELAYS) throw ngpu_exception("Too many distinct delays");
+  // STDP structures: stamps, target ids and per-target incoming plastic lists
+  if (plastic_) {
+    if (E >= 0xFFFFFFFFull) throw ngpu_exception("Too many connections for plastic synapses");
+    NGPU_CUDA(cudaMalloc(&d_e_syn_, E));
+    NGPU_CUDA(cudaMemcpy(d_e_syn_, syn.data(), E, cudaMemcpyHostToDevice));
+    NGPU_CUDA(cudaMalloc(&d_e_post_, sizeof(unsigned) * E));
+    NGPU_CUDA(cudaMemcpy(d_e_post_, post.data(), sizeof(unsigned) * E, cudaMemcpyHostToDevice));
+    NGPU_CUDA(cudaMalloc(&d_e_stamp_, sizeof(int) * E));
+    LaunchFillInt(d_e_stamp_, (long long)E, -(1 << 30), stream_);
+    std::vector<uint64_t> roff(N + 1, 0);
+    for (uint64_t k = 0; k < E; k++) if (syn[k] > 0) roff[post[k] + 1]++;
+    for (long long i = 0; i < N; i++) roff[i + 1] += roff[i];
+    std::vector<uint32_t> redge(roff[N]);
+    std::vector<uint64_t> fill(roff.begin(), roff.end() - 1);
+    for (uint64_t k = 0; k < E; k++) if (syn[k] > 0) redge[fill[post[k]]++] = (uint32_t)k;
+    NGPU_CUDA(cudaMalloc(&d_rev_off_, sizeof(unsigned long long) * (N + 1)));
+    NGPU_CUDA(cudaMemcpy(d_rev_off_, roff.data(), sizeof(unsigned long long) * (N + 1), cudaMemcpyHostToDevice));
+    NGPU_CUDA(cudaMalloc(&d_rev_edge_, sizeof(unsigned) * (redge.size() + 1)));
+    if (!redge.empty())
+      NGPU_CUDA(cudaMemcpy(d_rev_edge_, redge.data(), sizeof(unsigned) * redge.size(), cudaMemcpyHostToDevice));
+  }
+  // node-level arrays
+  NGPU_CUDA(cudaMalloc(&d_last_spike_T_, sizeof(int) * N));
+  NGPU_CUDA(cudaMalloc(&d_last_rev_T_, sizeof(int) * N));
+  NGPU_CUDA(cudaMalloc(&d_last_post_T_, sizeof(int) * N));
+  NGPU_CUDA(cudaMalloc(&d_last_spike_h_, sizeof(float) * N));
+  LaunchFillInt(d_last_spike_T_, N, (int)0x80000000, stream_);
+  LaunchFillInt(d_last_rev_T_, N, -(1 << 30), stream_);
+  LaunchFillInt(d_last_post_T_, N, (int)0x80000000, stream_);
+  LaunchFillFloat(d_last_spike_h_, N, 0.0f, stream_);
+  has_out_.assign(N, 0);
+  for (long long s = 0; s < N; s++)
+    has_out_[s] = (h_grp_off_[(s + 1) * nd] > h_grp_off_[s * nd]) ? 1 : 0;
+  // spike ring
+  int maxD = 1;
+  for (int d : delays_) maxD = std::max(maxD, d);
+  ring_R_ = maxD + 1;
+  ring_C_ = (int)std::min<long long>(0x7fffffffLL,
+                                     (long long)ceil((double)N * std::max(1.0f, max_spike_num_fact_)) + 64);
+  NGPU_CUDA(cudaMalloc(&d_ring_src_, sizeof(unsigned) * (size_t)ring_R_ * ring_C_));
+  NGPU_CUDA(cudaMalloc(&d_ring_h_, sizeof(float) * (size_t)ring_R_ * ring_C_));
+  NGPU_CUDA(cudaMalloc(&d_ring_cnt_, sizeof(int) * ring_R_));
+  NGPU_CUDA(cudaMemset(d_ring_cnt_, 0, sizeof(int) * ring_R_));
+  // Poisson direct connections: edges whose source is a poisson_generator
+  // node, ordered by (source, delay group, insertion) as in
+  // src/neurongpu.cu:1156-1192; grouped by target for the update kernels.
+  gen_nodes_.clear();
+  std::vector<int> gen_index(N, -1);
+  for (NodeGroup *g : groups_) {
+    if (g->mi->kind != MK_POISSON_GENERATOR) continue;
+    for (int i = 0; i < g->n_node; i++) {
+      gen_index[g->i_node_0 + i] = (int)gen_nodes_.size();
+      gen_nodes_.push_back(g->i_node_0 + i);
+    }
+  }
+  n_gen_ = (int)gen_nodes_.size();
+  if (n_gen_ > 0) {
+    struct DC { uint32_t tgt, gen; uint8_t port; float w, delay; uint64_t stream; };
+    std::vector<DC> dcs;
+    uint64_t stream = 0;
+    for (int gi = 0; gi < n_gen_; gi++) {
+      int s = gen_nodes_[gi];
+      for (int di = 0; di < nd; di++) {
+        for (uint64_t k = h_grp_off_[(uint64_t)s * nd + di]; k < h_grp_off_[(uint64_t)s * nd + di + 1]; k++) {
+          uint64_t o = h_order_[k];
+          DC c;
+          c.tgt = e_tgt_[o]; c.gen = gi; c.port = e_port_[o]; c.w = e_w_[o];
+          c.delay = time_resolution_ * (float)delays_[di];
+          c.stream = stream++;
+          dcs.push_back(c);
+        }
+      }
+    }
+    std::stable_sort(dcs.begin(), dcs.end(), [](const DC &a, const DC &b) { return a.tgt < b.tgt; });
+    size_t M = dcs.size();
+    std::vector<unsigned> off(N + 1, 0), gen(M);
+    std::vector<unsigned char> port(M);
+    std::vector<float> wv(M), dv(M);
+    std::vector<unsigned long long> st(M);
+    for (size_t k = 0; k < M; k++) {
+      off[dcs[k].tgt + 1]++;
+      gen[k] = dcs[k].gen; port[k] = dcs[k].port; wv[k] = dcs[k].w; dv[k] = dcs[k].delay;
+      st[k] = dcs[k].stream;
+    }
+    for (long long i = 0; i < N; i++) off[i + 1] += off[i];
+    NGPU_CUDA(cudaMalloc(&d_dc_off_, sizeof(unsigned) * (N + 1)));
+    NGPU_CUDA(cudaMemcpy(d_dc_off_, off.data(), sizeof(unsigned) * (N + 1), cudaMemcpyHostToDevice));
+    NGPU_CUDA(cudaMalloc(&d_dc_gen_, sizeof(unsigned) * (M + 1)));
+    NGPU_CUDA(cudaMalloc(&d_dc_port_, M + 1));
+    NGPU_CUDA(cudaMalloc(&d_dc_w_, sizeof(float) * (M + 1)));
+    NGPU_CUDA(cudaMalloc(&d_dc_delay_, sizeof(float) * (M + 1)));
+    NGPU_CUDA(cudaMalloc(&d_dc_stream_, sizeof(unsigned long long) * (M + 1)));
+    if (M > 0) {
+      NGPU_CUDA(cudaMemcpy(d_dc_gen_, gen.data(), sizeof(unsigned) * M, cudaMemcpyHostToDevice));
+      NGPU_CUDA(cudaMemcpy(d_dc_port_, port.data(), M, cudaMemcpyHostToDevice));
+      NGPU_CUDA(cudaMemcpy(d_dc_w_, wv.data(), sizeof(float) * M, cudaMemcpyHostToDevice));
+      NGPU_CUDA(cudaMemcpy(d_dc_delay_, dv.data(), sizeof(float) * M, cudaMemcpyHostToDevice));
+      NGPU_CUDA(cudaMemcpy(d_dc_stream_, st.data(), sizeof(unsigned long long) * M, cudaMemcpyHostToDevice));
+    }
+    for (NodeGroup *g : groups_) {
+      g->has_dc = off[g->i_node_0 + g->n_node] > off[g->i_node_0];
+      g->d_dc_off = d_dc_off_ + g->i_node_0;
+    }
+    NGPU_CUDA(cudaMalloc(&d_gen_rate_, sizeof(float) * n_gen_));
+    NGPU_CUDA(cudaMalloc(&d_gen_origin_, sizeof(float) * n_gen_));
+    NGPU_CUDA(cudaMalloc(&d_gen_start_, sizeof(float) * n_gen_));
+    NGPU_CUDA(cudaMalloc(&d_gen_stop_, sizeof(float) * n_gen_));
+    NGPU_CUDA(cudaMalloc(&d_gen_lambda_, sizeof(double) * n_gen_));
+    NGPU_CUDA(cudaMalloc(&d_gen_explam_, sizeof(double) * n_gen_));
+  }
+  // counters, per-group device extras and calibration
+  deliver_blocks_ = 148 * 8;
+  NGPU_CUDA(cudaMalloc(&d_blk_events_, sizeof(unsigned long long) * deliver_blocks_));
+  NGPU_CUDA(cudaMemset(d_blk_events_, 0, sizeof(unsigned long long) * deliver_blocks_));
+  for (NodeGroup *g : groups_) {
+    if (g->mi->kind == MK_RK5) {
+      g->n_blocks = (g->n_node + 127) / 128;
+      NGPU_CUDA(cudaMalloc(&g->d_blk_evals, sizeof(unsigned long long) * g->n_blocks));
+      NGPU_CUDA(cudaMemset(g->d_blk_evals, 0, sizeof(unsigned long long) * g->n_blocks));
+    }
+    calibrate_group(g, time_resolution_, stream_);
+    if (g->mi->den_delay_param >= 0 && g->nparam > g->mi->den_delay_param) {
+      std::vector<float> dd(g->n_node);
+      NGPU_CUDA(cudaMemcpy(dd.data(), g->d_param + (size_t)g->mi->den_delay_param * g->n_pad,
+                           sizeof(float) * g->n_node, cudaMemcpyDeviceToHost));
+      for (int i = 0; i < g->n_node; i++)
+        if ((int)roundf(dd[i] / time_resolution_) > 0) has_out_[g->i_node_0 + i] = 1;
+    }
+  }
+  // synapse group table
+  memset(&syn_table_, 0, sizeof(syn_table_));
+  syn_table_.n = (int)syn_groups_.size();
+  if (syn_table_.n > NGPU_MAX_SYN_GROUPS) throw ngpu_exception("Too many synapse groups");
+  for (int k = 0; k < syn_table_.n; k++) {
+    syn_table_.type[k] = syn_groups_[k].type;
+    for (size_t j = 0; j < syn_groups_[k].values.size() && j < NGPU_MAX_SYN_PARAM; j++)
+      syn_table_.param[k][j] = syn_groups_[k].values[j];
+  }
+  // recording columns
+  n_rec_cols_ = 0;
+  std::vector<RecCol> cols;
+  for (Record &r : records_) {
+    r.col0 = (int)cols.size();
+    for (size_t k = 0; k < r.nodes.size(); k++) {
+      int il;
+      NodeGroup *g = GroupOf(r.nodes[k], 1, il);
+      RecCol c;
+      memset(&c, 0, sizeof(c));
+      c.node = r.nodes[k];
+      const std::string &v = r.var_names[k];
+      if (v == "spike") {
+        c.spike = 1;
+        c.has_out = has_out_[c.node];
+      } else {
+        int col;
+        float *base;
+        if ((col = g->ScalVarIdx(v)) >= 0) base = g->d_var;
+        else if ((col = g->PortVarIdx(v)) >= 0) { col = g->NSV() + r.ports[k] * g->NPV() + col; base = g->d_var; }
+        else if ((col = g->ScalParamIdx(v)) >= 0) base = g->d_param;
+        else { col = g->NSP() + r.ports[k] * g->NPP() + g->PortParamIdx(v); base = g->d_param; }
+        c.ptr = base + (size_t)col * g->n_pad + il;
+      }
+      cols.push_back(c);
+    }
+    if (!r.file_name.empty()) {
+      r.fp = fopen(r.file_name.c_str(), "w");
+      if (!r.fp) throw ngpu_exception("Cannot open record file " + r.file_name);
+    }
+  }
+  n_rec_cols_ = (int)cols.size();
+  if (n_rec_cols_ > 0) {
+    NGPU_CUDA(cudaMalloc(&d_rec_cols_, sizeof(RecCol) * n_rec_cols_));
+    NGPU_CUDA(cudaMemcpy(d_rec_cols_, cols.data(), sizeof(RecCol) * n_rec_cols_, cudaMemcpyHostToDevice));
+    rec_cap_rows_ = std::max<long long>(4 * graph_chunk_ + 8, 4096);
+    NGPU_CUDA(cudaMalloc(&d_rec_buf_, sizeof(float) * (size_t)rec_cap_rows_ * (n_rec_cols_ + 1)));
+  }
+  // step context
+  NGPU_CUDA(cudaMalloc(&d_ctx_, sizeof(StepCtx)));
+  StepCtx c;
+  memset(&c, 0, sizeof(c));
+  NGPU_CUDA(cudaMemcpy(d_ctx_, &c, sizeof(StepCtx), cudaMemcpyHostToDevice));
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  NGPU_CUDA(cudaDeviceSynchronize());
+}
+
+void NeuronGPU::UploadGeneratorParams() {
+  if (n_gen_ == 0) return;
+  std::vector<float> rate(n_gen_), origin(n_gen_), start(n_gen_), stop(n_gen_);
+  std::vector<double> lam(n_gen_), explam(n_gen_);
+  const float time_step = (float)(time_resolution_ / 1000.0);
+  for (int k = 0; k < n_gen_; k++) {
+    int node = gen_nodes_[k];
+    NodeGroup *g = groups_[node_group_map_[node]];
+    int il = node - g->i_node_0;
+    float v[4];
+    for (int j = 0; j < 4; j++)
+      NGPU_CUDA(cudaMemcpy(&v[j], g->d_param + (size_t)j * g->n_pad + il, sizeof(float),
+                           cudaMemcpyDeviceToHost));
+    rate[k] = v[0]; origin[k] = v[1]; start[k] = v[2]; stop[k] = v[3];
+    float lf = time_step * rate[k];      // float product, as in src/poiss_gen.cu:62
+    lam[k] = (double)lf;
+    explam[k] = exp(-(double)lf);
+  }
+  NGPU_CUDA(cudaMemcpy(d_gen_rate_, rate.data(), sizeof(float) * n_gen_, cudaMemcpyHostToDevice));
+  NGPU_CUDA(cudaMemcpy(d_gen_origin_, origin.data(), sizeof(float) * n_gen_, cudaMemcpyHostToDevice));
+  NGPU_CUDA(cudaMemcpy(d_gen_start_, start.data(), sizeof(float) * n_gen_, cudaMemcpyHostToDevice));
+  NGPU_CUDA(cudaMemcpy(d_gen_stop_, stop.data(), sizeof(float) * n_gen_, cudaMemcpyHostToDevice));
+  NGPU_CUDA(cudaMemcpy(d_gen_lambda_, lam.data(), sizeof(double) * n_gen_, cudaMemcpyHostToDevice));
+  NGPU_CUDA(cudaMemcpy(d_gen_explam_, explam.data(), sizeof(double) * n_gen_, cudaMemcpyHostToDevice));
+}
+
+// ---------------------------------------------------------------------------
+// simulation loop
+// ---------------------------------------------------------------------------
+void NeuronGPU::InvalidateGraphs() {
+  for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
+  graphs_.clear();
+}
+
+void NeuronGPU::KEvent(int step_in_chunk, int j) {
+  size_t idx = (size_t)step_in_chunk * 5 + j;
+  while (kev_.size() <= idx) {
+    cudaEvent_t e;
+    NGPU_CUDA(cudaEventCreate(&e));
+    kev_.push_back(e);
+  }
+  NGPU_CUDA(cudaEventRecordWithFlags(kev_[idx], stream_,
+                                     capturing_ ? cudaEventRecordExternal : cudaEventRecordDefault));
+}
+
+void NeuronGPU::AccumulateKernelTiming(int n_steps) {
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  for (int k = 0; k < n_steps; k++) {
+    for (int j = 0; j < 4; j++) {
+      float ms = 0.0f;
+      NGPU_CUDA(cudaEventElapsedTime(&ms, kev_[(size_t)k * 5 + j], kev_[(size_t)k * 5 + j + 1]));
+      ktime_ms_[j] += ms;
+      klaunch_[j] += 1;
+    }
+  }
+}
+
+int NeuronGPU::SetKernelTiming(int on) {
+  ktime_ = on != 0;
+  for (int j = 0; j < 4; j++) { ktime_ms_[j] = 0; klaunch_[j] = 0; }
+  InvalidateGraphs();
+  return 0;
+}
+
+int NeuronGPU::GetKernelTiming(int kind, double *total_ms, long long *launches) {
+  if (kind < 0 || kind > 3) throw ngpu_exception("Unknown kernel class");
+  *total_ms = ktime_ms_[kind];
+  *launches = klaunch_[kind];
+  return 0;
+}
+
+// one time step on stream_ (kernel launches only, no host synchronisation)
+void NeuronGPU::EnqueueStep(int step_in_chunk) {
+  if (ktime_) KEvent(step_in_chunk, 0);
+  for (NodeGroup *g : groups_) {
+    const ModelInfo *mi = g->mi;
+    switch (mi->kind) {
+      case MK_RK5:
+        LaunchRk5Update(mi->rk5_model, g->n_port, MakeGroupArgs(g), MakeInputArgs(g),
+                        MakePushArgs(g), d_ctx_, stream_);
+        break;
+      case MK_IAF_PSC_EXP:
+        LaunchIafPscExpUpdate(MakeGroupArgs(g), MakeInputArgs(g), MakePushArgs(g), d_ctx_, stream_);
+        break;
+      case MK_SPIKE_GENERATOR:
+        if (g->d_sg_off) LaunchSpikeGeneratorUpdate(MakeGroupArgs(g), MakePushArgs(g), d_ctx_, stream_);
+        break;
+      case MK_PARROT:
+        LaunchParrotUpdate(MakeGroupArgs(g), MakeInputArgs(g), MakePushArgs(g), d_ctx_, stream_);
+        break;
+      case MK_SPIKE_DETECTOR:
+        LaunchSpikeDetectorUpdate(MakeGroupArgs(g), MakeInputArgs(g), d_ctx_, stream_);
+        break;
+      case MK_POISSON_NODES: {
+        double lam = (double)g->poisson_lambda;
+        LaunchPoissonNodesUpdate(MakeGroupArgs(g), MakePushArgs(g), lam, exp(-lam), kernel_seed_,
+                                 d_ctx_, stream_);
+        break;
+      }
+      default:
+        break;
+    }
+  }
+  if (ktime_) KEvent(step_in_chunk, 1);
+  DeliverArgs d = MakeDeliverArgs();
+  LaunchDeliver(d, syn_table_, d_ctx_, deliver_blocks_, stream_);
+  if (ktime_) KEvent(step_in_chunk, 2);
+  if (plastic_) LaunchStdpPost(d, syn_table_, d_ctx_, 148 * 2, stream_);
+  if (ktime_) KEvent(step_in_chunk, 3);
+  int flags = 1;
+  if (n_rec_cols_ > 0) {
+    LaunchRecord(d_rec_cols_, n_rec_cols_, d_rec_buf_, rec_cap_rows_, d_last_spike_T_,
+                 d_last_spike_h_, 0, time_resolution_, d_ctx_, stream_);
+    flags |= 2;
+  }
+  LaunchAdvance(d_ring_cnt_, ring_R_, ring_C_, flags, d_ctx_, stream_);
+  if (ktime_) KEvent(step_in_chunk, 4);
+}
+
+void NeuronGPU::LaunchSteps(int n_steps) {
+  if (n_steps <= 0) return;
+  if (n_rec_cols_ > 0 && rec_rows_used_ + n_steps > rec_cap_rows_) FlushRecords();
+  if (ktime_) {
+    // create the event pool before any capture
+    for (int k = (int)(kev_.size() / 5); k < n_steps; k++) {
+      for (int j = 0; j < 5; j++) {
+        cudaEvent_t e;
+        NGPU_CUDA(cudaEventCreate(&e));
+        kev_.push_back(e);
+      }
+    }
+  }
+  if (!use_graphs_) {
+    for (int k = 0; k < n_steps; k++) EnqueueStep(k);
+  } else {
+    auto it = graphs_.find(n_steps);
+    if (it == graphs_.end()) {
+      cudaGraph_t graph;
+      NGPU_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+      capturing_ = true;
+      try {
+        for (int k = 0; k < n_steps; k++) EnqueueStep(k);
+      } catch (...) {
+        capturing_ = false;
+        cudaStreamEndCapture(stream_, &graph);
+        throw;
+      }
+      capturing_ = false;
+      NGPU_CUDA(cudaStreamEndCapture(stream_, &graph));
+      cudaGraphExec_t exec;
+      NGPU_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+      cudaGraphDestroy(graph);
+      it = graphs_.emplace(n_steps, exec).first;
+    }
+    NGPU_CUDA(cudaGraphLaunch(it->second, stream_));
+  }
+  if (n_rec_cols_ > 0) rec_rows_used_ += n_steps;
+  NGPU_CUDA(cudaGetLastError());
+  if (ktime_) AccumulateKernelTiming(n_steps);
+}
+
+void NeuronGPU::WriteInitialRecord() {
+  if (n_rec_cols_ == 0) return;
+  if (rec_rows_used_ + 1 > rec_cap_rows_) FlushRecords();
+  LaunchRecord(d_rec_cols_, n_rec_cols_, d_rec_buf_, rec_cap_rows_, d_last_spike_T_,
+               d_last_spike_h_, 1, time_resolution_, d_ctx_, stream_);
+  LaunchAdvance(d_ring_cnt_, ring_R_, ring_C_, 2, d_ctx_, stream_);
+  rec_rows_used_ += 1;
+}
+
+void NeuronGPU::FlushRecords() {
+  if (n_rec_cols_ == 0 || d_rec_buf_ == nullptr) return;
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  if (rec_rows_used_ > 0) {
+    const int nc = n_rec_cols_ + 1;
+    std::vector<float> buf((size_t)rec_rows_used_ * nc);
+    NGPU_CUDA(cudaMemcpy(buf.data(), d_rec_buf_, sizeof(float) * buf.size(), cudaMemcpyDeviceToHost));
+    for (Record &r : records_) {
+      const int ncol = (int)r.nodes.size();
+      for (long long row = 0; row < rec_rows_used_; row++) {
+        const float *src = &buf[(size_t)row * nc];
+        std::vector<float> v(ncol + 1);
+        v[0] = src[0];
+        for (int k = 0; k < ncol; k++) v[k + 1] = src[1 + r.col0 + k];
+        if (r.fp) {
+          fprintf(r.fp, "%f", v[0]);
+          for (int k = 0; k < ncol; k++) fprintf(r.fp, "\t%f", v[k + 1]);
+          fprintf(r.fp, "\n");
+        }
+        r.data.push_back(std::move(v));
+      }
+      if (r.fp) fflush(r.fp);
+    }
+  }
+  rec_rows_used_ = 0;
+  long long zero = 0;
+  NGPU_CUDA(cudaMemcpy((char *)d_ctx_ + offsetof(StepCtx, rec_row), &zero, sizeof(long long),
+                       cudaMemcpyHostToDevice));
+}
+
+void NeuronGPU::CheckDeviceErrors() {
+  StepCtx c;
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  NGPU_CUDA(cudaMemcpy(&c, d_ctx_, sizeof(StepCtx), cudaMemcpyDeviceToHost));
+  if (c.err) {
+    unsigned e = c.err;
+    unsigned zero = 0;
+    NGPU_CUDA(cudaMemcpy((char *)d_ctx_ + offsetof(StepCtx, err), &zero, sizeof(unsigned),
+                         cudaMemcpyHostToDevice));
+    std::string m = "Simulation error:";
+    if (e & DERR_RING_OVERFLOW) m += " more spikes in one step than the spike list can hold (increase max_spike_num_fact);";
+    if (e & DERR_RK5_STUCK) m += " RK5 integration exceeded the substep limit;";
+    if (e & DERR_REC_OVERFLOW) m += " recording buffer overflow;";
+    throw ngpu_exception(m);
+  }
+}
+
+int NeuronGPU::FlushInput() {
+  if (!calibrate_flag_ || !input_pending_) return 0;
+  for (NodeGroup *g : groups_) {
+    if (g->n_port > 0 && g->mi->in_var >= 0)
+      LaunchFoldInput(MakeGroupArgs(g), MakeInputArgs(g), d_ctx_, stream_);
+  }
+  LaunchClearPending(d_ctx_, stream_);
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  input_pending_ = false;
+  return 0;
+}
+
+int NeuronGPU::StartSimulation() {
+  if (!calibrate_flag_) Calibrate();
+  FlushInput();
+  if (first_simulation_flag_) {
+    // ctx at t_min for the initial record
+    StepCtx c;
+    NGPU_CUDA(cudaMemcpy(&c, d_ctx_, sizeof(StepCtx), cudaMemcpyDeviceToHost));
+    c.it = 0;
+    c.t0 = neural_time_;
+    c.T0 = (long long)round(neural_time_ / time_resolution_);
+    NGPU_CUDA(cudaMemcpy(d_ctx_, &c, sizeof(StepCtx), cudaMemcpyHostToDevice));
+    WriteInitialRecord();
+    first_simulation_flag_ = false;
+  }
+  if (verbosity_level_ >= 1) {
+    printf("Simulating ...\n");
+    printf("Neural activity simulation time: %.3lf\n", (double)sim_time_);
+  }
+  UploadGeneratorParams();
+  neur_t0_ = neural_time_;
+  it_ = 0;
+  Nt_ = (long long)round(sim_time_ / time_resolution_);
+  StepCtx c;
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  NGPU_CUDA(cudaMemcpy(&c, d_ctx_, sizeof(StepCtx), cudaMemcpyDeviceToHost));
+  c.it = 0;
+  c.t0 = neur_t0_;
+  c.T0 = (long long)round(neur_t0_ / time_resolution_);
+  c.poisson_pending = 0;
+  NGPU_CUDA(cudaMemcpy(d_ctx_, &c, sizeof(StepCtx), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int NeuronGPU::SimulationStep() {
+  if (first_simulation_flag_) StartSimulation();
+  if (input_pending_ == false && it_ > 0) {
+    // state was read in between: the fold already consumed the pending
+    // input, so the device context says so (poisson_pending == 0)
+  }
+  LaunchSteps(1);
+  it_++;
+  input_pending_ = true;
+  neural_time_ = neur_t0_ + (double)time_resolution_ * (double)it_;
+  return 0;
+}
+
+int NeuronGPU::EndSimulation() {
+  FlushInput();
+  FlushRecords();
+  CheckDeviceErrors();
+  if (verbosity_level_ >= 2) printf("%.3lf\n", neural_time_);
+  return 0;
+}
+
+int NeuronGPU::Simulate() {
+  StartSimulation();
+  auto t_start = std::chrono::steady_clock::now();
+  if (!ev_start_) {
+    NGPU_CUDA(cudaEventCreate(&ev_start_));
+    NGPU_CUDA(cudaEventCreate(&ev_stop_));
+  }
+  NGPU_CUDA(cudaEventRecord(ev_start_, stream_));
+  long long done = 0;
+  while (done < Nt_) {
+    if (verbosity_level_ >= 2 && done % 100 == 0)
+      printf("%.3lf\n", neur_t0_ + (double)time_resolution_ * (double)done);
+    long long n = std::min<long long>(graph_chunk_, Nt_ - done);
+    if (verbosity_level_ >= 2) n = std::min<long long>(n, 100 - done % 100);
+    LaunchSteps((int)n);
+    done += n;
+    it_ = done;
+    input_pending_ = true;
+  }
+  neural_time_ = neur_t0_ + (double)time_resolution_ * (double)Nt_;
+  NGPU_CUDA(cudaEventRecord(ev_stop_, stream_));
+  NGPU_CUDA(cudaEventSynchronize(ev_stop_));
+  float dev_ms = 0.0f;
+  NGPU_CUDA(cudaEventElapsedTime(&dev_ms, ev_start_, ev_stop_));
+  last_sim_device_ms_ = dev_ms;
+  EndSimulation();
+  last_sim_seconds_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  return 0;
+}
+
+int NeuronGPU::PushSpikesToNodes(int n, const int *nodes) {
+  (void)n; (void)nodes;
+  throw ngpu_exception("PushSpikesToNodes is only available for external-neuron co-simulation, which this build does not provide");
+}
+
+unsigned long long NeuronGPU::StageEvaluations() {
+  unsigned long long tot = 0;
+  for (NodeGroup *g : groups_) {
+    if (!g->d_blk_evals) continue;
+    std::vector<unsigned long long> v(g->n_blocks);
+    NGPU_CUDA(cudaMemcpy(v.data(), g->d_blk_evals, sizeof(unsigned long long) * g->n_blocks,
+                         cudaMemcpyDeviceToHost));
+    for (auto x : v) tot += x;
+  }
+  return tot;
+}
+
+unsigned long long NeuronGPU::DeliveredEvents() {
+  if (!d_blk_events_) return 0;
+  std::vector<unsigned long long> v(deliver_blocks_);
+  NGPU_CUDA(cudaMemcpy(v.data(), d_blk_events_, sizeof(unsigned long long) * deliver_blocks_,
+                       cudaMemcpyDeviceToHost));
+  unsigned long long tot = 0;
+  for (auto x : v) tot += x;
+  return tot;
+}
+
+unsigned long long NeuronGPU::TotalSpikes() {
+  if (!d_ctx_) return 0;
+  StepCtx c;
+  NGPU_CUDA(cudaMemcpy(&c, d_ctx_, sizeof(StepCtx), cudaMemcpyDeviceToHost));
+  return c.n_spikes;
+}
+
+}  // namespace ngpu

@@ -1,0 +1,422 @@
+// NeuronGPU: host driver of the B200 simulation core.
+//
+// Public methods mirror the reference class NeuronGPU (src/neurongpu.h:94-679)
+// so the C ABI (src/neurongpu_C.h) maps one to one; the internals (SoA state,
+// CSR delivery graph, spike ring, device-side step counter, CUDA graphs) are
+// this build's own.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "ngpu_device.h"
+#include "ngpu_kernels.h"
+#include "ngpu_models.h"
+
+namespace ngpu {
+
+class ngpu_exception : public std::exception {
+  std::string msg_;
+
+ public:
+  explicit ngpu_exception(const std::string &m) : msg_(m) {}
+  const char *what() const noexcept override { return msg_.c_str(); }
+};
+
+#define NGPU_CUDA(call)                                                    \
+  do {                                                                     \
+    cudaError_t e_ = (call);                                               \
+    if (e_ != cudaSuccess) {                                               \
+      throw ngpu::ngpu_exception(std::string("CUDA error: ") +             \
+                                 cudaGetErrorString(e_) + " at " +         \
+                                 __FILE__ + ":" + std::to_string(__LINE__)); \
+    }                                                                      \
+  } while (0)
+
+enum { ON_EXCEPTION_EXIT = 0, ON_EXCEPTION_HANDLE = 1 };
+
+struct ConnectionId {
+  int i_source_;
+  int i_group_;
+  int i_conn_;
+};
+
+struct ConnectionStatus {
+  int i_source;
+  int i_target;
+  unsigned char port;
+  unsigned char syn_group;
+  float delay;
+  float weight;
+};
+
+enum ConnRule {
+  ONE_TO_ONE = 0, ALL_TO_ALL, FIXED_TOTAL_NUMBER, FIXED_INDEGREE,
+  FIXED_OUTDEGREE, N_CONN_RULE
+};
+
+struct ConnSpec {
+  int rule_ = ALL_TO_ALL;
+  int total_num_ = 0;
+  int indegree_ = 0;
+  int outdegree_ = 0;
+  void Init() { *this = ConnSpec(); }
+  int SetParam(const std::string &name, int value);
+  static bool IsParam(const std::string &name);
+};
+
+struct SynSpec {
+  unsigned char syn_group_ = 0;
+  unsigned char port_ = 0;
+  float weight_ = 0.0f;
+  float delay_ = 0.0f;
+  const float *weight_array_ = nullptr;
+  const float *delay_array_ = nullptr;
+  void Init() { *this = SynSpec(); }
+  int SetParam(const std::string &name, int value);
+  int SetParam(const std::string &name, float value);
+  int SetParam(const std::string &name, const float *arr);
+  static bool IsIntParam(const std::string &name);
+  static bool IsFloatParam(const std::string &name);
+  static bool IsFloatPtParam(const std::string &name);
+};
+
+struct SynGroupHost {
+  int type;                       // 1 test_syn_model, 2 stdp
+  std::vector<std::string> names;
+  std::vector<float> values;
+};
+
+// One node group (one Create call).
+struct NodeGroup {
+  int model = -1;                 // index into ModelCatalogue()
+  const ModelInfo *mi = nullptr;
+  int i_node_0 = 0, n_node = 0, n_port = 0, n_pad = 0;
+  int nvar = 0, nparam = 0;
+  float *d_var = nullptr, *d_param = nullptr, *d_h = nullptr, *d_dx = nullptr;
+  std::vector<char> p_uniform;
+  std::vector<float> p_uval;
+  std::vector<float> group_param;
+  float rk5_eps = 1.0e-6f;
+  long long acc_base = 0;
+  // spike count / spike-time recording
+  int *d_spike_count = nullptr;
+  float *d_rec_times = nullptr;
+  int *d_n_rec = nullptr;
+  int max_rec = 0;
+  std::vector<std::string> int_var_names;
+  // spike generator
+  std::vector<std::vector<float>> sg_times, sg_heights;
+  int *d_sg_off = nullptr, *d_sg_step = nullptr, *d_sg_next = nullptr;
+  float *d_sg_height = nullptr;
+  // Poisson direct connections into this group (CSR by local node)
+  unsigned *d_dc_off = nullptr;
+  bool has_dc = false;
+  // CreatePoissonGenerator nodes
+  float poisson_lambda = 0.0f;
+  // per-block RK5 derivative evaluation counters
+  unsigned long long *d_blk_evals = nullptr;
+  int n_blocks = 0;
+
+  int ScalVarIdx(const std::string &n) const;
+  int PortVarIdx(const std::string &n) const;
+  int ScalParamIdx(const std::string &n) const;
+  int PortParamIdx(const std::string &n) const;
+  int GroupParamIdx(const std::string &n) const;
+  int IntVarIdx(const std::string &n) const;
+  int ArrayParamIdx(const std::string &n) const;
+  int NSV() const { return (int)mi->scal_var.size(); }
+  int NPV() const { return (int)mi->port_var.size(); }
+  int NSP() const { return (int)mi->scal_param.size(); }
+  int NPP() const { return (int)mi->port_param.size(); }
+};
+
+struct Record {
+  std::string file_name;
+  std::vector<std::string> var_names;
+  std::vector<int> nodes, ports;
+  std::vector<std::vector<float>> data;   // rows: t, v1, v2, ...
+  FILE *fp = nullptr;
+  int col0 = 0;                           // first column in device buffer
+};
+
+class NeuronGPU {
+ public:
+  NeuronGPU();
+  ~NeuronGPU();
+
+  // errors
+  bool error_flag_ = false;
+  std::string error_message_;
+  unsigned char error_code_ = 0;
+  int on_exception_ = ON_EXCEPTION_EXIT;
+  void SetErrorFlag(bool f) { error_flag_ = f; }
+  void SetErrorMessage(const std::string &m) { error_message_ = m; }
+  void SetErrorCode(unsigned char c) { error_code_ = c; }
+  char *GetErrorMessage() { return (char *)error_message_.c_str(); }
+  unsigned char GetErrorCode() { return error_code_; }
+  void SetOnException(int v) { on_exception_ = v; }
+  int OnException() { return on_exception_; }
+
+  // kernel parameters
+  int SetRandomSeed(unsigned long long seed);
+  int SetTimeResolution(float t);
+  float GetTimeResolution() { return time_resolution_; }
+  int SetMaxSpikeBufferSize(int n) { max_spike_buffer_size_ = n; return 0; }
+  int GetMaxSpikeBufferSize() { return max_spike_buffer_size_; }
+  int SetSimTime(float t) { sim_time_ = t; return 0; }
+  int SetVerbosityLevel(int v) { verbosity_level_ = v; return 0; }
+  std::vector<std::string> GetFloatParamNames();
+  std::vector<std::string> GetIntParamNames();
+  bool IsFloatParam(const std::string &n);
+  bool IsIntParam(const std::string &n);
+  int GetFloatParamIdx(const std::string &n);
+  int GetIntParamIdx(const std::string &n);
+  float GetFloatParam(const std::string &n);
+  int GetIntParam(const std::string &n);
+  int SetFloatParam(const std::string &n, float v);
+  int SetIntParam(const std::string &n, int v);
+
+  // nodes
+  int Create(const std::string &model, int n_node, int n_port);
+  int CreatePoissonGenerator(int n_node, float rate);
+  int SetNeuronParam(int i_node, int n, const std::string &name, float val);
+  int SetNeuronParam(const int *nodes, int n, const std::string &name,
+                     float val);
+  int SetNeuronParam(int i_node, int n, const std::string &name,
+                     const float *arr, int size);
+  int SetNeuronParam(const int *nodes, int n, const std::string &name,
+                     const float *arr, int size);
+  int SetNeuronIntVar(int i_node, int n, const std::string &name, int val);
+  int SetNeuronIntVar(const int *nodes, int n, const std::string &name,
+                      int val);
+  int SetNeuronVar(int i_node, int n, const std::string &name, float val);
+  int SetNeuronVar(const int *nodes, int n, const std::string &name,
+                   float val);
+  int SetNeuronVar(int i_node, int n, const std::string &name,
+                   const float *arr, int size);
+  int SetNeuronVar(const int *nodes, int n, const std::string &name,
+                   const float *arr, int size);
+  int IsNeuronScalParam(int i_node, const std::string &n);
+  int IsNeuronPortParam(int i_node, const std::string &n);
+  int IsNeuronArrayParam(int i_node, const std::string &n);
+  int IsNeuronGroupParam(int i_node, const std::string &n);
+  int IsNeuronIntVar(int i_node, const std::string &n);
+  int IsNeuronScalVar(int i_node, const std::string &n);
+  int IsNeuronPortVar(int i_node, const std::string &n);
+  int IsNeuronArrayVar(int i_node, const std::string &n);
+  int GetNeuronParamSize(int i_node, const std::string &n);
+  int GetNeuronVarSize(int i_node, const std::string &n);
+  float *GetNeuronParam(int i_node, int n, const std::string &name);
+  float *GetNeuronParam(const int *nodes, int n, const std::string &name);
+  float *GetArrayParam(int i_node, const std::string &name);
+  int *GetNeuronIntVar(int i_node, int n, const std::string &name);
+  int *GetNeuronIntVar(const int *nodes, int n, const std::string &name);
+  float *GetNeuronVar(int i_node, int n, const std::string &name);
+  float *GetNeuronVar(const int *nodes, int n, const std::string &name);
+  float *GetArrayVar(int i_node, const std::string &name);
+  int SetNeuronGroupParam(int i_node, int n, const std::string &name,
+                          float val);
+  float GetNeuronGroupParam(int i_node, const std::string &name);
+  std::vector<std::string> GetIntVarNames(int i_node);
+  std::vector<std::string> GetScalVarNames(int i_node);
+  std::vector<std::string> GetPortVarNames(int i_node);
+  std::vector<std::string> GetScalParamNames(int i_node);
+  std::vector<std::string> GetPortParamNames(int i_node);
+  std::vector<std::string> GetGroupParamNames(int i_node);
+  std::vector<std::string> GetArrayParamNames(int i_node);
+  std::vector<std::string> GetArrayVarNames(int i_node);
+
+  // recording
+  int CreateRecord(const std::string &file, const std::vector<std::string> &vars,
+                   const int *nodes, const int *ports, int n);
+  std::vector<std::vector<float>> *GetRecordData(int i_record);
+  int ActivateSpikeCount(int i_node, int n);
+  int ActivateRecSpikeTimes(int i_node, int n, int max_n);
+  int GetNRecSpikeTimes(int i_node);
+  std::vector<float> GetRecSpikeTimes(int i_node);
+
+  // connections
+  int Connect(int i_source, int i_target, unsigned char port,
+              unsigned char syn_group, float weight, float delay);
+  int Connect(const int *src_arr, int i_src0, int n_source,
+              const int *tgt_arr, int i_tgt0, int n_target,
+              ConnSpec &cs, SynSpec &ss);
+  std::vector<ConnectionId> GetConnections(const int *src_arr, int i_src0,
+                                           int n_source, const int *tgt_arr,
+                                           int i_tgt0, int n_target,
+                                           int syn_group);
+  ConnectionStatus GetConnectionStatus(ConnectionId id);
+  int CreateSynGroup(const std::string &model);
+  int GetSynGroupNParam(int sg);
+  std::vector<std::string> GetSynGroupParamNames(int sg);
+  bool IsSynGroupParam(int sg, const std::string &n);
+  int GetSynGroupParamIdx(int sg, const std::string &n);
+  float GetSynGroupParam(int sg, const std::string &n);
+  int SetSynGroupParam(int sg, const std::string &n, float v);
+
+  // random arrays (host, counter-based)
+  unsigned int *RandomInt(size_t n);
+  float *RandomUniform(size_t n);
+  float *RandomNormal(size_t n, float mean, float stddev);
+  float *RandomNormalClipped(size_t n, float mean, float stddev, float vmin,
+                             float vmax, float vstep);
+
+  // simulation
+  int Calibrate();
+  int Simulate();
+  int Simulate(float sim_time) { sim_time_ = sim_time; return Simulate(); }
+  int StartSimulation();
+  int SimulationStep();
+  int EndSimulation();
+  int PushSpikesToNodes(int n, const int *nodes);
+
+  // statistics exposed through the extension entry points
+  unsigned long long StageEvaluations();
+  unsigned long long DeliveredEvents();
+  unsigned long long TotalSpikes();
+  double LastSimulateSeconds() { return last_sim_seconds_; }
+  double LastSimulateDeviceMs() { return last_sim_device_ms_; }
+  // per-kernel-class device timing (CUDA events around every launch)
+  int SetKernelTiming(int on);
+  int GetKernelTiming(int kind, double *total_ms, long long *launches);
+  int SetGraphChunk(int g) { graph_chunk_ = g > 0 ? g : 1; InvalidateGraphs(); return 0; }
+  long long NNodes() { return (long long)node_group_map_.size(); }
+  long long NConnections() { return (long long)e_src_.size(); }
+  int UseGraphs(int f) { use_graphs_ = f != 0; return 0; }
+  // synchronous device copy of a raw column (tests, bench)
+  cudaStream_t Stream() { return stream_; }
+  int FlushInput();
+
+  // public state read by the C layer
+  ConnSpec conn_spec_;
+  SynSpec syn_spec_;
+
+ private:
+  // kernel parameters
+  float time_resolution_ = 0.1f;
+  float sim_time_ = 1000.0f;
+  float max_spike_num_fact_ = 1.0f;
+  float max_spike_per_host_fact_ = 1.0f;
+  int verbosity_level_ = 4;
+  int max_spike_buffer_size_ = 20;
+  int remote_spike_height_flag_ = 0;
+  unsigned long long rnd_seed_ = 54321ULL;
+  unsigned long long kernel_seed_ = 54321ULL + 12345ULL;
+  unsigned long long rng_calls_ = 0;   // host RNG stream counter
+
+  // structure
+  std::vector<NodeGroup *> groups_;
+  std::vector<int> node_group_map_;
+  std::vector<SynGroupHost> syn_groups_;
+  std::vector<Record> records_;
+
+  // edges in insertion order (before calibration)
+  std::vector<uint32_t> e_src_, e_tgt_;
+  std::vector<uint8_t> e_port_, e_syn_;
+  std::vector<float> e_w_;
+  std::vector<uint16_t> e_d_;         // delay in steps (>= 1)
+  bool host_csr_valid_ = false;
+  // host CSR (by source, then delay index, insertion order inside)
+  std::vector<int> delays_;           // distinct delays (steps), sorted
+  std::vector<int> delay_index_;      // D -> di (or -1)
+  std::vector<uint64_t> h_grp_off_;   // [n_nodes*nd + 1]
+  std::vector<uint64_t> h_order_;     // csr position -> insertion index
+
+  // device state
+  bool calibrate_flag_ = false;
+  bool first_simulation_flag_ = true;
+  cudaStream_t stream_ = nullptr;
+  StepCtx *d_ctx_ = nullptr;
+  long long *d_acc_ = nullptr;
+  long long n_acc_ = 0;
+  unsigned *d_ring_src_ = nullptr;
+  float *d_ring_h_ = nullptr;
+  int *d_ring_cnt_ = nullptr;
+  int ring_R_ = 0, ring_C_ = 0;
+  int *d_last_spike_T_ = nullptr, *d_last_rev_T_ = nullptr;
+  int *d_last_post_T_ = nullptr;
+  float *d_last_spike_h_ = nullptr;
+  unsigned long long *d_grp_off_ = nullptr;
+  unsigned *d_e_slot_ = nullptr;
+  float *d_e_w_ = nullptr;
+  unsigned char *d_e_syn_ = nullptr;
+  int *d_e_stamp_ = nullptr;
+  unsigned *d_e_post_ = nullptr;
+  unsigned long long *d_rev_off_ = nullptr;
+  unsigned *d_rev_edge_ = nullptr;
+  int *d_delays_ = nullptr;
+  bool plastic_ = false;
+  std::vector<unsigned char> has_out_;
+  // Poisson direct connections (global arrays, CSR by target node)
+  unsigned *d_dc_off_ = nullptr, *d_dc_gen_ = nullptr;
+  unsigned char *d_dc_port_ = nullptr;
+  float *d_dc_w_ = nullptr, *d_dc_delay_ = nullptr;
+  unsigned long long *d_dc_stream_ = nullptr;
+  int n_gen_ = 0;
+  std::vector<int> gen_nodes_;        // generator index -> node
+  float *d_gen_rate_ = nullptr, *d_gen_origin_ = nullptr;
+  float *d_gen_start_ = nullptr, *d_gen_stop_ = nullptr;
+  double *d_gen_lambda_ = nullptr, *d_gen_explam_ = nullptr;
+  // delivery counters
+  unsigned long long *d_blk_events_ = nullptr;
+  int deliver_blocks_ = 0;
+  // recording
+  RecCol *d_rec_cols_ = nullptr;
+  int n_rec_cols_ = 0;
+  float *d_rec_buf_ = nullptr;
+  long long rec_cap_rows_ = 0;
+  long long rec_rows_used_ = 0;
+  SynGroupTable syn_table_;
+
+  // session
+  double neural_time_ = 0.0, neur_t0_ = 0.0, t_min_ = 0.0;
+  long long it_ = 0, Nt_ = 0;
+  bool input_pending_ = false;
+  double last_sim_seconds_ = 0.0;
+  double last_sim_device_ms_ = 0.0;
+  cudaEvent_t ev_start_ = nullptr, ev_stop_ = nullptr;
+  bool ktime_ = false;
+  bool capturing_ = false;
+  std::vector<cudaEvent_t> kev_;
+  double ktime_ms_[4] = {0, 0, 0, 0};
+  long long klaunch_[4] = {0, 0, 0, 0};
+  void KEvent(int step_in_chunk, int j);
+  void AccumulateKernelTiming(int n_steps);
+
+  // graphs
+  bool use_graphs_ = true;
+  int graph_chunk_ = 100;
+  std::map<int, cudaGraphExec_t> graphs_;
+  void InvalidateGraphs();
+  void LaunchSteps(int n_steps);
+  void EnqueueStep(int step_in_chunk);
+
+  // helpers
+  NodeGroup *GroupOf(int i_node, int n, int &i_local);
+  NodeGroup *GroupOfList(const int *nodes, int n, std::vector<int> &local);
+  void CheckUncalibrated(const std::string &msg);
+  void BuildHostCSR();
+  void BuildDevice();
+  void UploadGeneratorParams();
+  void FlushRecords();
+  void WriteInitialRecord();
+  GroupArgs MakeGroupArgs(NodeGroup *g);
+  InputArgs MakeInputArgs(NodeGroup *g);
+  PushArgs MakePushArgs(NodeGroup *g);
+  DeliverArgs MakeDeliverArgs();
+  void SetParamColumn(NodeGroup *g, int col, int i0, int n, const int *nodes,
+                      float val, const float *vals, int stride);
+  void GetParamColumn(NodeGroup *g, float *col_base, int i0, int n,
+                      const int *nodes, float *out, int stride);
+  void CheckDeviceErrors();
+  unsigned long long NextRngStream() { return rng_calls_++; }
+  void AddEdge(int s, int t, unsigned char port, unsigned char syn, float w,
+               float delay);
+  void FreeDevice();
+};
+
+}  // namespace ngpu

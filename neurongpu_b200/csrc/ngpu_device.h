@@ -1,0 +1,142 @@
+// Device-side data layout shared by the kernels and the host driver.
+//
+// Layout in HBM (one simulation instance):
+//   * per node group, state and parameters as structure-of-arrays columns of
+//     length n_pad (n rounded up to 128): var[j*n_pad + i], param[j*n_pad + i];
+//     RK5 groups add h[i] (adaptive step) and dx[i] (offset of the neuron's
+//     integration time from the step boundary, replacing the reference's FP64
+//     per-neuron time x, src/rk5.h:27-55).
+//   * acc[slot]: 64-bit fixed-point input accumulators (32 fractional bits),
+//     one per (target node, receptor port); slot = acc_base + port*n_pad + i.
+//     Integer addition is associative, so delivery order never changes results.
+//   * out-edges in CSR order by (source, delay): e_slot (u32 accumulator slot)
+//     and e_w (f32 weight) = 8 bytes per synapse; grp_off[src*nd + di] gives
+//     the edge range of source src for the di-th distinct delay.
+//   * a ring of per-step spike lists (R = max delay + 1 slots), replacing the
+//     per-source shift queues of src/spike_buffer.cu:143-302.
+#pragma once
+#include <stdint.h>
+
+namespace ngpu {
+
+#define NGPU_MAX_PARAM 128      // per-neuron parameters of one model
+#define NGPU_MAX_VAR 64         // per-neuron variables of one model
+#define NGPU_MAX_DELAYS 1024    // distinct delay values (steps)
+#define NGPU_MAX_SYN_GROUPS 32
+#define NGPU_MAX_SYN_PARAM 8
+#define NGPU_MAX_SYN_DT 16384   // STDP window in steps (src/syn_model.h:21)
+#define NGPU_RK5_MAX_SUBSTEPS 200000
+
+// error bits written by kernels into StepCtx::err
+enum DeviceError : unsigned {
+  DERR_RING_OVERFLOW = 1u,      // more spikes in one step than ring capacity
+  DERR_RK5_STUCK = 2u,          // adaptive integration exceeded substep cap
+  DERR_REC_OVERFLOW = 4u,       // recording buffer overflow
+  DERR_NAN_STATE = 8u
+};
+
+struct StepCtx {
+  long long it;                 // iteration index within the current session
+  long long T0;                 // time index at session start
+  double t0;                    // time (ms) at session start
+  int poisson_pending;          // Poisson draws of step it-1 not yet folded
+  unsigned err;                 // DeviceError bits
+  long long rec_row;            // next row of the recording buffer
+  unsigned long long n_spikes;  // spikes pushed (all time)
+};
+
+// Where a node's spike goes and what bookkeeping it updates.
+struct PushArgs {
+  unsigned *ring_src;
+  float *ring_h;
+  int *ring_cnt;
+  int ring_R;
+  int ring_C;
+  int *last_spike_T;
+  float *last_spike_h;
+  int *last_rev_T;
+  int *spike_count;             // per group-local node, may be null
+  float *rec_times;             // [n * max_rec], may be null
+  int *n_rec;
+  int max_rec;
+};
+
+// Per-group input folding: acc (+ Poisson direct connections) into state.
+struct InputArgs {
+  long long *acc;               // global accumulator array
+  long long acc_base;           // this group's first slot
+  int np;                       // receptor ports
+  int in_var;                   // var column of port-0 input
+  int in_step;                  // column stride between ports
+  int w_param;                  // weight from a port parameter?
+  int w_col;                    // param column of port-0 weight
+  int w_col_step;               // param column stride between ports
+  float w_const[4];             // constant weights (w_param == 0)
+  // Poisson direct connections into this group's nodes, CSR by local node
+  const unsigned *dc_off;       // [n+1] or null
+  const unsigned *dc_gen;       // generator index
+  const unsigned char *dc_port;
+  const float *dc_weight;
+  const float *dc_delay;
+  const unsigned long long *dc_stream;
+  const float *gen_rate;        // per generator node
+  const float *gen_origin;
+  const float *gen_start;
+  const float *gen_stop;
+  const double *gen_lambda;     // rate*dt/1000 as the reference computes it
+  const double *gen_explam;     // exp(-lambda)
+  unsigned long long seed;
+};
+
+struct GroupArgs {
+  int n;                        // nodes
+  int n_pad;                    // column length
+  int i_node_0;                 // first global node id
+  int nvar, nparam;             // per-neuron columns in use
+  float *var;                   // [nvar][n_pad]
+  float *param;                 // [nparam][n_pad]
+  float *h;                     // RK5 step size
+  float *dx;                    // RK5 time offset
+  unsigned pmask[NGPU_MAX_PARAM / 32];  // bit j: param j read per neuron
+  float puni[NGPU_MAX_PARAM];   // uniform parameter values
+  float h_min;
+  float dt;                     // time resolution (ms)
+  float eps;                    // RK5 tolerance
+  int den_delay_col;            // param column of den_delay or -1
+  unsigned long long *blk_evals;  // per-block RK5 derivative evaluations
+  // spike generator data
+  const int *sg_off;            // [n+1]
+  const int *sg_step;           // spike step index
+  const float *sg_height;
+  int *sg_next;
+};
+
+struct SynGroupTable {
+  int n;                        // number of synapse groups (index 1..n)
+  int type[NGPU_MAX_SYN_GROUPS];          // 1: test_syn_model, 2: stdp
+  float param[NGPU_MAX_SYN_GROUPS][NGPU_MAX_SYN_PARAM];
+};
+
+struct DeliverArgs {
+  const unsigned long long *grp_off;   // [n_src*nd + 1]
+  const unsigned *e_slot;
+  float *e_w;
+  const unsigned char *e_syn;          // null if no plastic synapse exists
+  int *e_stamp;                        // arrival step of last pre spike
+  const unsigned *e_post;              // target node id (plastic networks)
+  long long *acc;
+  const unsigned *ring_src;
+  const float *ring_h;
+  const int *ring_cnt;
+  int ring_R, ring_C;
+  int nd;
+  const int *delays;                   // [nd] distinct delays in steps
+  const int *last_rev_T;
+  int *last_post_T;
+  const unsigned long long *rev_off;   // [n_nodes+1] incoming plastic edges
+  const unsigned *rev_edge;
+  float dt;
+  unsigned long long *blk_events;      // per-block delivered events
+};
+
+}  // namespace ngpu

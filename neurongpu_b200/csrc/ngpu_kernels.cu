@@ -1,0 +1,926 @@
+// Simulation kernels for sm_100a.
+//
+// Per time step the driver launches (optionally captured in a CUDA graph):
+//   1. one update kernel per node group: folds the pending synaptic input of
+//      the previous step into the state (the reference's GetSpikes and
+//      PoissGenSendSpikeKernel, src/get_spike.cu:116-140,
+//      src/poiss_gen.cu:43-74), integrates the step (src/rk5.h:57-195 for
+//      RK5 groups) and appends emitted spikes to this step's ring slot
+//      (src/spike_buffer.cu:143-228);
+//   2. k_deliver: expands the (source, delay) groups that fall due in this
+//      step into fixed-point accumulator additions, with the STDP pre-spike
+//      rule (src/spike_buffer.cu:233-302, src/nested_loop.cu:39-167,
+//      src/get_spike.cu:48-85);
+//   3. k_stdp_post: STDP post-spike rule over incoming plastic synapses of the
+//      neurons that spiked (src/rev_spike.cu:41-75);
+//   4. k_record (multimeter columns) and k_advance (step counter).
+// No host synchronisation happens inside a step; every kernel reads the step
+// index from the device-resident StepCtx.
+#include <cuda_runtime.h>
+#include <math.h>
+#include "ngpu_device.h"
+#include "ngpu_kernels.h"
+#include "ngpu_models.h"
+#include "ngpu_rk5_models.cuh"
+#include "ngpu_rng.h"
+
+namespace ngpu {
+
+#define NGPU_BLOCK 128
+
+__device__ __forceinline__ bool pbit(const unsigned *mask, int j) {
+  return (mask[j >> 5] >> (j & 31)) & 1u;
+}
+
+// ---------------------------------------------------------------------------
+// spikes
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void push_spike(const PushArgs &pa, StepCtx *ctx,
+                                           int node, int local, float height,
+                                           long long T, double t_now,
+                                           int den_delay_steps) {
+  int slot = (int)(T % pa.ring_R);
+  int pos = atomicAdd(&pa.ring_cnt[slot], 1);
+  if (pos < pa.ring_C) {
+    long long k = (long long)slot * pa.ring_C + pos;
+    pa.ring_src[k] = (unsigned)node;
+    pa.ring_h[k] = height;
+  } else {
+    atomicOr(&ctx->err, (unsigned)DERR_RING_OVERFLOW);
+  }
+  pa.last_spike_T[node] = (int)T;
+  pa.last_spike_h[node] = height;
+  if (den_delay_steps == 0) pa.last_rev_T[node] = (int)T;
+  if (pa.spike_count != nullptr) pa.spike_count[local]++;
+  if (pa.rec_times != nullptr) {
+    int n = pa.n_rec[local];
+    // one slot is kept unused, as in src/spike_buffer.cu:183-186
+    if (n < pa.max_rec - 1) {
+      pa.rec_times[(long long)local * pa.max_rec + n] = (float)t_now;
+      pa.n_rec[local] = n + 1;
+    }
+  }
+}
+
+// Sum of the pending synaptic input of one node per port (fixed point):
+// accumulator contents (cleared here) plus the Poisson direct connections
+// drawn for the previous step.
+template <int NP>
+__device__ __forceinline__ void input_sum(const InputArgs &in, int i,
+                                          int n_pad, int np, long long it,
+                                          double t0, float dt, int pending,
+                                          long long T0, long long *s) {
+#pragma unroll
+  for (int q = 0; q < NP; q++) {
+    s[q] = 0;
+    if (q < np) {
+      long long *a = in.acc + in.acc_base + (long long)q * n_pad + i;
+      long long v = *a;
+      if (v != 0) *a = 0;
+      s[q] = v;
+    }
+  }
+  if (pending && in.dc_off != nullptr) {
+    unsigned b = in.dc_off[i], e = in.dc_off[i + 1];
+    if (b < e) {
+      // time of the step whose draws are pending (neural_time_ of that step)
+      double t = t0 + (double)dt * (double)it;
+      long long T_prev = T0 + it;
+      for (unsigned c = b; c < e; c++) {
+        unsigned gen = in.dc_gen[c];
+        double t_rel = t - (double)in.gen_origin[gen] - (double)in.dc_delay[c];
+        if (t_rel >= (double)in.gen_start[gen] &&
+            t_rel <= (double)in.gen_stop[gen]) {
+          unsigned n = ng_poisson(in.gen_lambda[gen], in.gen_explam[gen],
+                                  in.seed, RNG_TAG_POISSON_DIRECT,
+                                  in.dc_stream[c], T_prev);
+          if (n > 0) {
+            long long v = ng_to_fixed(in.dc_weight[c] * (float)n);
+            int port = in.dc_port[c];
+#pragma unroll
+            for (int q = 0; q < NP; q++) {
+              if (q == port) s[q] += v;
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ float fold_value(float var, long long s, float w) {
+  return (float)((double)var + (double)s * NGPU_ACC_INV_SCALE * (double)w);
+}
+
+// ---------------------------------------------------------------------------
+// RK5 (Cash-Karp) step and update, following src/rk5.h:57-162
+// ---------------------------------------------------------------------------
+template <class M, int NP>
+__device__ __forceinline__ void rk5_step(double &x, float *y, float &h,
+                                         float h_min, float h_max,
+                                         const float *p, int np, float eps,
+                                         unsigned &evals) {
+  using namespace rk5c;
+  constexpr int NV = M::NVAR;
+  float k1[NV], k2[NV], k3[NV], k4[NV], k5[NV], k6[NV], yn[NV], ys[NV];
+  M::deriv(y, k1, p, np);
+  evals++;
+#pragma unroll
+  for (int i = 0; i < NV; i++) ys[i] = fabsf(y[i]) + fabsf(k1[i] * h) + scal_min;
+  float err = 0.0f;
+  for (int guard = 0;; guard++) {
+    if (h > h_max) h = h_max;
+    if (h < h_min) h = h_min;
+#pragma unroll
+    for (int i = 0; i < NV; i++) yn[i] = y[i] + h * a21 * k1[i];
+    M::deriv(yn, k2, p, np);
+#pragma unroll
+    for (int i = 0; i < NV; i++) yn[i] = y[i] + h * (a31 * k1[i] + a32 * k2[i]);
+    M::deriv(yn, k3, p, np);
+#pragma unroll
+    for (int i = 0; i < NV; i++)
+      yn[i] = y[i] + h * (a41 * k1[i] + a42 * k2[i] + a43 * k3[i]);
+    M::deriv(yn, k4, p, np);
+#pragma unroll
+    for (int i = 0; i < NV; i++)
+      yn[i] = y[i] + h * (a51 * k1[i] + a52 * k2[i] + a53 * k3[i]
+                          + a54 * k4[i]);
+    M::deriv(yn, k5, p, np);
+#pragma unroll
+    for (int i = 0; i < NV; i++)
+      yn[i] = y[i] + h * (a61 * k1[i] + a62 * k2[i] + a63 * k3[i]
+                          + a64 * k4[i] + a65 * k5[i]);
+    M::deriv(yn, k6, p, np);
+#pragma unroll
+    for (int i = 0; i < NV; i++)
+      yn[i] = y[i] + h * (a71 * k1[i] + a73 * k3[i] + a74 * k4[i]
+                          + a76 * k6[i]);
+    evals += 5;
+    err = 0.0f;
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+      float val = h * (e1 * k1[i] + e3 * k3[i] + e4 * k4[i] + e5 * k5[i]
+                       + e6 * k6[i]);
+      val /= ys[i];
+      float av = fabsf(val);
+      err = (err > av) ? err : av;
+    }
+    err /= eps;
+    if (err <= 1.0f || (double)h <= (double)h_min * (1.0 + 1.0e-5)) break;
+    if (guard >= 256) break;
+    float h_new = h * coeff * powf(err, exp_dec);
+    double h01 = 0.1 * (double)h;
+    h = (float)(((double)h_new > h01) ? (double)h_new : h01);
+  }
+  x += h;
+  if (err > err_min) {
+    h = h * coeff * powf(err, exp_inc);
+  } else {
+    h = (float)(5.0 * (double)h);
+  }
+#pragma unroll
+  for (int i = 0; i < NV; i++) y[i] = yn[i];
+}
+
+template <class M>
+struct ModelTraits;
+
+// input var / weight mapping and the param column of den_delay and
+// refractory_step for every RK5 model
+#define NGPU_TRAITS(MODEL, IN_BASE, IN_STEP, W_BASE, W_STEP, REFR, DEN)   \
+  template <int NP>                                                       \
+  struct ModelTraits<MODEL<NP>> {                                         \
+    enum { in_base = IN_BASE, in_step = IN_STEP, w_base = W_BASE,         \
+           w_step = W_STEP, refr = REFR, den = DEN };                     \
+  };
+NGPU_TRAITS(AeifCondBeta, 3, 2, A_NSP + 3, 4, A_refr, A_den_delay)
+NGPU_TRAITS(AeifCondAlpha, 3, 2, A_NSP + 2, 3, A_refr, A_den_delay)
+NGPU_TRAITS(AeifPscAlpha, 3, 2, A_NSP + 1, 2, A_refr, A_den_delay)
+NGPU_TRAITS(AeifPscExp, 2, 1, -1, 0, A_refr, A_den_delay)
+NGPU_TRAITS(AeifPscDelta, 0, 0, -1, 0, A_refr, A_den_delay)
+NGPU_TRAITS(IzhCondBeta, 3, 2, I_NSP + 3, 4, I_refr, I_den_delay)
+
+__device__ __forceinline__ void block_add_u64(unsigned long long v,
+                                              unsigned long long *dst) {
+  __shared__ unsigned long long s_part[NGPU_BLOCK / 32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) s_part[wid] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += s_part[k];
+    dst[blockIdx.x] += t;
+  }
+}
+
+template <class M, int NP>
+__global__ void __launch_bounds__(NGPU_BLOCK)
+k_rk5_update(GroupArgs g, InputArgs in, PushArgs pa, StepCtx *ctx) {
+  using Tr = ModelTraits<M>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned evals = 0;
+  if (i < g.n) {
+    const int np = in.np;
+    const long long it = ctx->it;
+    const long long T0 = ctx->T0;
+    const double t0 = ctx->t0;
+    const int pending = ctx->poisson_pending;
+    const int n_pad = g.n_pad;
+    float y[M::NVAR];
+    float p[M::NPARAM];
+#pragma unroll
+    for (int j = 0; j < M::NVAR; j++) {
+      y[j] = (j < g.nvar) ? g.var[(long long)j * n_pad + i] : 0.0f;
+    }
+#pragma unroll
+    for (int j = 0; j < M::NPARAM; j++) {
+      if (j < g.nparam) {
+        p[j] = pbit(g.pmask, j) ? g.param[(long long)j * n_pad + i] : g.puni[j];
+      } else {
+        p[j] = 1.0f;
+      }
+    }
+    // fold the previous step's input
+    constexpr int NPI = (M::NPV == 0) ? 1 : NP;
+    long long s[NPI];
+    input_sum<NPI>(in, i, n_pad, np, it, t0, g.dt, pending, T0, s);
+#pragma unroll
+    for (int q = 0; q < NPI; q++) {
+      if (q < np && s[q] != 0) {
+        constexpr int dummy = 0;
+        (void)dummy;
+        const int vi = Tr::in_base + q * Tr::in_step;
+        const float w = (Tr::w_base >= 0) ? p[Tr::w_base + q * Tr::w_step]
+                                          : 1.0f;
+        y[vi] = fold_value(y[vi], s[q], w);
+      }
+    }
+    const float refr0 = p[Tr::refr];
+    const double x1 = t0 + (double)g.dt * (double)(it + 1);
+    double x = t0 + (double)g.dt * (double)it + (double)g.dx[i];
+    float h = g.h[i];
+    const float h_min = g.h_min;
+    const long long T = T0 + it + 1;
+    const int den = (int)roundf(p[Tr::den] / g.dt);
+    bool end_step = false;
+    int guard = 0;
+    while (!end_step) {
+      float hmax = (float)(x1 - x);
+      rk5_step<M, NP>(x, y, h, h_min, hmax, p, np, g.eps, evals);
+      end_step = (x >= x1 - (double)h_min);
+      if (M::external(y, p, end_step, g.dt)) {
+        push_spike(pa, ctx, g.i_node_0 + i, i, 1.0f, T, x1, den);
+      }
+      if (++guard > NGPU_RK5_MAX_SUBSTEPS) {
+        atomicOr(&ctx->err, (unsigned)DERR_RK5_STUCK);
+        break;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < M::NVAR; j++) {
+      if (j < g.nvar) g.var[(long long)j * n_pad + i] = y[j];
+    }
+    g.h[i] = h;
+    g.dx[i] = (float)(x - x1);
+    if (p[Tr::refr] != refr0) g.param[(long long)Tr::refr * n_pad + i] = p[Tr::refr];
+  }
+  if (g.blk_evals != nullptr) block_add_u64(evals, g.blk_evals);
+}
+
+template <template <int> class MT>
+static void launch_rk5_model(int np, const GroupArgs &g, const InputArgs &in,
+                             const PushArgs &pa, StepCtx *ctx,
+                             cudaStream_t s) {
+  dim3 grid((g.n + NGPU_BLOCK - 1) / NGPU_BLOCK), block(NGPU_BLOCK);
+  switch (np) {
+    case 0:
+    case 1: k_rk5_update<MT<1>, 1><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+    case 2: k_rk5_update<MT<2>, 2><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+    case 3: k_rk5_update<MT<3>, 3><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+    case 4: k_rk5_update<MT<4>, 4><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+    default:
+      if (np <= 8) {
+        k_rk5_update<MT<8>, 8><<<grid, block, 0, s>>>(g, in, pa, ctx);
+      } else {
+        k_rk5_update<MT<20>, 20><<<grid, block, 0, s>>>(g, in, pa, ctx);
+      }
+  }
+}
+
+void LaunchRk5Update(int model, int np, const GroupArgs &g,
+                     const InputArgs &in, const PushArgs &pa, StepCtx *ctx,
+                     cudaStream_t s) {
+  if (g.n <= 0) return;
+  switch (model) {
+    case RK5_AEIF_COND_BETA:
+      launch_rk5_model<AeifCondBeta>(np, g, in, pa, ctx, s); break;
+    case RK5_AEIF_COND_ALPHA:
+      launch_rk5_model<AeifCondAlpha>(np, g, in, pa, ctx, s); break;
+    case RK5_AEIF_PSC_ALPHA:
+      launch_rk5_model<AeifPscAlpha>(np, g, in, pa, ctx, s); break;
+    case RK5_AEIF_PSC_EXP:
+      launch_rk5_model<AeifPscExp>(np, g, in, pa, ctx, s); break;
+    case RK5_AEIF_PSC_DELTA: {
+      dim3 grid((g.n + NGPU_BLOCK - 1) / NGPU_BLOCK), block(NGPU_BLOCK);
+      k_rk5_update<AeifPscDelta<1>, 1><<<grid, block, 0, s>>>(g, in, pa, ctx);
+      break;
+    }
+    case RK5_IZHIKEVICH_COND_BETA:
+      launch_rk5_model<IzhCondBeta>(np, g, in, pa, ctx, s); break;
+    default: break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// iaf_psc_exp: exact propagator update (src/iaf_psc_exp.cu:94-119)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float gparam(const GroupArgs &g, int j, int i) {
+  return pbit(g.pmask, j) ? g.param[(long long)j * g.n_pad + i] : g.puni[j];
+}
+
+__global__ void __launch_bounds__(NGPU_BLOCK)
+k_iaf_psc_exp(GroupArgs g, InputArgs in, PushArgs pa, StepCtx *ctx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.n) return;
+  const long long it = ctx->it, T0 = ctx->T0;
+  const double t0 = ctx->t0;
+  const int n_pad = g.n_pad;
+  float *var = g.var;
+  float I_ex = var[i], I_in = var[n_pad + i];
+  float V = var[2 * n_pad + i], refr = var[3 * n_pad + i];
+  long long s[2];
+  input_sum<2>(in, i, n_pad, 2, it, t0, g.dt, ctx->poisson_pending, T0, s);
+  if (s[0] != 0) I_ex = fold_value(I_ex, s[0], 1.0f);
+  if (s[1] != 0) I_in = fold_value(I_in, s[1], 1.0f);
+  const float I_e = gparam(g, 3, i), Theta = gparam(g, 4, i);
+  const float V_reset = gparam(g, 5, i), t_ref = gparam(g, 8, i);
+  const float P20 = gparam(g, 10, i), P11ex = gparam(g, 11, i);
+  const float P11in = gparam(g, 12, i), P21ex = gparam(g, 13, i);
+  const float P21in = gparam(g, 14, i), P22 = gparam(g, 15, i);
+  if (refr > 0.0f) {
+    refr -= 1.0f;
+  } else {
+    V = V * P22 + I_ex * P21ex + I_in * P21in + I_e * P20;
+  }
+  I_ex *= P11ex;
+  I_in *= P11in;
+  if (V >= Theta) {
+    const long long T = T0 + it + 1;
+    const double t_now = t0 + (double)g.dt * (double)(it + 1);
+    const int den = (int)roundf(gparam(g, 9, i) / g.dt);
+    push_spike(pa, ctx, g.i_node_0 + i, i, 1.0f, T, t_now, den);
+    V = V_reset;
+    refr = (float)(int)roundf(t_ref / g.dt);
+  }
+  var[i] = I_ex;
+  var[n_pad + i] = I_in;
+  var[2 * n_pad + i] = V;
+  var[3 * n_pad + i] = refr;
+}
+
+void LaunchIafPscExpUpdate(const GroupArgs &g, const InputArgs &in,
+                           const PushArgs &pa, StepCtx *ctx, cudaStream_t s) {
+  if (g.n <= 0) return;
+  k_iaf_psc_exp<<<(g.n + NGPU_BLOCK - 1) / NGPU_BLOCK, NGPU_BLOCK, 0, s>>>(
+      g, in, pa, ctx);
+}
+
+// ---------------------------------------------------------------------------
+// spike_generator (src/spike_generator.cu:37-55)
+// ---------------------------------------------------------------------------
+__global__ void k_spike_generator(GroupArgs g, PushArgs pa, StepCtx *ctx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.n) return;
+  const long long it = ctx->it, T0 = ctx->T0;
+  const long long step = T0 + it;
+  int b = g.sg_next[i];
+  if (b < g.sg_off[i + 1] && (long long)g.sg_step[b] == step) {
+    const long long T = step + 1;
+    const double t_now = ctx->t0 + (double)g.dt * (double)(it + 1);
+    push_spike(pa, ctx, g.i_node_0 + i, i, g.sg_height[b], T, t_now, 0);
+    g.sg_next[i] = b + 1;
+  }
+}
+
+void LaunchSpikeGeneratorUpdate(const GroupArgs &g, const PushArgs &pa,
+                                StepCtx *ctx, cudaStream_t s) {
+  if (g.n <= 0) return;
+  k_spike_generator<<<(g.n + NGPU_BLOCK - 1) / NGPU_BLOCK, NGPU_BLOCK, 0, s>>>(
+      g, pa, ctx);
+}
+
+// ---------------------------------------------------------------------------
+// parrot_neuron (src/parrot_neuron.cu:48-70)
+// ---------------------------------------------------------------------------
+__global__ void k_parrot(GroupArgs g, InputArgs in, PushArgs pa,
+                         StepCtx *ctx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.n) return;
+  const long long it = ctx->it, T0 = ctx->T0;
+  const double t0 = ctx->t0;
+  const int n_pad = g.n_pad;
+  float *var = g.var;
+  long long s[2];
+  input_sum<2>(in, i, n_pad, 2, it, t0, g.dt, ctx->poisson_pending, T0, s);
+  float sh = var[i];
+  if (s[0] != 0) sh = fold_value(sh, s[0], 1.0f);
+  if (s[1] != 0) var[n_pad + i] = fold_value(var[n_pad + i], s[1], 0.0f);
+  var[2 * n_pad + i] = sh;
+  if (sh != 0.0f) {
+    if (gparam(g, 0, i) == 0.0f) sh = 1.0f;
+    const long long T = T0 + it + 1;
+    const double t_now = t0 + (double)g.dt * (double)(it + 1);
+    const int den = (int)roundf(gparam(g, 1, i) / g.dt);
+    push_spike(pa, ctx, g.i_node_0 + i, i, sh, T, t_now, den);
+    var[i] = 0.0f;
+  } else {
+    var[i] = sh;
+  }
+}
+
+void LaunchParrotUpdate(const GroupArgs &g, const InputArgs &in,
+                        const PushArgs &pa, StepCtx *ctx, cudaStream_t s) {
+  if (g.n <= 0) return;
+  k_parrot<<<(g.n + NGPU_BLOCK - 1) / NGPU_BLOCK, NGPU_BLOCK, 0, s>>>(g, in,
+                                                                     pa, ctx);
+}
+
+// ---------------------------------------------------------------------------
+// spike_detector (src/spike_detector.cu:43-66)
+// ---------------------------------------------------------------------------
+__global__ void k_spike_detector(GroupArgs g, InputArgs in, StepCtx *ctx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.n) return;
+  const int n_pad = g.n_pad;
+  float *var = g.var;
+  long long s[1];
+  input_sum<1>(in, i, n_pad, 1, ctx->it, ctx->t0, g.dt, ctx->poisson_pending,
+               ctx->T0, s);
+  float sh = var[i];
+  if (s[0] != 0) sh = fold_value(sh, s[0], 1.0f);
+  if (sh != 0.0f) {
+    if (gparam(g, 0, i) == 0.0f) sh = 1.0f;
+    var[i] = 0.0f;
+  } else {
+    var[i] = sh;
+  }
+  var[n_pad + i] = sh;
+}
+
+void LaunchSpikeDetectorUpdate(const GroupArgs &g, const InputArgs &in,
+                               StepCtx *ctx, cudaStream_t s) {
+  if (g.n <= 0) return;
+  k_spike_detector<<<(g.n + NGPU_BLOCK - 1) / NGPU_BLOCK, NGPU_BLOCK, 0, s>>>(
+      g, in, ctx);
+}
+
+// ---------------------------------------------------------------------------
+// CreatePoissonGenerator nodes: one count per node per step pushed as a
+// spike of that height (src/poisson.cu:26-54)
+// ---------------------------------------------------------------------------
+__global__ void k_poisson_nodes(GroupArgs g, PushArgs pa, double lambda,
+                                double explam, unsigned long long seed,
+                                StepCtx *ctx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.n) return;
+  const long long it = ctx->it, T0 = ctx->T0;
+  const long long T = T0 + it + 1;
+  unsigned n = ng_poisson(lambda, explam, seed, RNG_TAG_POISSON_NODE,
+                          (unsigned long long)(g.i_node_0 + i), T);
+  if ((float)n > (float)lambda * 5.0f) n = 0;
+  if (n > 0) {
+    const double t_now = ctx->t0 + (double)g.dt * (double)(it + 1);
+    push_spike(pa, ctx, g.i_node_0 + i, i, (float)n, T, t_now, 0);
+  }
+}
+
+void LaunchPoissonNodesUpdate(const GroupArgs &g, const PushArgs &pa,
+                              double lambda, double explam,
+                              unsigned long long seed, StepCtx *ctx,
+                              cudaStream_t s) {
+  if (g.n <= 0) return;
+  k_poisson_nodes<<<(g.n + NGPU_BLOCK - 1) / NGPU_BLOCK, NGPU_BLOCK, 0, s>>>(
+      g, pa, lambda, explam, seed, ctx);
+}
+
+// ---------------------------------------------------------------------------
+// input fold outside the step loop
+// ---------------------------------------------------------------------------
+__global__ void k_fold_input(GroupArgs g, InputArgs in, StepCtx *ctx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.n || in.np <= 0 || in.in_var < 0) return;
+  long long s[4];
+  const int np = in.np < 4 ? in.np : 4;
+  input_sum<4>(in, i, g.n_pad, np, ctx->it, ctx->t0, g.dt, ctx->poisson_pending,
+               ctx->T0, s);
+  for (int q = 0; q < np; q++) {
+    if (s[q] == 0) continue;
+    float w;
+    if (in.w_param) {
+      w = gparam(g, in.w_col + q * in.w_col_step, i);
+    } else {
+      w = in.w_const[q];
+    }
+    float *v = g.var + (long long)(in.in_var + q * in.in_step) * g.n_pad + i;
+    *v = fold_value(*v, s[q], w);
+  }
+  // ports beyond 4 (RK5 groups with many receptors)
+  for (int q = 4; q < in.np; q++) {
+    long long *a = in.acc + in.acc_base + (long long)q * g.n_pad + i;
+    long long sv = *a;
+    if (sv == 0) continue;
+    *a = 0;
+    float w = in.w_param ? gparam(g, in.w_col + q * in.w_col_step, i)
+                         : in.w_const[3];
+    float *v = g.var + (long long)(in.in_var + q * in.in_step) * g.n_pad + i;
+    *v = fold_value(*v, sv, w);
+  }
+}
+
+__global__ void k_clear_pending(StepCtx *ctx) { ctx->poisson_pending = 0; }
+
+void LaunchFoldInput(const GroupArgs &g, const InputArgs &in, StepCtx *ctx,
+                     cudaStream_t s) {
+  if (g.n <= 0) return;
+  k_fold_input<<<(g.n + NGPU_BLOCK - 1) / NGPU_BLOCK, NGPU_BLOCK, 0, s>>>(
+      g, in, ctx);
+}
+
+void LaunchClearPending(StepCtx *ctx, cudaStream_t s) {
+  k_clear_pending<<<1, 1, 0, s>>>(ctx);
+}
+
+// ---------------------------------------------------------------------------
+// synapse models (src/stdp.cu:24-51, src/test_syn_model.cu:24-30)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float syn_update(const SynGroupTable &syn, int sg,
+                                            float w, float Dt) {
+  int type = syn.type[sg - 1];
+  const float *prm = syn.param[sg - 1];
+  if (type == 2) {
+    double tau_plus = prm[0], tau_minus = prm[1], lambda = prm[2];
+    double alpha = prm[3], mu_plus = prm[4], mu_minus = prm[5];
+    double Wmax = prm[6];
+    double w0 = w, w1;
+    if (Dt >= 0.0f) {
+      double fact = lambda * exp(-(double)Dt / tau_plus);
+      w1 = w0 + fact * Wmax * pow(1.0 - w0 / Wmax, mu_plus);
+    } else {
+      double fact = -alpha * lambda * exp((double)Dt / tau_minus);
+      w1 = w0 + fact * Wmax * pow(w0 / Wmax, mu_minus);
+    }
+    w1 = w1 > 0.0 ? w1 : 0.0;
+    w1 = w1 < Wmax ? w1 : Wmax;
+    return (float)w1;
+  } else if (type == 1) {
+    return w + (prm[1] + prm[0] * Dt);
+  }
+  return w;
+}
+
+// ---------------------------------------------------------------------------
+// synaptic delivery: one warp per (spike, delay) group
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
+  __shared__ int s_pref[NGPU_MAX_DELAYS + 1];
+  __shared__ int s_slot[NGPU_MAX_DELAYS];
+  const long long T = ctx->T0 + ctx->it + 1;
+  for (int di = threadIdx.x; di < d.nd; di += blockDim.x) {
+    int slot = (int)((T - d.delays[di]) % d.ring_R);
+    if (slot < 0) slot += d.ring_R;
+    s_slot[di] = slot;
+    int c = d.ring_cnt[slot];
+    s_pref[di + 1] = c < d.ring_C ? c : d.ring_C;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_pref[0] = 0;
+    for (int di = 0; di < d.nd; di++) s_pref[di + 1] += s_pref[di];
+  }
+  __syncthreads();
+  const int total = s_pref[d.nd];
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int n_warps = (gridDim.x * blockDim.x) >> 5;
+  unsigned long long events = 0;
+  for (int item = warp; item < total; item += n_warps) {
+    int lo = 0, hi = d.nd;          // find di with s_pref[di] <= item
+    while (hi - lo > 1) {
+      int mid = (lo + hi) >> 1;
+      if (s_pref[mid] <= item) lo = mid; else hi = mid;
+    }
+    const int di = lo;
+    const long long k = (long long)s_slot[di] * d.ring_C + (item - s_pref[di]);
+    const unsigned src = d.ring_src[k];
+    const float height = d.ring_h[k];
+    const unsigned long long gi = (unsigned long long)src * d.nd + di;
+    const unsigned long long beg = d.grp_off[gi], end = d.grp_off[gi + 1];
+    if (lane == 0) events += end - beg;
+    if (d.e_syn == nullptr) {
+      for (unsigned long long e = beg + lane; e < end; e += 32) {
+        const unsigned slot = d.e_slot[e];
+        const float w = d.e_w[e];
+        atomicAdd((unsigned long long *)(d.acc + slot),
+                  (unsigned long long)ng_to_fixed(height * w));
+      }
+    } else {
+      for (unsigned long long e = beg + lane; e < end; e += 32) {
+        const unsigned slot = d.e_slot[e];
+        const float w = d.e_w[e];
+        atomicAdd((unsigned long long *)(d.acc + slot),
+                  (unsigned long long)ng_to_fixed(height * w));
+        const int sg = d.e_syn[e];
+        if (sg > 0) {
+          // pre-spike rule with the last post spike (src/get_spike.cu:73-83)
+          d.e_stamp[e] = (int)T;
+          long long Dt_int = T - (long long)d.last_rev_T[d.e_post[e]];
+          if (Dt_int > 0 && Dt_int < NGPU_MAX_SYN_DT) {
+            d.e_w[e] = syn_update(syn, sg, w, -d.dt * (float)Dt_int);
+          }
+        }
+      }
+    }
+  }
+  if (d.blk_events != nullptr) {
+    __shared__ unsigned long long s_ev[8];
+    for (int o = 16; o > 0; o >>= 1)
+      events += __shfl_down_sync(0xffffffffu, events, o);
+    if (lane == 0) s_ev[threadIdx.x >> 5] = events;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned long long t = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += s_ev[w];
+      d.blk_events[blockIdx.x] += t;
+    }
+  }
+}
+
+void LaunchDeliver(const DeliverArgs &d, const SynGroupTable &syn,
+                   StepCtx *ctx, int n_blocks, cudaStream_t s) {
+  if (d.nd <= 0) return;
+  k_deliver<<<n_blocks, 256, 0, s>>>(d, syn, ctx);
+}
+
+// ---------------------------------------------------------------------------
+// STDP post-spike rule: neurons that spiked in this step, over their
+// incoming plastic synapses (src/rev_spike.cu:41-75)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_stdp_post(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
+  const long long T = ctx->T0 + ctx->it + 1;
+  const int slot = (int)(T % d.ring_R);
+  int cnt = d.ring_cnt[slot];
+  cnt = cnt < d.ring_C ? cnt : d.ring_C;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int n_warps = (gridDim.x * blockDim.x) >> 5;
+  for (int item = warp; item < cnt; item += n_warps) {
+    const unsigned node = d.ring_src[(long long)slot * d.ring_C + item];
+    if (d.last_rev_T[node] != (int)T) continue;   // dendritic delay > 0
+    int first = 0;
+    if (lane == 0) first = (atomicExch(&d.last_post_T[node], (int)T) != (int)T);
+    first = __shfl_sync(0xffffffffu, first, 0);
+    if (!first) continue;
+    const unsigned long long beg = d.rev_off[node], end = d.rev_off[node + 1];
+    for (unsigned long long r = beg + lane; r < end; r += 32) {
+      const unsigned e = d.rev_edge[r];
+      const int sg = d.e_syn[e];
+      long long Dt_int = T - (long long)d.e_stamp[e];
+      if (sg > 0 && Dt_int >= 0 && Dt_int < NGPU_MAX_SYN_DT) {
+        d.e_w[e] = syn_update(syn, sg, d.e_w[e], d.dt * (float)Dt_int);
+      }
+    }
+  }
+}
+
+void LaunchStdpPost(const DeliverArgs &d, const SynGroupTable &syn,
+                    StepCtx *ctx, int n_blocks, cudaStream_t s) {
+  k_stdp_post<<<n_blocks, 256, 0, s>>>(d, syn, ctx);
+}
+
+// ---------------------------------------------------------------------------
+// multimeter records and step bookkeeping
+// ---------------------------------------------------------------------------
+__global__ void k_record(const RecCol *cols, int n_cols, float *buf,
+                         long long cap_rows, const int *last_spike_T,
+                         const float *last_spike_h, int initial, float dt,
+                         StepCtx *ctx) {
+  const long long row = ctx->rec_row;
+  if (row >= cap_rows) {
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+      atomicOr(&ctx->err, (unsigned)DERR_REC_OVERFLOW);
+    return;
+  }
+  const long long it = ctx->it;
+  const long long T = ctx->T0 + it + 1;
+  float *r = buf + row * (n_cols + 1);
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c == 0) {
+    double t = initial ? ctx->t0 : ctx->t0 + (double)dt * (double)(it + 1);
+    r[0] = (float)t;
+  }
+  if (c < n_cols) {
+    RecCol col = cols[c];
+    float v;
+    if (col.spike) {
+      v = (!initial && col.has_out && last_spike_T[col.node] == (int)T)
+              ? last_spike_h[col.node] : 0.0f;
+    } else {
+      v = *col.ptr;
+    }
+    r[1 + c] = v;
+  }
+}
+
+void LaunchRecord(const RecCol *cols, int n_cols, float *buf, long long cap_rows,
+                  const int *last_spike_T, const float *last_spike_h,
+                  int initial, float dt, StepCtx *ctx, cudaStream_t s) {
+  int nb = (n_cols + 1 + 255) / 256;
+  k_record<<<nb, 256, 0, s>>>(cols, n_cols, buf, cap_rows, last_spike_T,
+                              last_spike_h, initial, dt, ctx);
+}
+
+__global__ void k_advance(int *ring_cnt, int ring_R, int ring_C, int flags,
+                          StepCtx *ctx) {
+  if (flags & 1) {
+    const long long T = ctx->T0 + ctx->it + 1;
+    int c = ring_cnt[(int)(T % ring_R)];
+    ctx->n_spikes += (unsigned long long)(c < ring_C ? c : ring_C);
+    ring_cnt[(int)((T + 1) % ring_R)] = 0;
+    ctx->it += 1;
+    ctx->poisson_pending = 1;
+  }
+  if (flags & 2) ctx->rec_row += 1;
+}
+
+void LaunchAdvance(int *ring_cnt, int ring_R, int ring_C, int flags,
+                   StepCtx *ctx, cudaStream_t s) {
+  k_advance<<<1, 1, 0, s>>>(ring_cnt, ring_R, ring_C, flags, ctx);
+}
+
+// ---------------------------------------------------------------------------
+// calibration kernels
+// ---------------------------------------------------------------------------
+// beta-function conductance normalisation (src/aeif_cond_beta.cu:58-87)
+__global__ void k_calib_beta(int n, int n_pad, float *param, int np,
+                             int nsp, int npp, int col_rise, int col_decay,
+                             int col_g0, int col_refr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  param[(long long)col_refr * n_pad + i] = 0.0f;
+  for (int q = 0; q < np; q++) {
+    float tr = param[(long long)(nsp + npp * q + col_rise) * n_pad + i];
+    float td = param[(long long)(nsp + npp * q + col_decay) * n_pad + i];
+    float denom1 = td - tr;
+    float denom2 = 0.0f;
+    if (denom1 != 0.0f) {
+      float t_p = td * tr * logf(td / tr) / denom1;
+      denom2 = expf(-t_p / td) - expf(-t_p / tr);
+    }
+    float g0;
+    if (denom2 == 0.0f) {
+      g0 = (float)(M_E / (double)td);
+    } else {
+      g0 = (float)((1.0 / (double)tr - 1.0 / (double)td) / (double)denom2);
+    }
+    param[(long long)(nsp + npp * q + col_g0) * n_pad + i] = g0;
+  }
+}
+
+// alpha-function normalisation e/tau (src/aeif_cond_alpha.cu:63-68)
+__global__ void k_calib_alpha(int n, int n_pad, float *param, int np, int nsp,
+                              int npp, int col_tau, int col_out, int col_refr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  param[(long long)col_refr * n_pad + i] = 0.0f;
+  for (int q = 0; q < np; q++) {
+    float tau = param[(long long)(nsp + npp * q + col_tau) * n_pad + i];
+    param[(long long)(nsp + npp * q + col_out) * n_pad + i] =
+        (float)(M_E / (double)tau);
+  }
+}
+
+__global__ void k_calib_refr(int n, int n_pad, float *param, int col_refr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  param[(long long)col_refr * n_pad + i] = 0.0f;
+}
+
+void LaunchCalibrateRk5(int model, const GroupArgs &g, int np,
+                        cudaStream_t s) {
+  if (g.n <= 0) return;
+  int nb = (g.n + NGPU_BLOCK - 1) / NGPU_BLOCK;
+  switch (model) {
+    case RK5_AEIF_COND_BETA:
+      k_calib_beta<<<nb, NGPU_BLOCK, 0, s>>>(g.n, g.n_pad, g.param, np, A_NSP,
+                                             4, 1, 2, 3, A_refr);
+      break;
+    case RK5_IZHIKEVICH_COND_BETA:
+      k_calib_beta<<<nb, NGPU_BLOCK, 0, s>>>(g.n, g.n_pad, g.param, np, I_NSP,
+                                             4, 1, 2, 3, I_refr);
+      break;
+    case RK5_AEIF_COND_ALPHA:
+      k_calib_alpha<<<nb, NGPU_BLOCK, 0, s>>>(g.n, g.n_pad, g.param, np, A_NSP,
+                                              3, 1, 2, A_refr);
+      break;
+    case RK5_AEIF_PSC_ALPHA:
+      k_calib_alpha<<<nb, NGPU_BLOCK, 0, s>>>(g.n, g.n_pad, g.param, np, A_NSP,
+                                              2, 0, 1, A_refr);
+      break;
+    default:
+      k_calib_refr<<<nb, NGPU_BLOCK, 0, s>>>(g.n, g.n_pad, g.param, A_refr);
+  }
+}
+
+// exact-integration propagators (src/iaf_psc_exp.cu:53-91)
+__device__ double propagator_32(double tau_syn, double tau, double C,
+                                double h) {
+  const double P32_linear = 1.0 / (2.0 * C * tau * tau) * h * h
+                            * (tau_syn - tau) * exp(-h / tau);
+  const double P32_singular = h / C * exp(-h / tau);
+  const double P32 = -tau / (C * (1.0 - tau / tau_syn)) * exp(-h / tau_syn)
+                     * expm1(h * (1.0 / tau_syn - 1.0 / tau));
+  const double dev_P32 = fabs(P32 - P32_singular);
+  if (tau == tau_syn ||
+      (fabs(tau - tau_syn) < 0.1 && dev_P32 > 2.0 * fabs(P32_linear))) {
+    return P32_singular;
+  }
+  return P32;
+}
+
+__global__ void k_calib_iaf(int n, int n_pad, float *param, float h) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float *col = param + i;
+  const long long P = n_pad;
+  float tau_m = col[0 * P], C_m = col[1 * P];
+  float tau_ex = col[6 * P], tau_in = col[7 * P];
+  float P22 = expf(-h / tau_m);
+  col[11 * P] = expf(-h / tau_ex);
+  col[12 * P] = expf(-h / tau_in);
+  col[15 * P] = P22;
+  col[13 * P] = (float)propagator_32(tau_ex, tau_m, C_m, h);
+  col[14 * P] = (float)propagator_32(tau_in, tau_m, C_m, h);
+  col[10 * P] = (float)((double)(tau_m / C_m) * (1.0 - (double)P22));
+}
+
+void LaunchCalibrateIaf(const GroupArgs &g, float h, cudaStream_t s) {
+  if (g.n <= 0) return;
+  k_calib_iaf<<<(g.n + NGPU_BLOCK - 1) / NGPU_BLOCK, NGPU_BLOCK, 0, s>>>(
+      g.n, g.n_pad, g.param, h);
+}
+
+// ---------------------------------------------------------------------------
+// parameter / variable access helpers
+// ---------------------------------------------------------------------------
+__global__ void k_fill_float(float *p, long long n, float v) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i < n; i += (long long)gridDim.x * blockDim.x) p[i] = v;
+}
+__global__ void k_fill_int(int *p, long long n, int v) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i < n; i += (long long)gridDim.x * blockDim.x) p[i] = v;
+}
+__global__ void k_scatter_float(float *col, const int *idx, int n, float v,
+                                const float *vals, int stride) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  col[idx[k]] = vals ? vals[(long long)k * stride] : v;
+}
+__global__ void k_gather_float(const float *col, const int *idx, int n,
+                               float *out, int stride) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  out[(long long)k * stride] = col[idx[k]];
+}
+
+static int grid_for(long long n) {
+  long long b = (n + 255) / 256;
+  if (b > 148 * 32) b = 148 * 32;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+void LaunchFillFloat(float *p, long long n, float v, cudaStream_t s) {
+  if (n <= 0) return;
+  k_fill_float<<<grid_for(n), 256, 0, s>>>(p, n, v);
+}
+void LaunchFillInt(int *p, long long n, int v, cudaStream_t s) {
+  if (n <= 0) return;
+  k_fill_int<<<grid_for(n), 256, 0, s>>>(p, n, v);
+}
+void LaunchScatterFloat(float *col, const int *idx, int n, float v,
+                        const float *vals, int vals_stride, cudaStream_t s) {
+  if (n <= 0) return;
+  k_scatter_float<<<(n + 255) / 256, 256, 0, s>>>(col, idx, n, v, vals,
+                                                  vals_stride);
+}
+void LaunchGatherFloat(const float *col, const int *idx, int n, float *out,
+                       int out_stride, cudaStream_t s) {
+  if (n <= 0) return;
+  k_gather_float<<<(n + 255) / 256, 256, 0, s>>>(col, idx, n, out, out_stride);
+}
+
+}  // namespace ngpu

@@ -1,0 +1,62 @@
+// Host-callable launchers for the simulation kernels (ngpu_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include "ngpu_device.h"
+
+namespace ngpu {
+
+struct RecCol {
+  const float *ptr;   // address of the recorded value (null for "spike")
+  int node;           // global node id (for "spike")
+  int spike;          // 1: spike height recorded in this step, else 0
+  int has_out;        // node stores spikes (reference quirk of "spike")
+};
+
+// per-step node updates
+void LaunchRk5Update(int model, int np, const GroupArgs &g,
+                     const InputArgs &in, const PushArgs &pa,
+                     StepCtx *ctx, cudaStream_t s);
+void LaunchIafPscExpUpdate(const GroupArgs &g, const InputArgs &in,
+                           const PushArgs &pa, StepCtx *ctx, cudaStream_t s);
+void LaunchSpikeGeneratorUpdate(const GroupArgs &g, const PushArgs &pa,
+                                StepCtx *ctx, cudaStream_t s);
+void LaunchParrotUpdate(const GroupArgs &g, const InputArgs &in,
+                        const PushArgs &pa, StepCtx *ctx, cudaStream_t s);
+void LaunchSpikeDetectorUpdate(const GroupArgs &g, const InputArgs &in,
+                               StepCtx *ctx, cudaStream_t s);
+void LaunchPoissonNodesUpdate(const GroupArgs &g, const PushArgs &pa,
+                              double lambda, double explam,
+                              unsigned long long seed, StepCtx *ctx,
+                              cudaStream_t s);
+// folds pending input outside the step loop (end of a session)
+void LaunchFoldInput(const GroupArgs &g, const InputArgs &in, StepCtx *ctx,
+                     cudaStream_t s);
+void LaunchClearPending(StepCtx *ctx, cudaStream_t s);
+
+// synaptic delivery and plasticity
+void LaunchDeliver(const DeliverArgs &d, const SynGroupTable &syn,
+                   StepCtx *ctx, int n_blocks, cudaStream_t s);
+void LaunchStdpPost(const DeliverArgs &d, const SynGroupTable &syn,
+                    StepCtx *ctx, int n_blocks, cudaStream_t s);
+
+// recording and step bookkeeping
+void LaunchRecord(const RecCol *cols, int n_cols, float *buf, long long cap_rows,
+                  const int *last_spike_T, const float *last_spike_h,
+                  int initial, float dt, StepCtx *ctx, cudaStream_t s);
+void LaunchAdvance(int *ring_cnt, int ring_R, int ring_C, int flags,
+                   StepCtx *ctx, cudaStream_t s);
+
+// calibration
+void LaunchCalibrateRk5(int model, const GroupArgs &g, int np,
+                        cudaStream_t s);
+void LaunchCalibrateIaf(const GroupArgs &g, float h, cudaStream_t s);
+
+// utilities
+void LaunchFillFloat(float *p, long long n, float v, cudaStream_t s);
+void LaunchFillInt(int *p, long long n, int v, cudaStream_t s);
+void LaunchScatterFloat(float *col, const int *idx, int n, float v,
+                        const float *vals, int vals_stride, cudaStream_t s);
+void LaunchGatherFloat(const float *col, const int *idx, int n, float *out,
+                       int out_stride, cudaStream_t s);
+
+}  // namespace ngpu

@@ -1,0 +1,242 @@
+"""Parity of the CUDA core (through the drop-in API / C ABI) with the FP64
+oracle and with the reference's golden vectors. Needs a B200.
+
+Tolerances:
+  * membrane traces: the reference's own metric against NEST
+    (std(dV)/|mean V| <= 5e-4, python/test/test_aeif_cond_beta.py:4) and a
+    max relative deviation <= 2e-5 from the FP64 oracle of the same RK5 scheme;
+  * spike routing, delivered input and Poisson counts: bit-exact;
+  * STDP weights: 1e-5 absolute against the closed form
+    (python/test/test_stdp.py:21) and against the oracle.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from tests import netdefs
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", sorted(netdefs.SINGLE))
+def test_single_neuron_trace(ngpu, name):
+    t, v = netdefs.run_single_api(ngpu, name)
+    assert len(v) == 8001
+    rmse = netdefs.nest_rmse(v, name)
+    assert rmse <= netdefs.SINGLE[name]["tol"], (name, rmse)
+    t_o, v_o, _ = netdefs.run_single_oracle(name)
+    np.testing.assert_allclose(t, t_o, rtol=0, atol=1e-3)
+    scale = max(1.0, float(np.max(np.abs(v_o))))
+    err = float(np.max(np.abs(v - v_o))) / scale
+    assert err <= 2e-5, (name, err)
+
+
+def _routing_net(rng, n_sg=40, n_par=60, n_edges=900, max_delay=4.0):
+    sg_times = [sorted(set(np.round(rng.uniform(0.5, 40.0, size=rng.integers(1, 6)), 1)))
+                for _ in range(n_sg)]
+    heights = [[float(rng.choice([1.0, 2.0, 0.5])) for _ in ts] for ts in sg_times]
+    n = n_sg + n_par
+    src = rng.integers(0, n, size=n_edges)
+    tgt = rng.integers(n_sg, n, size=n_edges)
+    port = rng.integers(0, 2, size=n_edges)
+    w = rng.choice([0.25, 0.5, 1.0, -0.75, 3.0], size=n_edges).astype(np.float32)
+    d = (rng.integers(1, int(max_delay * 10) + 1, size=n_edges) * 0.1).astype(np.float32)
+    return sg_times, heights, src, tgt, port, w, d
+
+
+def test_spike_routing_bit_exact(ngpu):
+    """Spike generators and parrot neurons in a random recurrent graph:
+    every parrot's per-step summed input height and every emitted spike must
+    equal the oracle's exactly (integer routing, ordered-free fixed-point
+    accumulation)."""
+    from oracle import oracle as orc
+    rng = np.random.default_rng(7)
+    sg_times, heights, src, tgt, port, w, d = _routing_net(rng)
+    n_sg, n_par = len(sg_times), 60
+    n_steps = 600
+    # API
+    sg = ngpu.Create("spike_generator", n_sg)
+    for i in range(n_sg):
+        ngpu.SetStatus([sg[i]], {"spike_times": sg_times[i], "spike_heights": heights[i]})
+    par = ngpu.Create("parrot_neuron", n_par)
+    ngpu.SetStatus(par, {"hold_spike_height": 1.0})
+    for k in range(len(src)):
+        ngpu.Connect([int(src[k])], [int(tgt[k])], {"rule": "one_to_one"},
+                     {"weight": float(w[k]), "delay": float(d[k]), "receptor": int(port[k])})
+    rec = ngpu.CreateRecord("", ["V"] * n_par, list(range(n_sg, n_sg + n_par)), [0] * n_par)
+    ngpu.Simulate(n_steps * 0.1)
+    gpu = np.asarray(ngpu.GetRecordData(rec))[1:, 1:]
+    # oracle
+    net = orc.Network(dt=0.1)
+    osg = net.create(orc.SPIKE_GENERATOR, n_sg)
+    net.set_spikes(osg, sg_times, heights)
+    opar = net.create(orc.PARROT, n_par, 2, params={"hold_spike_height": 1.0})
+    net.connect(src, tgt, port, w, d)
+    ref = net.simulate(n_steps, record=[(n_sg + i, 2) for i in range(n_par)])
+    assert gpu.shape == ref.shape
+    assert np.count_nonzero(ref) > 50
+    np.testing.assert_array_equal(gpu.astype(np.float32), ref.astype(np.float32))
+
+
+def test_poisson_counts_bit_exact(ngpu):
+    """poisson_generator -> parrot (hold height): the per-step input equals the
+    Poisson count; GPU and oracle draw the same counts."""
+    from oracle import oracle as orc
+    n = 500
+    ngpu.SetKernelStatus("rnd_seed", 1234)
+    pg = ngpu.Create("poisson_generator")
+    ngpu.SetStatus(pg, "rate", 20000.0)
+    par = ngpu.Create("parrot_neuron", n)
+    ngpu.SetStatus(par, {"hold_spike_height": 1.0})
+    ngpu.Connect(pg, par, {"rule": "all_to_all"}, {"weight": 1.0, "delay": 0.1, "receptor": 0})
+    rec = ngpu.CreateRecord("", ["V"] * n, par.ToList(), [0] * n)
+    ngpu.Simulate(30.0)
+    gpu = np.asarray(ngpu.GetRecordData(rec))[1:, 1:]
+    net = orc.Network(dt=0.1, seed=1234)
+    opg = net.create(orc.POISSON_GENERATOR, 1, params={"rate": 20000.0})
+    opar = net.create(orc.PARROT, n, 2, params={"hold_spike_height": 1.0})
+    net.connect(np.zeros(n, dtype=np.int32), np.arange(n) + 1, 0, 1.0, 0.1)
+    ref = net.simulate(300, record=[(1 + i, 2) for i in range(n)])
+    np.testing.assert_array_equal(gpu, ref.astype(np.float32))
+    assert abs(gpu[1:].mean() - 2.0) < 0.05
+
+
+def _stdp_expect(w, Dt, tau_plus, tau_minus, Wplus, alpha, mu_plus, mu_minus, Wmax):
+    if Dt >= 0:
+        w1 = w + Wplus * math.exp(-Dt / tau_plus) * math.pow(1.0 - w / Wmax, mu_plus)
+        return min(w1, Wmax)
+    w1 = w - alpha * Wplus * math.exp(Dt / tau_minus) * math.pow(w / Wmax, mu_minus)
+    return max(w1, 0.0)
+
+
+def test_stdp_closed_form(ngpu):
+    """python/test/test_stdp.py restated: 50 neuron pairs with spike-time
+    differences -122.5 .. 122.5 ms; final weight vs the closed form."""
+    tau_plus = tau_minus = 20.0
+    lambd, alpha, mu_plus, mu_minus, Wmax = 1.0, 1.0, 1.0, 1.0, 0.001
+    N = 50
+    dt_list = [5.0 * (-0.5 * (N - 1) + i) for i in range(N)]
+    syn_group = ngpu.CreateSynGroup("stdp", {"tau_plus": tau_plus, "tau_minus": tau_minus,
+                                             "lambda": lambd, "alpha": alpha,
+                                             "mu_plus": mu_plus, "mu_minus": mu_minus,
+                                             "Wmax": Wmax})
+    sg = ngpu.Create("spike_generator", N)
+    neuron = ngpu.Create("aeif_cond_beta", 2 * N)
+    ngpu.SetStatus(neuron, {"t_ref": 1000.0, "den_delay": 0.0})
+    n0, n1 = neuron[0:N], neuron[N:2 * N]
+    ngpu.SetStatus(sg, {"spike_times": [50.0], "spike_heights": [1.0]})
+    ngpu.Connect(sg, n0, {"rule": "one_to_one"}, {"weight": 17.9, "delay": 1.0})
+    ngpu.Connect(sg, n1, {"rule": "one_to_one"}, {"weight": 17.9, "delay": 401.0})
+    for i in range(N):
+        ngpu.Connect([n0[i]], [n1[i]], {"rule": "one_to_one"},
+                     {"weight": Wmax / 2, "delay": 400.0 - dt_list[i],
+                      "synapse_group": syn_group})
+    ngpu.Simulate(1000.0)
+    conn = ngpu.GetConnections(n0, n1)
+    w = ngpu.GetStatus(conn, "weight")
+    assert len(w) == N
+    for i in range(N):
+        e = _stdp_expect(Wmax / 2, dt_list[i], tau_plus, tau_minus, lambd * Wmax, alpha,
+                         mu_plus, mu_minus, Wmax)
+        assert abs(e - w[i]) < 1e-5, (i, dt_list[i], e, w[i])
+
+
+def test_small_network_vs_oracle(ngpu):
+    """100 AdEx neurons with Poisson drive and random recurrent synapses:
+    traces agree with the FP64 oracle until the first spike, and the spike
+    trains agree (same neuron, within one step) for the first 30 ms."""
+    from oracle import oracle as orc
+    rng = np.random.default_rng(11)
+    n = 100
+    ne = 80
+    k = 20
+    src = np.concatenate([rng.choice(n, size=k, replace=False) for _ in range(n)])
+    tgt = np.repeat(np.arange(n), k)
+    port = (src >= ne).astype(np.int32)
+    w = np.where(src < ne, 0.5, 1.5).astype(np.float32)
+    d = (rng.integers(1, 3, size=len(src)) * 1.0).astype(np.float32)
+    params = {"E_rev": [0.0, -85.0], "tau_rise": [0.2, 0.5], "tau_decay": [2.0, 8.0]}
+    ngpu.SetKernelStatus("rnd_seed", 99)
+    pg = ngpu.Create("poisson_generator")
+    ngpu.SetStatus(pg, "rate", 20000.0)
+    nrn = ngpu.Create("aeif_cond_beta", n, 2)
+    ngpu.SetStatus(nrn, params)
+    ngpu.Connect(pg, nrn, {"rule": "all_to_all"}, {"weight": 0.5, "delay": 0.1, "receptor": 0})
+    for p in (0, 1):
+        m = port == p
+        ngpu.Connect((src[m] + 1).tolist(), (tgt[m] + 1).tolist(), {"rule": "one_to_one"},
+                     {"weight": {"array": w[m].tolist()}, "delay": {"array": d[m].tolist()},
+                      "receptor": p})
+    ngpu.ActivateRecSpikeTimes(nrn, 1000)
+    rec = ngpu.CreateRecord("", ["V_m"] * n, nrn.ToList(), [0] * n)
+    ngpu.Simulate(100.0)
+    gv = np.asarray(ngpu.GetRecordData(rec))[1:, 1:]
+    net = orc.Network(dt=0.1, seed=99)
+    net.create(orc.POISSON_GENERATOR, 1, params={"rate": 20000.0})
+    on = net.create(orc.AEIF_COND_BETA, n, 2,
+                    params={k2: [np.float32(x) for x in v2] for k2, v2 in params.items()})
+    net.connect(np.zeros(n, dtype=np.int32), np.arange(n) + 1, 0, 0.5, 0.1)
+    for p in (0, 1):
+        m = port == p
+        net.connect(src[m] + 1, tgt[m] + 1, p, w[m], d[m])
+    ov = net.simulate(1000, record=[(1 + i, 0) for i in range(n)])
+    steps, nodes = net.spikes()
+    first = int(steps.min()) if len(steps) else 1000
+    assert first > 10
+    # sub-threshold traces before the first spike
+    err = np.max(np.abs(gv[:first] - ov[:first])) / 70.0
+    assert err < 1e-4, err
+    # spike trains of the first 30 ms
+    g_sp = []
+    for i in range(n):
+        g_sp += [(round(t / 0.1) - 1, i) for t in ngpu.GetRecSpikeTimes(nrn[i]) if t <= 30.0]
+    o_sp = [(int(s), int(nd) - 1) for s, nd in zip(steps, nodes) if s < 300]
+    assert len(o_sp) > 0
+    matched = 0
+    for s, i in o_sp:
+        if any(abs(s - s2) <= 1 and i == i2 for s2, i2 in g_sp):
+            matched += 1
+    assert matched >= 0.99 * len(o_sp), (matched, len(o_sp), len(g_sp))
+
+
+def test_api_status_roundtrip(ngpu):
+    nrn = ngpu.Create("aeif_cond_beta", 10, 2)
+    ngpu.SetStatus(nrn, {"a": 3.0, "tau_decay": [3.0, 9.0]})
+    ngpu.SetStatus(nrn[2:4], {"V_m": -55.0})
+    assert ngpu.GetStatus(nrn[0], "a") == pytest.approx(3.0)
+    assert ngpu.GetStatus(nrn[3], "V_m") == pytest.approx(-55.0)
+    assert ngpu.GetStatus(nrn[5], "V_m") == pytest.approx(-70.6, abs=1e-5)
+    assert ngpu.GetStatus(nrn[1], "tau_decay") == pytest.approx([3.0, 9.0])
+    st = ngpu.GetStatus(nrn[0])
+    assert set(["V_m", "w", "g", "g1", "E_rev", "tau_rise", "h_min_rel"]) <= set(st)
+    with pytest.raises(ValueError):
+        ngpu.SetStatus(nrn, {"no_such_param": 1.0})
+    ngpu.SetStatus([nrn[1], nrn[7]], "b", 50.0)
+    b = ngpu.GetStatus(nrn, "b")
+    assert b[1] == pytest.approx(50.0) and b[7] == pytest.approx(50.0)
+    assert b[0] == pytest.approx(80.5)
+
+
+def test_connection_queries(ngpu):
+    a = ngpu.Create("aeif_cond_beta", 20, 2)
+    b = ngpu.Create("aeif_cond_beta", 30, 2)
+    ngpu.SetKernelStatus("rnd_seed", 5)
+    ngpu.Connect(a, b, {"rule": "fixed_indegree", "indegree": 7},
+                 {"weight": 0.1, "delay": {"distribution": "normal_clipped", "mu": 1.0,
+                                           "low": 0.5, "high": 1.5, "sigma": 0.3},
+                  "receptor": 1})
+    conns = ngpu.GetConnections(a, b)
+    assert len(conns) == 30 * 7
+    for i in range(3):
+        assert len(ngpu.GetConnections(target=b[i])) == 7
+    st = ngpu.GetStatus(conns[0])
+    assert st["port"] == 1 and st["weight"] == pytest.approx(0.1)
+    assert 0.5 - 1e-6 <= st["delay"] <= 1.5 + 1e-6
+    # no multapses per target
+    for i in range(30):
+        srcs = [c.i_source for c in ngpu.GetConnections(target=[b[i]])]
+        assert len(set(srcs)) == 7
+    ngpu.Simulate(5.0)
+    st2 = ngpu.GetStatus(conns[0])
+    assert st2 == st
