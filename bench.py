@@ -246,7 +246,10 @@ def main():
     ap.add_argument("--cpu-ms", type=float, default=200.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-gpu", action="store_true")
+    ap.add_argument("--n", type=int, default=0, help="override the number of neurons")
     args = ap.parse_args()
+    if args.n > 0:
+        SCALE["n"] = SMALL["n"] = args.n
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         return run_reference(args, world, rank)

@@ -286,26 +286,50 @@ void NeuronGPU::BuildHostCSR() {
   }
   for (uint64_t k = 0; k < nkeys; k++) h_grp_off_[k + 1] += h_grp_off_[k];
   h_order_.assign(E, 0);
-  // stable scatter, parallel over disjoint source ranges
+  // Stable scatter. The edge list is split into T contiguous chunks; each
+  // chunk's edges of a key go after those of the earlier chunks, so the
+  // result keeps insertion order for any T.
   int nthr = 1;
 #ifdef _OPENMP
   nthr = omp_get_max_threads();
-  if (E < 1000000) nthr = 1;
+  if (E < 4000000) nthr = 1;
+  while (nthr > 1 && (uint64_t)nthr * nkeys > (1ull << 30)) nthr /= 2;
 #endif
-  std::vector<uint64_t> fill(h_grp_off_.begin(), h_grp_off_.end() - 1);
-#pragma omp parallel num_threads(nthr)
-  {
-    int tid = 0, nt = 1;
-#ifdef _OPENMP
-    tid = omp_get_thread_num();
-    nt = omp_get_num_threads();
-#endif
-    long long s_lo = N * tid / nt, s_hi = N * (tid + 1) / nt;
+  if (nthr <= 1) {
+    std::vector<uint64_t> fill(h_grp_off_.begin(), h_grp_off_.end() - 1);
     for (uint64_t k = 0; k < E; k++) {
-      long long s = e_src_[k];
-      if (s < s_lo || s >= s_hi) continue;
-      uint64_t key = (uint64_t)s * nd + delay_index_[e_d_[k]];
+      uint64_t key = (uint64_t)e_src_[k] * nd + delay_index_[e_d_[k]];
       h_order_[fill[key]++] = k;
+    }
+  } else {
+    std::vector<std::vector<uint32_t>> cnt(nthr);
+#pragma omp parallel num_threads(nthr)
+    {
+      int tid = 0;
+#ifdef _OPENMP
+      tid = omp_get_thread_num();
+#endif
+      uint64_t lo = E * tid / nthr, hi = E * (tid + 1) / nthr;
+      std::vector<uint32_t> &c = cnt[tid];
+      c.assign(nkeys, 0);
+      for (uint64_t k = lo; k < hi; k++)
+        c[(uint64_t)e_src_[k] * nd + delay_index_[e_d_[k]]]++;
+#pragma omp barrier
+      // exclusive prefix over chunks, per key (offset inside the group)
+      uint64_t k_lo = nkeys * tid / nthr, k_hi = nkeys * (tid + 1) / nthr;
+      for (uint64_t key = k_lo; key < k_hi; key++) {
+        uint32_t run = 0;
+        for (int t = 0; t < nthr; t++) {
+          uint32_t v = cnt[t][key];
+          cnt[t][key] = run;
+          run += v;
+        }
+      }
+#pragma omp barrier
+      for (uint64_t k = lo; k < hi; k++) {
+        uint64_t key = (uint64_t)e_src_[k] * nd + delay_index_[e_d_[k]];
+        h_order_[h_grp_off_[key] + c[key]++] = k;
+      }
     }
   }
   host_csr_valid_ = true;

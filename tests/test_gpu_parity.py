@@ -60,7 +60,9 @@ def test_spike_routing_bit_exact(ngpu):
     for i in range(n_sg):
         ngpu.SetStatus([sg[i]], {"spike_times": sg_times[i], "spike_heights": heights[i]})
     par = ngpu.Create("parrot_neuron", n_par)
-    ngpu.SetStatus(par, {"hold_spike_height": 1.0})
+    # parrots re-emit height 1 (hold_spike_height 0): heights stay bounded
+    # in recurrent loops, while V records the raw summed input
+    ngpu.SetStatus(par, {"hold_spike_height": 0.0})
     for k in range(len(src)):
         ngpu.Connect([int(src[k])], [int(tgt[k])], {"rule": "one_to_one"},
                      {"weight": float(w[k]), "delay": float(d[k]), "receptor": int(port[k])})
@@ -71,7 +73,7 @@ def test_spike_routing_bit_exact(ngpu):
     net = orc.Network(dt=0.1)
     osg = net.create(orc.SPIKE_GENERATOR, n_sg)
     net.set_spikes(osg, sg_times, heights)
-    opar = net.create(orc.PARROT, n_par, 2, params={"hold_spike_height": 1.0})
+    opar = net.create(orc.PARROT, n_par, 2, params={"hold_spike_height": 0.0})
     net.connect(src, tgt, port, w, d)
     ref = net.simulate(n_steps, record=[(n_sg + i, 2) for i in range(n_par)])
     assert gpu.shape == ref.shape
