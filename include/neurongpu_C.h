@@ -229,6 +229,26 @@ double NGB200_LastSimulateDeviceMs();
 int NGB200_SetKernelTiming(int on);
 int NGB200_GetKernelTiming(int kind, double *total_ms, long long *launches);
 
+/* Standalone synaptic delivery, the simulator's delivery kernel applied to a
+ * caller-owned graph and spike batch (all pointers are device memory):
+ *   grp_off[n_src*nd + 1]  edge range of (source s, delay index di) is
+ *                          [grp_off[s*nd+di], grp_off[s*nd+di+1])
+ *   e_slot[E], e_w[E]      accumulator index and weight of every synapse
+ *   spike_src[k], spike_h[k], spike_di[k]   source, height and delay index
+ *                          (0 <= di < nd, nd <= 1024) of spike k
+ *   acc[]                  64-bit fixed-point accumulators (32 fractional
+ *                          bits), zeroed by the caller; every synapse of
+ *                          every spike adds round(h*w * 2^32)
+ * Scratch device memory for the per-delay spike lists is allocated and
+ * released inside the call; the call returns after the stream is drained.
+ * Returns 0 on success, 1 bad arguments, 2 allocation failure, 3 CUDA
+ * error, 4 a spike with an out-of-range delay index. */
+int NGB200_DeliverSpikes(const unsigned long long *grp_off,
+                         const unsigned *e_slot, const float *e_w, int nd,
+                         const unsigned *spike_src, const float *spike_h,
+                         const int *spike_di, int n_spikes, long long *acc,
+                         void *stream);
+
 #ifdef __cplusplus
 }
 #endif

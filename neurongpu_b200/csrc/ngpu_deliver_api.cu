@@ -1,0 +1,125 @@
+// Standalone spike delivery through the C ABI: one batch of spikes through a
+// caller-owned CSR synapse graph into caller-owned fixed-point accumulators,
+// using the simulator's delivery kernel (k_deliver in ngpu_kernels.cu).
+//
+// The kernel reads spikes from per-delay slots of a spike ring; this entry
+// point builds that ring in scratch device memory (allocated per call),
+// buckets the caller's spikes into it by delay index, runs the delivery and
+// releases the scratch.
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include "ngpu_device.h"
+#include "ngpu_kernels.h"
+
+namespace ngpu {
+
+// spike k of the batch goes to ring slot (nd - di[k]) so that the kernel,
+// run at time index T = nd + 1 with delays[di] = di + 1, finds it there
+__global__ void k_bucket_spikes(const unsigned *src, const float *h, const int *di, int n,
+                                int nd, unsigned *ring_src, float *ring_h, int *ring_cnt,
+                                int C, unsigned *err) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int d = di[k];
+  if (d < 0 || d >= nd) {
+    atomicOr(err, 1u);
+    return;
+  }
+  int slot = nd - d;
+  int pos = atomicAdd(&ring_cnt[slot], 1);
+  if (pos < C) {
+    ring_src[(long long)slot * C + pos] = src[k];
+    ring_h[(long long)slot * C + pos] = h[k];
+  } else {
+    atomicOr(err, 2u);
+  }
+}
+
+__global__ void k_prepare_batch(StepCtx *ctx, int *delays, int *ring_cnt, int nd) {
+  int t = threadIdx.x;
+  if (t == 0) {
+    ctx->it = 0;
+    ctx->T0 = nd;          // T = T0 + it + 1 = nd + 1
+    ctx->t0 = 0.0;
+    ctx->err = 0;
+  }
+  for (int k = t; k < nd; k += blockDim.x) delays[k] = k + 1;
+  for (int k = t; k < nd + 1; k += blockDim.x) ring_cnt[k] = 0;
+}
+
+int DeliverBatch(const unsigned long long *grp_off, const unsigned *e_slot, const float *e_w,
+                 int nd, const unsigned *spike_src, const float *spike_h, const int *spike_di,
+                 int n_spikes, long long *acc, cudaStream_t stream, unsigned *ring_src,
+                 float *ring_h, int *ring_cnt, int *delays, StepCtx *ctx, unsigned *err) {
+  const int C = n_spikes > 0 ? n_spikes : 1;
+  k_prepare_batch<<<1, 128, 0, stream>>>(ctx, delays, ring_cnt, nd);
+  if (n_spikes > 0) {
+    k_bucket_spikes<<<(n_spikes + 255) / 256, 256, 0, stream>>>(
+        spike_src, spike_h, spike_di, n_spikes, nd, ring_src, ring_h, ring_cnt, C, err);
+  }
+  DeliverArgs d;
+  memset(&d, 0, sizeof(d));
+  d.grp_off = grp_off;
+  d.e_slot = e_slot;
+  d.e_w = (float *)e_w;
+  d.acc = acc;
+  d.ring_src = ring_src;
+  d.ring_h = ring_h;
+  d.ring_cnt = ring_cnt;
+  d.ring_R = nd + 1;
+  d.ring_C = C;
+  d.nd = nd;
+  d.delays = delays;
+  SynGroupTable syn;
+  memset(&syn, 0, sizeof(syn));
+  LaunchDeliver(d, syn, ctx, 148 * 8, stream);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+}  // namespace ngpu
+
+using namespace ngpu;
+
+extern "C" int NGB200_DeliverSpikes(const unsigned long long *grp_off, const unsigned *e_slot,
+                                    const float *e_w, int nd, const unsigned *spike_src,
+                                    const float *spike_h, const int *spike_di, int n_spikes,
+                                    long long *acc, void *stream) {
+  if (nd <= 0 || nd > NGPU_MAX_DELAYS || n_spikes < 0) return 1;
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long C = n_spikes > 0 ? n_spikes : 1;
+  const long long R = nd + 1;
+  unsigned *ring_src = nullptr, *err = nullptr;
+  float *ring_h = nullptr;
+  int *ring_cnt = nullptr, *delays = nullptr;
+  StepCtx *ctx = nullptr;
+  int rc = 0;
+  if (cudaMalloc(&ring_src, sizeof(unsigned) * R * C) != cudaSuccess ||
+      cudaMalloc(&ring_h, sizeof(float) * R * C) != cudaSuccess ||
+      cudaMalloc(&ring_cnt, sizeof(int) * R) != cudaSuccess ||
+      cudaMalloc(&delays, sizeof(int) * nd) != cudaSuccess ||
+      cudaMalloc(&ctx, sizeof(StepCtx)) != cudaSuccess ||
+      cudaMalloc(&err, sizeof(unsigned)) != cudaSuccess) {
+    rc = 2;
+  } else {
+    cudaMemsetAsync(err, 0, sizeof(unsigned), s);
+    if (DeliverBatch(grp_off, e_slot, e_w, nd, spike_src, spike_h, spike_di, n_spikes, acc, s,
+                     ring_src, ring_h, ring_cnt, delays, ctx, err) != 0) {
+      rc = 3;
+    }
+    unsigned h_err = 0;
+    if (cudaMemcpyAsync(&h_err, err, sizeof(unsigned), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+      rc = 3;
+    } else if (h_err) {
+      rc = 4;
+    }
+  }
+  cudaFree(ring_src);
+  cudaFree(ring_h);
+  cudaFree(ring_cnt);
+  cudaFree(delays);
+  cudaFree(ctx);
+  cudaFree(err);
+  return rc;
+}
