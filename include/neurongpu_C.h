@@ -249,6 +249,26 @@ int NGB200_DeliverSpikes(const unsigned long long *grp_off,
                          const int *spike_di, int n_spikes, long long *acc,
                          void *stream);
 
+/* NGB200_DeliverSpikes without any device allocation. This entry point has
+ * no counterpart in the reference. It is for callers that cannot allocate
+ * device memory while they run: a host program whose own allocator owns the
+ * device memory, or a loop that must not stall, where a cudaMalloc / cudaFree
+ * could fail or would synchronise the device and block the caller's other
+ * streams. Same arguments and result as NGB200_DeliverSpikes. Its scratch is
+ * a file-scope __device__ array of about 8 MiB that every GPU loading the
+ * library keeps until the process exits; a batch may use at most
+ * (nd + 1) * n_spikes <= 1048576 spike-list entries, larger batches are
+ * rejected with return code 5 before any work is queued. The first call on a
+ * device looks up the array's device address with that device current; make
+ * that first call before any stream capture. All calls share the array:
+ * each call clears its counters and error word first, and calls that
+ * overlap on the GPU race on it. Returns after the stream is drained. */
+int NGB200_DeliverSpikesNoAlloc(const unsigned long long *grp_off,
+                                const unsigned *e_slot, const float *e_w,
+                                int nd, const unsigned *spike_src,
+                                const float *spike_h, const int *spike_di,
+                                int n_spikes, long long *acc, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
