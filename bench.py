@@ -247,9 +247,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-gpu", action="store_true")
     ap.add_argument("--n", type=int, default=0, help="override the number of neurons")
+    ap.add_argument("--w-pg", type=float, default=0.0,
+                    help="override the Poisson drive weight (nS) for an active network")
     args = ap.parse_args()
     if args.n > 0:
         SCALE["n"] = SMALL["n"] = args.n
+    if args.w_pg > 0:
+        SCALE["w_pg"] = SMALL["w_pg"] = args.w_pg
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         return run_reference(args, world, rank)
@@ -268,7 +272,8 @@ def main():
     for _ in range(args.warmup):
         ngpu.Simulate(step_ms)
     # timed region (device time of the step loops), per-kernel events on
-    b.SetKernelTiming(True)
+    # timed region: device time of the step loops (CUDA events on the
+    # simulation stream), no per-kernel instrumentation
     ev0 = b.DeliveredEvents()
     evals0 = b.StageEvaluations()
     spikes0 = b.TotalSpikes()
@@ -285,8 +290,16 @@ def main():
     events = b.DeliveredEvents() - ev0
     evals = b.StageEvaluations() - evals0
     spikes = b.TotalSpikes() - spikes0
+    # same number of steps again with CUDA events around every kernel class
+    # of every step, for the per-kernel launch durations of the roofline
+    b.SetKernelTiming(True)
+    ev1 = b.DeliveredEvents()
+    for _ in range(args.steps):
+        ngpu.Simulate(step_ms)
+    events_instr = b.DeliveredEvents() - ev1
     upd_ms, upd_n = b.GetKernelTiming(0)
     del_ms, del_n = b.GetKernelTiming(1)
+    stdp_ms, stdp_n = b.GetKernelTiming(2)
     oth_ms, oth_n = b.GetKernelTiming(3)
     b.SetKernelTiming(False)
     bio_s = args.steps * step_ms / 1000.0
@@ -304,7 +317,7 @@ def main():
         traffic = tpu * cfg["n"] if tpu else None
     else:
         kname = "deliver"
-        ev_launch = events / max(del_n, 1)
+        ev_launch = events_instr / max(del_n, 1)
         bytes_launch = BYTES_PER_EVENT * ev_launch
         avg_ms = del_ms / max(del_n, 1)
         tpu = tr.get("deliver_bytes_per_event")
@@ -313,8 +326,11 @@ def main():
     roof = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
             "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "avg_launch_ms": avg_ms,
-            "kernel_ms": {"update": upd_ms, "deliver": del_ms, "bookkeeping": oth_ms},
-            "launches": {"update": upd_n, "deliver": del_n, "bookkeeping": oth_n}}
+            "kernel_ms": {"update": upd_ms, "deliver": del_ms, "stdp": stdp_ms,
+                          "bookkeeping": oth_ms},
+            "launches": {"update": upd_n, "deliver": del_n, "stdp": stdp_n,
+                         "bookkeeping": oth_n},
+            "timing": "kernel events over a second run of the timed steps"}
     # end-to-end through the public API: H2D of the generator parameters,
     # the simulation call, D2H of the per-neuron spike counts
     e2e_steps = max(1, min(args.steps, 3))
@@ -343,8 +359,9 @@ def main():
         "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": ("scale" if args.config == "scale" else "small")
-                   + ": %d aeif_cond_beta x %d synapses, Poisson %.0f Hz, dt 0.1 ms, RK5 eps %g"
-                   % (cfg["n"], cfg["k_exc"] + cfg["k_inh"], cfg["rate"], cfg["eps"]),
+                   + ": %d aeif_cond_beta x %d synapses, Poisson %.0f Hz w %g nS, dt 0.1 ms, "
+                   "RK5 eps %g" % (cfg["n"], cfg["k_exc"] + cfg["k_inh"], cfg["rate"],
+                                   cfg["w_pg"], cfg["eps"]),
                    "step_bio_ms": step_ms, "integration_steps": n_steps,
                    "l2": "inputs larger than L2 (1e9 synapses, 8 GB)",
                    "parallelism": "replicas" if world > 1 else "single"},
@@ -352,8 +369,9 @@ def main():
         "mean_rate_hz": rate_hz,
         "rk5_stage_evals_per_neuron_step": evals / (cfg["n"] * n_steps),
         "wall_per_bio_s": (dev_ms_max / 1000.0) / bio_s,
+        "rk5_tuning": b.GetRk5Tuning(nrn.i0),
         "build_s": build_s,
-        "gpu_launches": int(upd_n + del_n + oth_n),
+        "gpu_launches": int(2 * n_steps),
         "roofline": roof,
         "cpu_baseline": cpu,
         "e2e": e2e,

@@ -77,7 +77,7 @@ void NeuronGPU::FreeDevice() {
   F(d_e_post_); F(d_rev_off_); F(d_rev_edge_); F(d_delays_);
   F(d_dc_off_); F(d_dc_gen_); F(d_dc_port_); F(d_dc_w_); F(d_dc_delay_);
   F(d_dc_stream_); F(d_gen_rate_); F(d_gen_origin_); F(d_gen_start_);
-  F(d_gen_stop_); F(d_gen_lambda_); F(d_gen_explam_); F(d_blk_events_);
+  F(d_gen_stop_); F(d_gen_lambda_); F(d_gen_explam_); F(d_gen_cdf_); F(d_blk_events_); F(d_done_);
   F(d_rec_cols_); F(d_rec_buf_);
   for (cudaEvent_t e : kev_) cudaEventDestroy(e);
   kev_.clear();
@@ -859,16 +859,24 @@ GroupArgs NeuronGPU::MakeGroupArgs(NodeGroup *g) {
   a.param = g->d_param;
   a.h = g->d_h;
   a.dx = g->d_dx;
+  a.all_uniform = 1;
   for (int j = 0; j < g->nparam; j++) {
     bool per_neuron = !g->p_uniform[j] || j == g->mi->refr_param;
     if (per_neuron) a.pmask[j >> 5] |= (1u << (j & 31));
+    if (!g->p_uniform[j] && j != g->mi->refr_param) a.all_uniform = 0;
     a.puni[j] = g->p_uval[j];
+    // reciprocals for the RK5 right-hand sides (IEEE float division, the
+    // same value the kernel forms for per-neuron parameters)
+    volatile float one = 1.0f;
+    a.pinv[j] = one / g->p_uval[j];
   }
   if (g->mi->kind == MK_RK5) {
     a.h_min = g->group_param[0] * time_resolution_;
     a.eps = g->rk5_eps;
   }
   a.dt = time_resolution_;
+  a.variant = g->rk5_variant;
+  a.dry = 0;
   a.den_delay_col = g->mi->den_delay_param;
   a.blk_evals = g->d_blk_evals;
   a.sg_off = g->d_sg_off;
@@ -910,6 +918,21 @@ InputArgs NeuronGPU::MakeInputArgs(NodeGroup *g) {
     in.gen_stop = d_gen_stop_;
     in.gen_lambda = d_gen_lambda_;
     in.gen_explam = d_gen_explam_;
+    in.gen_cdf = d_gen_cdf_;
+  }
+  if (g->ud && g->ud_gen < (int)gen_lam_h_.size()) {
+    const int k = g->ud_gen;
+    in.ud = 1;
+    in.ud_port = g->ud_port;
+    in.ud_w = g->ud_w;
+    in.ud_delay = g->ud_delay;
+    in.ud_origin = gen_origin_h_[k];
+    in.ud_start = gen_start_h_[k];
+    in.ud_stop = gen_stop_h_[k];
+    in.ud_lambda = gen_lam_h_[k];
+    in.ud_explam = gen_explam_h_[k];
+    in.ud_cdf = d_gen_cdf_ + (size_t)k * NGPU_CDF_LEN;
+    in.ud_stream0 = g->ud_stream0;
   }
   in.seed = kernel_seed_;
   return in;
@@ -956,6 +979,9 @@ DeliverArgs NeuronGPU::MakeDeliverArgs() {
   d.rev_edge = d_rev_edge_;
   d.dt = time_resolution_;
   d.blk_events = d_blk_events_;
+  d.advance_flags = 0;
+  d.ring_cnt_w = d_ring_cnt_;
+  d.done = d_done_;
   return d;
 }
 
@@ -1226,6 +1252,27 @@ void NeuronGPU::BuildDevice() {
     for (NodeGroup *g : groups_) {
       g->has_dc = off[g->i_node_0 + g->n_node] > off[g->i_node_0];
       g->d_dc_off = d_dc_off_ + g->i_node_0;
+      // uniform drive: one connection per node, identical except for the
+      // random stream, which must run consecutively with the node index
+      g->ud = false;
+      if (g->has_dc && g->n_port > 0) {
+        const size_t b0 = off[g->i_node_0];
+        bool ok = true;
+        for (int i = 0; i < g->n_node && ok; i++) {
+          size_t b = off[g->i_node_0 + i];
+          ok = (off[g->i_node_0 + i + 1] - b == 1) && gen[b] == gen[b0] &&
+               port[b] == port[b0] && wv[b] == wv[b0] && dv[b] == dv[b0] &&
+               st[b] == st[b0] + (unsigned long long)i;
+        }
+        if (ok) {
+          g->ud = true;
+          g->ud_gen = (int)gen[b0];
+          g->ud_port = port[b0];
+          g->ud_w = wv[b0];
+          g->ud_delay = dv[b0];
+          g->ud_stream0 = st[b0];
+        }
+      }
     }
     NGPU_CUDA(cudaMalloc(&d_gen_rate_, sizeof(float) * n_gen_));
     NGPU_CUDA(cudaMalloc(&d_gen_origin_, sizeof(float) * n_gen_));
@@ -1233,9 +1280,19 @@ void NeuronGPU::BuildDevice() {
     NGPU_CUDA(cudaMalloc(&d_gen_stop_, sizeof(float) * n_gen_));
     NGPU_CUDA(cudaMalloc(&d_gen_lambda_, sizeof(double) * n_gen_));
     NGPU_CUDA(cudaMalloc(&d_gen_explam_, sizeof(double) * n_gen_));
+    NGPU_CUDA(cudaMalloc(&d_gen_cdf_, sizeof(double) * n_gen_ * NGPU_CDF_LEN));
   }
   // counters, per-group device extras and calibration
-  deliver_blocks_ = 148 * 8;
+  // one full wave of resident delivery blocks (grid-stride over the items)
+  int n_sm = 148;
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  }
+  deliver_blocks_ = n_sm * DeliverBlocksPerSM();
+  NGPU_CUDA(cudaMalloc(&d_done_, sizeof(unsigned)));
+  NGPU_CUDA(cudaMemset(d_done_, 0, sizeof(unsigned)));
   NGPU_CUDA(cudaMalloc(&d_blk_events_, sizeof(unsigned long long) * deliver_blocks_));
   NGPU_CUDA(cudaMemset(d_blk_events_, 0, sizeof(unsigned long long) * deliver_blocks_));
   for (NodeGroup *g : groups_) {
@@ -1313,6 +1370,7 @@ void NeuronGPU::UploadGeneratorParams() {
   if (n_gen_ == 0) return;
   std::vector<float> rate(n_gen_), origin(n_gen_), start(n_gen_), stop(n_gen_);
   std::vector<double> lam(n_gen_), explam(n_gen_);
+  std::vector<double> cdf((size_t)n_gen_ * NGPU_CDF_LEN);
   const float time_step = (float)(time_resolution_ / 1000.0);
   for (int k = 0; k < n_gen_; k++) {
     int node = gen_nodes_[k];
@@ -1326,7 +1384,22 @@ void NeuronGPU::UploadGeneratorParams() {
     float lf = time_step * rate[k];      // float product, as in src/poiss_gen.cu:62
     lam[k] = (double)lf;
     explam[k] = exp(-(double)lf);
+    // CDF by the recurrence of ng_poisson_inversion (same double operations)
+    double pk = explam[k], F = pk;
+    cdf[(size_t)k * NGPU_CDF_LEN] = F;
+    for (int n = 1; n < NGPU_CDF_LEN; n++) {
+      pk = (pk * lam[k]) / (double)n;
+      F = F + pk;
+      cdf[(size_t)k * NGPU_CDF_LEN + n] = F;
+    }
   }
+  NGPU_CUDA(cudaMemcpy(d_gen_cdf_, cdf.data(), sizeof(double) * cdf.size(), cudaMemcpyHostToDevice));
+  gen_origin_h_ = origin;
+  gen_start_h_ = start;
+  gen_stop_h_ = stop;
+  gen_lam_h_ = lam;
+  gen_explam_h_ = explam;
+  InvalidateGraphs();
   NGPU_CUDA(cudaMemcpy(d_gen_rate_, rate.data(), sizeof(float) * n_gen_, cudaMemcpyHostToDevice));
   NGPU_CUDA(cudaMemcpy(d_gen_origin_, origin.data(), sizeof(float) * n_gen_, cudaMemcpyHostToDevice));
   NGPU_CUDA(cudaMemcpy(d_gen_start_, start.data(), sizeof(float) * n_gen_, cudaMemcpyHostToDevice));
@@ -1412,19 +1485,27 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
         break;
     }
   }
-  if (ktime_) KEvent(step_in_chunk, 1);
-  DeliverArgs d = MakeDeliverArgs();
-  LaunchDeliver(d, syn_table_, d_ctx_, deliver_blocks_, stream_);
-  if (ktime_) KEvent(step_in_chunk, 2);
-  if (plastic_) LaunchStdpPost(d, syn_table_, d_ctx_, 148 * 2, stream_);
-  if (ktime_) KEvent(step_in_chunk, 3);
+  // multimeter columns: state after the update, before this step's input is
+  // delivered (the reference records between the two, src/neurongpu.cu:488)
   int flags = 1;
   if (n_rec_cols_ > 0) {
     LaunchRecord(d_rec_cols_, n_rec_cols_, d_rec_buf_, rec_cap_rows_, d_last_spike_T_,
                  d_last_spike_h_, 0, time_resolution_, d_ctx_, stream_);
     flags |= 2;
   }
-  LaunchAdvance(d_ring_cnt_, ring_R_, ring_C_, flags, d_ctx_, stream_);
+  if (ktime_) KEvent(step_in_chunk, 1);
+  // the step's last kernel also does the step bookkeeping (finish_step)
+  DeliverArgs d = MakeDeliverArgs();
+  const bool has_delivery = d.nd > 0;
+  if (has_delivery && !plastic_) d.advance_flags = flags;
+  LaunchDeliver(d, syn_table_, d_ctx_, deliver_blocks_, stream_);
+  if (ktime_) KEvent(step_in_chunk, 2);
+  if (plastic_) {
+    d.advance_flags = flags;
+    LaunchStdpPost(d, syn_table_, d_ctx_, 148 * 2, stream_);
+  }
+  if (ktime_) KEvent(step_in_chunk, 3);
+  if (!has_delivery && !plastic_) LaunchAdvance(d_ring_cnt_, ring_R_, ring_C_, flags, d_ctx_, stream_);
   if (ktime_) KEvent(step_in_chunk, 4);
 }
 
@@ -1538,6 +1619,64 @@ int NeuronGPU::FlushInput() {
   return 0;
 }
 
+// RK5 autotuner: times every kernel variant of a group on the live state in
+// dry mode (full computation, no stores) and keeps the fastest. The variants
+// differ only in their register cap (occupancy), not in arithmetic.
+void NeuronGPU::TuneRk5(NodeGroup *g) {
+  g->tuned = true;
+  const char *force = getenv("NGB200_RK5_VARIANT");
+  GroupArgs a = MakeGroupArgs(g);
+  int nv = Rk5VariantCount(g->n_port, a.all_uniform);
+  if (force != nullptr) {
+    g->rk5_variant = std::max(0, std::min(nv - 1, atoi(force)));
+    InvalidateGraphs();
+    return;
+  }
+  const char *off = getenv("NGB200_AUTOTUNE");
+  if ((off != nullptr && atoi(off) == 0) || nv <= 1 || g->n_node < 16384) return;
+  InputArgs in = MakeInputArgs(g);
+  PushArgs pa = MakePushArgs(g);
+  a.dry = 1;
+  in.dry = 1;
+  a.blk_evals = nullptr;
+  cudaEvent_t e0, e1;
+  NGPU_CUDA(cudaEventCreate(&e0));
+  NGPU_CUDA(cudaEventCreate(&e1));
+  int best = 0;
+  float best_ms = 1e30f;
+  for (int v = 0; v < nv; v++) {
+    a.variant = v;
+    LaunchRk5Update(g->mi->rk5_model, g->n_port, a, in, pa, d_ctx_, stream_);
+    float t[3];
+    for (int r = 0; r < 3; r++) {
+      NGPU_CUDA(cudaEventRecord(e0, stream_));
+      LaunchRk5Update(g->mi->rk5_model, g->n_port, a, in, pa, d_ctx_, stream_);
+      NGPU_CUDA(cudaEventRecord(e1, stream_));
+      NGPU_CUDA(cudaEventSynchronize(e1));
+      NGPU_CUDA(cudaEventElapsedTime(&t[r], e0, e1));
+    }
+    std::sort(t, t + 3);
+    g->tune_ms[v] = t[1];
+    if (t[1] < best_ms) {
+      best_ms = t[1];
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  NGPU_CUDA(cudaGetLastError());
+  g->rk5_variant = best;
+  InvalidateGraphs();
+}
+
+int NeuronGPU::GetRk5Tuning(int i_node, int *variant, float *ms4) {
+  int il;
+  NodeGroup *g = GroupOf(i_node, 1, il);
+  *variant = g->rk5_variant;
+  for (int v = 0; v < 4; v++) ms4[v] = g->tune_ms[v];
+  return 0;
+}
+
 int NeuronGPU::StartSimulation() {
   if (!calibrate_flag_) Calibrate();
   FlushInput();
@@ -1557,6 +1696,8 @@ int NeuronGPU::StartSimulation() {
     printf("Neural activity simulation time: %.3lf\n", (double)sim_time_);
   }
   UploadGeneratorParams();
+  for (NodeGroup *g : groups_)
+    if (g->mi->kind == MK_RK5 && !g->tuned) TuneRk5(g);
   neur_t0_ = neural_time_;
   it_ = 0;
   Nt_ = (long long)round(sim_time_ / time_resolution_);

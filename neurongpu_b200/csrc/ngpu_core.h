@@ -115,11 +115,20 @@ struct NodeGroup {
   // Poisson direct connections into this group (CSR by local node)
   unsigned *d_dc_off = nullptr;
   bool has_dc = false;
+  // uniform drive (one identical direct connection per node, see InputArgs)
+  bool ud = false;
+  int ud_gen = -1, ud_port = 0;
+  float ud_w = 0.0f, ud_delay = 0.0f;
+  unsigned long long ud_stream0 = 0;
   // CreatePoissonGenerator nodes
   float poisson_lambda = 0.0f;
   // per-block RK5 derivative evaluation counters
   unsigned long long *d_blk_evals = nullptr;
   int n_blocks = 0;
+  // autotuned RK5 kernel variant and the timings it was chosen from
+  int rk5_variant = 0;
+  bool tuned = false;
+  float tune_ms[4] = {0, 0, 0, 0};
 
   int ScalVarIdx(const std::string &n) const;
   int PortVarIdx(const std::string &n) const;
@@ -283,6 +292,9 @@ class NeuronGPU {
   // per-kernel-class device timing (CUDA events around every launch)
   int SetKernelTiming(int on);
   int GetKernelTiming(int kind, double *total_ms, long long *launches);
+  // RK5 kernel variant chosen for the group of i_node and its timings
+  int GetRk5Tuning(int i_node, int *variant, float *ms4);
+  void TuneRk5(NodeGroup *g);
   int SetGraphChunk(int g) { graph_chunk_ = g > 0 ? g : 1; InvalidateGraphs(); return 0; }
   long long NNodes() { return (long long)node_group_map_.size(); }
   long long NConnections() { return (long long)e_src_.size(); }
@@ -360,9 +372,12 @@ class NeuronGPU {
   std::vector<int> gen_nodes_;        // generator index -> node
   float *d_gen_rate_ = nullptr, *d_gen_origin_ = nullptr;
   float *d_gen_start_ = nullptr, *d_gen_stop_ = nullptr;
-  double *d_gen_lambda_ = nullptr, *d_gen_explam_ = nullptr;
+  double *d_gen_lambda_ = nullptr, *d_gen_explam_ = nullptr, *d_gen_cdf_ = nullptr;
+  std::vector<float> gen_origin_h_, gen_start_h_, gen_stop_h_;
+  std::vector<double> gen_lam_h_, gen_explam_h_;
   // delivery counters
   unsigned long long *d_blk_events_ = nullptr;
+  unsigned *d_done_ = nullptr;
   int deliver_blocks_ = 0;
   // recording
   RecCol *d_rec_cols_ = nullptr;

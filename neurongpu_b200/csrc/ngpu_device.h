@@ -85,8 +85,25 @@ struct InputArgs {
   const float *gen_stop;
   const double *gen_lambda;     // rate*dt/1000 as the reference computes it
   const double *gen_explam;     // exp(-lambda)
+  const double *gen_cdf;        // [gen * NGPU_CDF_LEN + k] Poisson CDF F(k)
   unsigned long long seed;
+  int dry;                      // timing run: leave the accumulators as they are
+  // Uniform drive: every node of the group has exactly one direct connection,
+  // all from generator ud_gen with the same port, weight and delay and with
+  // consecutive random streams ud_stream0 + i. The per-node connection
+  // arrays are then not read at all.
+  int ud;
+  int ud_port;
+  float ud_w, ud_delay, ud_origin, ud_start, ud_stop;
+  double ud_lambda, ud_explam;
+  const double *ud_cdf;
+  unsigned long long ud_stream0;
 };
+
+// Poisson CDF table entries per generator: F(0..200), built on the host by
+// the recurrence of ng_poisson_inversion so that searching it returns the
+// same counts as the sequential-search sampler
+#define NGPU_CDF_LEN 201
 
 struct GroupArgs {
   int n;                        // nodes
@@ -99,6 +116,10 @@ struct GroupArgs {
   float *dx;                    // RK5 time offset
   unsigned pmask[NGPU_MAX_PARAM / 32];  // bit j: param j read per neuron
   float puni[NGPU_MAX_PARAM];   // uniform parameter values
+  float pinv[NGPU_MAX_PARAM];   // 1 / puni[j] (IEEE division on the host)
+  int all_uniform;              // every parameter but refractory_step uniform
+  int variant;                  // RK5 kernel variant (occupancy target)
+  int dry;                      // timing run: compute everything, store nothing
   float h_min;
   float dt;                     // time resolution (ms)
   float eps;                    // RK5 tolerance
@@ -137,6 +158,11 @@ struct DeliverArgs {
   const unsigned *rev_edge;
   float dt;
   unsigned long long *blk_events;      // per-block delivered events
+  // step bookkeeping done by the last block of the step's last kernel:
+  // bit 0 advance the step, bit 1 advance the recording row
+  int advance_flags;
+  int *ring_cnt_w;
+  unsigned *done;                      // blocks finished (reset by the last)
 };
 
 }  // namespace ngpu

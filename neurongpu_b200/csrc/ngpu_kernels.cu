@@ -76,11 +76,37 @@ __device__ __forceinline__ void input_sum(const InputArgs &in, int i,
     if (q < np) {
       long long *a = in.acc + in.acc_base + (long long)q * n_pad + i;
       long long v = *a;
-      if (v != 0) *a = 0;
+      if (v != 0 && !in.dry) *a = 0;
       s[q] = v;
     }
   }
-  if (pending && in.dc_off != nullptr) {
+  if (pending && in.ud) {
+    const double t = t0 + (double)dt * (double)it;
+    const double t_rel = t - (double)in.ud_origin - (double)in.ud_delay;
+    if (t_rel >= (double)in.ud_start && t_rel <= (double)in.ud_stop) {
+      const double lam = in.ud_lambda;
+      unsigned n;
+      if (lam < NGPU_POISSON_INV_MAX) {
+        Philox4 r = ng_random_block(in.seed, RNG_TAG_POISSON_DIRECT,
+                                    in.ud_stream0 + (unsigned long long)i, T0 + it, 0);
+        const double u = ng_u01(r.v[0], r.v[1]);
+        n = 0;
+        if (lam > 0.0) {
+          while (n < NGPU_CDF_LEN - 1 && u > in.ud_cdf[n]) n++;
+        }
+      } else {
+        n = ng_poisson(lam, in.ud_explam, in.seed, RNG_TAG_POISSON_DIRECT,
+                       in.ud_stream0 + (unsigned long long)i, T0 + it);
+      }
+      if (n > 0) {
+        const long long v = ng_to_fixed(in.ud_w * (float)n);
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+          if (q == in.ud_port) s[q] += v;
+        }
+      }
+    }
+  } else if (pending && in.dc_off != nullptr) {
     unsigned b = in.dc_off[i], e = in.dc_off[i + 1];
     if (b < e) {
       // time of the step whose draws are pending (neural_time_ of that step)
@@ -91,9 +117,23 @@ __device__ __forceinline__ void input_sum(const InputArgs &in, int i,
         double t_rel = t - (double)in.gen_origin[gen] - (double)in.dc_delay[c];
         if (t_rel >= (double)in.gen_start[gen] &&
             t_rel <= (double)in.gen_stop[gen]) {
-          unsigned n = ng_poisson(in.gen_lambda[gen], in.gen_explam[gen],
-                                  in.seed, RNG_TAG_POISSON_DIRECT,
-                                  in.dc_stream[c], T_prev);
+          const double lam = in.gen_lambda[gen];
+          unsigned n;
+          if (lam < NGPU_POISSON_INV_MAX) {
+            // inversion against the host-built CDF table: the same counts as
+            // ng_poisson_inversion, without device double divisions
+            Philox4 r = ng_random_block(in.seed, RNG_TAG_POISSON_DIRECT,
+                                        in.dc_stream[c], T_prev, 0);
+            const double u = ng_u01(r.v[0], r.v[1]);
+            const double *cdf = in.gen_cdf + (size_t)gen * NGPU_CDF_LEN;
+            n = 0;
+            if (lam > 0.0) {
+              while (n < NGPU_CDF_LEN - 1 && u > cdf[n]) n++;
+            }
+          } else {
+            n = ng_poisson(lam, in.gen_explam[gen], in.seed,
+                           RNG_TAG_POISSON_DIRECT, in.dc_stream[c], T_prev);
+          }
           if (n > 0) {
             long long v = ng_to_fixed(in.dc_weight[c] * (float)n);
             int port = in.dc_port[c];
@@ -115,15 +155,21 @@ __device__ __forceinline__ float fold_value(float var, long long s, float w) {
 // ---------------------------------------------------------------------------
 // RK5 (Cash-Karp) step and update, following src/rk5.h:57-162
 // ---------------------------------------------------------------------------
+// err^e for err > 0 with e = -0.2 or -0.25 (step-size controller)
+__device__ __forceinline__ float ctrl_pow(float err, float e) {
+  return exp2f(e * log2f(err));
+}
+
 template <class M, int NP>
 __device__ __forceinline__ void rk5_step(double &x, float *y, float &h,
                                          float h_min, float h_max,
-                                         const float *p, int np, float eps,
+                                         const float *p, const float *q,
+                                         float refr, int np, float eps,
                                          unsigned &evals) {
   using namespace rk5c;
   constexpr int NV = M::NVAR;
   float k1[NV], k2[NV], k3[NV], k4[NV], k5[NV], k6[NV], yn[NV], ys[NV];
-  M::deriv(y, k1, p, np);
+  M::deriv(y, k1, p, q, refr, np);
   evals++;
 #pragma unroll
   for (int i = 0; i < NV; i++) ys[i] = fabsf(y[i]) + fabsf(k1[i] * h) + scal_min;
@@ -133,24 +179,24 @@ __device__ __forceinline__ void rk5_step(double &x, float *y, float &h,
     if (h < h_min) h = h_min;
 #pragma unroll
     for (int i = 0; i < NV; i++) yn[i] = y[i] + h * a21 * k1[i];
-    M::deriv(yn, k2, p, np);
+    M::deriv(yn, k2, p, q, refr, np);
 #pragma unroll
     for (int i = 0; i < NV; i++) yn[i] = y[i] + h * (a31 * k1[i] + a32 * k2[i]);
-    M::deriv(yn, k3, p, np);
+    M::deriv(yn, k3, p, q, refr, np);
 #pragma unroll
     for (int i = 0; i < NV; i++)
       yn[i] = y[i] + h * (a41 * k1[i] + a42 * k2[i] + a43 * k3[i]);
-    M::deriv(yn, k4, p, np);
+    M::deriv(yn, k4, p, q, refr, np);
 #pragma unroll
     for (int i = 0; i < NV; i++)
       yn[i] = y[i] + h * (a51 * k1[i] + a52 * k2[i] + a53 * k3[i]
                           + a54 * k4[i]);
-    M::deriv(yn, k5, p, np);
+    M::deriv(yn, k5, p, q, refr, np);
 #pragma unroll
     for (int i = 0; i < NV; i++)
       yn[i] = y[i] + h * (a61 * k1[i] + a62 * k2[i] + a63 * k3[i]
                           + a64 * k4[i] + a65 * k5[i]);
-    M::deriv(yn, k6, p, np);
+    M::deriv(yn, k6, p, q, refr, np);
 #pragma unroll
     for (int i = 0; i < NV; i++)
       yn[i] = y[i] + h * (a71 * k1[i] + a73 * k3[i] + a74 * k4[i]
@@ -168,13 +214,13 @@ __device__ __forceinline__ void rk5_step(double &x, float *y, float &h,
     err /= eps;
     if (err <= 1.0f || (double)h <= (double)h_min * (1.0 + 1.0e-5)) break;
     if (guard >= 256) break;
-    float h_new = h * coeff * powf(err, exp_dec);
+    float h_new = h * coeff * ctrl_pow(err, exp_dec);
     double h01 = 0.1 * (double)h;
     h = (float)(((double)h_new > h01) ? (double)h_new : h01);
   }
   x += h;
   if (err > err_min) {
-    h = h * coeff * powf(err, exp_inc);
+    h = h * coeff * ctrl_pow(err, exp_inc);
   } else {
     h = (float)(5.0 * (double)h);
   }
@@ -214,9 +260,14 @@ __device__ __forceinline__ void block_add_u64(unsigned long long v,
   }
 }
 
-template <class M, int NP>
-__global__ void __launch_bounds__(NGPU_BLOCK)
-k_rk5_update(GroupArgs g, InputArgs in, PushArgs pa, StepCtx *ctx) {
+// One thread per neuron. UNI: every parameter except the refractory
+// counter is group-uniform, so p and its reciprocals q are read from the
+// constant kernel-parameter block (no per-neuron loads, no registers);
+// otherwise they are loaded per neuron and q is formed in registers.
+template <class M, int NP, bool UNI, int MINB>
+__global__ void __launch_bounds__(NGPU_BLOCK, MINB)
+k_rk5_update(const __grid_constant__ GroupArgs g, const __grid_constant__ InputArgs in,
+             const __grid_constant__ PushArgs pa, StepCtx *ctx) {
   using Tr = ModelTraits<M>;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned evals = 0;
@@ -228,35 +279,39 @@ k_rk5_update(GroupArgs g, InputArgs in, PushArgs pa, StepCtx *ctx) {
     const int pending = ctx->poisson_pending;
     const int n_pad = g.n_pad;
     float y[M::NVAR];
-    float p[M::NPARAM];
 #pragma unroll
     for (int j = 0; j < M::NVAR; j++) {
       y[j] = (j < g.nvar) ? g.var[(long long)j * n_pad + i] : 0.0f;
     }
+    float p_loc[UNI ? 1 : M::NPARAM];
+    float q_loc[UNI ? 1 : M::NPARAM];
+    if (!UNI) {
 #pragma unroll
-    for (int j = 0; j < M::NPARAM; j++) {
-      if (j < g.nparam) {
-        p[j] = pbit(g.pmask, j) ? g.param[(long long)j * n_pad + i] : g.puni[j];
-      } else {
-        p[j] = 1.0f;
+      for (int j = 0; j < (UNI ? 1 : M::NPARAM); j++) {
+        if (j < g.nparam) {
+          p_loc[j] = pbit(g.pmask, j) ? g.param[(long long)j * n_pad + i] : g.puni[j];
+        } else {
+          p_loc[j] = 1.0f;
+        }
+        q_loc[j] = 1.0f / p_loc[j];
       }
     }
+    const float *p = UNI ? g.puni : p_loc;
+    const float *q = UNI ? g.pinv : q_loc;
+    float refr = g.param[(long long)Tr::refr * n_pad + i];
     // fold the previous step's input
     constexpr int NPI = (M::NPV == 0) ? 1 : NP;
     long long s[NPI];
     input_sum<NPI>(in, i, n_pad, np, it, t0, g.dt, pending, T0, s);
 #pragma unroll
-    for (int q = 0; q < NPI; q++) {
-      if (q < np && s[q] != 0) {
-        constexpr int dummy = 0;
-        (void)dummy;
-        const int vi = Tr::in_base + q * Tr::in_step;
-        const float w = (Tr::w_base >= 0) ? p[Tr::w_base + q * Tr::w_step]
-                                          : 1.0f;
-        y[vi] = fold_value(y[vi], s[q], w);
+    for (int qq = 0; qq < NPI; qq++) {
+      if (qq < np && s[qq] != 0) {
+        const int vi = Tr::in_base + qq * Tr::in_step;
+        const float w = (Tr::w_base >= 0) ? p[Tr::w_base + qq * Tr::w_step] : 1.0f;
+        y[vi] = fold_value(y[vi], s[qq], w);
       }
     }
-    const float refr0 = p[Tr::refr];
+    const float refr0 = refr;
     const double x1 = t0 + (double)g.dt * (double)(it + 1);
     double x = t0 + (double)g.dt * (double)it + (double)g.dx[i];
     float h = g.h[i];
@@ -267,43 +322,70 @@ k_rk5_update(GroupArgs g, InputArgs in, PushArgs pa, StepCtx *ctx) {
     int guard = 0;
     while (!end_step) {
       float hmax = (float)(x1 - x);
-      rk5_step<M, NP>(x, y, h, h_min, hmax, p, np, g.eps, evals);
+      rk5_step<M, NP>(x, y, h, h_min, hmax, p, q, refr, np, g.eps, evals);
       end_step = (x >= x1 - (double)h_min);
-      if (M::external(y, p, end_step, g.dt)) {
-        push_spike(pa, ctx, g.i_node_0 + i, i, 1.0f, T, x1, den);
+      if (M::external(y, p, refr, end_step, g.dt)) {
+        if (!g.dry) push_spike(pa, ctx, g.i_node_0 + i, i, 1.0f, T, x1, den);
       }
       if (++guard > NGPU_RK5_MAX_SUBSTEPS) {
         atomicOr(&ctx->err, (unsigned)DERR_RK5_STUCK);
         break;
       }
     }
+    if (!g.dry) {
 #pragma unroll
-    for (int j = 0; j < M::NVAR; j++) {
-      if (j < g.nvar) g.var[(long long)j * n_pad + i] = y[j];
+      for (int j = 0; j < M::NVAR; j++) {
+        if (j < g.nvar) g.var[(long long)j * n_pad + i] = y[j];
+      }
+      g.h[i] = h;
+      g.dx[i] = (float)(x - x1);
+      if (refr != refr0) g.param[(long long)Tr::refr * n_pad + i] = refr;
+    } else if (y[0] == 1.2345e30f) {
+      // keeps the dry run from being optimised away; never true in practice
+      g.h[i] = h + (float)x;
     }
-    g.h[i] = h;
-    g.dx[i] = (float)(x - x1);
-    if (p[Tr::refr] != refr0) g.param[(long long)Tr::refr * n_pad + i] = p[Tr::refr];
   }
   if (g.blk_evals != nullptr) block_add_u64(evals, g.blk_evals);
 }
+
+template <class M, int NP>
+static void launch_rk5(const GroupArgs &g, const InputArgs &in, const PushArgs &pa,
+                       StepCtx *ctx, cudaStream_t s) {
+  dim3 grid((g.n + NGPU_BLOCK - 1) / NGPU_BLOCK), block(NGPU_BLOCK);
+  if (g.all_uniform) {
+    if constexpr (NP <= 4) {
+      // occupancy variants chosen by the autotuner (register cap per thread)
+      switch (g.variant) {
+        case 1: k_rk5_update<M, NP, true, 5><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+        case 2: k_rk5_update<M, NP, true, 6><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+        case 3: k_rk5_update<M, NP, true, 8><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+        default: k_rk5_update<M, NP, true, 1><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+      }
+    } else {
+      k_rk5_update<M, NP, true, 1><<<grid, block, 0, s>>>(g, in, pa, ctx);
+    }
+  } else {
+    k_rk5_update<M, NP, false, 1><<<grid, block, 0, s>>>(g, in, pa, ctx);
+  }
+}
+
+int Rk5VariantCount(int np, int all_uniform) { return (all_uniform && np <= 4) ? 4 : 1; }
 
 template <template <int> class MT>
 static void launch_rk5_model(int np, const GroupArgs &g, const InputArgs &in,
                              const PushArgs &pa, StepCtx *ctx,
                              cudaStream_t s) {
-  dim3 grid((g.n + NGPU_BLOCK - 1) / NGPU_BLOCK), block(NGPU_BLOCK);
   switch (np) {
     case 0:
-    case 1: k_rk5_update<MT<1>, 1><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
-    case 2: k_rk5_update<MT<2>, 2><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
-    case 3: k_rk5_update<MT<3>, 3><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
-    case 4: k_rk5_update<MT<4>, 4><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+    case 1: launch_rk5<MT<1>, 1>(g, in, pa, ctx, s); break;
+    case 2: launch_rk5<MT<2>, 2>(g, in, pa, ctx, s); break;
+    case 3: launch_rk5<MT<3>, 3>(g, in, pa, ctx, s); break;
+    case 4: launch_rk5<MT<4>, 4>(g, in, pa, ctx, s); break;
     default:
       if (np <= 8) {
-        k_rk5_update<MT<8>, 8><<<grid, block, 0, s>>>(g, in, pa, ctx);
+        launch_rk5<MT<8>, 8>(g, in, pa, ctx, s);
       } else {
-        k_rk5_update<MT<20>, 20><<<grid, block, 0, s>>>(g, in, pa, ctx);
+        launch_rk5<MT<20>, 20>(g, in, pa, ctx, s);
       }
   }
 }
@@ -321,11 +403,9 @@ void LaunchRk5Update(int model, int np, const GroupArgs &g,
       launch_rk5_model<AeifPscAlpha>(np, g, in, pa, ctx, s); break;
     case RK5_AEIF_PSC_EXP:
       launch_rk5_model<AeifPscExp>(np, g, in, pa, ctx, s); break;
-    case RK5_AEIF_PSC_DELTA: {
-      dim3 grid((g.n + NGPU_BLOCK - 1) / NGPU_BLOCK), block(NGPU_BLOCK);
-      k_rk5_update<AeifPscDelta<1>, 1><<<grid, block, 0, s>>>(g, in, pa, ctx);
+    case RK5_AEIF_PSC_DELTA:
+      launch_rk5<AeifPscDelta<1>, 1>(g, in, pa, ctx, s);
       break;
-    }
     case RK5_IZHIKEVICH_COND_BETA:
       launch_rk5_model<IzhCondBeta>(np, g, in, pa, ctx, s); break;
     default: break;
@@ -579,6 +659,33 @@ __device__ __forceinline__ float syn_update(const SynGroupTable &syn, int sg,
   return w;
 }
 
+// Step bookkeeping fused into the step's last kernel: the last block to
+// finish counts the step's spikes, clears the next ring slot and advances the
+// step (and recording row). Every other block has read the step index and
+// finished by then, so nothing reads the context while it changes.
+__device__ __forceinline__ void finish_step(const DeliverArgs &d, StepCtx *ctx) {
+  if (d.advance_flags == 0) return;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned prev = atomicAdd(d.done, 1u);
+    if (prev == gridDim.x - 1) {
+      __threadfence();
+      if (d.advance_flags & 1) {
+        const long long T = ctx->T0 + ctx->it + 1;
+        int c = d.ring_cnt_w[(int)(T % d.ring_R)];
+        ctx->n_spikes += (unsigned long long)(c < d.ring_C ? c : d.ring_C);
+        d.ring_cnt_w[(int)((T + 1) % d.ring_R)] = 0;
+        ctx->it += 1;
+        ctx->poisson_pending = 1;
+      }
+      if (d.advance_flags & 2) ctx->rec_row += 1;
+      *d.done = 0u;
+      __threadfence();
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // synaptic delivery: one warp per (spike, delay) group
 // ---------------------------------------------------------------------------
@@ -587,49 +694,100 @@ k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
   __shared__ int s_pref[NGPU_MAX_DELAYS + 1];
   __shared__ int s_slot[NGPU_MAX_DELAYS];
   const long long T = ctx->T0 + ctx->it + 1;
-  for (int di = threadIdx.x; di < d.nd; di += blockDim.x) {
-    int slot = (int)((T - d.delays[di]) % d.ring_R);
-    if (slot < 0) slot += d.ring_R;
-    s_slot[di] = slot;
-    int c = d.ring_cnt[slot];
-    s_pref[di + 1] = c < d.ring_C ? c : d.ring_C;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    s_pref[0] = 0;
-    for (int di = 0; di < d.nd; di++) s_pref[di + 1] += s_pref[di];
-  }
-  __syncthreads();
-  const int total = s_pref[d.nd];
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int n_warps = (gridDim.x * blockDim.x) >> 5;
+  const bool warp_scan = d.nd <= 32;
+  // per-delay spike counts and their prefix: in registers of every warp when
+  // there are at most 32 distinct delays, else in shared memory
+  int my_slot = 0, my_incl = 0, total;
+  if (warp_scan) {
+    int c = 0;
+    if (lane < d.nd) {
+      int slot = (int)((T - d.delays[lane]) % d.ring_R);
+      if (slot < 0) slot += d.ring_R;
+      my_slot = slot;
+      c = d.ring_cnt[slot];
+      c = c < d.ring_C ? c : d.ring_C;
+    }
+    my_incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int v = __shfl_up_sync(0xffffffffu, my_incl, o);
+      if (lane >= o) my_incl += v;
+    }
+    total = __shfl_sync(0xffffffffu, my_incl, 31);
+  } else {
+    for (int di = threadIdx.x; di < d.nd; di += blockDim.x) {
+      int slot = (int)((T - d.delays[di]) % d.ring_R);
+      if (slot < 0) slot += d.ring_R;
+      s_slot[di] = slot;
+      int c = d.ring_cnt[slot];
+      s_pref[di + 1] = c < d.ring_C ? c : d.ring_C;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_pref[0] = 0;
+      for (int di = 0; di < d.nd; di++) s_pref[di + 1] += s_pref[di];
+    }
+    __syncthreads();
+    total = s_pref[d.nd];
+  }
   unsigned long long events = 0;
   for (int item = warp; item < total; item += n_warps) {
-    int lo = 0, hi = d.nd;          // find di with s_pref[di] <= item
-    while (hi - lo > 1) {
-      int mid = (lo + hi) >> 1;
-      if (s_pref[mid] <= item) lo = mid; else hi = mid;
+    int di, slot, base;
+    if (warp_scan) {
+      // first delay whose inclusive prefix exceeds the item
+      // (item < total, so some lane's inclusive prefix exceeds it)
+      unsigned m = __ballot_sync(0xffffffffu, my_incl > item);
+      di = __ffs(m) - 1;
+      slot = __shfl_sync(0xffffffffu, my_slot, di);
+      const int prev = __shfl_sync(0xffffffffu, my_incl, di > 0 ? di - 1 : 0);
+      base = di > 0 ? prev : 0;
+    } else {
+      int lo = 0, hi = d.nd;          // find di with s_pref[di] <= item
+      while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (s_pref[mid] <= item) lo = mid; else hi = mid;
+      }
+      di = lo;
+      slot = s_slot[di];
+      base = s_pref[di];
     }
-    const int di = lo;
-    const long long k = (long long)s_slot[di] * d.ring_C + (item - s_pref[di]);
+    const long long k = (long long)slot * d.ring_C + (item - base);
     const unsigned src = d.ring_src[k];
     const float height = d.ring_h[k];
     const unsigned long long gi = (unsigned long long)src * d.nd + di;
     const unsigned long long beg = d.grp_off[gi], end = d.grp_off[gi + 1];
     if (lane == 0) events += end - beg;
     if (d.e_syn == nullptr) {
-      for (unsigned long long e = beg + lane; e < end; e += 32) {
-        const unsigned slot = d.e_slot[e];
-        const float w = d.e_w[e];
-        atomicAdd((unsigned long long *)(d.acc + slot),
-                  (unsigned long long)ng_to_fixed(height * w));
+      // four edges per lane in flight; edges are read once per spike, so
+      // they are loaded with the streaming (evict-first) hint
+      for (unsigned long long e0 = beg + lane; e0 < end; e0 += 128) {
+        unsigned sl[4];
+        float wv[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const unsigned long long e = e0 + 32 * u;
+          if (e < end) {
+            sl[u] = __ldcs(d.e_slot + e);
+            wv[u] = __ldcs(d.e_w + e);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const unsigned long long e = e0 + 32 * u;
+          if (e < end) {
+            atomicAdd((unsigned long long *)(d.acc + sl[u]),
+                      (unsigned long long)ng_to_fixed(height * wv[u]));
+          }
+        }
       }
     } else {
       for (unsigned long long e = beg + lane; e < end; e += 32) {
-        const unsigned slot = d.e_slot[e];
+        const unsigned slot_t = d.e_slot[e];
         const float w = d.e_w[e];
-        atomicAdd((unsigned long long *)(d.acc + slot),
+        atomicAdd((unsigned long long *)(d.acc + slot_t),
                   (unsigned long long)ng_to_fixed(height * w));
         const int sg = d.e_syn[e];
         if (sg > 0) {
@@ -655,6 +813,14 @@ k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
       d.blk_events[blockIdx.x] += t;
     }
   }
+  finish_step(d, ctx);
+}
+
+int DeliverBlocksPerSM() {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_deliver, 256, 0) != cudaSuccess)
+    return 4;
+  return nb > 0 ? nb : 1;
 }
 
 void LaunchDeliver(const DeliverArgs &d, const SynGroupTable &syn,
@@ -693,6 +859,7 @@ k_stdp_post(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
       }
     }
   }
+  finish_step(d, ctx);
 }
 
 void LaunchStdpPost(const DeliverArgs &d, const SynGroupTable &syn,

@@ -16,6 +16,8 @@ struct RecCol {
 void LaunchRk5Update(int model, int np, const GroupArgs &g,
                      const InputArgs &in, const PushArgs &pa,
                      StepCtx *ctx, cudaStream_t s);
+// number of RK5 kernel variants (GroupArgs::variant) for a group
+int Rk5VariantCount(int np, int all_uniform);
 void LaunchIafPscExpUpdate(const GroupArgs &g, const InputArgs &in,
                            const PushArgs &pa, StepCtx *ctx, cudaStream_t s);
 void LaunchSpikeGeneratorUpdate(const GroupArgs &g, const PushArgs &pa,
@@ -36,6 +38,8 @@ void LaunchClearPending(StepCtx *ctx, cudaStream_t s);
 // synaptic delivery and plasticity
 void LaunchDeliver(const DeliverArgs &d, const SynGroupTable &syn,
                    StepCtx *ctx, int n_blocks, cudaStream_t s);
+// resident 256-thread delivery blocks per SM (grid = SMs x this)
+int DeliverBlocksPerSM();
 void LaunchStdpPost(const DeliverArgs &d, const SynGroupTable &syn,
                     StepCtx *ctx, int n_blocks, cudaStream_t s);
 

@@ -2,11 +2,19 @@
 //
 // Each model exposes, for a compile-time port bound NP and a runtime port
 // count np <= NP:
-//   deriv(y, dydx, p, np)        -- the model ODE
-//   external(y, p, end, dt)      -- post-substep update; returns the number
-//                                   of spikes emitted (0 or 1)
-// Index layout of y and p (scalar entries first, then per-port blocks) is
-// the reference's, e.g. src/aeif_cond_beta_kernel.h:30-72.
+//   deriv(y, dydx, p, q, refr, np) -- the model ODE
+//   external(y, p, refr, end, dt)  -- post-substep update; returns 1 when the
+//                                     neuron spiked
+// p[j] is parameter j and q[j] its reciprocal 1/p[j]; both point either into
+// the kernel's constant parameter block (group-uniform parameters) or to
+// per-neuron register arrays. Divisions by parameters are written as
+// multiplications by q[j], which the caller computes once per step (or the
+// host once per launch) instead of once per right-hand-side evaluation.
+// refr is the neuron's refractory counter (the reference keeps it in the
+// parameter array as "refractory_step").
+// Index layout of y and p (scalar entries first, then per-port blocks) is the
+// reference's, e.g. src/aeif_cond_beta_kernel.h:30-72; the equations follow
+// src/aeif_cond_beta_kernel.h:153-214 and the other *_kernel.h files.
 #pragma once
 #include <math.h>
 
@@ -47,8 +55,8 @@ enum AeifScal {
   A_V_peak, A_V_reset, A_t_ref, A_refr, A_den_delay, A_NSP
 };
 
-__device__ __forceinline__ int aeif_external(float *y, float *p, bool end,
-                                             float dt) {
+__device__ __forceinline__ int aeif_external(float *y, const float *p,
+                                             float &refr, bool end, float dt) {
   float &V_m = y[0];
   float &w = y[1];
   if (V_m < -1.0e3f) {           // numerical instability guard
@@ -61,19 +69,36 @@ __device__ __forceinline__ int aeif_external(float *y, float *p, bool end,
     w = 0.0f;
     return 0;
   }
-  if (p[A_refr] > 0.0f) {
+  if (refr > 0.0f) {
     V_m = p[A_V_reset];
-    if (end) p[A_refr] -= 1.0f;
+    if (end) refr -= 1.0f;
     return 0;
   }
   if (V_m >= p[A_V_peak]) {
     V_m = p[A_V_reset];
     w += p[A_b];
     float r = (float)(int)roundf(p[A_t_ref] / dt);
-    p[A_refr] = r < 0.0f ? 0.0f : r;
+    refr = r < 0.0f ? 0.0f : r;
     return 1;
   }
   return 0;
+}
+
+// membrane and adaptation derivatives shared by the AdEx models
+__device__ __forceinline__ void aeif_vw(const float *y, float *dydx,
+                                        const float *p, const float *q,
+                                        float refr, float V, float I_in,
+                                        bool exp_guard) {
+  float V_spike;
+  if (exp_guard && p[A_Delta_T] == 0.0f) {
+    V_spike = 0.0f;
+  } else {
+    V_spike = p[A_Delta_T] * expf((V - p[A_V_th]) * q[A_Delta_T]);
+  }
+  dydx[0] = (refr > 0.0f) ? 0.0f
+      : (-p[A_g_L] * (V - p[A_E_L] - V_spike) + I_in - y[1] + p[A_I_e])
+        * q[A_C_m];
+  dydx[1] = (p[A_a] * (V - p[A_E_L]) - y[1]) * q[A_tau_w];
 }
 
 template <int NP>
@@ -81,31 +106,28 @@ struct AeifCondBeta {
   enum { NSV = 2, NPV = 2, NSP = A_NSP, NPP = 4,
          NVAR = NSV + NPV * NP, NPARAM = NSP + NPP * NP };
   __device__ __forceinline__ static void deriv(const float *y, float *dydx,
-                                               const float *p, int np) {
-    float refr = p[A_refr];
+                                               const float *p, const float *q,
+                                               float refr, int np) {
     float V = (refr > 0.0f) ? p[A_V_reset] : fminf(y[0], p[A_V_peak]);
     float I_syn = 0.0f;
 #pragma unroll
     for (int i = 0; i < NP; i++) {
       if (i < np) I_syn += y[NSV + NPV * i] * (p[NSP + NPP * i] - V);
     }
-    float V_spike = p[A_Delta_T] * expf((V - p[A_V_th]) / p[A_Delta_T]);
-    dydx[0] = (refr > 0.0f) ? 0.0f
-        : (-p[A_g_L] * (V - p[A_E_L] - V_spike) + I_syn - y[1] + p[A_I_e])
-          / p[A_C_m];
-    dydx[1] = (p[A_a] * (V - p[A_E_L]) - y[1]) / p[A_tau_w];
+    aeif_vw(y, dydx, p, q, refr, V, I_syn, false);
 #pragma unroll
     for (int i = 0; i < NP; i++) {
       if (i < np) {
         float g = y[NSV + NPV * i], g1 = y[NSV + NPV * i + 1];
-        dydx[NSV + NPV * i + 1] = -g1 / p[NSP + NPP * i + 1];
-        dydx[NSV + NPV * i] = g1 - g / p[NSP + NPP * i + 2];
+        dydx[NSV + NPV * i + 1] = -g1 * q[NSP + NPP * i + 1];
+        dydx[NSV + NPV * i] = g1 - g * q[NSP + NPP * i + 2];
       }
     }
   }
-  __device__ __forceinline__ static int external(float *y, float *p, bool end,
+  __device__ __forceinline__ static int external(float *y, const float *p,
+                                                 float &refr, bool end,
                                                  float dt) {
-    return aeif_external(y, p, end, dt);
+    return aeif_external(y, p, refr, end, dt);
   }
 };
 
@@ -114,32 +136,29 @@ struct AeifCondAlpha {
   enum { NSV = 2, NPV = 2, NSP = A_NSP, NPP = 3,
          NVAR = NSV + NPV * NP, NPARAM = NSP + NPP * NP };
   __device__ __forceinline__ static void deriv(const float *y, float *dydx,
-                                               const float *p, int np) {
-    float refr = p[A_refr];
+                                               const float *p, const float *q,
+                                               float refr, int np) {
     float V = (refr > 0.0f) ? p[A_V_reset] : fminf(y[0], p[A_V_peak]);
     float I_syn = 0.0f;
 #pragma unroll
     for (int i = 0; i < NP; i++) {
       if (i < np) I_syn += y[NSV + NPV * i] * (p[NSP + NPP * i] - V);
     }
-    float V_spike = p[A_Delta_T] * expf((V - p[A_V_th]) / p[A_Delta_T]);
-    dydx[0] = (refr > 0.0f) ? 0.0f
-        : (-p[A_g_L] * (V - p[A_E_L] - V_spike) + I_syn - y[1] + p[A_I_e])
-          / p[A_C_m];
-    dydx[1] = (p[A_a] * (V - p[A_E_L]) - y[1]) / p[A_tau_w];
+    aeif_vw(y, dydx, p, q, refr, V, I_syn, false);
 #pragma unroll
     for (int i = 0; i < NP; i++) {
       if (i < np) {
         float g = y[NSV + NPV * i], g1 = y[NSV + NPV * i + 1];
-        float tau = p[NSP + NPP * i + 1];
-        dydx[NSV + NPV * i + 1] = -g1 / tau;
-        dydx[NSV + NPV * i] = g1 - g / tau;
+        float itau = q[NSP + NPP * i + 1];
+        dydx[NSV + NPV * i + 1] = -g1 * itau;
+        dydx[NSV + NPV * i] = g1 - g * itau;
       }
     }
   }
-  __device__ __forceinline__ static int external(float *y, float *p, bool end,
+  __device__ __forceinline__ static int external(float *y, const float *p,
+                                                 float &refr, bool end,
                                                  float dt) {
-    return aeif_external(y, p, end, dt);
+    return aeif_external(y, p, refr, end, dt);
   }
 };
 
@@ -148,33 +167,29 @@ struct AeifPscAlpha {
   enum { NSV = 2, NPV = 2, NSP = A_NSP, NPP = 2,
          NVAR = NSV + NPV * NP, NPARAM = NSP + NPP * NP };
   __device__ __forceinline__ static void deriv(const float *y, float *dydx,
-                                               const float *p, int np) {
-    float refr = p[A_refr];
+                                               const float *p, const float *q,
+                                               float refr, int np) {
     float V = (refr > 0.0f) ? p[A_V_reset] : fminf(y[0], p[A_V_peak]);
     float I_tot = 0.0f;
 #pragma unroll
     for (int i = 0; i < NP; i++) {
       if (i < np) I_tot += y[NSV + NPV * i];
     }
-    float V_spike = p[A_Delta_T] == 0.0f ? 0.0f
-        : p[A_Delta_T] * expf((V - p[A_V_th]) / p[A_Delta_T]);
-    dydx[0] = (refr > 0.0f) ? 0.0f
-        : (-p[A_g_L] * (V - p[A_E_L] - V_spike) + I_tot - y[1] + p[A_I_e])
-          / p[A_C_m];
-    dydx[1] = (p[A_a] * (V - p[A_E_L]) - y[1]) / p[A_tau_w];
+    aeif_vw(y, dydx, p, q, refr, V, I_tot, true);
 #pragma unroll
     for (int i = 0; i < NP; i++) {
       if (i < np) {
         float I = y[NSV + NPV * i], I1 = y[NSV + NPV * i + 1];
-        float tau = p[NSP + NPP * i];
-        dydx[NSV + NPV * i + 1] = -I1 / tau;
-        dydx[NSV + NPV * i] = I1 - I / tau;
+        float itau = q[NSP + NPP * i];
+        dydx[NSV + NPV * i + 1] = -I1 * itau;
+        dydx[NSV + NPV * i] = I1 - I * itau;
       }
     }
   }
-  __device__ __forceinline__ static int external(float *y, float *p, bool end,
+  __device__ __forceinline__ static int external(float *y, const float *p,
+                                                 float &refr, bool end,
                                                  float dt) {
-    return aeif_external(y, p, end, dt);
+    return aeif_external(y, p, refr, end, dt);
   }
 };
 
@@ -183,28 +198,24 @@ struct AeifPscExp {
   enum { NSV = 2, NPV = 1, NSP = A_NSP, NPP = 1,
          NVAR = NSV + NPV * NP, NPARAM = NSP + NPP * NP };
   __device__ __forceinline__ static void deriv(const float *y, float *dydx,
-                                               const float *p, int np) {
-    float refr = p[A_refr];
+                                               const float *p, const float *q,
+                                               float refr, int np) {
     float V = (refr > 0.0f) ? p[A_V_reset] : fminf(y[0], p[A_V_peak]);
     float I_tot = 0.0f;
 #pragma unroll
     for (int i = 0; i < NP; i++) {
       if (i < np) I_tot += y[NSV + i];
     }
-    float V_spike = p[A_Delta_T] == 0.0f ? 0.0f
-        : p[A_Delta_T] * expf((V - p[A_V_th]) / p[A_Delta_T]);
-    dydx[0] = (refr > 0.0f) ? 0.0f
-        : (-p[A_g_L] * (V - p[A_E_L] - V_spike) + I_tot - y[1] + p[A_I_e])
-          / p[A_C_m];
-    dydx[1] = (p[A_a] * (V - p[A_E_L]) - y[1]) / p[A_tau_w];
+    aeif_vw(y, dydx, p, q, refr, V, I_tot, true);
 #pragma unroll
     for (int i = 0; i < NP; i++) {
-      if (i < np) dydx[NSV + i] = -y[NSV + i] / p[NSP + i];
+      if (i < np) dydx[NSV + i] = -y[NSV + i] * q[NSP + i];
     }
   }
-  __device__ __forceinline__ static int external(float *y, float *p, bool end,
+  __device__ __forceinline__ static int external(float *y, const float *p,
+                                                 float &refr, bool end,
                                                  float dt) {
-    return aeif_external(y, p, end, dt);
+    return aeif_external(y, p, refr, end, dt);
   }
 };
 
@@ -212,18 +223,15 @@ template <int NP>
 struct AeifPscDelta {
   enum { NSV = 2, NPV = 0, NSP = A_NSP, NPP = 0, NVAR = 2, NPARAM = A_NSP };
   __device__ __forceinline__ static void deriv(const float *y, float *dydx,
-                                               const float *p, int np) {
-    float refr = p[A_refr];
+                                               const float *p, const float *q,
+                                               float refr, int np) {
     float V = (refr > 0.0f) ? p[A_V_reset] : fminf(y[0], p[A_V_peak]);
-    float V_spike = p[A_Delta_T] == 0.0f ? 0.0f
-        : p[A_Delta_T] * expf((V - p[A_V_th]) / p[A_Delta_T]);
-    dydx[0] = (refr > 0.0f) ? 0.0f
-        : (-p[A_g_L] * (V - p[A_E_L] - V_spike) - y[1] + p[A_I_e]) / p[A_C_m];
-    dydx[1] = (p[A_a] * (V - p[A_E_L]) - y[1]) / p[A_tau_w];
+    aeif_vw(y, dydx, p, q, refr, V, 0.0f, true);
   }
-  __device__ __forceinline__ static int external(float *y, float *p, bool end,
+  __device__ __forceinline__ static int external(float *y, const float *p,
+                                                 float &refr, bool end,
                                                  float dt) {
-    return aeif_external(y, p, end, dt);
+    return aeif_external(y, p, refr, end, dt);
   }
 };
 
@@ -237,8 +245,8 @@ struct IzhCondBeta {
   enum { NSV = 2, NPV = 2, NSP = I_NSP, NPP = 4,
          NVAR = NSV + NPV * NP, NPARAM = NSP + NPP * NP };
   __device__ __forceinline__ static void deriv(const float *y, float *dydx,
-                                               const float *p, int np) {
-    float refr = p[I_refr];
+                                               const float *p, const float *q,
+                                               float refr, int np) {
     float V = (refr > 0.0f) ? p[I_c] : y[0];
     float I_syn = 0.0f;
 #pragma unroll
@@ -252,12 +260,13 @@ struct IzhCondBeta {
     for (int i = 0; i < NP; i++) {
       if (i < np) {
         float g = y[NSV + NPV * i], g1 = y[NSV + NPV * i + 1];
-        dydx[NSV + NPV * i + 1] = -g1 / p[NSP + NPP * i + 1];
-        dydx[NSV + NPV * i] = g1 - g / p[NSP + NPP * i + 2];
+        dydx[NSV + NPV * i + 1] = -g1 * q[NSP + NPP * i + 1];
+        dydx[NSV + NPV * i] = g1 - g * q[NSP + NPP * i + 2];
       }
     }
   }
-  __device__ __forceinline__ static int external(float *y, float *p, bool end,
+  __device__ __forceinline__ static int external(float *y, const float *p,
+                                                 float &refr, bool end,
                                                  float dt) {
     float &V_m = y[0];
     float &u = y[1];
@@ -266,16 +275,16 @@ struct IzhCondBeta {
       u = 0.0f;
       return 0;
     }
-    if (p[I_refr] > 0.0f) {
+    if (refr > 0.0f) {
       V_m = p[I_c];
-      if (end) p[I_refr] -= 1.0f;
+      if (end) refr -= 1.0f;
       return 0;
     }
     if (V_m >= p[I_V_th]) {
       V_m = p[I_c];
       u += p[I_d];
       float r = (float)(int)roundf(p[I_t_ref] / dt);
-      p[I_refr] = r < 0.0f ? 0.0f : r;
+      refr = r < 0.0f ? 0.0f : r;
       return 1;
     }
     return 0;

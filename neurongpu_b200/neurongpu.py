@@ -243,6 +243,8 @@ _EXT_SIG = {
     "NGB200_SetKernelTiming": (_I, (_I,)),
     "NGB200_GetKernelTiming": (_I, (_I, ctypes.POINTER(ctypes.c_double),
                                     ctypes.POINTER(ctypes.c_longlong))),
+    "NGB200_GetRk5Tuning": (_I, (_I, ctypes.POINTER(ctypes.c_int),
+                                 ctypes.POINTER(ctypes.c_float))),
 }
 
 
@@ -1178,6 +1180,13 @@ class Binding(object):
         n = ctypes.c_longlong(0)
         self._call("NGB200_GetKernelTiming", ctypes.c_int(kind), ctypes.byref(t), ctypes.byref(n))
         return t.value, n.value
+
+    def GetRk5Tuning(self, i_node):
+        "(chosen RK5 kernel variant, [ms of variants 0..3]) for the group of i_node"
+        v = ctypes.c_int(0)
+        ms = (ctypes.c_float * 4)()
+        self._call("NGB200_GetRk5Tuning", ctypes.c_int(i_node), ctypes.byref(v), ms)
+        return v.value, list(ms)
 
 
 _default = None
