@@ -339,7 +339,7 @@ def main():
     for _ in range(e2e_steps):
         ngpu.SetStatus(pg, "rate", cfg["rate"])
         ngpu.Simulate(step_ms)
-        counts = ngpu.GetNeuronIntVar(nrn.i0, nrn.n, "spike_count")
+        counts = ngpu.GetNeuronIntVarArray(nrn.i0, nrn.n, "spike_count")
     e2e_wall = reduce_max(time.perf_counter() - t0, world)
     e2e = {"value": world * e2e_steps * step_ms / 1000.0 / e2e_wall, "unit": "bio_s/wall_s",
            "h2d_bytes_per_step": 48, "d2h_bytes_per_step": 4 * cfg["n"]}

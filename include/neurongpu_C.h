@@ -220,6 +220,14 @@ int NGB200_SetGraphChunk(int n_steps);
 /* Total number of nodes and of connections. */
 long long NGB200_NNodes();
 long long NGB200_NConnections();
+/* Every connection in one call, in delivery order (source, delay group,
+ * insertion; the order of NeuronGPU_GetSeqSeqConnections over all nodes).
+ * Each non-null array must hold NGB200_NConnections() elements; weights are
+ * the current device values once the network is calibrated. Returns the
+ * number of connections. No reference counterpart (the reference returns
+ * connections one status call at a time, src/neurongpu_C.h:294-331). */
+long long NGB200_GetAllConnections(int *src, int *tgt, int *port, int *syn,
+                                   float *delay, float *weight);
 /* Device time (CUDA events on the simulation stream) of the step loop of the
  * last NeuronGPU_Simulate call, in ms. */
 double NGB200_LastSimulateDeviceMs();

@@ -568,6 +568,12 @@ long long NGB200_NNodes() {
 long long NGB200_NConnections() {
   return guarded(0LL, [&](NeuronGPU *n) { return n->NConnections(); });
 }
+long long NGB200_GetAllConnections(int *src, int *tgt, int *port, int *syn,
+                                   float *delay, float *weight) {
+  return guarded(0LL, [&](NeuronGPU *n) {
+    return n->ExportConnections(src, tgt, port, syn, delay, weight);
+  });
+}
 double NGB200_LastSimulateDeviceMs() {
   return guarded(0.0, [&](NeuronGPU *n) { return n->LastSimulateDeviceMs(); });
 }

@@ -379,6 +379,36 @@ std::vector<ConnectionId> NeuronGPU::GetConnections(const int *src_arr, int i_sr
   return out;
 }
 
+long long NeuronGPU::ExportConnections(int *src, int *tgt, int *port, int *syn,
+                                       float *delay, float *weight) {
+  const long long N = (long long)node_group_map_.size();
+  if (!calibrate_flag_) BuildHostCSR();
+  const int nd = (int)delays_.size();
+  const long long M = (long long)e_src_.size();
+  std::vector<float> dev_w;
+  if (weight && calibrate_flag_ && M > 0) {
+    dev_w.resize((size_t)M);
+    NGPU_CUDA(cudaMemcpy(dev_w.data(), d_e_w_, sizeof(float) * M, cudaMemcpyDeviceToHost));
+  }
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (long long s = 0; s < N; s++) {
+    for (int di = 0; di < nd; di++) {
+      const uint64_t b = h_grp_off_[(uint64_t)s * nd + di];
+      const uint64_t e = h_grp_off_[(uint64_t)s * nd + di + 1];
+      for (uint64_t k = b; k < e; k++) {
+        const uint64_t o = h_order_[k];
+        if (src) src[k] = (int)s;
+        if (tgt) tgt[k] = (int)e_tgt_[o];
+        if (port) port[k] = e_port_[o];
+        if (syn) syn[k] = e_syn_[o];
+        if (delay) delay[k] = time_resolution_ * (float)delays_[di];
+        if (weight) weight[k] = dev_w.empty() ? e_w_[o] : dev_w[k];
+      }
+    }
+  }
+  return M;
+}
+
 ConnectionStatus NeuronGPU::GetConnectionStatus(ConnectionId id) {
   const int N = (int)node_group_map_.size();
   if (!calibrate_flag_) BuildHostCSR();

@@ -1393,6 +1393,10 @@ void NeuronGPU::UploadGeneratorParams() {
       cdf[(size_t)k * NGPU_CDF_LEN + n] = F;
     }
   }
+  // unchanged generator parameters keep the captured step graphs valid
+  if (gen_lam_h_ == lam && gen_origin_h_ == origin && gen_start_h_ == start &&
+      gen_stop_h_ == stop)
+    return;
   NGPU_CUDA(cudaMemcpy(d_gen_cdf_, cdf.data(), sizeof(double) * cdf.size(), cudaMemcpyHostToDevice));
   gen_origin_h_ = origin;
   gen_start_h_ = start;

@@ -298,6 +298,10 @@ class NeuronGPU {
   int SetGraphChunk(int g) { graph_chunk_ = g > 0 ? g : 1; InvalidateGraphs(); return 0; }
   long long NNodes() { return (long long)node_group_map_.size(); }
   long long NConnections() { return (long long)e_src_.size(); }
+  // every connection in delivery order (source, delay group, insertion);
+  // null outputs are skipped; weights are the device values once calibrated
+  long long ExportConnections(int *src, int *tgt, int *port, int *syn,
+                              float *delay, float *weight);
   int UseGraphs(int f) { use_graphs_ = f != 0; return 0; }
   // synchronous device copy of a raw column (tests, bench)
   cudaStream_t Stream() { return stream_; }

@@ -239,6 +239,8 @@ _EXT_SIG = {
     "NGB200_SetGraphChunk": (_I, (_I,)),
     "NGB200_NNodes": (ctypes.c_longlong, ()),
     "NGB200_NConnections": (ctypes.c_longlong, ()),
+    "NGB200_GetAllConnections": (ctypes.c_longlong, (c_int_p, c_int_p, c_int_p, c_int_p,
+                                                     c_float_p, c_float_p)),
     "NGB200_LastSimulateDeviceMs": (ctypes.c_double, ()),
     "NGB200_SetKernelTiming": (_I, (_I,)),
     "NGB200_GetKernelTiming": (_I, (_I, ctypes.POINTER(ctypes.c_double),
@@ -514,13 +516,13 @@ class Binding(object):
 
     @staticmethod
     def _rows(data_pt, n_node, array_size):
-        out = []
-        for i in range(n_node):
-            if array_size > 1:
-                out.append([data_pt[i * array_size + k] for k in range(array_size)])
-            else:
-                out.append(data_pt[i])
-        return out
+        import numpy as np
+        if n_node <= 0:
+            return []
+        a = np.ctypeslib.as_array(data_pt, shape=(n_node * max(array_size, 1),))
+        if array_size > 1:
+            return a.reshape(n_node, array_size).tolist()
+        return a.tolist()
 
     def GetNeuronParam(self, i_node, n_node, param_name):
         "Get neuron parameter value"
@@ -554,9 +556,15 @@ class Binding(object):
         return self._call("GetNeuronGroupParam", ctypes.c_int(i_node), _cstr(param_name))
 
     def GetNeuronIntVar(self, i_node, n_node, var_name):
+        return self.GetNeuronIntVarArray(i_node, n_node, var_name).reshape(-1, 1).tolist()
+
+    def GetNeuronIntVarArray(self, i_node, n_node, var_name):
+        """GetNeuronIntVar as a numpy int32 array of n_node values (extension:
+        one copy instead of a Python list of lists)."""
+        import numpy as np
         pt = self._call("GetNeuronIntVar", ctypes.c_int(i_node), ctypes.c_int(n_node),
                         _cstr(var_name))
-        return [[pt[i]] for i in range(n_node)]
+        return np.ctypeslib.as_array(pt, shape=(n_node,)).copy()
 
     def GetNeuronVar(self, i_node, n_node, var_name):
         pt = self._call("GetNeuronVar", ctypes.c_int(i_node), ctypes.c_int(n_node),
@@ -895,6 +903,16 @@ class Binding(object):
             return self.RandomNormal(array_size, mu, sigma)
         if dist_name == "normal_clipped":
             return self.RandomNormalClipped(array_size, mu, sigma, low, high, vstep)
+        if dist_name == "uniform":
+            # extension: uniform in [low, high) from the library generator
+            import numpy as np
+            if low <= -1.0e35 or high >= 1.0e35:
+                raise ValueError("uniform distribution needs low and high")
+            pt = self.RandomUniform(array_size)
+            a = np.ctypeslib.as_array(pt, shape=(array_size,))
+            a *= np.float32(high - low)
+            a += np.float32(low)
+            return pt
         raise ValueError("Unknown distribution")
 
     @staticmethod
@@ -1170,6 +1188,18 @@ class Binding(object):
 
     def NConnections(self):
         return self._call("NGB200_NConnections")
+
+    def GetAllConnections(self):
+        """Every connection as numpy arrays (source, target, port, syn_group,
+        delay, weight) in delivery order, in one library call."""
+        import numpy as np
+        m = self.NConnections()
+        cols = [np.zeros(m, dtype=np.int32) for _ in range(4)] + \
+               [np.zeros(m, dtype=np.float32) for _ in range(2)]
+        ptrs = [c.ctypes.data_as(c_int_p) for c in cols[:4]] + \
+               [c.ctypes.data_as(c_float_p) for c in cols[4:]]
+        self._call("NGB200_GetAllConnections", *ptrs)
+        return dict(zip(("source", "target", "port", "syn", "delay", "weight"), cols))
 
     def SetKernelTiming(self, on):
         return self._call("NGB200_SetKernelTiming", ctypes.c_int(1 if on else 0))
