@@ -220,6 +220,48 @@ int NGB200_SetGraphChunk(int n_steps);
 /* Total number of nodes and of connections. */
 long long NGB200_NNodes();
 long long NGB200_NConnections();
+/* RK5 node groups of the same model and port count are integrated by one
+ * kernel launch per time step through a device segment table (many
+ * independent networks, e.g. a parameter sweep). on = 0 gives every group
+ * its own launch; must be called before the first simulation. Default on.
+ * No reference counterpart (the reference launches one kernel per node
+ * group, src/neurongpu.cu:481-483). */
+int NGB200_SetRk5Batching(int on);
+/* Index of the batched RK5 launch the node's group belongs to, -1 if the
+ * group has its own launch (valid after the first simulation). */
+int NGB200_Rk5BatchOf(int i_node);
+/* Learned RK5 step proposer (no reference counterpart; the reference sizes
+ * every RK5 sub-step with the embedded-error controller of src/rk5.h:57-147
+ * only). A 6 -> 32 -> 32 -> 1 MLP over (V, w, conductances, previous step)
+ * proposes the next sub-step of aeif_cond_beta / aeif_cond_alpha neurons
+ * (1 or 2 ports) whenever the controller's own guess is shorter than the rest
+ * of the time step; the RK5 error test still accepts or rejects every step.
+ * i_node selects the node's group; -1 selects every supported group. */
+/* Log accepted sub-steps of the plain controller (capacity rows of 8 floats:
+ * 6 features, target log2(h/dt), 0); capacity 0 stops logging. */
+int NGB200_SetStepLog(int i_node, int capacity);
+/* Number of sub-steps logged so far (may exceed the capacity). */
+long long NGB200_GetStepLogCount(int i_node);
+/* Copies up to max_rows logged rows; returns the number copied. */
+int NGB200_GetStepLog(int i_node, float *out, int max_rows);
+/* Trains the proposer on every logged row (GPU forward / backward kernels,
+ * FP32 Adam, steps mini-batches of blocks x 64 rows); logging stops. Returns
+ * the number of rows; losses are mean squared errors of log2(h/dt) averaged
+ * over the first and the last 5% of the steps. */
+int NGB200_TrainStepProposer(int steps, int blocks, float lr, unsigned long long seed,
+                             float *loss_first, float *loss_last);
+/* Uses (on != 0) or stops using the trained proposer for the group. */
+int NGB200_SetStepProposer(int i_node, int on);
+/* The 1313 FP32 parameters: W1[32][6], b1[32], W2[32][32], b2[32], w3[32], b3. */
+int NGB200_SetStepProposerParams(const float *params);
+int NGB200_GetStepProposerParams(float *params);
+/* Proposed step = dt * 2^(output - margin); default margin 0.25. */
+int NGB200_SetStepProposerMargin(float margin);
+/* Test entry points: mean gradient (1313 floats) and loss of the training
+ * kernels over n samples of 8 floats; tensor-core inference of n rows of 6
+ * features with the given parameters. */
+float NGB200_MlpGradients(const float *data, int n_samples, const float *params, float *grad);
+int NGB200_MlpInfer(const float *x6, int n_rows, const float *params, float *out);
 /* Every connection in one call, in delivery order (source, delay group,
  * insertion; the order of NeuronGPU_GetSeqSeqConnections over all nodes).
  * Each non-null array must hold NGB200_NConnections() elements; weights are

@@ -568,6 +568,47 @@ long long NGB200_NNodes() {
 long long NGB200_NConnections() {
   return guarded(0LL, [&](NeuronGPU *n) { return n->NConnections(); });
 }
+int NGB200_SetRk5Batching(int on) {
+  return guarded(0, [&](NeuronGPU *n) { return n->SetRk5Batching(on); });
+}
+int NGB200_Rk5BatchOf(int i_node) {
+  return guarded(-1, [&](NeuronGPU *n) { return n->Rk5BatchOf(i_node); });
+}
+int NGB200_SetStepLog(int i_node, int capacity) {
+  return guarded(0, [&](NeuronGPU *n) { return n->SetStepLog(i_node, capacity); });
+}
+long long NGB200_GetStepLogCount(int i_node) {
+  return guarded(0LL, [&](NeuronGPU *n) { return n->GetStepLogCount(i_node); });
+}
+int NGB200_GetStepLog(int i_node, float *out, int max_rows) {
+  return guarded(0, [&](NeuronGPU *n) { return n->GetStepLog(i_node, out, max_rows); });
+}
+int NGB200_TrainStepProposer(int steps, int blocks, float lr, unsigned long long seed,
+                             float *loss_first, float *loss_last) {
+  return guarded(0, [&](NeuronGPU *n) {
+    return n->TrainStepProposer(steps, blocks, lr, seed, loss_first, loss_last);
+  });
+}
+int NGB200_SetStepProposer(int i_node, int on) {
+  return guarded(0, [&](NeuronGPU *n) { return n->SetStepProposer(i_node, on); });
+}
+int NGB200_SetStepProposerParams(const float *params) {
+  return guarded(0, [&](NeuronGPU *n) { return n->SetStepProposerParams(params); });
+}
+int NGB200_GetStepProposerParams(float *params) {
+  return guarded(0, [&](NeuronGPU *n) { return n->GetStepProposerParams(params); });
+}
+int NGB200_SetStepProposerMargin(float margin) {
+  return guarded(0, [&](NeuronGPU *n) { return n->SetStepProposerMargin(margin); });
+}
+float NGB200_MlpGradients(const float *data, int n_samples, const float *params, float *grad) {
+  return guarded(0.0f, [&](NeuronGPU *n) {
+    return n->MlpGradientsHost(data, n_samples, params, grad);
+  });
+}
+int NGB200_MlpInfer(const float *x6, int n_rows, const float *params, float *out) {
+  return guarded(0, [&](NeuronGPU *n) { return n->MlpInferHost(x6, n_rows, params, out); });
+}
 long long NGB200_GetAllConnections(int *src, int *tgt, int *port, int *syn,
                                    float *delay, float *weight) {
   return guarded(0LL, [&](NeuronGPU *n) {

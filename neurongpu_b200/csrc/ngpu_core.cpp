@@ -63,12 +63,18 @@ NeuronGPU::~NeuronGPU() {
 
 void NeuronGPU::FreeDevice() {
   InvalidateGraphs();
+  FreeRk5Batches();
   auto F = [](void *p) { if (p) cudaFree(p); };
   for (NodeGroup *g : groups_) {
     F(g->d_var); F(g->d_param); F(g->d_h); F(g->d_dx);
     F(g->d_spike_count); F(g->d_rec_times); F(g->d_n_rec);
     F(g->d_sg_off); F(g->d_sg_step); F(g->d_sg_next); F(g->d_sg_height);
     F(g->d_blk_evals);
+    F(g->d_log_buf); F(g->d_log_count);
+    g->d_log_buf = nullptr;
+    g->d_log_count = nullptr;
+    g->log_cap = 0;
+    if (g->step_mode == STEP_LOG) g->step_mode = STEP_PLAIN;
     g->d_var = g->d_param = g->d_h = g->d_dx = nullptr;
   }
   F(d_ctx_); F(d_acc_); F(d_ring_src_); F(d_ring_h_); F(d_ring_cnt_);
@@ -79,6 +85,8 @@ void NeuronGPU::FreeDevice() {
   F(d_dc_stream_); F(d_gen_rate_); F(d_gen_origin_); F(d_gen_start_);
   F(d_gen_stop_); F(d_gen_lambda_); F(d_gen_explam_); F(d_gen_cdf_); F(d_blk_events_); F(d_done_);
   F(d_rec_cols_); F(d_rec_buf_);
+  F(d_mlp_img_);
+  d_mlp_img_ = nullptr;
   for (cudaEvent_t e : kev_) cudaEventDestroy(e);
   kev_.clear();
   if (ev_start_) cudaEventDestroy(ev_start_);
@@ -879,6 +887,14 @@ GroupArgs NeuronGPU::MakeGroupArgs(NodeGroup *g) {
   a.dry = 0;
   a.den_delay_col = g->mi->den_delay_param;
   a.blk_evals = g->d_blk_evals;
+  a.step_mode = g->step_mode;
+  a.mlp_margin = mlp_margin_;
+  a.mlp = d_mlp_img_;
+  a.log_buf = g->d_log_buf;
+  a.log_count = g->d_log_count;
+  a.log_cap = g->log_cap;
+  if (a.step_mode == STEP_LEARNED && a.mlp == nullptr)
+    throw ngpu_exception("the learned step proposer has no parameters (train or set them first)");
   a.sg_off = g->d_sg_off;
   a.sg_step = g->d_sg_step;
   a.sg_height = g->d_sg_height;
@@ -1418,6 +1434,7 @@ void NeuronGPU::UploadGeneratorParams() {
 void NeuronGPU::InvalidateGraphs() {
   for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
   graphs_.clear();
+  batch_tables_dirty_ = true;
 }
 
 void NeuronGPU::KEvent(int step_in_chunk, int j) {
@@ -1464,8 +1481,14 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
     const ModelInfo *mi = g->mi;
     switch (mi->kind) {
       case MK_RK5:
-        LaunchRk5Update(mi->rk5_model, g->n_port, MakeGroupArgs(g), MakeInputArgs(g),
-                        MakePushArgs(g), d_ctx_, stream_);
+        if (g->batch >= 0) {
+          // the whole batch is launched once, at its first group
+          const Rk5BatchHost &b = batches_[g->batch];
+          if (b.groups[0] == g) LaunchRk5Batch(MakeRk5Batch(b), d_ctx_, stream_);
+        } else {
+          LaunchRk5Update(mi->rk5_model, g->n_port, MakeGroupArgs(g), MakeInputArgs(g),
+                          MakePushArgs(g), d_ctx_, stream_);
+        }
         break;
       case MK_IAF_PSC_EXP:
         LaunchIafPscExpUpdate(MakeGroupArgs(g), MakeInputArgs(g), MakePushArgs(g), d_ctx_, stream_);
@@ -1515,6 +1538,7 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
 
 void NeuronGPU::LaunchSteps(int n_steps) {
   if (n_steps <= 0) return;
+  if (batch_tables_dirty_) RefreshRk5BatchTables();
   if (n_rec_cols_ > 0 && rec_rows_used_ + n_steps > rec_cap_rows_) FlushRecords();
   if (ktime_) {
     // create the event pool before any capture
@@ -1607,6 +1631,7 @@ void NeuronGPU::CheckDeviceErrors() {
     if (e & DERR_RING_OVERFLOW) m += " more spikes in one step than the spike list can hold (increase max_spike_num_fact);";
     if (e & DERR_RK5_STUCK) m += " RK5 integration exceeded the substep limit;";
     if (e & DERR_REC_OVERFLOW) m += " recording buffer overflow;";
+    if (e & DERR_PROPOSER_TIMEOUT) m += " a tensor-core wait of the step proposer timed out;";
     throw ngpu_exception(m);
   }
 }
@@ -1643,6 +1668,7 @@ void NeuronGPU::TuneRk5(NodeGroup *g) {
   a.dry = 1;
   in.dry = 1;
   a.blk_evals = nullptr;
+  a.step_mode = STEP_PLAIN;       // the variants exist for the plain controller
   cudaEvent_t e0, e1;
   NGPU_CUDA(cudaEventCreate(&e0));
   NGPU_CUDA(cudaEventCreate(&e1));
@@ -1676,9 +1702,172 @@ void NeuronGPU::TuneRk5(NodeGroup *g) {
 int NeuronGPU::GetRk5Tuning(int i_node, int *variant, float *ms4) {
   int il;
   NodeGroup *g = GroupOf(i_node, 1, il);
+  if (g->batch >= 0) {
+    const Rk5BatchHost &b = batches_[g->batch];
+    *variant = b.variant;
+    for (int v = 0; v < 4; v++) ms4[v] = b.tune_ms[v];
+    return 0;
+  }
   *variant = g->rk5_variant;
   for (int v = 0; v < 4; v++) ms4[v] = g->tune_ms[v];
   return 0;
+}
+
+int NeuronGPU::SetRk5Batching(int on) {
+  if (batches_built_)
+    throw ngpu_exception("RK5 batching must be chosen before the first simulation");
+  rk5_batching_ = on != 0;
+  return 0;
+}
+
+int NeuronGPU::Rk5BatchOf(int i_node) {
+  int il;
+  NodeGroup *g = GroupOf(i_node, 1, il);
+  return g->batch;
+}
+
+// Groups with the same RK5 model and port count form one batch (launched
+// once per step through a segment table) when there are at least two of
+// them; a single group keeps its own launch with constant-bank arguments.
+void NeuronGPU::BuildRk5Batches() {
+  batches_built_ = true;
+  const char *env = getenv("NGB200_RK5_BATCH");
+  if (!rk5_batching_ || (env != nullptr && atoi(env) == 0)) return;
+  std::map<std::pair<int, int>, std::vector<NodeGroup *>> by_key;
+  for (NodeGroup *g : groups_) {
+    if (g->mi->kind != MK_RK5 || g->n_node <= 0) continue;
+    if (!Rk5BatchSupported(g->mi->rk5_model, g->n_port)) continue;
+    by_key[{g->mi->rk5_model, g->n_port}].push_back(g);
+  }
+  for (auto &kv : by_key) {
+    if (kv.second.size() < 2) continue;
+    Rk5BatchHost b;
+    b.model = kv.first.first;
+    b.np = kv.first.second;
+    b.groups = kv.second;
+    for (NodeGroup *g : b.groups) b.n_blocks += (g->n_node + 127) / 128;
+    const int k = (int)batches_.size();
+    for (NodeGroup *g : b.groups) g->batch = k;
+    NGPU_CUDA(cudaMalloc(&b.d_segs, sizeof(SegArgs) * b.groups.size()));
+    NGPU_CUDA(cudaMalloc(&b.d_blk_seg, sizeof(int) * b.n_blocks));
+    NGPU_CUDA(cudaMalloc(&b.d_blk_evals, sizeof(unsigned long long) * b.n_blocks));
+    NGPU_CUDA(cudaMemset(b.d_blk_evals, 0, sizeof(unsigned long long) * b.n_blocks));
+    std::vector<int> map(b.n_blocks);
+    int blk = 0;
+    for (size_t si = 0; si < b.groups.size(); si++) {
+      const int nb = (b.groups[si]->n_node + 127) / 128;
+      for (int j = 0; j < nb; j++) map[blk + j] = (int)si;
+      blk += nb;
+    }
+    NGPU_CUDA(cudaMemcpy(b.d_blk_seg, map.data(), sizeof(int) * b.n_blocks,
+                         cudaMemcpyHostToDevice));
+    batches_.push_back(b);
+  }
+  batch_tables_dirty_ = true;
+}
+
+// (Re)writes every batch's segment table from the groups' current
+// arguments; captured graphs read the tables at run time, so they stay valid.
+void NeuronGPU::RefreshRk5BatchTables() {
+  batch_tables_dirty_ = false;
+  for (Rk5BatchHost &b : batches_) {
+    std::vector<SegArgs> segs(b.groups.size());
+    int blk = 0;
+    for (size_t si = 0; si < b.groups.size(); si++) {
+      NodeGroup *g = b.groups[si];
+      memset(&segs[si], 0, sizeof(SegArgs));
+      segs[si].g = MakeGroupArgs(g);
+      segs[si].g.blk_evals = nullptr;
+      segs[si].in = MakeInputArgs(g);
+      segs[si].pa = MakePushArgs(g);
+      segs[si].blk0 = blk;
+      blk += (g->n_node + 127) / 128;
+    }
+    NGPU_CUDA(cudaMemcpy(b.d_segs, segs.data(), sizeof(SegArgs) * segs.size(),
+                         cudaMemcpyHostToDevice));
+  }
+}
+
+Rk5Batch NeuronGPU::MakeRk5Batch(const Rk5BatchHost &b) {
+  Rk5Batch r;
+  r.model = b.model;
+  r.np = b.np;
+  r.uni = 1;
+  for (NodeGroup *g : b.groups) {
+    GroupArgs a = MakeGroupArgs(g);
+    if (!a.all_uniform) r.uni = 0;
+  }
+  r.variant = r.uni ? b.variant : 0;
+  r.dry = 0;
+  r.mode = b.groups[0]->step_mode;
+  for (NodeGroup *g : b.groups)
+    if (g->step_mode != r.mode)
+      throw ngpu_exception("all node groups of a batched RK5 launch must use the same step "
+                           "mode (or switch batching off before the first simulation)");
+  r.n_blocks = b.n_blocks;
+  r.segs = b.d_segs;
+  r.blk_seg = b.d_blk_seg;
+  r.blk_evals = b.d_blk_evals;
+  return r;
+}
+
+// autotuner of a batch: as TuneRk5, over the whole segment table
+void NeuronGPU::TuneRk5Batch(Rk5BatchHost &b) {
+  b.tuned = true;
+  Rk5Batch r = MakeRk5Batch(b);
+  const int nv = r.uni ? Rk5VariantCount(b.np, 1) : 1;
+  const char *force = getenv("NGB200_RK5_VARIANT");
+  if (force != nullptr) {
+    b.variant = std::max(0, std::min(nv - 1, atoi(force)));
+    InvalidateGraphs();
+    return;
+  }
+  long long n_total = 0;
+  for (NodeGroup *g : b.groups) n_total += g->n_node;
+  const char *off = getenv("NGB200_AUTOTUNE");
+  if ((off != nullptr && atoi(off) == 0) || nv <= 1 || n_total < 16384) return;
+  r.dry = 1;
+  r.blk_evals = nullptr;
+  r.mode = STEP_PLAIN;
+  cudaEvent_t e0, e1;
+  NGPU_CUDA(cudaEventCreate(&e0));
+  NGPU_CUDA(cudaEventCreate(&e1));
+  int best = 0;
+  float best_ms = 1e30f;
+  for (int v = 0; v < nv; v++) {
+    r.variant = v;
+    LaunchRk5Batch(r, d_ctx_, stream_);
+    float t[3];
+    for (int k = 0; k < 3; k++) {
+      NGPU_CUDA(cudaEventRecord(e0, stream_));
+      LaunchRk5Batch(r, d_ctx_, stream_);
+      NGPU_CUDA(cudaEventRecord(e1, stream_));
+      NGPU_CUDA(cudaEventSynchronize(e1));
+      NGPU_CUDA(cudaEventElapsedTime(&t[k], e0, e1));
+    }
+    std::sort(t, t + 3);
+    b.tune_ms[v] = t[1];
+    if (t[1] < best_ms) {
+      best_ms = t[1];
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  NGPU_CUDA(cudaGetLastError());
+  b.variant = best;
+  InvalidateGraphs();
+}
+
+void NeuronGPU::FreeRk5Batches() {
+  for (Rk5BatchHost &b : batches_) {
+    if (b.d_segs) cudaFree(b.d_segs);
+    if (b.d_blk_seg) cudaFree(b.d_blk_seg);
+    if (b.d_blk_evals) cudaFree(b.d_blk_evals);
+  }
+  for (NodeGroup *g : groups_) g->batch = -1;
+  batches_.clear();
+  batches_built_ = false;
 }
 
 int NeuronGPU::StartSimulation() {
@@ -1700,8 +1889,12 @@ int NeuronGPU::StartSimulation() {
     printf("Neural activity simulation time: %.3lf\n", (double)sim_time_);
   }
   UploadGeneratorParams();
+  if (!batches_built_) BuildRk5Batches();
+  if (batch_tables_dirty_) RefreshRk5BatchTables();
+  for (Rk5BatchHost &b : batches_)
+    if (!b.tuned) TuneRk5Batch(b);
   for (NodeGroup *g : groups_)
-    if (g->mi->kind == MK_RK5 && !g->tuned) TuneRk5(g);
+    if (g->mi->kind == MK_RK5 && g->batch < 0 && !g->tuned) TuneRk5(g);
   neur_t0_ = neural_time_;
   it_ = 0;
   Nt_ = (long long)round(sim_time_ / time_resolution_);
@@ -1774,6 +1967,12 @@ int NeuronGPU::PushSpikesToNodes(int n, const int *nodes) {
 
 unsigned long long NeuronGPU::StageEvaluations() {
   unsigned long long tot = 0;
+  for (const Rk5BatchHost &b : batches_) {
+    std::vector<unsigned long long> v(b.n_blocks);
+    NGPU_CUDA(cudaMemcpy(v.data(), b.d_blk_evals, sizeof(unsigned long long) * b.n_blocks,
+                         cudaMemcpyDeviceToHost));
+    for (auto x : v) tot += x;
+  }
   for (NodeGroup *g : groups_) {
     if (!g->d_blk_evals) continue;
     std::vector<unsigned long long> v(g->n_blocks);
@@ -1799,6 +1998,220 @@ unsigned long long NeuronGPU::TotalSpikes() {
   StepCtx c;
   NGPU_CUDA(cudaMemcpy(&c, d_ctx_, sizeof(StepCtx), cudaMemcpyDeviceToHost));
   return c.n_spikes;
+}
+
+}  // namespace ngpu
+
+namespace ngpu {
+
+// ---------------------------------------------------------------------------
+// learned RK5 step proposer
+// ---------------------------------------------------------------------------
+std::vector<NodeGroup *> NeuronGPU::ProposerGroups(int i_node) {
+  std::vector<NodeGroup *> out;
+  if (i_node < 0) {
+    for (NodeGroup *g : groups_)
+      if (g->mi->kind == MK_RK5 && StepProposerSupported(g->mi->rk5_model, g->n_port))
+        out.push_back(g);
+    if (out.empty()) throw ngpu_exception("no node group supports the step proposer");
+    return out;
+  }
+  int il;
+  NodeGroup *g = GroupOf(i_node, 1, il);
+  if (g->mi->kind != MK_RK5 || !StepProposerSupported(g->mi->rk5_model, g->n_port))
+    throw ngpu_exception("the step proposer supports aeif_cond_beta and aeif_cond_alpha "
+                         "groups with 1 or 2 receptor ports");
+  out.push_back(g);
+  return out;
+}
+
+int NeuronGPU::SetStepLog(int i_node, int capacity) {
+  if (capacity < 0 || capacity > (1 << 26)) throw ngpu_exception("step log capacity out of range");
+  for (NodeGroup *g : ProposerGroups(i_node)) {
+    if (g->d_log_buf) cudaFree(g->d_log_buf);
+    if (g->d_log_count) cudaFree(g->d_log_count);
+    g->d_log_buf = nullptr;
+    g->d_log_count = nullptr;
+    g->log_cap = 0;
+    if (capacity > 0) {
+      NGPU_CUDA(cudaMalloc(&g->d_log_buf, sizeof(float) * 8 * (size_t)capacity));
+      NGPU_CUDA(cudaMalloc(&g->d_log_count, sizeof(unsigned)));
+      NGPU_CUDA(cudaMemset(g->d_log_count, 0, sizeof(unsigned)));
+      g->log_cap = capacity;
+      g->step_mode = STEP_LOG;
+    } else if (g->step_mode == STEP_LOG) {
+      g->step_mode = STEP_PLAIN;
+    }
+  }
+  InvalidateGraphs();
+  return 0;
+}
+
+long long NeuronGPU::GetStepLogCount(int i_node) {
+  long long tot = 0;
+  if (stream_) NGPU_CUDA(cudaStreamSynchronize(stream_));
+  for (NodeGroup *g : ProposerGroups(i_node)) {
+    if (!g->d_log_count) continue;
+    unsigned c = 0;
+    NGPU_CUDA(cudaMemcpy(&c, g->d_log_count, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    tot += c;
+  }
+  return tot;
+}
+
+int NeuronGPU::GetStepLog(int i_node, float *out, int max_rows) {
+  int rows = 0;
+  if (stream_) NGPU_CUDA(cudaStreamSynchronize(stream_));
+  for (NodeGroup *g : ProposerGroups(i_node)) {
+    if (!g->d_log_count || rows >= max_rows) continue;
+    unsigned c = 0;
+    NGPU_CUDA(cudaMemcpy(&c, g->d_log_count, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    int k = (int)std::min<long long>(std::min<long long>((long long)c, (long long)g->log_cap),
+                                     (long long)(max_rows - rows));
+    if (k > 0)
+      NGPU_CUDA(cudaMemcpy(out + (size_t)rows * 8, g->d_log_buf, sizeof(float) * 8 * (size_t)k,
+                           cudaMemcpyDeviceToHost));
+    rows += k;
+  }
+  return rows;
+}
+
+void NeuronGPU::UploadMlpImage() {
+  MlpImage img;
+  MlpBuildImage(mlp_params_.data(), &img);
+  if (!d_mlp_img_) NGPU_CUDA(cudaMalloc(&d_mlp_img_, sizeof(MlpImage)));
+  NGPU_CUDA(cudaMemcpy(d_mlp_img_, &img, sizeof(MlpImage), cudaMemcpyHostToDevice));
+  InvalidateGraphs();
+}
+
+// Trains the proposer on every logged sample of every group (GPU kernels,
+// FP32 Adam); logging is switched off afterwards.
+int NeuronGPU::TrainStepProposer(int steps, int blocks, float lr, unsigned long long seed,
+                                 float *loss_first, float *loss_last) {
+  if (steps <= 0 || blocks <= 0 || !(lr > 0.0f)) throw ngpu_exception("invalid training settings");
+  if (!stream_) NGPU_CUDA(cudaStreamCreate(&stream_));
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  std::vector<std::pair<NodeGroup *, int>> parts;
+  long long n = 0;
+  for (NodeGroup *g : groups_) {
+    if (!g->d_log_count) continue;
+    unsigned c = 0;
+    NGPU_CUDA(cudaMemcpy(&c, g->d_log_count, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    int k = (int)std::min<long long>((long long)c, (long long)g->log_cap);
+    if (k > 0) parts.push_back({g, k});
+    n += k;
+  }
+  if (n < 64) throw ngpu_exception("too few logged RK5 steps to train the step proposer");
+  float *d_data = nullptr;
+  NGPU_CUDA(cudaMalloc(&d_data, sizeof(float) * 8 * (size_t)n));
+  long long off = 0;
+  double tsum = 0.0;
+  std::vector<float> tmp;
+  for (auto &pk : parts) {
+    NGPU_CUDA(cudaMemcpy(d_data + off * 8, pk.first->d_log_buf, sizeof(float) * 8 * (size_t)pk.second,
+                         cudaMemcpyDeviceToDevice));
+    tmp.resize((size_t)pk.second * 8);
+    NGPU_CUDA(cudaMemcpy(tmp.data(), pk.first->d_log_buf, sizeof(float) * 8 * (size_t)pk.second,
+                         cudaMemcpyDeviceToHost));
+    for (int r = 0; r < pk.second; r++) tsum += tmp[(size_t)r * 8 + 6];
+    off += pk.second;
+  }
+  mlp_params_.assign(NGPU_MLP_NPARAM, 0.0f);
+  MlpInitParams(mlp_params_.data(), seed, (float)(tsum / (double)n));
+  float l0 = 0.0f, l1 = 0.0f;
+  try {
+    MlpTrain(d_data, (int)std::min<long long>(n, 0x7fffffffLL), mlp_params_.data(), steps, blocks,
+             lr, seed, &l0, &l1, stream_);
+  } catch (const std::exception &e) {
+    cudaFree(d_data);
+    throw ngpu_exception(e.what());
+  }
+  cudaFree(d_data);
+  for (NodeGroup *g : groups_) {
+    if (g->step_mode == STEP_LOG) g->step_mode = STEP_PLAIN;
+  }
+  UploadMlpImage();
+  if (loss_first) *loss_first = l0;
+  if (loss_last) *loss_last = l1;
+  return (int)std::min<long long>(n, 0x7fffffffLL);
+}
+
+int NeuronGPU::SetStepProposer(int i_node, int on) {
+  if (on && mlp_params_.empty())
+    throw ngpu_exception("the learned step proposer has no parameters (train or set them first)");
+  for (NodeGroup *g : ProposerGroups(i_node)) {
+    g->step_mode = on ? STEP_LEARNED : (g->d_log_buf ? STEP_LOG : STEP_PLAIN);
+  }
+  InvalidateGraphs();
+  return 0;
+}
+
+int NeuronGPU::SetStepProposerParams(const float *params) {
+  mlp_params_.assign(params, params + NGPU_MLP_NPARAM);
+  if (!stream_) NGPU_CUDA(cudaStreamCreate(&stream_));
+  UploadMlpImage();
+  return 0;
+}
+
+int NeuronGPU::GetStepProposerParams(float *params) {
+  if (mlp_params_.empty()) throw ngpu_exception("the step proposer has no parameters");
+  std::copy(mlp_params_.begin(), mlp_params_.end(), params);
+  return 0;
+}
+
+int NeuronGPU::SetStepProposerMargin(float margin) {
+  if (!(margin > -4.0f && margin < 8.0f)) throw ngpu_exception("margin out of range");
+  mlp_margin_ = margin;
+  InvalidateGraphs();
+  return 0;
+}
+
+// test entry points: gradients of the training kernels and tensor-core
+// inference on caller data (host arrays)
+float NeuronGPU::MlpGradientsHost(const float *data, int n, const float *params, float *grad) {
+  if (n <= 0) throw ngpu_exception("no samples");
+  if (!stream_) NGPU_CUDA(cudaStreamCreate(&stream_));
+  float *d = nullptr;
+  NGPU_CUDA(cudaMalloc(&d, sizeof(float) * 8 * (size_t)n));
+  NGPU_CUDA(cudaMemcpy(d, data, sizeof(float) * 8 * (size_t)n, cudaMemcpyHostToDevice));
+  float loss = 0.0f;
+  try {
+    loss = MlpGradients(d, n, params, grad, stream_);
+  } catch (const std::exception &e) {
+    cudaFree(d);
+    throw ngpu_exception(e.what());
+  }
+  cudaFree(d);
+  return loss;
+}
+
+int NeuronGPU::MlpInferHost(const float *x6, int n, const float *params, float *out) {
+  if (n <= 0) throw ngpu_exception("no samples");
+  if (!stream_) NGPU_CUDA(cudaStreamCreate(&stream_));
+  MlpImage img;
+  MlpBuildImage(params, &img);
+  MlpImage *d_img = nullptr;
+  float *d_x = nullptr, *d_out = nullptr;
+  unsigned *d_err = nullptr;
+  NGPU_CUDA(cudaMalloc(&d_img, sizeof(MlpImage)));
+  NGPU_CUDA(cudaMalloc(&d_x, sizeof(float) * 6 * (size_t)n));
+  NGPU_CUDA(cudaMalloc(&d_out, sizeof(float) * (size_t)n));
+  NGPU_CUDA(cudaMalloc(&d_err, sizeof(unsigned)));
+  NGPU_CUDA(cudaMemset(d_err, 0, sizeof(unsigned)));
+  NGPU_CUDA(cudaMemcpy(d_img, &img, sizeof(MlpImage), cudaMemcpyHostToDevice));
+  NGPU_CUDA(cudaMemcpy(d_x, x6, sizeof(float) * 6 * (size_t)n, cudaMemcpyHostToDevice));
+  MlpInfer(d_x, n, d_img, d_out, d_err, stream_);
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  NGPU_CUDA(cudaGetLastError());
+  unsigned err = 0;
+  NGPU_CUDA(cudaMemcpy(out, d_out, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost));
+  NGPU_CUDA(cudaMemcpy(&err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  cudaFree(d_img);
+  cudaFree(d_x);
+  cudaFree(d_out);
+  cudaFree(d_err);
+  if (err) throw ngpu_exception("tensor-core completion wait timed out in the step proposer");
+  return 0;
 }
 
 }  // namespace ngpu

@@ -129,6 +129,13 @@ struct NodeGroup {
   int rk5_variant = 0;
   bool tuned = false;
   float tune_ms[4] = {0, 0, 0, 0};
+  // index of the batched RK5 launch this group belongs to, or -1
+  int batch = -1;
+  // RK5 step mode (StepMode) and the accepted-step log of STEP_LOG
+  int step_mode = 0;
+  float *d_log_buf = nullptr;
+  unsigned *d_log_count = nullptr;
+  int log_cap = 0;
 
   int ScalVarIdx(const std::string &n) const;
   int PortVarIdx(const std::string &n) const;
@@ -295,6 +302,22 @@ class NeuronGPU {
   // RK5 kernel variant chosen for the group of i_node and its timings
   int GetRk5Tuning(int i_node, int *variant, float *ms4);
   void TuneRk5(NodeGroup *g);
+  // RK5 groups of one model and port count are integrated by one launch
+  // per step (segment table) unless batching is switched off
+  int SetRk5Batching(int on);
+  int Rk5BatchOf(int i_node);
+  // learned RK5 step proposer: accepted-step logging, GPU training, use
+  int SetStepLog(int i_node, int capacity);
+  long long GetStepLogCount(int i_node);
+  int GetStepLog(int i_node, float *out, int max_rows);
+  int TrainStepProposer(int steps, int blocks, float lr, unsigned long long seed,
+                        float *loss_first, float *loss_last);
+  int SetStepProposer(int i_node, int on);
+  int SetStepProposerParams(const float *params);
+  int GetStepProposerParams(float *params);
+  int SetStepProposerMargin(float margin);
+  float MlpGradientsHost(const float *data, int n, const float *params, float *grad);
+  int MlpInferHost(const float *x6, int n, const float *params, float *out);
   int SetGraphChunk(int g) { graph_chunk_ = g > 0 ? g : 1; InvalidateGraphs(); return 0; }
   long long NNodes() { return (long long)node_group_map_.size(); }
   long long NConnections() { return (long long)e_src_.size(); }
@@ -326,6 +349,31 @@ class NeuronGPU {
 
   // structure
   std::vector<NodeGroup *> groups_;
+  struct Rk5BatchHost {
+    int model = 0, np = 0;
+    std::vector<NodeGroup *> groups;
+    int n_blocks = 0;
+    int variant = 0;
+    bool tuned = false;
+    float tune_ms[4] = {0, 0, 0, 0};
+    SegArgs *d_segs = nullptr;
+    int *d_blk_seg = nullptr;
+    unsigned long long *d_blk_evals = nullptr;
+  };
+  std::vector<Rk5BatchHost> batches_;
+  bool batches_built_ = false;
+  bool batch_tables_dirty_ = true;
+  bool rk5_batching_ = true;
+  void BuildRk5Batches();
+  void RefreshRk5BatchTables();
+  void TuneRk5Batch(Rk5BatchHost &b);
+  Rk5Batch MakeRk5Batch(const Rk5BatchHost &b);
+  void FreeRk5Batches();
+  std::vector<float> mlp_params_;       // FP32 proposer parameters (empty: none)
+  MlpImage *d_mlp_img_ = nullptr;
+  float mlp_margin_ = 0.25f;
+  void UploadMlpImage();
+  std::vector<NodeGroup *> ProposerGroups(int i_node);
   std::vector<int> node_group_map_;
   std::vector<SynGroupHost> syn_groups_;
   std::vector<Record> records_;

@@ -32,7 +32,8 @@ enum DeviceError : unsigned {
   DERR_RING_OVERFLOW = 1u,      // more spikes in one step than ring capacity
   DERR_RK5_STUCK = 2u,          // adaptive integration exceeded substep cap
   DERR_REC_OVERFLOW = 4u,       // recording buffer overflow
-  DERR_NAN_STATE = 8u
+  DERR_NAN_STATE = 8u,
+  DERR_PROPOSER_TIMEOUT = 16u   // a tensor-core completion wait of the step proposer timed out
 };
 
 struct StepCtx {
@@ -105,6 +106,25 @@ struct InputArgs {
 // same counts as the sequential-search sampler
 #define NGPU_CDF_LEN 201
 
+// Inference image of the learned RK5 step proposer (6 -> 32 -> 32 -> 1 MLP):
+// BF16 weight tiles already in the UMMA K-major layout of the kernels' shared
+// memory, FP32 output-layer parameters.
+#define NGPU_MLP_NPARAM 1313      // FP32 parameters: W1 32x6, b1 32, W2 32x32, b2 32, w3 32, b3
+enum MlpParamOffset {
+  MLP_W1 = 0, MLP_B1 = 192, MLP_W2 = 224, MLP_B2 = 1248, MLP_W3 = 1280, MLP_B3 = 1312
+};
+struct MlpImage {
+  unsigned w1[32 * 16 / 2];     // N 32 x K 16 bf16 (K 0..5 weights, K 6 bias)
+  unsigned w2[32 * 32 / 2];     // N 32 x K 32 bf16
+  float b2[32];
+  float w3[32];
+  float b3;
+  float pad_[31];
+};
+
+// RK5 update modes
+enum StepMode { STEP_PLAIN = 0, STEP_LOG = 1, STEP_LEARNED = 2 };
+
 struct GroupArgs {
   int n;                        // nodes
   int n_pad;                    // column length
@@ -125,11 +145,27 @@ struct GroupArgs {
   float eps;                    // RK5 tolerance
   int den_delay_col;            // param column of den_delay or -1
   unsigned long long *blk_evals;  // per-block RK5 derivative evaluations
+  // learned step proposer (STEP_LEARNED) and accepted-step logging (STEP_LOG)
+  int step_mode;
+  float mlp_margin;             // proposal = dt * 2^(output - margin)
+  const MlpImage *mlp;
+  float *log_buf;               // [log_cap][8]: 6 features, target, 0
+  unsigned *log_count;
+  int log_cap;
   // spike generator data
   const int *sg_off;            // [n+1]
   const int *sg_step;           // spike step index
   const float *sg_height;
   int *sg_next;
+};
+
+// One RK5 group of a batched launch: its arguments and its first block.
+struct SegArgs {
+  GroupArgs g;
+  InputArgs in;
+  PushArgs pa;
+  int blk0;
+  int pad_;
 };
 
 struct SynGroupTable {

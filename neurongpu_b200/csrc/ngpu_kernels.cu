@@ -23,349 +23,41 @@
 #include "ngpu_models.h"
 #include "ngpu_rk5_models.cuh"
 #include "ngpu_rng.h"
+#include "ngpu_kernels_common.cuh"
 
 namespace ngpu {
-
-#define NGPU_BLOCK 128
-
-__device__ __forceinline__ bool pbit(const unsigned *mask, int j) {
-  return (mask[j >> 5] >> (j & 31)) & 1u;
-}
-
-// ---------------------------------------------------------------------------
-// spikes
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void push_spike(const PushArgs &pa, StepCtx *ctx,
-                                           int node, int local, float height,
-                                           long long T, double t_now,
-                                           int den_delay_steps) {
-  int slot = (int)(T % pa.ring_R);
-  int pos = atomicAdd(&pa.ring_cnt[slot], 1);
-  if (pos < pa.ring_C) {
-    long long k = (long long)slot * pa.ring_C + pos;
-    pa.ring_src[k] = (unsigned)node;
-    pa.ring_h[k] = height;
-  } else {
-    atomicOr(&ctx->err, (unsigned)DERR_RING_OVERFLOW);
-  }
-  pa.last_spike_T[node] = (int)T;
-  pa.last_spike_h[node] = height;
-  if (den_delay_steps == 0) pa.last_rev_T[node] = (int)T;
-  if (pa.spike_count != nullptr) pa.spike_count[local]++;
-  if (pa.rec_times != nullptr) {
-    int n = pa.n_rec[local];
-    // one slot is kept unused, as in src/spike_buffer.cu:183-186
-    if (n < pa.max_rec - 1) {
-      pa.rec_times[(long long)local * pa.max_rec + n] = (float)t_now;
-      pa.n_rec[local] = n + 1;
-    }
-  }
-}
-
-// Sum of the pending synaptic input of one node per port (fixed point):
-// accumulator contents (cleared here) plus the Poisson direct connections
-// drawn for the previous step.
-template <int NP>
-__device__ __forceinline__ void input_sum(const InputArgs &in, int i,
-                                          int n_pad, int np, long long it,
-                                          double t0, float dt, int pending,
-                                          long long T0, long long *s) {
-#pragma unroll
-  for (int q = 0; q < NP; q++) {
-    s[q] = 0;
-    if (q < np) {
-      long long *a = in.acc + in.acc_base + (long long)q * n_pad + i;
-      long long v = *a;
-      if (v != 0 && !in.dry) *a = 0;
-      s[q] = v;
-    }
-  }
-  if (pending && in.ud) {
-    const double t = t0 + (double)dt * (double)it;
-    const double t_rel = t - (double)in.ud_origin - (double)in.ud_delay;
-    if (t_rel >= (double)in.ud_start && t_rel <= (double)in.ud_stop) {
-      const double lam = in.ud_lambda;
-      unsigned n;
-      if (lam < NGPU_POISSON_INV_MAX) {
-        Philox4 r = ng_random_block(in.seed, RNG_TAG_POISSON_DIRECT,
-                                    in.ud_stream0 + (unsigned long long)i, T0 + it, 0);
-        const double u = ng_u01(r.v[0], r.v[1]);
-        n = 0;
-        if (lam > 0.0) {
-          while (n < NGPU_CDF_LEN - 1 && u > in.ud_cdf[n]) n++;
-        }
-      } else {
-        n = ng_poisson(lam, in.ud_explam, in.seed, RNG_TAG_POISSON_DIRECT,
-                       in.ud_stream0 + (unsigned long long)i, T0 + it);
-      }
-      if (n > 0) {
-        const long long v = ng_to_fixed(in.ud_w * (float)n);
-#pragma unroll
-        for (int q = 0; q < NP; q++) {
-          if (q == in.ud_port) s[q] += v;
-        }
-      }
-    }
-  } else if (pending && in.dc_off != nullptr) {
-    unsigned b = in.dc_off[i], e = in.dc_off[i + 1];
-    if (b < e) {
-      // time of the step whose draws are pending (neural_time_ of that step)
-      double t = t0 + (double)dt * (double)it;
-      long long T_prev = T0 + it;
-      for (unsigned c = b; c < e; c++) {
-        unsigned gen = in.dc_gen[c];
-        double t_rel = t - (double)in.gen_origin[gen] - (double)in.dc_delay[c];
-        if (t_rel >= (double)in.gen_start[gen] &&
-            t_rel <= (double)in.gen_stop[gen]) {
-          const double lam = in.gen_lambda[gen];
-          unsigned n;
-          if (lam < NGPU_POISSON_INV_MAX) {
-            // inversion against the host-built CDF table: the same counts as
-            // ng_poisson_inversion, without device double divisions
-            Philox4 r = ng_random_block(in.seed, RNG_TAG_POISSON_DIRECT,
-                                        in.dc_stream[c], T_prev, 0);
-            const double u = ng_u01(r.v[0], r.v[1]);
-            const double *cdf = in.gen_cdf + (size_t)gen * NGPU_CDF_LEN;
-            n = 0;
-            if (lam > 0.0) {
-              while (n < NGPU_CDF_LEN - 1 && u > cdf[n]) n++;
-            }
-          } else {
-            n = ng_poisson(lam, in.gen_explam[gen], in.seed,
-                           RNG_TAG_POISSON_DIRECT, in.dc_stream[c], T_prev);
-          }
-          if (n > 0) {
-            long long v = ng_to_fixed(in.dc_weight[c] * (float)n);
-            int port = in.dc_port[c];
-#pragma unroll
-            for (int q = 0; q < NP; q++) {
-              if (q == port) s[q] += v;
-            }
-          }
-        }
-      }
-    }
-  }
-}
-
-__device__ __forceinline__ float fold_value(float var, long long s, float w) {
-  return (float)((double)var + (double)s * NGPU_ACC_INV_SCALE * (double)w);
-}
-
-// ---------------------------------------------------------------------------
-// RK5 (Cash-Karp) step and update, following src/rk5.h:57-162
-// ---------------------------------------------------------------------------
-// err^e for err > 0 with e = -0.2 or -0.25 (step-size controller)
-__device__ __forceinline__ float ctrl_pow(float err, float e) {
-  return exp2f(e * log2f(err));
-}
-
-template <class M, int NP>
-__device__ __forceinline__ void rk5_step(double &x, float *y, float &h,
-                                         float h_min, float h_max,
-                                         const float *p, const float *q,
-                                         float refr, int np, float eps,
-                                         unsigned &evals) {
-  using namespace rk5c;
-  constexpr int NV = M::NVAR;
-  float k1[NV], k2[NV], k3[NV], k4[NV], k5[NV], k6[NV], yn[NV], ys[NV];
-  M::deriv(y, k1, p, q, refr, np);
-  evals++;
-#pragma unroll
-  for (int i = 0; i < NV; i++) ys[i] = fabsf(y[i]) + fabsf(k1[i] * h) + scal_min;
-  float err = 0.0f;
-  for (int guard = 0;; guard++) {
-    if (h > h_max) h = h_max;
-    if (h < h_min) h = h_min;
-#pragma unroll
-    for (int i = 0; i < NV; i++) yn[i] = y[i] + h * a21 * k1[i];
-    M::deriv(yn, k2, p, q, refr, np);
-#pragma unroll
-    for (int i = 0; i < NV; i++) yn[i] = y[i] + h * (a31 * k1[i] + a32 * k2[i]);
-    M::deriv(yn, k3, p, q, refr, np);
-#pragma unroll
-    for (int i = 0; i < NV; i++)
-      yn[i] = y[i] + h * (a41 * k1[i] + a42 * k2[i] + a43 * k3[i]);
-    M::deriv(yn, k4, p, q, refr, np);
-#pragma unroll
-    for (int i = 0; i < NV; i++)
-      yn[i] = y[i] + h * (a51 * k1[i] + a52 * k2[i] + a53 * k3[i]
-                          + a54 * k4[i]);
-    M::deriv(yn, k5, p, q, refr, np);
-#pragma unroll
-    for (int i = 0; i < NV; i++)
-      yn[i] = y[i] + h * (a61 * k1[i] + a62 * k2[i] + a63 * k3[i]
-                          + a64 * k4[i] + a65 * k5[i]);
-    M::deriv(yn, k6, p, q, refr, np);
-#pragma unroll
-    for (int i = 0; i < NV; i++)
-      yn[i] = y[i] + h * (a71 * k1[i] + a73 * k3[i] + a74 * k4[i]
-                          + a76 * k6[i]);
-    evals += 5;
-    err = 0.0f;
-#pragma unroll
-    for (int i = 0; i < NV; i++) {
-      float val = h * (e1 * k1[i] + e3 * k3[i] + e4 * k4[i] + e5 * k5[i]
-                       + e6 * k6[i]);
-      val /= ys[i];
-      float av = fabsf(val);
-      err = (err > av) ? err : av;
-    }
-    err /= eps;
-    if (err <= 1.0f || (double)h <= (double)h_min * (1.0 + 1.0e-5)) break;
-    if (guard >= 256) break;
-    float h_new = h * coeff * ctrl_pow(err, exp_dec);
-    double h01 = 0.1 * (double)h;
-    h = (float)(((double)h_new > h01) ? (double)h_new : h01);
-  }
-  x += h;
-  if (err > err_min) {
-    h = h * coeff * ctrl_pow(err, exp_inc);
-  } else {
-    h = (float)(5.0 * (double)h);
-  }
-#pragma unroll
-  for (int i = 0; i < NV; i++) y[i] = yn[i];
-}
-
-template <class M>
-struct ModelTraits;
-
-// input var / weight mapping and the param column of den_delay and
-// refractory_step for every RK5 model
-#define NGPU_TRAITS(MODEL, IN_BASE, IN_STEP, W_BASE, W_STEP, REFR, DEN)   \
-  template <int NP>                                                       \
-  struct ModelTraits<MODEL<NP>> {                                         \
-    enum { in_base = IN_BASE, in_step = IN_STEP, w_base = W_BASE,         \
-           w_step = W_STEP, refr = REFR, den = DEN };                     \
-  };
-NGPU_TRAITS(AeifCondBeta, 3, 2, A_NSP + 3, 4, A_refr, A_den_delay)
-NGPU_TRAITS(AeifCondAlpha, 3, 2, A_NSP + 2, 3, A_refr, A_den_delay)
-NGPU_TRAITS(AeifPscAlpha, 3, 2, A_NSP + 1, 2, A_refr, A_den_delay)
-NGPU_TRAITS(AeifPscExp, 2, 1, -1, 0, A_refr, A_den_delay)
-NGPU_TRAITS(AeifPscDelta, 0, 0, -1, 0, A_refr, A_den_delay)
-NGPU_TRAITS(IzhCondBeta, 3, 2, I_NSP + 3, 4, I_refr, I_den_delay)
-
-__device__ __forceinline__ void block_add_u64(unsigned long long v,
-                                              unsigned long long *dst) {
-  __shared__ unsigned long long s_part[NGPU_BLOCK / 32];
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0) s_part[wid] = v;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned long long t = 0;
-    for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += s_part[k];
-    dst[blockIdx.x] += t;
-  }
-}
-
-// One thread per neuron. UNI: every parameter except the refractory
-// counter is group-uniform, so p and its reciprocals q are read from the
-// constant kernel-parameter block (no per-neuron loads, no registers);
-// otherwise they are loaded per neuron and q is formed in registers.
-template <class M, int NP, bool UNI, int MINB>
-__global__ void __launch_bounds__(NGPU_BLOCK, MINB)
-k_rk5_update(const __grid_constant__ GroupArgs g, const __grid_constant__ InputArgs in,
-             const __grid_constant__ PushArgs pa, StepCtx *ctx) {
-  using Tr = ModelTraits<M>;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned evals = 0;
-  if (i < g.n) {
-    const int np = in.np;
-    const long long it = ctx->it;
-    const long long T0 = ctx->T0;
-    const double t0 = ctx->t0;
-    const int pending = ctx->poisson_pending;
-    const int n_pad = g.n_pad;
-    float y[M::NVAR];
-#pragma unroll
-    for (int j = 0; j < M::NVAR; j++) {
-      y[j] = (j < g.nvar) ? g.var[(long long)j * n_pad + i] : 0.0f;
-    }
-    float p_loc[UNI ? 1 : M::NPARAM];
-    float q_loc[UNI ? 1 : M::NPARAM];
-    if (!UNI) {
-#pragma unroll
-      for (int j = 0; j < (UNI ? 1 : M::NPARAM); j++) {
-        if (j < g.nparam) {
-          p_loc[j] = pbit(g.pmask, j) ? g.param[(long long)j * n_pad + i] : g.puni[j];
-        } else {
-          p_loc[j] = 1.0f;
-        }
-        q_loc[j] = 1.0f / p_loc[j];
-      }
-    }
-    const float *p = UNI ? g.puni : p_loc;
-    const float *q = UNI ? g.pinv : q_loc;
-    float refr = g.param[(long long)Tr::refr * n_pad + i];
-    // fold the previous step's input
-    constexpr int NPI = (M::NPV == 0) ? 1 : NP;
-    long long s[NPI];
-    input_sum<NPI>(in, i, n_pad, np, it, t0, g.dt, pending, T0, s);
-#pragma unroll
-    for (int qq = 0; qq < NPI; qq++) {
-      if (qq < np && s[qq] != 0) {
-        const int vi = Tr::in_base + qq * Tr::in_step;
-        const float w = (Tr::w_base >= 0) ? p[Tr::w_base + qq * Tr::w_step] : 1.0f;
-        y[vi] = fold_value(y[vi], s[qq], w);
-      }
-    }
-    const float refr0 = refr;
-    const double x1 = t0 + (double)g.dt * (double)(it + 1);
-    double x = t0 + (double)g.dt * (double)it + (double)g.dx[i];
-    float h = g.h[i];
-    const float h_min = g.h_min;
-    const long long T = T0 + it + 1;
-    const int den = (int)roundf(p[Tr::den] / g.dt);
-    bool end_step = false;
-    int guard = 0;
-    while (!end_step) {
-      float hmax = (float)(x1 - x);
-      rk5_step<M, NP>(x, y, h, h_min, hmax, p, q, refr, np, g.eps, evals);
-      end_step = (x >= x1 - (double)h_min);
-      if (M::external(y, p, refr, end_step, g.dt)) {
-        if (!g.dry) push_spike(pa, ctx, g.i_node_0 + i, i, 1.0f, T, x1, den);
-      }
-      if (++guard > NGPU_RK5_MAX_SUBSTEPS) {
-        atomicOr(&ctx->err, (unsigned)DERR_RK5_STUCK);
-        break;
-      }
-    }
-    if (!g.dry) {
-#pragma unroll
-      for (int j = 0; j < M::NVAR; j++) {
-        if (j < g.nvar) g.var[(long long)j * n_pad + i] = y[j];
-      }
-      g.h[i] = h;
-      g.dx[i] = (float)(x - x1);
-      if (refr != refr0) g.param[(long long)Tr::refr * n_pad + i] = refr;
-    } else if (y[0] == 1.2345e30f) {
-      // keeps the dry run from being optimised away; never true in practice
-      g.h[i] = h + (float)x;
-    }
-  }
-  if (g.blk_evals != nullptr) block_add_u64(evals, g.blk_evals);
-}
 
 template <class M, int NP>
 static void launch_rk5(const GroupArgs &g, const InputArgs &in, const PushArgs &pa,
                        StepCtx *ctx, cudaStream_t s) {
   dim3 grid((g.n + NGPU_BLOCK - 1) / NGPU_BLOCK), block(NGPU_BLOCK);
+  if (g.step_mode != STEP_PLAIN) {
+    // step logging and the learned proposer: conductance AdEx, <= 2 ports
+    if constexpr (ProposerFeatures<M>::supported && NP <= 2) {
+      if (g.step_mode == STEP_LOG) {
+        if (g.all_uniform) k_rk5_update<M, NP, true, 1, STEP_LOG><<<grid, block, 0, s>>>(g, in, pa, ctx);
+        else k_rk5_update<M, NP, false, 1, STEP_LOG><<<grid, block, 0, s>>>(g, in, pa, ctx);
+      } else {
+        if (g.all_uniform) k_rk5_update<M, NP, true, 4, STEP_LEARNED><<<grid, block, 0, s>>>(g, in, pa, ctx);
+        else k_rk5_update<M, NP, false, 4, STEP_LEARNED><<<grid, block, 0, s>>>(g, in, pa, ctx);
+      }
+    }
+    return;
+  }
   if (g.all_uniform) {
     if constexpr (NP <= 4) {
       // occupancy variants chosen by the autotuner (register cap per thread)
       switch (g.variant) {
-        case 1: k_rk5_update<M, NP, true, 5><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
-        case 2: k_rk5_update<M, NP, true, 6><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
-        case 3: k_rk5_update<M, NP, true, 8><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
-        default: k_rk5_update<M, NP, true, 1><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+        case 1: k_rk5_update<M, NP, true, 5, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+        case 2: k_rk5_update<M, NP, true, 6, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+        case 3: k_rk5_update<M, NP, true, 8, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+        default: k_rk5_update<M, NP, true, 1, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
       }
     } else {
-      k_rk5_update<M, NP, true, 1><<<grid, block, 0, s>>>(g, in, pa, ctx);
+      k_rk5_update<M, NP, true, 1, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx);
     }
   } else {
-    k_rk5_update<M, NP, false, 1><<<grid, block, 0, s>>>(g, in, pa, ctx);
+    k_rk5_update<M, NP, false, 1, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx);
   }
 }
 

@@ -18,6 +18,24 @@ void LaunchRk5Update(int model, int np, const GroupArgs &g,
                      StepCtx *ctx, cudaStream_t s);
 // number of RK5 kernel variants (GroupArgs::variant) for a group
 int Rk5VariantCount(int np, int all_uniform);
+
+// several RK5 groups of one model and port count in one launch: a device
+// segment table (one SegArgs per group) and a block -> segment map
+struct Rk5Batch {
+  int model, np;
+  int uni;                        // every segment has all_uniform set
+  int variant;                    // occupancy variant (as GroupArgs::variant)
+  int dry;                        // timing run: compute, store nothing
+  int mode;                       // StepMode shared by every segment
+  int n_blocks;
+  const SegArgs *segs;
+  const int *blk_seg;
+  unsigned long long *blk_evals;  // [n_blocks] or null
+};
+bool Rk5BatchSupported(int model, int np);
+void LaunchRk5Batch(const Rk5Batch &b, StepCtx *ctx, cudaStream_t s);
+// step logging / learned proposer available for this model and port count
+bool StepProposerSupported(int model, int np);
 void LaunchIafPscExpUpdate(const GroupArgs &g, const InputArgs &in,
                            const PushArgs &pa, StepCtx *ctx, cudaStream_t s);
 void LaunchSpikeGeneratorUpdate(const GroupArgs &g, const PushArgs &pa,
@@ -54,6 +72,19 @@ void LaunchAdvance(int *ring_cnt, int ring_R, int ring_C, int flags,
 void LaunchCalibrateRk5(int model, const GroupArgs &g, int np,
                         cudaStream_t s);
 void LaunchCalibrateIaf(const GroupArgs &g, float h, cudaStream_t s);
+
+// learned RK5 step proposer (ngpu_step_proposer.cu)
+void MlpBuildImage(const float *params, MlpImage *img);
+void MlpInitParams(float *params, unsigned long long seed, float b3);
+// mean gradient and loss over n samples [n][8] (features, target)
+float MlpGradients(const float *d_data, int n, const float *params, float *grad,
+                   cudaStream_t s);
+// Adam on FP32 params (in/out), mini-batches of blocks x 64 samples
+void MlpTrain(const float *d_data, int n, float *params, int steps, int blocks, float lr,
+              unsigned long long seed, float *loss_first, float *loss_last, cudaStream_t s);
+// tensor-core inference on n feature rows [n][6]
+void MlpInfer(const float *d_x6, int n, const MlpImage *d_img, float *d_out, unsigned *d_err,
+              cudaStream_t s);
 
 // utilities
 void LaunchFillFloat(float *p, long long n, float v, cudaStream_t s);

@@ -1,0 +1,466 @@
+// Device-side building blocks shared by the kernel translation units:
+// spike push, input folding, the RK5 (Cash-Karp) step and the per-neuron RK5
+// update with its single-group and batched (segment-table) kernels.
+// Included by ngpu_kernels.cu and ngpu_rk5_batch.cu only.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include "ngpu_device.h"
+#include "ngpu_kernels.h"
+#include "ngpu_models.h"
+#include "ngpu_rk5_models.cuh"
+#include "ngpu_rng.h"
+#include "ngpu_step_proposer.cuh"
+
+namespace ngpu {
+
+#define NGPU_BLOCK 128
+
+__device__ __forceinline__ bool pbit(const unsigned *mask, int j) {
+  return (mask[j >> 5] >> (j & 31)) & 1u;
+}
+
+// ---------------------------------------------------------------------------
+// spikes
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void push_spike(const PushArgs &pa, StepCtx *ctx,
+                                           int node, int local, float height,
+                                           long long T, double t_now,
+                                           int den_delay_steps) {
+  int slot = (int)(T % pa.ring_R);
+  int pos = atomicAdd(&pa.ring_cnt[slot], 1);
+  if (pos < pa.ring_C) {
+    long long k = (long long)slot * pa.ring_C + pos;
+    pa.ring_src[k] = (unsigned)node;
+    pa.ring_h[k] = height;
+  } else {
+    atomicOr(&ctx->err, (unsigned)DERR_RING_OVERFLOW);
+  }
+  pa.last_spike_T[node] = (int)T;
+  pa.last_spike_h[node] = height;
+  if (den_delay_steps == 0) pa.last_rev_T[node] = (int)T;
+  if (pa.spike_count != nullptr) pa.spike_count[local]++;
+  if (pa.rec_times != nullptr) {
+    int n = pa.n_rec[local];
+    // one slot is kept unused, as in src/spike_buffer.cu:183-186
+    if (n < pa.max_rec - 1) {
+      pa.rec_times[(long long)local * pa.max_rec + n] = (float)t_now;
+      pa.n_rec[local] = n + 1;
+    }
+  }
+}
+
+// Sum of the pending synaptic input of one node per port (fixed point):
+// accumulator contents (cleared here) plus the Poisson direct connections
+// drawn for the previous step.
+template <int NP>
+__device__ __forceinline__ void input_sum(const InputArgs &in, int i,
+                                          int n_pad, int np, long long it,
+                                          double t0, float dt, int pending,
+                                          long long T0, long long *s,
+                                          bool dry = false) {
+#pragma unroll
+  for (int q = 0; q < NP; q++) {
+    s[q] = 0;
+    if (q < np) {
+      long long *a = in.acc + in.acc_base + (long long)q * n_pad + i;
+      long long v = *a;
+      if (v != 0 && !(in.dry || dry)) *a = 0;
+      s[q] = v;
+    }
+  }
+  if (pending && in.ud) {
+    const double t = t0 + (double)dt * (double)it;
+    const double t_rel = t - (double)in.ud_origin - (double)in.ud_delay;
+    if (t_rel >= (double)in.ud_start && t_rel <= (double)in.ud_stop) {
+      const double lam = in.ud_lambda;
+      unsigned n;
+      if (lam < NGPU_POISSON_INV_MAX) {
+        Philox4 r = ng_random_block(in.seed, RNG_TAG_POISSON_DIRECT,
+                                    in.ud_stream0 + (unsigned long long)i, T0 + it, 0);
+        const double u = ng_u01(r.v[0], r.v[1]);
+        n = 0;
+        if (lam > 0.0) {
+          while (n < NGPU_CDF_LEN - 1 && u > in.ud_cdf[n]) n++;
+        }
+      } else {
+        n = ng_poisson(lam, in.ud_explam, in.seed, RNG_TAG_POISSON_DIRECT,
+                       in.ud_stream0 + (unsigned long long)i, T0 + it);
+      }
+      if (n > 0) {
+        const long long v = ng_to_fixed(in.ud_w * (float)n);
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+          if (q == in.ud_port) s[q] += v;
+        }
+      }
+    }
+  } else if (pending && in.dc_off != nullptr) {
+    unsigned b = in.dc_off[i], e = in.dc_off[i + 1];
+    if (b < e) {
+      // time of the step whose draws are pending (neural_time_ of that step)
+      double t = t0 + (double)dt * (double)it;
+      long long T_prev = T0 + it;
+      for (unsigned c = b; c < e; c++) {
+        unsigned gen = in.dc_gen[c];
+        double t_rel = t - (double)in.gen_origin[gen] - (double)in.dc_delay[c];
+        if (t_rel >= (double)in.gen_start[gen] &&
+            t_rel <= (double)in.gen_stop[gen]) {
+          const double lam = in.gen_lambda[gen];
+          unsigned n;
+          if (lam < NGPU_POISSON_INV_MAX) {
+            // inversion against the host-built CDF table: the same counts as
+            // ng_poisson_inversion, without device double divisions
+            Philox4 r = ng_random_block(in.seed, RNG_TAG_POISSON_DIRECT,
+                                        in.dc_stream[c], T_prev, 0);
+            const double u = ng_u01(r.v[0], r.v[1]);
+            const double *cdf = in.gen_cdf + (size_t)gen * NGPU_CDF_LEN;
+            n = 0;
+            if (lam > 0.0) {
+              while (n < NGPU_CDF_LEN - 1 && u > cdf[n]) n++;
+            }
+          } else {
+            n = ng_poisson(lam, in.gen_explam[gen], in.seed,
+                           RNG_TAG_POISSON_DIRECT, in.dc_stream[c], T_prev);
+          }
+          if (n > 0) {
+            long long v = ng_to_fixed(in.dc_weight[c] * (float)n);
+            int port = in.dc_port[c];
+#pragma unroll
+            for (int q = 0; q < NP; q++) {
+              if (q == port) s[q] += v;
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ float fold_value(float var, long long s, float w) {
+  return (float)((double)var + (double)s * NGPU_ACC_INV_SCALE * (double)w);
+}
+
+// ---------------------------------------------------------------------------
+// RK5 (Cash-Karp) step and update, following src/rk5.h:57-162
+// ---------------------------------------------------------------------------
+// err^e for err > 0 with e = -0.2 or -0.25 (step-size controller)
+__device__ __forceinline__ float ctrl_pow(float err, float e) {
+  return exp2f(e * log2f(err));
+}
+
+template <class M, int NP>
+__device__ __forceinline__ void rk5_step(double &x, float *y, float &h,
+                                         float h_min, float h_max,
+                                         const float *p, const float *q,
+                                         float refr, int np, float eps,
+                                         unsigned &evals, float &h_acc, float &err_acc) {
+  using namespace rk5c;
+  constexpr int NV = M::NVAR;
+  float k1[NV], k2[NV], k3[NV], k4[NV], k5[NV], k6[NV], yn[NV], ys[NV];
+  M::deriv(y, k1, p, q, refr, np);
+  evals++;
+#pragma unroll
+  for (int i = 0; i < NV; i++) ys[i] = fabsf(y[i]) + fabsf(k1[i] * h) + scal_min;
+  float err = 0.0f;
+  for (int guard = 0;; guard++) {
+    if (h > h_max) h = h_max;
+    if (h < h_min) h = h_min;
+#pragma unroll
+    for (int i = 0; i < NV; i++) yn[i] = y[i] + h * a21 * k1[i];
+    M::deriv(yn, k2, p, q, refr, np);
+#pragma unroll
+    for (int i = 0; i < NV; i++) yn[i] = y[i] + h * (a31 * k1[i] + a32 * k2[i]);
+    M::deriv(yn, k3, p, q, refr, np);
+#pragma unroll
+    for (int i = 0; i < NV; i++)
+      yn[i] = y[i] + h * (a41 * k1[i] + a42 * k2[i] + a43 * k3[i]);
+    M::deriv(yn, k4, p, q, refr, np);
+#pragma unroll
+    for (int i = 0; i < NV; i++)
+      yn[i] = y[i] + h * (a51 * k1[i] + a52 * k2[i] + a53 * k3[i]
+                          + a54 * k4[i]);
+    M::deriv(yn, k5, p, q, refr, np);
+#pragma unroll
+    for (int i = 0; i < NV; i++)
+      yn[i] = y[i] + h * (a61 * k1[i] + a62 * k2[i] + a63 * k3[i]
+                          + a64 * k4[i] + a65 * k5[i]);
+    M::deriv(yn, k6, p, q, refr, np);
+#pragma unroll
+    for (int i = 0; i < NV; i++)
+      yn[i] = y[i] + h * (a71 * k1[i] + a73 * k3[i] + a74 * k4[i]
+                          + a76 * k6[i]);
+    evals += 5;
+    err = 0.0f;
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+      float val = h * (e1 * k1[i] + e3 * k3[i] + e4 * k4[i] + e5 * k5[i]
+                       + e6 * k6[i]);
+      val /= ys[i];
+      float av = fabsf(val);
+      err = (err > av) ? err : av;
+    }
+    err /= eps;
+    if (err <= 1.0f || (double)h <= (double)h_min * (1.0 + 1.0e-5)) break;
+    if (guard >= 256) break;
+    float h_new = h * coeff * ctrl_pow(err, exp_dec);
+    double h01 = 0.1 * (double)h;
+    h = (float)(((double)h_new > h01) ? (double)h_new : h01);
+  }
+  x += h;
+  h_acc = h;
+  err_acc = err;
+  if (err > err_min) {
+    h = h * coeff * ctrl_pow(err, exp_inc);
+  } else {
+    h = (float)(5.0 * (double)h);
+  }
+#pragma unroll
+  for (int i = 0; i < NV; i++) y[i] = yn[i];
+}
+
+template <class M>
+struct ModelTraits;
+
+// input var / weight mapping and the param column of den_delay and
+// refractory_step for every RK5 model
+#define NGPU_TRAITS(MODEL, IN_BASE, IN_STEP, W_BASE, W_STEP, REFR, DEN)   \
+  template <int NP>                                                       \
+  struct ModelTraits<MODEL<NP>> {                                         \
+    enum { in_base = IN_BASE, in_step = IN_STEP, w_base = W_BASE,         \
+           w_step = W_STEP, refr = REFR, den = DEN };                     \
+  };
+NGPU_TRAITS(AeifCondBeta, 3, 2, A_NSP + 3, 4, A_refr, A_den_delay)
+NGPU_TRAITS(AeifCondAlpha, 3, 2, A_NSP + 2, 3, A_refr, A_den_delay)
+NGPU_TRAITS(AeifPscAlpha, 3, 2, A_NSP + 1, 2, A_refr, A_den_delay)
+NGPU_TRAITS(AeifPscExp, 2, 1, -1, 0, A_refr, A_den_delay)
+NGPU_TRAITS(AeifPscDelta, 0, 0, -1, 0, A_refr, A_den_delay)
+NGPU_TRAITS(IzhCondBeta, 3, 2, I_NSP + 3, 4, I_refr, I_den_delay)
+
+__device__ __forceinline__ void block_add_u64(unsigned long long v,
+                                              unsigned long long *dst) {
+  __shared__ unsigned long long s_part[NGPU_BLOCK / 32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) s_part[wid] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += s_part[k];
+    dst[blockIdx.x] += t;
+  }
+}
+
+// Appends one accepted sub-step (features at its start, training target) to
+// the group's step log; one atomic per warp.
+__device__ __forceinline__ void log_step_sample(const GroupArgs &g, const float *f,
+                                                float target) {
+  const unsigned mask = __activemask();
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  const unsigned rank = __popc(mask & ((1u << lane) - 1u));
+  unsigned base = 0;
+  if (lane == leader) base = atomicAdd(g.log_count, (unsigned)__popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  const unsigned idx = base + rank;
+  if (idx < (unsigned)g.log_cap) {
+    float4 *dst = reinterpret_cast<float4 *>(g.log_buf + (size_t)idx * 8);
+    dst[0] = make_float4(f[0], f[1], f[2], f[3]);
+    dst[1] = make_float4(f[4], f[5], target, 0.0f);
+  }
+}
+
+// Integrates neuron i of group g over one time step (one thread per
+// neuron). UNI: every parameter except the refractory counter is
+// group-uniform and is read from p_uni / q_uni (reciprocals); otherwise the
+// parameters are loaded per neuron and q is formed in registers.
+// MODE STEP_PLAIN: the reference's controller; STEP_LOG: the same, and every
+// sub-step that starts with a controller guess shorter than the rest of the
+// time step is logged for training the proposer; STEP_LEARNED: that guess is
+// replaced by the learned proposer's (the error test still accepts or
+// rejects). STEP_LEARNED is called by every thread of the CTA, in lock-step
+// rounds of one accepted sub-step, because each proposal round is one
+// CTA-wide tensor-core MMA; threads past the group end only take part.
+template <class M, int NP, bool UNI, int MODE>
+__device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &in,
+                                           const PushArgs &pa, StepCtx *ctx, int i,
+                                           const float *p_uni, const float *q_uni,
+                                           unsigned &evals, bool dry_run,
+                                           ProposerSmem *ps) {
+  using Tr = ModelTraits<M>;
+  const bool active = (MODE != STEP_LEARNED) || (i < g.n);
+  const bool dry = g.dry || dry_run;
+  const int np = in.np;
+  const long long it = ctx->it;
+  const long long T0 = ctx->T0;
+  const double t0 = ctx->t0;
+  const int pending = ctx->poisson_pending;
+  const int n_pad = g.n_pad;
+  float y[M::NVAR];
+#pragma unroll
+  for (int j = 0; j < M::NVAR; j++) {
+    y[j] = (active && j < g.nvar) ? g.var[(long long)j * n_pad + i] : 0.0f;
+  }
+  float p_loc[UNI ? 1 : M::NPARAM];
+  float q_loc[UNI ? 1 : M::NPARAM];
+  if (!UNI) {
+#pragma unroll
+    for (int j = 0; j < (UNI ? 1 : M::NPARAM); j++) {
+      if (j < g.nparam) {
+        p_loc[j] = (active && pbit(g.pmask, j)) ? g.param[(long long)j * n_pad + i] : g.puni[j];
+      } else {
+        p_loc[j] = 1.0f;
+      }
+      q_loc[j] = 1.0f / p_loc[j];
+    }
+  }
+  const float *p = UNI ? p_uni : p_loc;
+  const float *q = UNI ? q_uni : q_loc;
+  float refr = active ? g.param[(long long)Tr::refr * n_pad + i] : 0.0f;
+  // fold the previous step's input
+  constexpr int NPI = (M::NPV == 0) ? 1 : NP;
+  if (active) {
+    long long s[NPI];
+    input_sum<NPI>(in, i, n_pad, np, it, t0, g.dt, pending, T0, s, dry);
+#pragma unroll
+    for (int qq = 0; qq < NPI; qq++) {
+      if (qq < np && s[qq] != 0) {
+        const int vi = Tr::in_base + qq * Tr::in_step;
+        const float w = (Tr::w_base >= 0) ? p[Tr::w_base + qq * Tr::w_step] : 1.0f;
+        y[vi] = fold_value(y[vi], s[qq], w);
+      }
+    }
+  }
+  const float refr0 = refr;
+  const double x1 = t0 + (double)g.dt * (double)(it + 1);
+  double x = t0 + (double)g.dt * (double)it + (active ? (double)g.dx[i] : 0.0);
+  float h = active ? g.h[i] : 0.0f;
+  const float h_min = g.h_min;
+  const long long T = T0 + it + 1;
+  const int den = (int)roundf(p[Tr::den] / g.dt);
+  bool end_step = !active;
+  int guard = 0;
+  float h_acc, err_acc;
+  if constexpr (MODE == STEP_LEARNED) {
+    bool ready = false, failed = false;
+    while (__syncthreads_or(!end_step)) {
+      const float hmax = active ? (float)(x1 - x) : 0.0f;
+      const bool want = !end_step && !failed && h < hmax;
+      if (__syncthreads_or(want)) {
+        if (!ready) {
+          proposer_setup(*ps, g.mlp);
+          ready = true;
+        }
+        float f[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        if (want) ProposerFeatures<M>::get(y, p, h, g.dt, f);
+        float o = 0.0f;
+        if (proposer_round(*ps, want, f, o, &ctx->err)) {
+          if (want) {
+            const float hp = g.dt * exp2f(o - g.mlp_margin);
+            h = fminf(fmaxf(hp, h_min), hmax);
+          }
+        } else {
+          failed = true;
+        }
+      }
+      if (!end_step) {
+        rk5_step<M, NP>(x, y, h, h_min, hmax, p, q, refr, np, g.eps, evals, h_acc, err_acc);
+        end_step = (x >= x1 - (double)h_min);
+        if (M::external(y, p, refr, end_step, g.dt)) {
+          if (!dry) push_spike(pa, ctx, g.i_node_0 + i, i, 1.0f, T, x1, den);
+        }
+        if (++guard > NGPU_RK5_MAX_SUBSTEPS) {
+          atomicOr(&ctx->err, (unsigned)DERR_RK5_STUCK);
+          end_step = true;
+        }
+      }
+    }
+    proposer_teardown(*ps, ready, failed);
+  } else {
+    while (!end_step) {
+      const float hmax = (float)(x1 - x);
+      float f[6];
+      bool lg = false;
+      if constexpr (MODE == STEP_LOG) {
+        if (h < hmax && !dry) {
+          ProposerFeatures<M>::get(y, p, h, g.dt, f);
+          lg = true;
+        }
+      }
+      rk5_step<M, NP>(x, y, h, h_min, hmax, p, q, refr, np, g.eps, evals, h_acc, err_acc);
+      if constexpr (MODE == STEP_LOG) {
+        if (lg) log_step_sample(g, f, proposer_target(h_acc, err_acc, g.dt));
+      }
+      end_step = (x >= x1 - (double)h_min);
+      if (M::external(y, p, refr, end_step, g.dt)) {
+        if (!dry) push_spike(pa, ctx, g.i_node_0 + i, i, 1.0f, T, x1, den);
+      }
+      if (++guard > NGPU_RK5_MAX_SUBSTEPS) {
+        atomicOr(&ctx->err, (unsigned)DERR_RK5_STUCK);
+        break;
+      }
+    }
+  }
+  if (!active) return;
+  if (!dry) {
+#pragma unroll
+    for (int j = 0; j < M::NVAR; j++) {
+      if (j < g.nvar) g.var[(long long)j * n_pad + i] = y[j];
+    }
+    g.h[i] = h;
+    g.dx[i] = (float)(x - x1);
+    if (refr != refr0) g.param[(long long)Tr::refr * n_pad + i] = refr;
+  } else if (y[0] == 1.2345e30f) {
+    // keeps the dry run from being optimised away; never true in practice
+    g.h[i] = h + (float)x;
+  }
+}
+
+// One RK5 group per launch; its arguments live in the constant
+// kernel-parameter block, so uniform parameters cost no loads.
+template <class M, int NP, bool UNI, int MINB, int MODE>
+__global__ void __launch_bounds__(NGPU_BLOCK, MINB)
+k_rk5_update(const __grid_constant__ GroupArgs g, const __grid_constant__ InputArgs in,
+             const __grid_constant__ PushArgs pa, StepCtx *ctx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned evals = 0;
+  if constexpr (MODE == STEP_LEARNED) {
+    __shared__ ProposerSmem ps;
+    rk5_neuron<M, NP, UNI, MODE>(g, in, pa, ctx, i, g.puni, g.pinv, evals, false, &ps);
+  } else {
+    if (i < g.n) rk5_neuron<M, NP, UNI, MODE>(g, in, pa, ctx, i, g.puni, g.pinv, evals, false,
+                                              nullptr);
+  }
+  if (g.blk_evals != nullptr) block_add_u64(evals, g.blk_evals);
+}
+
+// Many RK5 groups of one model in one launch (independent networks of a
+// parameter sweep, for instance): block b integrates segment blk_seg[b],
+// whose arguments are read from the device segment table; the segment's
+// uniform parameters are staged in shared memory.
+template <class M, int NP, bool UNI, int MINB, int MODE>
+__global__ void __launch_bounds__(NGPU_BLOCK, MINB)
+k_rk5_update_seg(const SegArgs *__restrict__ segs, const int *__restrict__ blk_seg,
+                 unsigned long long *blk_evals, int dry, StepCtx *ctx) {
+  __shared__ float s_p[M::NPARAM], s_q[M::NPARAM];
+  const SegArgs &S = segs[blk_seg[blockIdx.x]];
+  if (UNI) {
+    for (int j = threadIdx.x; j < M::NPARAM; j += blockDim.x) {
+      s_p[j] = S.g.puni[j];
+      s_q[j] = S.g.pinv[j];
+    }
+    __syncthreads();
+  }
+  const int i = (blockIdx.x - S.blk0) * blockDim.x + threadIdx.x;
+  unsigned evals = 0;
+  if constexpr (MODE == STEP_LEARNED) {
+    __shared__ ProposerSmem ps;
+    rk5_neuron<M, NP, UNI, MODE>(S.g, S.in, S.pa, ctx, i, s_p, s_q, evals, dry != 0, &ps);
+  } else {
+    if (i < S.g.n)
+      rk5_neuron<M, NP, UNI, MODE>(S.g, S.in, S.pa, ctx, i, s_p, s_q, evals, dry != 0, nullptr);
+  }
+  if (blk_evals != nullptr) block_add_u64(evals, blk_evals);
+}
+
+}  // namespace ngpu

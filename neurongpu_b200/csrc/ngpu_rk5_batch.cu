@@ -1,0 +1,71 @@
+// Batched RK5 update: many node groups of one model and port count in one
+// launch through a device segment table (k_rk5_update_seg), e.g. the
+// independent networks of a parameter sweep. Kept in its own translation unit
+// so that its template instances compile in parallel with ngpu_kernels.cu.
+#include "ngpu_kernels_common.cuh"
+
+namespace ngpu {
+
+template <class M, int NP>
+static void launch_rk5_seg(const Rk5Batch &b, StepCtx *ctx, cudaStream_t s) {
+  dim3 grid(b.n_blocks), block(NGPU_BLOCK);
+  if (b.mode != STEP_PLAIN) {
+    if constexpr (ProposerFeatures<M>::supported && NP <= 2) {
+      if (b.mode == STEP_LOG) {
+        if (b.uni) k_rk5_update_seg<M, NP, true, 1, STEP_LOG><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx);
+        else k_rk5_update_seg<M, NP, false, 1, STEP_LOG><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx);
+      } else {
+        if (b.uni) k_rk5_update_seg<M, NP, true, 4, STEP_LEARNED><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx);
+        else k_rk5_update_seg<M, NP, false, 4, STEP_LEARNED><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx);
+      }
+    }
+    return;
+  }
+  if constexpr (NP <= 4) {
+    if (b.uni) {
+      switch (b.variant) {
+        case 1: k_rk5_update_seg<M, NP, true, 5, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx); break;
+        case 2: k_rk5_update_seg<M, NP, true, 6, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx); break;
+        case 3: k_rk5_update_seg<M, NP, true, 8, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx); break;
+        default: k_rk5_update_seg<M, NP, true, 1, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx); break;
+      }
+    } else {
+      k_rk5_update_seg<M, NP, false, 1, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx);
+    }
+  }
+}
+
+template <template <int> class MT>
+static void launch_rk5_seg_model(const Rk5Batch &b, StepCtx *ctx, cudaStream_t s) {
+  switch (b.np) {
+    case 0:
+    case 1: launch_rk5_seg<MT<1>, 1>(b, ctx, s); break;
+    case 2: launch_rk5_seg<MT<2>, 2>(b, ctx, s); break;
+    case 3: launch_rk5_seg<MT<3>, 3>(b, ctx, s); break;
+    case 4: launch_rk5_seg<MT<4>, 4>(b, ctx, s); break;
+    default: break;
+  }
+}
+
+bool StepProposerSupported(int model, int np) {
+  return np >= 1 && np <= 2 && (model == RK5_AEIF_COND_BETA || model == RK5_AEIF_COND_ALPHA);
+}
+
+bool Rk5BatchSupported(int model, int np) {
+  return np <= 4 && model >= RK5_AEIF_COND_BETA && model <= RK5_IZHIKEVICH_COND_BETA;
+}
+
+void LaunchRk5Batch(const Rk5Batch &b, StepCtx *ctx, cudaStream_t s) {
+  if (b.n_blocks <= 0) return;
+  switch (b.model) {
+    case RK5_AEIF_COND_BETA: launch_rk5_seg_model<AeifCondBeta>(b, ctx, s); break;
+    case RK5_AEIF_COND_ALPHA: launch_rk5_seg_model<AeifCondAlpha>(b, ctx, s); break;
+    case RK5_AEIF_PSC_ALPHA: launch_rk5_seg_model<AeifPscAlpha>(b, ctx, s); break;
+    case RK5_AEIF_PSC_EXP: launch_rk5_seg_model<AeifPscExp>(b, ctx, s); break;
+    case RK5_AEIF_PSC_DELTA: launch_rk5_seg<AeifPscDelta<1>, 1>(b, ctx, s); break;
+    case RK5_IZHIKEVICH_COND_BETA: launch_rk5_seg_model<IzhCondBeta>(b, ctx, s); break;
+    default: break;
+  }
+}
+
+}  // namespace ngpu

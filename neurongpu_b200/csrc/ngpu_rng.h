@@ -34,7 +34,8 @@ enum RngTag : uint32_t {
   RNG_TAG_POISSON_NODE = 2,     // CreatePoissonGenerator nodes
   RNG_TAG_CONNECT = 3,          // host connection rules
   RNG_TAG_ARRAY = 4,            // RandomUniform / RandomNormal arrays
-  RNG_TAG_SOURCE_SET = 5        // per-target source sampling
+  RNG_TAG_SOURCE_SET = 5,       // per-target source sampling
+  RNG_TAG_MLP = 6               // step-proposer training samples
 };
 
 struct Philox4 {

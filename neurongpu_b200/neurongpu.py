@@ -241,6 +241,18 @@ _EXT_SIG = {
     "NGB200_NConnections": (ctypes.c_longlong, ()),
     "NGB200_GetAllConnections": (ctypes.c_longlong, (c_int_p, c_int_p, c_int_p, c_int_p,
                                                      c_float_p, c_float_p)),
+    "NGB200_SetRk5Batching": (_I, (_I,)),
+    "NGB200_Rk5BatchOf": (_I, (_I,)),
+    "NGB200_SetStepLog": (_I, (_I, _I)),
+    "NGB200_GetStepLogCount": (ctypes.c_longlong, (_I,)),
+    "NGB200_GetStepLog": (_I, (_I, c_float_p, _I)),
+    "NGB200_TrainStepProposer": (_I, (_I, _I, _F, ctypes.c_ulonglong, c_float_p, c_float_p)),
+    "NGB200_SetStepProposer": (_I, (_I, _I)),
+    "NGB200_SetStepProposerParams": (_I, (c_float_p,)),
+    "NGB200_GetStepProposerParams": (_I, (c_float_p,)),
+    "NGB200_SetStepProposerMargin": (_I, (_F,)),
+    "NGB200_MlpGradients": (_F, (c_float_p, _I, c_float_p, c_float_p)),
+    "NGB200_MlpInfer": (_I, (c_float_p, _I, c_float_p, c_float_p)),
     "NGB200_LastSimulateDeviceMs": (ctypes.c_double, ()),
     "NGB200_SetKernelTiming": (_I, (_I,)),
     "NGB200_GetKernelTiming": (_I, (_I, ctypes.POINTER(ctypes.c_double),
@@ -1188,6 +1200,92 @@ class Binding(object):
 
     def NConnections(self):
         return self._call("NGB200_NConnections")
+
+    def SetRk5Batching(self, on):
+        """Extension: one RK5 launch per step for all groups of one model and
+        port count (default on); call before the first simulation."""
+        return self._call("NGB200_SetRk5Batching", ctypes.c_int(1 if on else 0))
+
+    def Rk5BatchOf(self, i_node):
+        return self._call("NGB200_Rk5BatchOf", ctypes.c_int(i_node))
+
+    # -- learned RK5 step proposer (extension) ------------------------------
+    MLP_NPARAM = 1313
+
+    @staticmethod
+    def _node_index(nodes):
+        if nodes is None:
+            return -1
+        if isinstance(nodes, NodeSeq):
+            return nodes.i0
+        return int(nodes)
+
+    def SetStepLog(self, nodes, capacity):
+        """Log accepted RK5 sub-steps of the group of `nodes` (None: every
+        supported group) for training the step proposer."""
+        return self._call("NGB200_SetStepLog", ctypes.c_int(self._node_index(nodes)),
+                          ctypes.c_int(capacity))
+
+    def GetStepLogCount(self, nodes=None):
+        return self._call("NGB200_GetStepLogCount", ctypes.c_int(self._node_index(nodes)))
+
+    def GetStepLog(self, nodes=None, max_rows=1 << 20):
+        import numpy as np
+        out = np.zeros((max_rows, 8), dtype=np.float32)
+        n = self._call("NGB200_GetStepLog", ctypes.c_int(self._node_index(nodes)),
+                       out.ctypes.data_as(c_float_p), ctypes.c_int(max_rows))
+        return out[:n]
+
+    def TrainStepProposer(self, steps=4000, blocks=64, lr=3e-3, seed=1):
+        """Trains the proposer on the logged sub-steps on the GPU; returns
+        (rows, loss over the first 5% of steps, loss over the last 5%)."""
+        l0, l1 = ctypes.c_float(0.0), ctypes.c_float(0.0)
+        n = self._call("NGB200_TrainStepProposer", ctypes.c_int(steps), ctypes.c_int(blocks),
+                       ctypes.c_float(lr), ctypes.c_ulonglong(seed), ctypes.byref(l0),
+                       ctypes.byref(l1))
+        return n, l0.value, l1.value
+
+    def SetStepProposer(self, nodes, on=True):
+        return self._call("NGB200_SetStepProposer", ctypes.c_int(self._node_index(nodes)),
+                          ctypes.c_int(1 if on else 0))
+
+    def SetStepProposerParams(self, params):
+        import numpy as np
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        if p.size != self.MLP_NPARAM:
+            raise ValueError("the step proposer has %d parameters" % self.MLP_NPARAM)
+        return self._call("NGB200_SetStepProposerParams", p.ctypes.data_as(c_float_p))
+
+    def GetStepProposerParams(self):
+        import numpy as np
+        p = np.zeros(self.MLP_NPARAM, dtype=np.float32)
+        self._call("NGB200_GetStepProposerParams", p.ctypes.data_as(c_float_p))
+        return p
+
+    def SetStepProposerMargin(self, margin):
+        return self._call("NGB200_SetStepProposerMargin", ctypes.c_float(margin))
+
+    def MlpGradients(self, data, params):
+        """Mean gradient and loss of the GPU training kernels over the rows
+        of `data` ([n, 8]: 6 features, target, unused)."""
+        import numpy as np
+        d = np.ascontiguousarray(data, dtype=np.float32)
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        g = np.zeros(self.MLP_NPARAM, dtype=np.float32)
+        loss = self._call("NGB200_MlpGradients", d.ctypes.data_as(c_float_p),
+                          ctypes.c_int(d.shape[0]), p.ctypes.data_as(c_float_p),
+                          g.ctypes.data_as(c_float_p))
+        return g, loss
+
+    def MlpInfer(self, x6, params):
+        """Tensor-core inference of the proposer network on rows of 6 features."""
+        import numpy as np
+        x = np.ascontiguousarray(x6, dtype=np.float32)
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        out = np.zeros(x.shape[0], dtype=np.float32)
+        self._call("NGB200_MlpInfer", x.ctypes.data_as(c_float_p), ctypes.c_int(x.shape[0]),
+                   p.ctypes.data_as(c_float_p), out.ctypes.data_as(c_float_p))
+        return out
 
     def GetAllConnections(self):
         """Every connection as numpy arrays (source, target, port, syn_group,

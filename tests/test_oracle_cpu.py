@@ -107,3 +107,30 @@ def test_oracle_poisson_drive_statistics():
         p = math.exp(-2.0) * 2.0 ** k / math.factorial(k)
         f = np.mean(counts == k)
         assert abs(f - p) < 4 * math.sqrt(p * (1 - p) / counts.size) + 1e-4
+
+
+def test_mlp_oracle_gradient_finite_differences():
+    """The FP64 proposer-network oracle's backpropagation agrees with central
+    finite differences (pins the oracle used to check the GPU kernels)."""
+    from oracle import mlp
+    rng = np.random.default_rng(5)
+    P = rng.normal(0.0, 0.3, mlp.NPARAM)
+    data = np.concatenate([rng.normal(0.0, 1.0, (50, 6)), rng.normal(-2.0, 1.0, (50, 1))], axis=1)
+    loss, g = mlp.loss_and_grad(P, data)
+    eps = 1e-6
+    for k in list(range(0, mlp.NPARAM, 37)) + [mlp.B3, mlp.W3 + 3, mlp.B1 + 5]:
+        Pp, Pm = P.copy(), P.copy()
+        Pp[k] += eps
+        Pm[k] -= eps
+        fd = (mlp.loss_and_grad(Pp, data)[0] - mlp.loss_and_grad(Pm, data)[0]) / (2 * eps)
+        assert abs(fd - g[k]) <= 1e-6 + 1e-5 * abs(fd), (k, fd, g[k])
+
+
+def test_mlp_oracle_bf16_rounding():
+    from oracle import mlp
+    x = np.array([1.0, 1.00390625, 1.005859375, -3.14159, 1e-3], dtype=np.float32)
+    r = mlp.bf16(x)
+    assert r[0] == 1.0 and r[1] == 1.0           # tie rounds to even
+    assert r[2] == 1.0078125
+    assert abs(r[3] + 3.140625) < 1e-12
+    assert abs(r[4] - 1e-3) < 1e-5
