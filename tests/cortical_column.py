@@ -128,7 +128,8 @@ def build(ngpu, n_scaling=1.0, k_scaling=1.0, seed=12349, dt=0.1):
 def oracle_network(ngpu, pops, gens, d, seed, dt=0.1):
     """The same network on the FP64 oracle: identical nodes, initial
     membrane potentials, parameters and every connection (read back in bulk),
-    so that the Poisson draws agree draw by draw."""
+    so that the Poisson draws agree draw by draw. Call it before the first
+    simulation: it copies the current membrane potentials."""
     from oracle import oracle as orc
     net = orc.Network(dt=dt, seed=seed)
     E_L = NEURON["E_L"]

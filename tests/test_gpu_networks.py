@@ -66,9 +66,10 @@ def test_cortical_column_scaled_vs_oracle(ngpu):
     n_total = int(sum(sizes))
     for p in pops:
         ngpu.ActivateRecSpikeTimes(p, 500)
+    # the oracle copies the initial state, so it is built before simulating
+    net = cc.oracle_network(ngpu, pops, gens, d, seed=seed)
     ngpu.Simulate(1200.0)
     g_steps, g_nodes = _gpu_spikes(ngpu, first[0], n_total)
-    net = cc.oracle_network(ngpu, pops, gens, d, seed=seed)
     net.simulate(12000)
     o_steps, o_nodes = net.spikes()
     assert len(o_steps) > 1000
