@@ -234,13 +234,79 @@ def run_reference(args, world, rank):
     return 0
 
 
+def run_sweep(args, world, rank):
+    """Batched + learned workload: 256 independent AdEx networks (sizes
+    log-uniform in 1k-50k, in-degree 100-500, a, b and Poisson rate on a
+    seeded grid), all RK5 groups integrated by one batched launch per step.
+    Phases: plain controller with accepted-step logging, GPU training of the
+    step proposer, then the same networks continued with the plain and with
+    the learned controller; prints one JSON line comparing them."""
+    from tests import sweep
+    from neurongpu_b200 import neurongpu as ngpu
+    b = ngpu.default_binding()
+    b.SetVerbosityLevel(0)
+    if args.no_batch:
+        b.SetRk5Batching(False)
+    grid = sweep.sweep_grid(args.nets, 1000, 50000, 100, 500, seed=2024)
+    t0 = time.perf_counter()
+    nets = sweep.build_sweep(b, grid, w_pg=args.sweep_w_pg)
+    ngpu.Calibrate()
+    build_s = time.perf_counter() - t0
+    n_tot = sum(p["n"] for p in grid)
+    b.SetStepLog(None, args.log_cap)
+    b.Simulate(args.step_ms)
+    logged = b.GetStepLogCount(None)
+    t1 = time.perf_counter()
+    rows, l0, l1 = b.TrainStepProposer(steps=args.train_steps, blocks=64, lr=3e-3, seed=5)
+    train_s = time.perf_counter() - t1
+
+    def phase():
+        e0, s0, ms = b.StageEvaluations(), b.TotalSpikes(), 0.0
+        for _ in range(args.steps):
+            b.Simulate(args.step_ms)
+            ms += b.LastSimulateDeviceMs()
+        steps = n_tot * args.steps * args.step_ms / 0.1
+        bio = args.steps * args.step_ms / 1000.0
+        return {"bio_s_per_wall_s": bio / (ms / 1000.0), "device_ms": ms,
+                "stage_evals_per_neuron_step": (b.StageEvaluations() - e0) / steps,
+                "mean_rate_hz": (b.TotalSpikes() - s0) / (n_tot * bio)}
+    for _ in range(args.warmup):
+        b.Simulate(args.step_ms)
+    plain = phase()
+    b.SetStepProposer(None, True)
+    for _ in range(args.warmup):
+        b.Simulate(args.step_ms)
+    learned = phase()
+    line = {"metric": "sweep_bio_s_per_wall_s", "value": plain["bio_s_per_wall_s"],
+            "unit": "bio_s/wall_s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "sweep: %d aeif_cond_beta networks, %d neurons, sizes "
+                                   "log-uniform 1k-50k, in-degree 100-500, a 0-8 nS, b 0-150 pA, "
+                                   "Poisson 10-30 kHz w %g nS, dt 0.1 ms, RK5 eps 1e-3"
+                                   % (len(grid), n_tot, args.sweep_w_pg),
+                       "batched_launch": not args.no_batch, "step_bio_ms": args.step_ms},
+            "build_s": build_s, "logged_substeps": logged, "train_rows": rows,
+            "train_loss_first": l0, "train_loss_last": l1, "train_s": train_s,
+            "plain": plain, "learned": learned,
+            "stage_eval_reduction": 1.0 - learned["stage_evals_per_neuron_step"]
+            / plain["stage_evals_per_neuron_step"],
+            "rk5_tuning": b.GetRk5Tuning(nets[0].i0)}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours")
-    ap.add_argument("--config", default="scale", choices=["scale", "small"])
+    ap.add_argument("--config", default="scale", choices=["scale", "small", "sweep"])
+    ap.add_argument("--nets", type=int, default=256, help="sweep: number of networks")
+    ap.add_argument("--sweep-w-pg", type=float, default=0.2, help="sweep: Poisson weight (nS)")
+    ap.add_argument("--log-cap", type=int, default=65536, help="sweep: logged sub-steps per group")
+    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--no-batch", action="store_true", help="sweep: one RK5 launch per network")
     ap.add_argument("--step-ms", type=float, default=100.0)
     ap.add_argument("--cpu-sample", type=int, default=4000)
     ap.add_argument("--cpu-ms", type=float, default=200.0)
@@ -258,6 +324,8 @@ def main():
     if args.impl == "reference":
         return run_reference(args, world, rank)
     os.environ.setdefault("CUDA_VISIBLE_DEVICES", str(local))
+    if args.config == "sweep":
+        return run_sweep(args, world, rank)
     cfg = SCALE if args.config == "scale" else SMALL
     from neurongpu_b200 import neurongpu as ngpu
     b = ngpu.default_binding()
