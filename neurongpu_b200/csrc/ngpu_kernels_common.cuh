@@ -153,7 +153,7 @@ template <class M, int NP>
 __device__ __forceinline__ void rk5_step(double &x, float *y, float &h,
                                          float h_min, float h_max,
                                          const float *p, const float *q,
-                                         float refr, int np, float eps,
+                                         float refr, int np, float inv_eps,
                                          unsigned &evals, float &h_acc, float &err_acc) {
   using namespace rk5c;
   constexpr int NV = M::NVAR;
@@ -196,11 +196,12 @@ __device__ __forceinline__ void rk5_step(double &x, float *y, float &h,
     for (int i = 0; i < NV; i++) {
       float val = h * (e1 * k1[i] + e3 * k3[i] + e4 * k4[i] + e5 * k5[i]
                        + e6 * k6[i]);
-      val /= ys[i];
-      float av = fabsf(val);
+      // scaled error |val| / ys: an approximate quotient (2 ulp) instead of
+      // the IEEE division, which costs a dozen instructions per variable
+      float av = fabsf(__fdividef(val, ys[i]));
       err = (err > av) ? err : av;
     }
-    err /= eps;
+    err *= inv_eps;
     if (err <= 1.0f || (double)h <= (double)h_min * (1.0 + 1.0e-5)) break;
     if (guard >= 256) break;
     float h_new = h * coeff * ctrl_pow(err, exp_dec);
@@ -336,35 +337,41 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
   double x = t0 + (double)g.dt * (double)it + (active ? (double)g.dx[i] : 0.0);
   float h = active ? g.h[i] : 0.0f;
   const float h_min = g.h_min;
+  const float inv_eps = 1.0f / g.eps;
   const long long T = T0 + it + 1;
   const int den = (int)roundf(p[Tr::den] / g.dt);
   bool end_step = !active;
   int guard = 0;
   float h_acc, err_acc;
   if constexpr (MODE == STEP_LEARNED) {
-    bool ready = false, failed = false;
+    bool staged = false, failed = false;
+    proposer_alloc(*ps);
     while (__syncthreads_or(!end_step)) {
       const float hmax = active ? (float)(x1 - x) : 0.0f;
       const bool want = !end_step && !failed && h < hmax;
       if (__syncthreads_or(want)) {
-        if (!ready) {
-          proposer_setup(*ps, g.mlp);
-          ready = true;
+        if (!staged) {
+          proposer_stage_weights(*ps, g.mlp);
+          staged = true;
         }
         float f[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
         if (want) ProposerFeatures<M>::get(y, p, h, g.dt, f);
         float o = 0.0f;
         if (proposer_round(*ps, want, f, o, &ctx->err)) {
           if (want) {
+            // the proposal may shrink the controller's guess by at most 4x
+            // (after a low-error step it then still grows, >= 1.25x) and
+            // enlarge it by at most 16x: a network queried outside its
+            // training distribution cannot stall or blow up the integration
             const float hp = g.dt * exp2f(o - g.mlp_margin);
-            h = fminf(fmaxf(hp, h_min), hmax);
+            h = fminf(fmaxf(fminf(fmaxf(hp, 0.25f * h), 16.0f * h), h_min), hmax);
           }
         } else {
           failed = true;
         }
       }
       if (!end_step) {
-        rk5_step<M, NP>(x, y, h, h_min, hmax, p, q, refr, np, g.eps, evals, h_acc, err_acc);
+        rk5_step<M, NP>(x, y, h, h_min, hmax, p, q, refr, np, inv_eps, evals, h_acc, err_acc);
         end_step = (x >= x1 - (double)h_min);
         if (M::external(y, p, refr, end_step, g.dt)) {
           if (!dry) push_spike(pa, ctx, g.i_node_0 + i, i, 1.0f, T, x1, den);
@@ -375,7 +382,7 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
         }
       }
     }
-    proposer_teardown(*ps, ready, failed);
+    proposer_teardown(*ps, failed);
   } else {
     while (!end_step) {
       const float hmax = (float)(x1 - x);
@@ -387,7 +394,7 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
           lg = true;
         }
       }
-      rk5_step<M, NP>(x, y, h, h_min, hmax, p, q, refr, np, g.eps, evals, h_acc, err_acc);
+      rk5_step<M, NP>(x, y, h, h_min, hmax, p, q, refr, np, inv_eps, evals, h_acc, err_acc);
       if constexpr (MODE == STEP_LOG) {
         if (lg) log_step_sample(g, f, proposer_target(h_acc, err_acc, g.dt));
       }

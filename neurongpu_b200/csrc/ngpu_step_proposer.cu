@@ -167,11 +167,12 @@ k_mlp_infer(const float *__restrict__ x6, int n, const MlpImage *img, float *out
 #pragma unroll
     for (int k = 0; k < 6; k++) f[k] = x6[(size_t)i * 6 + k];
   }
-  proposer_setup(ps, img);
+  proposer_alloc(ps);
+  proposer_stage_weights(ps, img);
   float o = 0.0f;
   const bool ok = proposer_round(ps, want, f, o, err);
   if (want) out[i] = ok ? o : __int_as_float(0x7fc00000);
-  proposer_teardown(ps, true, !ok);
+  proposer_teardown(ps, !ok);
 }
 
 // ---------------------------------------------------------------------------

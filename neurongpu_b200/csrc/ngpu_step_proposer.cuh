@@ -210,9 +210,30 @@ struct __align__(1024) ProposerSmem {
   uint32_t phase;               // parity of the barrier phase to wait for next
 };
 
-// Stages the weights, allocates 32 TMEM columns (warp 0) and initialises the
-// completion barrier. Called by every thread of the CTA (CTA-uniform branch).
-__device__ __forceinline__ void proposer_setup(ProposerSmem &s, const MlpImage *img) {
+// Allocates the CTA's 32 TMEM columns (warp 0) and initialises the completion
+// barrier; called by every thread at kernel start. The allocation is made
+// and its permit relinquished up front in every CTA: a CTA that still holds
+// the allocation permit would keep further CTAs of the kernel from starting
+// on its SM.
+__device__ __forceinline__ void proposer_alloc(ProposerSmem &s) {
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    s.phase = 0;
+    mbar_init(&s.mbar, 1);
+  }
+  // K columns 8..15 of the feature tile stay zero
+  if (tid < 128) {
+    *reinterpret_cast<uint4 *>(s.a + umma_kmajor_off(tid, 8, 16)) = make_uint4(0, 0, 0, 0);
+  }
+  if ((tid >> 5) == 0) tmem_alloc32(&s.tmem);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+}
+
+// Stages the weights in shared memory (every thread; CTA-uniform branch,
+// before the first proposal round of the launch).
+__device__ __forceinline__ void proposer_stage_weights(ProposerSmem &s, const MlpImage *img) {
   const int tid = threadIdx.x;
   const uint32_t *src1 = img->w1;
   const uint32_t *src2 = img->w2;
@@ -224,20 +245,9 @@ __device__ __forceinline__ void proposer_setup(ProposerSmem &s, const MlpImage *
     s.b2[tid] = img->b2[tid];
     s.w3[tid] = img->w3[tid];
   }
-  if (tid == 0) {
-    s.b3 = img->b3;
-    s.phase = 0;
-    mbar_init(&s.mbar, 1);
-  }
-  // K columns 8..15 of the feature tile stay zero
-  if (tid < 128) {
-    *reinterpret_cast<uint4 *>(s.a + umma_kmajor_off(tid, 8, 16)) = make_uint4(0, 0, 0, 0);
-  }
-  if ((tid >> 5) == 0) tmem_alloc32(&s.tmem);
+  if (tid == 0) s.b3 = img->b3;
   proxy_fence_async_smem();
-  tc_fence_before();
   __syncthreads();
-  tc_fence_after();
 }
 
 // One proposal round for the whole CTA: every thread with want != 0 passes
@@ -324,8 +334,7 @@ __device__ __forceinline__ bool proposer_round(ProposerSmem &s, bool want, const
 // Releases the CTA's tensor memory (all threads; warp 0 deallocates). After
 // a timed-out wait the tensor-core work may still be in flight: wait for the
 // outstanding completion (bounded) before the columns are released.
-__device__ __forceinline__ void proposer_teardown(ProposerSmem &s, bool ready, bool failed) {
-  if (!ready) return;
+__device__ __forceinline__ void proposer_teardown(ProposerSmem &s, bool failed) {
   if (failed) mbar_wait(&s.mbar, s.phase, 1 << 22);
   tc_fence_before();
   __syncthreads();
