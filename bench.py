@@ -136,13 +136,15 @@ def traffic_per_unit():
         return {}
 
 
-def cpu_baseline(cfg, n_sample=2000, sim_ms=20.0, threads=1):
+def cpu_baseline(cfg, n_sample=2000, sim_ms=20.0, threads=0):
     """FP64 CPU oracle on a bounded sample of the workload: n_sample neurons
     with the same in-degree, rates and delays, sim_ms of biological time.
     Returns bio-s per wall-s scaled to the full network size (cost linear in
     the number of neurons at fixed in-degree)."""
     import numpy as np
     from oracle import oracle as orc
+    orc.set_threads(threads if threads > 0 else (os.cpu_count() or 1))
+    threads = orc.get_threads()
     rng = np.random.default_rng(1234)
     n = n_sample
     ne = int(0.8 * n)
@@ -160,6 +162,7 @@ def cpu_baseline(cfg, n_sample=2000, sim_ms=20.0, threads=1):
         src = np.concatenate([ne + rng.choice(n - ne, size=ki, replace=False) for _ in range(n)])
         net.connect(src + 1, np.repeat(np.arange(n) + 1, ki), 1, cfg["w_inh"], float(d))
     steps = int(round(sim_ms / 0.1))
+    net.simulate(1)             # builds the oracle's connection tables (untimed)
     t0 = time.perf_counter()
     net.simulate(steps)
     wall = time.perf_counter() - t0
@@ -308,8 +311,8 @@ def main():
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--no-batch", action="store_true", help="sweep: one RK5 launch per network")
     ap.add_argument("--step-ms", type=float, default=100.0)
-    ap.add_argument("--cpu-sample", type=int, default=4000)
-    ap.add_argument("--cpu-ms", type=float, default=200.0)
+    ap.add_argument("--cpu-sample", type=int, default=16000)
+    ap.add_argument("--cpu-ms", type=float, default=100.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-gpu", action="store_true")
     ap.add_argument("--n", type=int, default=0, help="override the number of neurons")

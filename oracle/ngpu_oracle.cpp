@@ -32,7 +32,11 @@
 #include <stdint.h>
 #include <string.h>
 #include <algorithm>
+#include <utility>
 #include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 #include "../neurongpu_b200/csrc/ngpu_rng.h"
 
@@ -407,6 +411,8 @@ static void prepare(Oracle &o) {
 static void fold(Oracle &o, long long T_pending, bool poisson) {
   const int N = (int)o.node_group.size();
   double t = (double)T_pending * (double)(float)o.dt;
+  // every node folds only its own accumulators and state
+#pragma omp parallel for schedule(static)
   for (int n = 0; n < N; n++) {
     Group &g = o.groups[o.node_group[n]];
     int i = n - g.i0;
@@ -439,6 +445,62 @@ static void step(Oracle &o, int it_in_session) {
   o.spikes_at[(size_t)(T % o.spikes_at.size())].clear();
   (void)it_in_session;
   for (Group &g : o.groups) {
+    // node updates are independent: RK5 and iaf groups are updated in
+    // parallel, each thread collecting its spikes in node order; the lists
+    // are merged in thread (= node) order, so the result does not depend on
+    // the number of threads
+    if (g.model <= O_IZH_COND_BETA || g.model == O_IAF_PSC_EXP) {
+      int nthr = 1;
+#ifdef _OPENMP
+      nthr = omp_get_max_threads();
+#endif
+      std::vector<std::vector<std::pair<int, real>>> part(nthr);
+      std::vector<long long> evals(nthr, 0);
+#pragma omp parallel num_threads(nthr)
+      {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        const int chunk = (g.n + nthr - 1) / nthr;
+        const int i0 = std::min(g.n, tid * chunk), i1 = std::min(g.n, i0 + chunk);
+        for (int i = i0; i < i1; i++) {
+          real *y = &g.var[(size_t)i * g.nvar];
+          real *p = &g.param[(size_t)i * g.nparam];
+          int node = g.i0 + i;
+          if (g.model <= O_IZH_COND_BETA) {
+            real h_min = g.h_min_rel * o.dt;
+            real &x = g.x[i];
+            real &h = g.h[i];
+            bool end = false;
+            int guard = 0;
+            while (!end && guard++ < 200000) {
+              real hmax = x1 - x;
+              rk5_step(g.model, g.model == O_AEIF_PSC_DELTA ? 0 : g.np, g.nvar, x, y, h, h_min,
+                       hmax, p, g.eps, evals[tid]);
+              end = (x >= x1 - h_min);
+              if (external_update(g.model, y, p, end, o.dt)) part[tid].push_back({node, 1.0});
+            }
+          } else {
+            real &I_ex = y[0], &I_in = y[1], &V = y[2], &refr = y[3];
+            if (refr > 0) refr -= 1;
+            else V = V * p[15] + I_ex * p[13] + I_in * p[14] + p[3] * p[10];
+            I_ex *= p[11];
+            I_in *= p[12];
+            if (V >= p[4]) {
+              part[tid].push_back({node, 1.0});
+              V = p[5];
+              refr = round(p[8] / o.dt);
+            }
+          }
+        }
+      }
+      for (int t = 0; t < nthr; t++) {
+        g.evals += evals[t];
+        for (const auto &sp : part[t]) push(o, sp.first, sp.second, T);
+      }
+      continue;
+    }
     for (int i = 0; i < g.n; i++) {
       real *y = &g.var[(size_t)i * g.nvar];
       real *p = &g.param[(size_t)i * g.nparam];
@@ -542,6 +604,24 @@ void *orc_create(double dt, unsigned long long seed) {
 }
 
 void orc_free(void *h) { delete (Oracle *)h; }
+
+// host threads of the parallel node-update and fold loops (results do not
+// depend on it)
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+int orc_get_threads() {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
 
 // params: [n][nparam]; vars: [n][nvar]
 int orc_add_group(void *h, int model, int n, int np, int nvar, int nparam,

@@ -88,6 +88,8 @@ def _load():
     lib.orc_get_state.argtypes = (ctypes.c_void_p, ctypes.c_int, _dp, _dp)
     lib.orc_stage_evals.restype = ctypes.c_longlong
     lib.orc_stage_evals.argtypes = (ctypes.c_void_p,)
+    lib.orc_set_threads.argtypes = (ctypes.c_int,)
+    lib.orc_get_threads.restype = ctypes.c_int
     return lib
 
 
@@ -99,6 +101,16 @@ def lib():
     if _lib is None:
         _lib = _load()
     return _lib
+
+
+def set_threads(n):
+    """Host threads of the oracle's parallel node-update loops (results are
+    independent of the thread count)."""
+    lib().orc_set_threads(int(n))
+
+
+def get_threads():
+    return lib().orc_get_threads()
 
 
 def _ptr(a, t):

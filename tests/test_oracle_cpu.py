@@ -134,3 +134,28 @@ def test_mlp_oracle_bf16_rounding():
     assert r[2] == 1.0078125
     assert abs(r[3] + 3.140625) < 1e-12
     assert abs(r[4] - 1e-3) < 1e-5
+
+
+def test_oracle_thread_count_independent():
+    """The oracle's parallel node updates give identical results for any
+    number of host threads (spikes merged in node order)."""
+    def run(threads):
+        orc.set_threads(threads)
+        rng = np.random.default_rng(3)
+        n = 300
+        net = orc.Network(dt=0.1, seed=9)
+        net.create(orc.POISSON_GENERATOR, 1, params={"rate": 20000.0})
+        net.create(orc.AEIF_COND_BETA, n, 2, params={"E_rev": [0.0, -85.0]}, eps=1e-3)
+        src = rng.integers(1, n + 1, 20 * n)
+        tgt = np.repeat(np.arange(1, n + 1), 20)
+        net.connect(src, tgt, 0, 0.5, 1.0)
+        net.connect(np.zeros(n, dtype=np.int32), np.arange(1, n + 1), 0, 0.5, 0.1)
+        out = net.simulate(300, record=[(5, 0), (77, 0)])
+        s, nd = net.spikes()
+        return out, s, nd, net.stage_evals()
+    a = run(1)
+    b = run(4)
+    orc.set_threads(1)
+    assert len(a[1]) > 0
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    assert np.array_equal(a[2], b[2]) and a[3] == b[3]
