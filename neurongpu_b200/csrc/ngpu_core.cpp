@@ -81,6 +81,10 @@ void NeuronGPU::FreeDevice() {
   F(d_last_spike_T_); F(d_last_rev_T_); F(d_last_post_T_); F(d_last_spike_h_);
   F(d_grp_off_); F(d_e_slot_); F(d_e_w_); F(d_e_syn_); F(d_e_stamp_);
   F(d_e_post_); F(d_rev_off_); F(d_rev_edge_); F(d_delays_);
+  F(d_rev_src_); F(d_rev_cnt_);
+  d_rev_src_ = nullptr;
+  d_rev_cnt_ = nullptr;
+  rev_R_ = rev_C_ = 0;
   F(d_dc_off_); F(d_dc_gen_); F(d_dc_port_); F(d_dc_w_); F(d_dc_delay_);
   F(d_dc_stream_); F(d_gen_rate_); F(d_gen_origin_); F(d_gen_start_);
   F(d_gen_stop_); F(d_gen_lambda_); F(d_gen_explam_); F(d_gen_cdf_); F(d_blk_events_); F(d_done_);
@@ -969,6 +973,10 @@ PushArgs NeuronGPU::MakePushArgs(NodeGroup *g) {
   pa.rec_times = g->d_rec_times;
   pa.n_rec = g->d_n_rec;
   pa.max_rec = g->max_rec;
+  pa.rev_src = d_rev_src_;
+  pa.rev_cnt = d_rev_cnt_;
+  pa.rev_R = rev_R_;
+  pa.rev_C = rev_C_;
   return pa;
 }
 
@@ -998,6 +1006,10 @@ DeliverArgs NeuronGPU::MakeDeliverArgs() {
   d.advance_flags = 0;
   d.ring_cnt_w = d_ring_cnt_;
   d.done = d_done_;
+  d.rev_src = d_rev_src_;
+  d.rev_cnt = d_rev_cnt_;
+  d.rev_R = rev_R_;
+  d.rev_C = rev_C_;
   return d;
 }
 
@@ -1311,6 +1323,7 @@ void NeuronGPU::BuildDevice() {
   NGPU_CUDA(cudaMemset(d_done_, 0, sizeof(unsigned)));
   NGPU_CUDA(cudaMalloc(&d_blk_events_, sizeof(unsigned long long) * deliver_blocks_));
   NGPU_CUDA(cudaMemset(d_blk_events_, 0, sizeof(unsigned long long) * deliver_blocks_));
+  int max_den_steps = 0;
   for (NodeGroup *g : groups_) {
     if (g->mi->kind == MK_RK5) {
       g->n_blocks = (g->n_node + 127) / 128;
@@ -1322,9 +1335,21 @@ void NeuronGPU::BuildDevice() {
       std::vector<float> dd(g->n_node);
       NGPU_CUDA(cudaMemcpy(dd.data(), g->d_param + (size_t)g->mi->den_delay_param * g->n_pad,
                            sizeof(float) * g->n_node, cudaMemcpyDeviceToHost));
-      for (int i = 0; i < g->n_node; i++)
-        if ((int)roundf(dd[i] / time_resolution_) > 0) has_out_[g->i_node_0 + i] = 1;
+      for (int i = 0; i < g->n_node; i++) {
+        const int dsteps = (int)roundf(dd[i] / time_resolution_);
+        if (dsteps > 0) has_out_[g->i_node_0 + i] = 1;
+        max_den_steps = std::max(max_den_steps, dsteps);
+      }
     }
+  }
+  // dendritic-delay ring: spikes reaching their own node's dendrites
+  // (STDP post rule) up to max_den_steps steps later
+  if (plastic_) {
+    rev_R_ = max_den_steps + 1;
+    rev_C_ = ring_C_;
+    NGPU_CUDA(cudaMalloc(&d_rev_src_, sizeof(unsigned) * (size_t)rev_R_ * rev_C_));
+    NGPU_CUDA(cudaMalloc(&d_rev_cnt_, sizeof(int) * rev_R_));
+    NGPU_CUDA(cudaMemset(d_rev_cnt_, 0, sizeof(int) * rev_R_));
   }
   // synapse group table
   memset(&syn_table_, 0, sizeof(syn_table_));
@@ -1525,6 +1550,7 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
   DeliverArgs d = MakeDeliverArgs();
   const bool has_delivery = d.nd > 0;
   if (has_delivery && !plastic_) d.advance_flags = flags;
+  if (plastic_ && rev_R_ > 1) LaunchRevArrive(d, d_ctx_, stream_);
   LaunchDeliver(d, syn_table_, d_ctx_, deliver_blocks_, stream_);
   if (ktime_) KEvent(step_in_chunk, 2);
   if (plastic_) {
@@ -1632,6 +1658,7 @@ void NeuronGPU::CheckDeviceErrors() {
     if (e & DERR_RK5_STUCK) m += " RK5 integration exceeded the substep limit;";
     if (e & DERR_REC_OVERFLOW) m += " recording buffer overflow;";
     if (e & DERR_PROPOSER_TIMEOUT) m += " a tensor-core wait of the step proposer timed out;";
+    if (e & DERR_REV_OVERFLOW) m += " a dendritic delay exceeds the one at calibration (or too many dendritic arrivals in one step);";
     throw ngpu_exception(m);
   }
 }

@@ -403,6 +403,10 @@ class NeuronGPU {
   int ring_R_ = 0, ring_C_ = 0;
   int *d_last_spike_T_ = nullptr, *d_last_rev_T_ = nullptr;
   int *d_last_post_T_ = nullptr;
+  // dendritic-delay ring of plastic networks (rev_R_ = max delay steps + 1)
+  unsigned *d_rev_src_ = nullptr;
+  int *d_rev_cnt_ = nullptr;
+  int rev_R_ = 0, rev_C_ = 0;
   float *d_last_spike_h_ = nullptr;
   unsigned long long *d_grp_off_ = nullptr;
   unsigned *d_e_slot_ = nullptr;

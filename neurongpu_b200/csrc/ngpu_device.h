@@ -33,7 +33,8 @@ enum DeviceError : unsigned {
   DERR_RK5_STUCK = 2u,          // adaptive integration exceeded substep cap
   DERR_REC_OVERFLOW = 4u,       // recording buffer overflow
   DERR_NAN_STATE = 8u,
-  DERR_PROPOSER_TIMEOUT = 16u   // a tensor-core completion wait of the step proposer timed out
+  DERR_PROPOSER_TIMEOUT = 16u,  // a tensor-core completion wait of the step proposer timed out
+  DERR_REV_OVERFLOW = 32u       // dendritic delay above its maximum or too many dendritic arrivals
 };
 
 struct StepCtx {
@@ -60,6 +61,11 @@ struct PushArgs {
   float *rec_times;             // [n * max_rec], may be null
   int *n_rec;
   int max_rec;
+  // dendritic-delay ring (plastic networks): nodes whose spike reaches their
+  // own dendrites in step T are listed in slot T % rev_R
+  unsigned *rev_src;
+  int *rev_cnt;
+  int rev_R, rev_C;
 };
 
 // Per-group input folding: acc (+ Poisson direct connections) into state.
@@ -188,8 +194,11 @@ struct DeliverArgs {
   int ring_R, ring_C;
   int nd;
   const int *delays;                   // [nd] distinct delays in steps
-  const int *last_rev_T;
+  int *last_rev_T;
   int *last_post_T;
+  const unsigned *rev_src;             // dendritic-delay ring (see PushArgs)
+  int *rev_cnt;
+  int rev_R, rev_C;
   const unsigned long long *rev_off;   // [n_nodes+1] incoming plastic edges
   const unsigned *rev_edge;
   float dt;

@@ -365,6 +365,7 @@ __device__ __forceinline__ void finish_step(const DeliverArgs &d, StepCtx *ctx) 
       __threadfence();
       if (d.advance_flags & 1) {
         const long long T = ctx->T0 + ctx->it + 1;
+        if (d.rev_cnt != nullptr) d.rev_cnt[(int)(T % d.rev_R)] = 0;
         int c = d.ring_cnt_w[(int)(T % d.ring_R)];
         ctx->n_spikes += (unsigned long long)(c < d.ring_C ? c : d.ring_C);
         d.ring_cnt_w[(int)((T + 1) % d.ring_R)] = 0;
@@ -525,6 +526,43 @@ void LaunchDeliver(const DeliverArgs &d, const SynGroupTable &syn,
 // STDP post-spike rule: neurons that spiked in this step, over their
 // incoming plastic synapses (src/rev_spike.cu:41-75)
 // ---------------------------------------------------------------------------
+// STDP post rule for one node whose spike reached its dendrites in step T:
+// every incoming plastic synapse with a pre-synaptic arrival stamp
+// 0 <= T - stamp < 16384 (src/rev_spike.cu:41-55); one warp per node,
+// a node is handled once per step.
+__device__ __forceinline__ void post_rule_node(const DeliverArgs &d, const SynGroupTable &syn,
+                                               unsigned node, long long T, int lane) {
+  int first = 0;
+  if (lane == 0) first = (atomicExch(&d.last_post_T[node], (int)T) != (int)T);
+  first = __shfl_sync(0xffffffffu, first, 0);
+  if (!first) return;
+  const unsigned long long beg = d.rev_off[node], end = d.rev_off[node + 1];
+  for (unsigned long long r = beg + lane; r < end; r += 32) {
+    const unsigned e = d.rev_edge[r];
+    const int sg = d.e_syn[e];
+    long long Dt_int = T - (long long)d.e_stamp[e];
+    if (sg > 0 && Dt_int >= 0 && Dt_int < NGPU_MAX_SYN_DT) {
+      d.e_w[e] = syn_update(syn, sg, d.e_w[e], d.dt * (float)Dt_int);
+    }
+  }
+}
+
+// Nodes whose spike reaches their dendrites in this step after a dendritic
+// delay: their last post-spike step is set before this step's deliveries
+// (src/spike_buffer.cu:299-301 runs before the delivery of the step).
+__global__ void k_rev_arrive(DeliverArgs d, StepCtx *ctx) {
+  const long long T = ctx->T0 + ctx->it + 1;
+  const int slot = (int)(T % d.rev_R);
+  int cnt = d.rev_cnt[slot];
+  cnt = cnt < d.rev_C ? cnt : d.rev_C;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x)
+    d.last_rev_T[d.rev_src[(long long)slot * d.rev_C + k]] = (int)T;
+}
+
+void LaunchRevArrive(const DeliverArgs &d, StepCtx *ctx, cudaStream_t s) {
+  k_rev_arrive<<<148, 256, 0, s>>>(d, ctx);
+}
+
 __global__ void __launch_bounds__(256)
 k_stdp_post(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
   const long long T = ctx->T0 + ctx->it + 1;
@@ -534,22 +572,19 @@ k_stdp_post(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int n_warps = (gridDim.x * blockDim.x) >> 5;
+  // spikes of this step without dendritic delay
   for (int item = warp; item < cnt; item += n_warps) {
     const unsigned node = d.ring_src[(long long)slot * d.ring_C + item];
     if (d.last_rev_T[node] != (int)T) continue;   // dendritic delay > 0
-    int first = 0;
-    if (lane == 0) first = (atomicExch(&d.last_post_T[node], (int)T) != (int)T);
-    first = __shfl_sync(0xffffffffu, first, 0);
-    if (!first) continue;
-    const unsigned long long beg = d.rev_off[node], end = d.rev_off[node + 1];
-    for (unsigned long long r = beg + lane; r < end; r += 32) {
-      const unsigned e = d.rev_edge[r];
-      const int sg = d.e_syn[e];
-      long long Dt_int = T - (long long)d.e_stamp[e];
-      if (sg > 0 && Dt_int >= 0 && Dt_int < NGPU_MAX_SYN_DT) {
-        d.e_w[e] = syn_update(syn, sg, d.e_w[e], d.dt * (float)Dt_int);
-      }
-    }
+    post_rule_node(d, syn, node, T, lane);
+  }
+  // spikes of earlier steps reaching the dendrites now
+  if (d.rev_cnt != nullptr) {
+    const int rslot = (int)(T % d.rev_R);
+    int rcnt = d.rev_cnt[rslot];
+    rcnt = rcnt < d.rev_C ? rcnt : d.rev_C;
+    for (int item = warp; item < rcnt; item += n_warps)
+      post_rule_node(d, syn, d.rev_src[(long long)rslot * d.rev_C + item], T, lane);
   }
   finish_step(d, ctx);
 }

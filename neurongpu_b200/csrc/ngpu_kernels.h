@@ -58,6 +58,8 @@ void LaunchDeliver(const DeliverArgs &d, const SynGroupTable &syn,
                    StepCtx *ctx, int n_blocks, cudaStream_t s);
 // resident 256-thread delivery blocks per SM (grid = SMs x this)
 int DeliverBlocksPerSM();
+// dendritic-delay arrivals of this step (before the delivery kernel)
+void LaunchRevArrive(const DeliverArgs &d, StepCtx *ctx, cudaStream_t s);
 void LaunchStdpPost(const DeliverArgs &d, const SynGroupTable &syn,
                     StepCtx *ctx, int n_blocks, cudaStream_t s);
 

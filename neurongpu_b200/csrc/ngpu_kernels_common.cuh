@@ -38,7 +38,20 @@ __device__ __forceinline__ void push_spike(const PushArgs &pa, StepCtx *ctx,
   }
   pa.last_spike_T[node] = (int)T;
   pa.last_spike_h[node] = height;
-  if (den_delay_steps == 0) pa.last_rev_T[node] = (int)T;
+  // the spike reaches the node's own dendrites (STDP post rule) at once or
+  // den_delay_steps later (src/spike_buffer.cu:164-167, 265-300)
+  if (den_delay_steps == 0) {
+    pa.last_rev_T[node] = (int)T;
+  } else if (pa.rev_cnt != nullptr) {
+    if (den_delay_steps < pa.rev_R) {
+      const int rs = (int)((T + den_delay_steps) % pa.rev_R);
+      const int rp = atomicAdd(&pa.rev_cnt[rs], 1);
+      if (rp < pa.rev_C) pa.rev_src[(long long)rs * pa.rev_C + rp] = (unsigned)node;
+      else atomicOr(&ctx->err, (unsigned)DERR_REV_OVERFLOW);
+    } else {
+      atomicOr(&ctx->err, (unsigned)DERR_REV_OVERFLOW);
+    }
+  }
   if (pa.spike_count != nullptr) pa.spike_count[local]++;
   if (pa.rec_times != nullptr) {
     int n = pa.n_rec[local];

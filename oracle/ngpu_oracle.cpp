@@ -32,6 +32,7 @@
 #include <stdint.h>
 #include <string.h>
 #include <algorithm>
+#include <map>
 #include <utility>
 #include <vector>
 #ifdef _OPENMP
@@ -87,7 +88,8 @@ struct Oracle {
   std::vector<real> acc;          // [node*maxport + port]
   int maxport = 1;
   std::vector<std::vector<std::pair<int, real>>> spikes_at;  // per step: (node, height)
-  std::vector<long long> last_rev;    // per node
+  std::vector<long long> last_rev;    // per node: step its last spike reached the dendrites
+  std::map<long long, std::vector<int>> rev_at;  // step -> nodes whose spike reaches them then
   long long T = 0;                    // time index of the last finished step
   bool prepared = false;
   // records
@@ -312,9 +314,32 @@ static void syn_update(const Oracle &o, int sg, real &w, real Dt) {
   }
 }
 
+// dendritic delay of a node in steps (src/spike_buffer.cu:148-166)
+static int den_steps(const Oracle &o, int node) {
+  const Group &g = o.groups[o.node_group[node]];
+  const real *p = &g.param[(size_t)(node - g.i0) * g.nparam];
+  real d = 0.0;
+  switch (g.model) {
+    case O_AEIF_COND_BETA: case O_AEIF_COND_ALPHA: case O_AEIF_PSC_ALPHA:
+    case O_AEIF_PSC_EXP: case O_AEIF_PSC_DELTA: d = p[A_den_delay]; break;
+    case O_IZH_COND_BETA: d = p[I_den_delay]; break;
+    case O_IAF_PSC_EXP: d = p[9]; break;
+    case O_PARROT: d = p[1]; break;
+    default: return 0;
+  }
+  return (int)round((float)d / (float)o.dt);
+}
+
+// A spike of step T reaches the node's own dendrites (STDP post rule) in
+// step T + den_delay: at once for den_delay 0 (src/spike_buffer.cu:164-167),
+// otherwise when the spike buffer's age reaches it (src/spike_buffer.cu:
+// 265-300), which sets the node's last post-spike time to that step before
+// that step's deliveries.
 static void push(Oracle &o, int node, real height, long long T) {
   o.spikes_at[(size_t)(T % o.spikes_at.size())].push_back(std::make_pair(node, height));
-  o.last_rev[node] = T;
+  const int den = den_steps(o, node);
+  if (den == 0) o.last_rev[node] = T;
+  else o.rev_at[T + den].push_back(node);
   o.log_step.push_back(T - 1);
   o.log_node.push_back(node);
 }
@@ -546,6 +571,16 @@ static void step(Oracle &o, int it_in_session) {
       }
     }
   }
+  // spikes reaching dendrites now (dendritic delay > 0)
+  std::vector<int> arrivals;
+  {
+    auto it = o.rev_at.find(T);
+    if (it != o.rev_at.end()) {
+      arrivals = it->second;
+      o.rev_at.erase(it);
+      for (int n : arrivals) o.last_rev[n] = T;
+    }
+  }
   // delivery of spikes emitted D steps ago, with the STDP pre rule
   const size_t R = o.spikes_at.size();
   for (size_t D = 1; D < R; D++) {
@@ -569,12 +604,16 @@ static void step(Oracle &o, int it_in_session) {
       }
     }
   }
-  // STDP post rule for neurons that spiked in this step
+  // STDP post rule for neurons whose spike reaches their dendrites in this
+  // step: spikes of this step without dendritic delay, then the arrivals
   {
     const auto &lst = o.spikes_at[(size_t)(T % (long long)R)];
+    std::vector<int> cand;
+    for (const auto &sp : lst)
+      if (den_steps(o, sp.first) == 0) cand.push_back(sp.first);
+    cand.insert(cand.end(), arrivals.begin(), arrivals.end());
     std::vector<int> seen;
-    for (const auto &sp : lst) {
-      int n = sp.first;
+    for (int n : cand) {
       if (std::find(seen.begin(), seen.end(), n) != seen.end()) continue;
       seen.push_back(n);
       for (size_t k : o.in_plastic[n]) {

@@ -112,9 +112,12 @@ def _stdp_expect(w, Dt, tau_plus, tau_minus, Wplus, alpha, mu_plus, mu_minus, Wm
     return max(w1, 0.0)
 
 
-def test_stdp_closed_form(ngpu):
+@pytest.mark.parametrize("den_delay", [0.0, 3.0])
+def test_stdp_closed_form(ngpu, den_delay):
     """python/test/test_stdp.py restated: 50 neuron pairs with spike-time
-    differences -122.5 .. 122.5 ms; final weight vs the closed form."""
+    differences -122.5 .. 122.5 ms; final weight vs the closed form. With a
+    dendritic delay d the post-synaptic spike reaches the synapse d later,
+    so the pair's time difference is Dt + d (src/spike_buffer.cu:265-300)."""
     tau_plus = tau_minus = 20.0
     lambd, alpha, mu_plus, mu_minus, Wmax = 1.0, 1.0, 1.0, 1.0, 0.001
     N = 50
@@ -125,7 +128,7 @@ def test_stdp_closed_form(ngpu):
                                              "Wmax": Wmax})
     sg = ngpu.Create("spike_generator", N)
     neuron = ngpu.Create("aeif_cond_beta", 2 * N)
-    ngpu.SetStatus(neuron, {"t_ref": 1000.0, "den_delay": 0.0})
+    ngpu.SetStatus(neuron, {"t_ref": 1000.0, "den_delay": den_delay})
     n0, n1 = neuron[0:N], neuron[N:2 * N]
     ngpu.SetStatus(sg, {"spike_times": [50.0], "spike_heights": [1.0]})
     ngpu.Connect(sg, n0, {"rule": "one_to_one"}, {"weight": 17.9, "delay": 1.0})
@@ -139,7 +142,7 @@ def test_stdp_closed_form(ngpu):
     w = ngpu.GetStatus(conn, "weight")
     assert len(w) == N
     for i in range(N):
-        e = _stdp_expect(Wmax / 2, dt_list[i], tau_plus, tau_minus, lambd * Wmax, alpha,
+        e = _stdp_expect(Wmax / 2, dt_list[i] + den_delay, tau_plus, tau_minus, lambd * Wmax, alpha,
                          mu_plus, mu_minus, Wmax)
         assert abs(e - w[i]) < 1e-5, (i, dt_list[i], e, w[i])
 

@@ -39,14 +39,17 @@ def stdp_pair_network(net_builder_n=50, dt_step=5.0):
     return N, dts
 
 
-def test_oracle_stdp_closed_form():
+@pytest.mark.parametrize("den_delay", [0.0, 3.0])
+def test_oracle_stdp_closed_form(den_delay):
+    """With a dendritic delay d of the post-synaptic neurons their spikes
+    reach the synapses d later: the pair difference becomes Dt + d."""
     N, dts = stdp_pair_network()
     tau_plus = tau_minus = 20.0
     Wmax = 0.001
     net = orc.Network(dt=0.1)
     sg = net.create(orc.SPIKE_GENERATOR, N)
     n0 = net.create(orc.AEIF_COND_BETA, N, 1, params={"t_ref": 1000.0})
-    n1 = net.create(orc.AEIF_COND_BETA, N, 1, params={"t_ref": 1000.0})
+    n1 = net.create(orc.AEIF_COND_BETA, N, 1, params={"t_ref": 1000.0, "den_delay": den_delay})
     net.set_spikes(sg, [[50.0]] * N)
     syn = net.syn_group("stdp", {"tau_plus": tau_plus, "tau_minus": tau_minus, "lambda": 1.0,
                                  "alpha": 1.0, "mu_plus": 1.0, "mu_minus": 1.0, "Wmax": Wmax})
@@ -57,7 +60,8 @@ def test_oracle_stdp_closed_form():
     net.simulate(10000)
     w = net.weights(3 * N)[2 * N:]
     for i in range(N):
-        e = _stdp_expect(Wmax / 2, dts[i], tau_plus, tau_minus, 1.0 * Wmax, 1.0, 1.0, 1.0, Wmax)
+        e = _stdp_expect(Wmax / 2, dts[i] + den_delay, tau_plus, tau_minus, 1.0 * Wmax, 1.0, 1.0,
+                         1.0, Wmax)
         assert abs(e - w[i]) < 1e-5, (i, dts[i], e, w[i])
 
 
