@@ -126,14 +126,30 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def traffic_per_unit():
-    """DRAM bytes per unit of the dominant kernels from the committed ncu
-    summary (profiles/roofline_traffic.json), or None."""
-    try:
-        with open(os.path.join(ROOT, "profiles", "roofline_traffic.json")) as f:
-            return json.load(f)
-    except Exception:
-        return {}
+# DRAM traffic and executed instructions per unit, from ncu captures of the
+# same kernels (dram__bytes_read.sum + dram__bytes_write.sum and
+# smsp__inst_executed.sum per launch, divided by the neurons / warps / events
+# of the launch): RK5 update on the silent network at 200,000 neurons,
+# delivery on the active network at 400,000 neurons.
+TRAFFIC_RK5_PER_NEURON_STEP = 77.3       # bytes
+TRAFFIC_DELIVER_PER_EVENT = 11.3         # bytes
+INST_RK5_PER_WARP_STEP = 1190.0          # warp instructions per 32 neuron-steps
+SM_COUNT, SMSP_PER_SM = 148, 4
+
+
+def issue_roofline(kname, n, avg_ms, clocks):
+    """Instruction-issue view of the RK5 update (it is issue and latency
+    bound, not HBM bound): warp instructions per launch from the ncu count
+    per warp-step, against one instruction per cycle per SM sub-partition at
+    the median SM clock sampled during the timed region."""
+    if kname != "rk5_update" or avg_ms <= 0:
+        return None
+    mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    inst = INST_RK5_PER_WARP_STEP * ((n + 31) // 32)
+    achieved = inst / (avg_ms / 1000.0) / 1e9
+    peak = SM_COUNT * SMSP_PER_SM * mhz * 1e6 / 1e9
+    return {"unit": "Ginst/s", "achieved": achieved, "peak": peak, "frac": achieved / peak,
+            "inst_per_launch": inst, "sm_mhz": mhz}
 
 
 def cpu_baseline(cfg, n_sample=2000, sim_ms=20.0, threads=0):
@@ -379,24 +395,22 @@ def main():
     n_steps = int(round(args.steps * step_ms / 0.1))
     # roofline of the dominant kernel
     peak, peak_kind = measured_peaks()
-    tr = traffic_per_unit()
     if upd_ms >= del_ms:
         kname = "rk5_update"
         bytes_launch = BYTES_PER_NEURON_STEP * cfg["n"]
         avg_ms = upd_ms / max(upd_n, 1)
-        tpu = tr.get("rk5_update_bytes_per_neuron_step")
-        traffic = tpu * cfg["n"] if tpu else None
+        traffic = TRAFFIC_RK5_PER_NEURON_STEP * cfg["n"]
     else:
         kname = "deliver"
         ev_launch = events_instr / max(del_n, 1)
         bytes_launch = BYTES_PER_EVENT * ev_launch
         avg_ms = del_ms / max(del_n, 1)
-        tpu = tr.get("deliver_bytes_per_event")
-        traffic = tpu * ev_launch if tpu else None
+        traffic = TRAFFIC_DELIVER_PER_EVENT * ev_launch
     achieved = bytes_launch / (avg_ms / 1000.0) / 1e9
     roof = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
             "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "avg_launch_ms": avg_ms,
+            "issue": issue_roofline(kname, cfg["n"], avg_ms, clocks),
             "kernel_ms": {"update": upd_ms, "deliver": del_ms, "stdp": stdp_ms,
                           "bookkeeping": oth_ms},
             "launches": {"update": upd_n, "deliver": del_n, "stdp": stdp_n,
