@@ -352,6 +352,7 @@ def main():
     t_build = time.perf_counter()
     pg, nrn = build_network(ngpu, cfg)
     ngpu.ActivateSpikeCount(nrn)
+    connect_s = time.perf_counter() - t_build
     ngpu.Calibrate()
     build_s = time.perf_counter() - t_build
     step_ms = args.step_ms
@@ -455,7 +456,7 @@ def main():
         "rk5_stage_evals_per_neuron_step": evals / (cfg["n"] * n_steps),
         "wall_per_bio_s": (dev_ms_max / 1000.0) / bio_s,
         "rk5_tuning": b.GetRk5Tuning(nrn.i0),
-        "build_s": build_s,
+        "build_s": build_s, "connect_s": connect_s, "calibrate_s": build_s - connect_s,
         "gpu_launches": int(2 * n_steps),
         "roofline": roof,
         "cpu_baseline": cpu,
