@@ -20,7 +20,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["ngpu_kernels.cu", "ngpu_rk5_batch.cu", "ngpu_step_proposer.cu",
+CU_SOURCES = ["ngpu_kernels.cu", "ngpu_rk5_batch.cu", "ngpu_step_proposer.cu", "ngpu_connect_device.cu",
               "ngpu_deliver_api.cu", "ngpu_deliver_static.cu"]
 CPP_SOURCES = ["ngpu_core.cpp", "ngpu_connect.cpp", "neurongpu_C.cpp"]
 

@@ -20,7 +20,6 @@
 #include <string.h>
 #include <algorithm>
 #include <numeric>
-#include <unordered_set>
 
 #include "ngpu_core.h"
 #include "ngpu_rng.h"
@@ -94,19 +93,71 @@ bool SynSpec::IsFloatParam(const std::string &n) { return n == "weight" || n == 
 bool SynSpec::IsFloatPtParam(const std::string &n) { return n == "weight_array" || n == "delay_array"; }
 
 // ---------------------------------------------------------------------------
-// edges
+// edges: device edge store in insertion order
 // ---------------------------------------------------------------------------
+void NeuronGPU::GrowRaw(long long need) {
+  if (need <= raw_cap_) return;
+  if (need >= 0x7fffffffLL) throw ngpu_exception("Too many connections (at most 2^31 - 1)");
+  if (!stream_) NGPU_CUDA(cudaStreamCreate(&stream_));
+  long long cap = std::max<long long>(need, std::max<long long>(1 << 16, raw_cap_ * 2));
+  cap = std::min<long long>(cap, 0x7fffffffLL);
+  EdgeStore e;
+  NGPU_CUDA(cudaMalloc(&e.src, sizeof(uint32_t) * cap));
+  NGPU_CUDA(cudaMalloc(&e.tgt, sizeof(uint32_t) * cap));
+  NGPU_CUDA(cudaMalloc(&e.port, cap));
+  NGPU_CUDA(cudaMalloc(&e.syn, cap));
+  NGPU_CUDA(cudaMalloc(&e.w, sizeof(float) * cap));
+  NGPU_CUDA(cudaMalloc(&e.d, sizeof(uint16_t) * cap));
+  if (n_raw_ > 0) {
+    NGPU_CUDA(cudaMemcpyAsync(e.src, d_raw_.src, sizeof(uint32_t) * n_raw_, cudaMemcpyDeviceToDevice, stream_));
+    NGPU_CUDA(cudaMemcpyAsync(e.tgt, d_raw_.tgt, sizeof(uint32_t) * n_raw_, cudaMemcpyDeviceToDevice, stream_));
+    NGPU_CUDA(cudaMemcpyAsync(e.port, d_raw_.port, n_raw_, cudaMemcpyDeviceToDevice, stream_));
+    NGPU_CUDA(cudaMemcpyAsync(e.syn, d_raw_.syn, n_raw_, cudaMemcpyDeviceToDevice, stream_));
+    NGPU_CUDA(cudaMemcpyAsync(e.w, d_raw_.w, sizeof(float) * n_raw_, cudaMemcpyDeviceToDevice, stream_));
+    NGPU_CUDA(cudaMemcpyAsync(e.d, d_raw_.d, sizeof(uint16_t) * n_raw_, cudaMemcpyDeviceToDevice, stream_));
+    NGPU_CUDA(cudaStreamSynchronize(stream_));
+  }
+  FreeRaw();
+  d_raw_ = e;
+  raw_cap_ = cap;
+}
+
+void NeuronGPU::FreeRaw() {
+  auto F = [](void *p) { if (p) cudaFree(p); };
+  F(d_raw_.src); F(d_raw_.tgt); F(d_raw_.port); F(d_raw_.syn); F(d_raw_.w); F(d_raw_.d);
+  d_raw_ = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  raw_cap_ = 0;
+}
+
+// single connections buffered on the host go to the store in call order
+void NeuronGPU::FlushPending() {
+  const long long n = (long long)p_src_.size();
+  if (n == 0) return;
+  GrowRaw(n_raw_ + n);
+  const long long b = n_raw_;
+  NGPU_CUDA(cudaMemcpy(d_raw_.src + b, p_src_.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+  NGPU_CUDA(cudaMemcpy(d_raw_.tgt + b, p_tgt_.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+  NGPU_CUDA(cudaMemcpy(d_raw_.port + b, p_port_.data(), n, cudaMemcpyHostToDevice));
+  NGPU_CUDA(cudaMemcpy(d_raw_.syn + b, p_syn_.data(), n, cudaMemcpyHostToDevice));
+  NGPU_CUDA(cudaMemcpy(d_raw_.w + b, p_w_.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+  NGPU_CUDA(cudaMemcpy(d_raw_.d + b, p_d_.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice));
+  n_raw_ += n;
+  p_src_.clear(); p_tgt_.clear(); p_port_.clear(); p_syn_.clear(); p_w_.clear(); p_d_.clear();
+}
+
 void NeuronGPU::AddEdge(int s, int t, unsigned char port, unsigned char syn, float w,
                         float delay) {
   if (delay < time_resolution_) throw ngpu_exception("Delay must be >= time resolution");
   float r = roundf(delay / time_resolution_);
   if (r > 65535.0f) throw ngpu_exception("Delay too large");
-  e_src_.push_back((uint32_t)s);
-  e_tgt_.push_back((uint32_t)t);
-  e_port_.push_back(port);
-  e_syn_.push_back(syn);
-  e_w_.push_back(w);
-  e_d_.push_back((uint16_t)r);
+  p_src_.push_back((uint32_t)s);
+  p_tgt_.push_back((uint32_t)t);
+  p_port_.push_back(port);
+  p_syn_.push_back(syn);
+  p_w_.push_back(w);
+  p_d_.push_back((uint16_t)r);
+  if (syn > 0) any_plastic_ = true;
+  csr_valid_ = false;
 }
 
 int NeuronGPU::Connect(int i_source, int i_target, unsigned char port,
@@ -116,223 +167,195 @@ int NeuronGPU::Connect(int i_source, int i_target, unsigned char port,
   if (i_source < 0 || i_source >= N || i_target < 0 || i_target >= N)
     throw ngpu_exception("Unrecognized node in connection");
   AddEdge(i_source, i_target, port, syn_group, weight, delay);
-  host_csr_valid_ = false;
   return 0;
 }
 
-// Generic rule driver. Edges are appended in the reference's i_array order
-// so weight_array / delay_array index the same connection.
+namespace {
+// device copy of a host array for the duration of one rule call
+template <class T>
+struct DevArray {
+  T *p = nullptr;
+  DevArray(const T *h, long long n, cudaStream_t s) {
+    if (!h || n <= 0) return;
+    if (cudaMalloc(&p, sizeof(T) * n) != cudaSuccess) throw ngpu_exception("cudaMalloc failed");
+    if (cudaMemcpyAsync(p, h, sizeof(T) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+      throw ngpu_exception("cudaMemcpy failed");
+  }
+  ~DevArray() { if (p) cudaFree(p); }
+};
+}  // namespace
+
+// Generic rule driver: the rule kernels append to the device edge store;
+// edge ia of a call lands at store index base + ia, in the reference's
+// i_array order, so weight_array / delay_array index the same connection.
 int NeuronGPU::Connect(const int *src_arr, int i_src0, int n_source, const int *tgt_arr,
                        int i_tgt0, int n_target, ConnSpec &cs, SynSpec &ss) {
   CheckUncalibrated("Connections cannot be created after calibration");
   const long long N = (long long)node_group_map_.size();
-  auto S = [&](long long k) -> int { return src_arr ? src_arr[k] : i_src0 + (int)k; };
-  auto Tn = [&](long long k) -> int { return tgt_arr ? tgt_arr[k] : i_tgt0 + (int)k; };
-  for (long long k = 0; k < n_source; k++)
-    if (S(k) < 0 || S(k) >= N) throw ngpu_exception("Unrecognized source node");
-  for (long long k = 0; k < n_target; k++)
-    if (Tn(k) < 0 || Tn(k) >= N) throw ngpu_exception("Unrecognized target node");
-  if (ss.syn_group_ > syn_groups_.size()) throw ngpu_exception("Unknown synapse group");
-  auto W = [&](size_t ia) { return ss.weight_array_ ? ss.weight_array_[ia] : ss.weight_; };
-  auto D = [&](size_t ia) { return ss.delay_array_ ? ss.delay_array_[ia] : ss.delay_; };
-  const unsigned long long seed = rnd_seed_;
-  const unsigned long long call = NextRngStream();
-  size_t base = e_src_.size();
-  auto reserve = [&](size_t n) {
-    e_src_.resize(base + n); e_tgt_.resize(base + n); e_port_.resize(base + n);
-    e_syn_.resize(base + n); e_w_.resize(base + n); e_d_.resize(base + n);
-  };
-  auto put = [&](size_t ia, int s, int t) {
-    float delay = D(ia);
-    if (delay < time_resolution_) throw ngpu_exception("Delay must be >= time resolution");
-    float r = roundf(delay / time_resolution_);
-    if (r > 65535.0f) throw ngpu_exception("Delay too large");
-    size_t k = base + ia;
-    e_src_[k] = (uint32_t)s; e_tgt_[k] = (uint32_t)t; e_port_[k] = ss.port_;
-    e_syn_[k] = ss.syn_group_; e_w_[k] = W(ia); e_d_[k] = (uint16_t)r;
-  };
-  host_csr_valid_ = false;
-  try {
-    switch (cs.rule_) {
-      case ONE_TO_ONE: {
-        if (n_source != n_target)
-          throw ngpu_exception("Number of source and target nodes must be equal for the one-to-one connection rule");
-        reserve(n_source);
-        for (long long k = 0; k < n_source; k++) put(k, S(k), Tn(k));
-        break;
-      }
-      case ALL_TO_ALL: {
-        size_t n = (size_t)n_source * n_target;
-        reserve(n);
-        for (long long it = 0; it < n_target; it++)
-          for (long long is = 0; is < n_source; is++) put((size_t)it * n_source + is, S(is), Tn(it));
-        break;
-      }
-      case FIXED_TOTAL_NUMBER: {
-        size_t n = (size_t)cs.total_num_;
-        reserve(n);
-        if (n > 0 && (n_source <= 0 || n_target <= 0))
-          throw ngpu_exception("Empty source or target list");
-        for (size_t k = 0; k < n; k++) {
-          Philox4 r = ng_random_block(seed, RNG_TAG_CONNECT, call, (int64_t)k, 0);
-          int is = (int)(r.v[0] % (uint32_t)n_source);
-          int it = (int)(r.v[1] % (uint32_t)n_target);
-          put(k, S(is), Tn(it));
-        }
-        break;
-      }
-      case FIXED_INDEGREE:
-      case FIXED_OUTDEGREE: {
-        const bool indeg = cs.rule_ == FIXED_INDEGREE;
-        const int K = indeg ? cs.indegree_ : cs.outdegree_;
-        const long long n_outer = indeg ? n_target : n_source;
-        const long long n_pool = indeg ? n_source : n_target;
-        if (K > n_pool)
-          throw ngpu_exception(indeg ? "Indegree larger than number of source nodes"
-                                     : "Outdegree larger than number of target nodes");
-        reserve((size_t)n_outer * K);
-        bool err = false;
-#pragma omp parallel for schedule(dynamic, 64)
-        for (long long o = 0; o < n_outer; o++) {
-          // sample K distinct pool indices for this target (source)
-          std::vector<int> pick(K);
-          if (n_pool < 5LL * K) {
-            std::vector<int> perm(n_pool);
-            std::iota(perm.begin(), perm.end(), 0);
-            for (int i = 0; i < K; i++) {
-              Philox4 r = ng_random_block(seed, RNG_TAG_SOURCE_SET, call, o, (uint32_t)i);
-              long long j = i + (long long)(r.v[0] % (uint32_t)(n_pool - i));
-              std::swap(perm[i], perm[j]);
-              pick[i] = perm[i];
-            }
-          } else {
-            // rejection of repeats with a small open-addressing set
-            int cap = 16;
-            while (cap < 2 * K) cap <<= 1;
-            std::vector<int> table(cap, -1);
-            uint32_t draw = 0;
-            for (int i = 0; i < K; i++) {
-              int j;
-              for (;;) {
-                Philox4 r = ng_random_block(seed, RNG_TAG_SOURCE_SET, call, o, draw++);
-                j = (int)(r.v[0] % (uint32_t)n_pool);
-                uint32_t hsh = ((uint32_t)j * 0x9E3779B1u) & (uint32_t)(cap - 1);
-                bool dup = false;
-                while (table[hsh] >= 0) {
-                  if (table[hsh] == j) { dup = true; break; }
-                  hsh = (hsh + 1) & (uint32_t)(cap - 1);
-                }
-                if (!dup) {
-                  table[hsh] = j;
-                  break;
-                }
-              }
-              pick[i] = j;
-            }
-          }
-          for (int i = 0; i < K; i++) {
-            size_t ia = (size_t)o * K + i;
-            float delay = D(ia);
-            if (delay < time_resolution_) { err = true; continue; }
-            size_t k = base + ia;
-            e_src_[k] = (uint32_t)(indeg ? S(pick[i]) : S(o));
-            e_tgt_[k] = (uint32_t)(indeg ? Tn(o) : Tn(pick[i]));
-            e_port_[k] = ss.port_;
-            e_syn_[k] = ss.syn_group_;
-            e_w_[k] = W(ia);
-            e_d_[k] = (uint16_t)std::min(65535.0f, roundf(delay / time_resolution_));
-          }
-        }
-        if (err) throw ngpu_exception("Delay must be >= time resolution");
-        break;
-      }
-      default:
-        throw ngpu_exception("Unknown connection rule");
-    }
-  } catch (...) {
-    e_src_.resize(base); e_tgt_.resize(base); e_port_.resize(base);
-    e_syn_.resize(base); e_w_.resize(base); e_d_.resize(base);
-    throw;
+  for (long long k = 0; k < n_source; k++) {
+    int v = src_arr ? src_arr[k] : i_src0 + (int)k;
+    if (v < 0 || v >= N) throw ngpu_exception("Unrecognized source node");
   }
+  for (long long k = 0; k < n_target; k++) {
+    int v = tgt_arr ? tgt_arr[k] : i_tgt0 + (int)k;
+    if (v < 0 || v >= N) throw ngpu_exception("Unrecognized target node");
+  }
+  if (ss.syn_group_ > syn_groups_.size()) throw ngpu_exception("Unknown synapse group");
+  if (!stream_) NGPU_CUDA(cudaStreamCreate(&stream_));
+  long long n_conn = 0;
+  switch (cs.rule_) {
+    case ONE_TO_ONE:
+      if (n_source != n_target)
+        throw ngpu_exception("Number of source and target nodes must be equal for the one-to-one connection rule");
+      n_conn = n_source;
+      break;
+    case ALL_TO_ALL: n_conn = (long long)n_source * n_target; break;
+    case FIXED_TOTAL_NUMBER:
+      n_conn = cs.total_num_;
+      if (n_conn > 0 && (n_source <= 0 || n_target <= 0))
+        throw ngpu_exception("Empty source or target list");
+      break;
+    case FIXED_INDEGREE:
+      if (cs.indegree_ > n_source) throw ngpu_exception("Indegree larger than number of source nodes");
+      n_conn = (long long)n_target * cs.indegree_;
+      break;
+    case FIXED_OUTDEGREE:
+      if (cs.outdegree_ > n_target) throw ngpu_exception("Outdegree larger than number of target nodes");
+      n_conn = (long long)n_source * cs.outdegree_;
+      break;
+    default:
+      throw ngpu_exception("Unknown connection rule");
+  }
+  const unsigned long long call = NextRngStream();
+  if (n_conn <= 0) return 0;
+  FlushPending();
+  GrowRaw(n_raw_ + n_conn);
+  DevArray<int> dsrc(src_arr, n_source, stream_), dtgt(tgt_arr, n_target, stream_);
+  DevArray<float> dw(ss.weight_array_, n_conn, stream_), dd(ss.delay_array_, n_conn, stream_);
+  unsigned *d_err = nullptr;
+  NGPU_CUDA(cudaMalloc(&d_err, sizeof(unsigned)));
+  NGPU_CUDA(cudaMemsetAsync(d_err, 0, sizeof(unsigned), stream_));
+  RuleArgs a;
+  a.e = d_raw_;
+  a.base = n_raw_;
+  a.src_arr = dsrc.p; a.src0 = i_src0;
+  a.tgt_arr = dtgt.p; a.tgt0 = i_tgt0;
+  a.w_arr = dw.p; a.w = ss.weight_;
+  a.d_arr = dd.p; a.delay = ss.delay_;
+  a.port = ss.port_; a.syn = ss.syn_group_;
+  a.dt = time_resolution_;
+  a.seed = rnd_seed_;
+  a.call = call;
+  a.err = d_err;
+  int *scratch = nullptr;
+  switch (cs.rule_) {
+    case ONE_TO_ONE: DevRuleOneToOne(a, n_conn, stream_); break;
+    case ALL_TO_ALL: DevRuleAllToAll(a, n_source, n_target, stream_); break;
+    case FIXED_TOTAL_NUMBER: DevRuleFixedTotal(a, n_conn, n_source, n_target, stream_); break;
+    default: {
+      const bool indeg = cs.rule_ == FIXED_INDEGREE;
+      const int K = indeg ? cs.indegree_ : cs.outdegree_;
+      const long long n_outer = indeg ? n_target : n_source;
+      const long long n_pool = indeg ? n_source : n_target;
+      const long long slice = DevRuleFixedDegreeScratchInts(n_pool, K);
+      // as many sampling threads as fit in 1 GB of scratch, at most 148 x 1024
+      long long thr = std::min<long long>(n_outer, 148LL * 1024);
+      thr = std::min<long long>(thr, std::max<long long>(1, (1LL << 28) / std::max<long long>(slice, 1)));
+      NGPU_CUDA(cudaMalloc(&scratch, sizeof(int) * (size_t)(slice * thr)));
+      DevRuleFixedDegree(a, n_outer, n_pool, K, indeg ? 1 : 0, scratch, slice, (int)thr, stream_);
+      break;
+    }
+  }
+  unsigned err = 0;
+  cudaError_t ce = cudaGetLastError();
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(&err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(stream_);
+  if (scratch) cudaFree(scratch);
+  cudaFree(d_err);
+  if (ce != cudaSuccess) throw ngpu_exception(std::string("CUDA error in Connect: ") + cudaGetErrorString(ce));
+  if (err & 1u) throw ngpu_exception("Delay must be >= time resolution");
+  if (err & 2u) throw ngpu_exception("Delay too large");
+  n_raw_ += n_conn;
+  if (ss.syn_group_ > 0) any_plastic_ = true;
+  csr_valid_ = false;
   return 0;
 }
 
 // ---------------------------------------------------------------------------
-// host CSR by (source, delay index); stable in insertion order
+// CSR by (source, delay index), stable in insertion order (device build)
 // ---------------------------------------------------------------------------
-void NeuronGPU::BuildHostCSR() {
-  if (host_csr_valid_) return;
-  const uint64_t E = e_src_.size();
+void NeuronGPU::FreeCSR() {
+  auto F = [](void *p) { if (p) cudaFree(p); };
+  F(d_grp_off_); F(d_e_post_); F(d_c_port_); F(d_e_syn_); F(d_e_w_);
+  d_grp_off_ = nullptr; d_e_post_ = nullptr; d_c_port_ = nullptr; d_e_syn_ = nullptr;
+  d_e_w_ = nullptr;
+  mirror_valid_ = false;
+  csr_valid_ = false;
+}
+
+void NeuronGPU::BuildCSR() {
+  if (csr_valid_) return;
+  if (!stream_) NGPU_CUDA(cudaStreamCreate(&stream_));
+  FlushPending();
+  FreeCSR();
+  const long long E = n_raw_;
   const long long N = (long long)node_group_map_.size();
-  int maxD = 0;
-  for (uint64_t k = 0; k < E; k++) maxD = std::max<int>(maxD, e_d_[k]);
-  std::vector<char> present(maxD + 1, 0);
-  for (uint64_t k = 0; k < E; k++) present[e_d_[k]] = 1;
+  // distinct delays
+  std::vector<unsigned> hist(65536, 0);
+  if (E > 0) {
+    unsigned *d_hist = nullptr;
+    NGPU_CUDA(cudaMalloc(&d_hist, sizeof(unsigned) * 65536));
+    DevDelayHistogram(d_raw_.d, E, d_hist, stream_);
+    NGPU_CUDA(cudaMemcpyAsync(hist.data(), d_hist, sizeof(unsigned) * 65536, cudaMemcpyDeviceToHost, stream_));
+    NGPU_CUDA(cudaStreamSynchronize(stream_));
+    cudaFree(d_hist);
+  }
   delays_.clear();
-  delay_index_.assign(maxD + 1, -1);
-  for (int d = 1; d <= maxD; d++) {
-    if (present[d]) {
+  delay_index_.assign(65536, -1);
+  for (int d = 1; d < 65536; d++) {
+    if (hist[d]) {
       delay_index_[d] = (int)delays_.size();
       delays_.push_back(d);
     }
   }
   const int nd = (int)delays_.size();
-  const uint64_t nkeys = (uint64_t)N * nd;
-  h_grp_off_.assign(nkeys + 1, 0);
-  // counts per (source, delay)
-  for (uint64_t k = 0; k < E; k++) {
-    uint64_t key = (uint64_t)e_src_[k] * nd + delay_index_[e_d_[k]];
-    h_grp_off_[key + 1]++;
+  const long long nkeys = N * nd;
+  if (nkeys >= 0xFFFFFFFFLL) throw ngpu_exception("Too many (source, delay) groups");
+  int *d_dix = nullptr;
+  NGPU_CUDA(cudaMalloc(&d_dix, sizeof(int) * 65536));
+  NGPU_CUDA(cudaMemcpy(d_dix, delay_index_.data(), sizeof(int) * 65536, cudaMemcpyHostToDevice));
+  NGPU_CUDA(cudaMalloc(&d_grp_off_, sizeof(unsigned long long) * (size_t)(nkeys + 1)));
+  const size_t ne = (size_t)(E > 0 ? E : 1);
+  NGPU_CUDA(cudaMalloc(&d_e_post_, sizeof(unsigned) * ne));
+  NGPU_CUDA(cudaMalloc(&d_c_port_, ne));
+  NGPU_CUDA(cudaMalloc(&d_e_syn_, ne));
+  NGPU_CUDA(cudaMalloc(&d_e_w_, sizeof(float) * ne));
+  cudaError_t ce = DevBuildCSR(d_raw_, E, d_dix, nd, nkeys, d_grp_off_, d_e_post_, d_c_port_,
+                               d_e_syn_, d_e_w_, stream_);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(stream_);
+  cudaFree(d_dix);
+  if (ce != cudaSuccess) throw ngpu_exception(std::string("CUDA error in the CSR build: ") + cudaGetErrorString(ce));
+  h_grp_off_.resize((size_t)(nkeys + 1));
+  NGPU_CUDA(cudaMemcpy(h_grp_off_.data(), d_grp_off_, sizeof(unsigned long long) * (size_t)(nkeys + 1),
+                       cudaMemcpyDeviceToHost));
+  mirror_valid_ = false;
+  csr_valid_ = true;
+}
+
+// host copies of the CSR targets, ports and synapse groups (queries)
+void NeuronGPU::EnsureMirror() {
+  if (!calibrate_flag_) BuildCSR();
+  if (mirror_valid_) return;
+  const long long E = n_raw_;
+  h_c_tgt_.resize((size_t)E);
+  h_c_port_.resize((size_t)E);
+  h_c_syn_.resize((size_t)E);
+  if (E > 0) {
+    NGPU_CUDA(cudaMemcpy(h_c_tgt_.data(), d_e_post_, sizeof(uint32_t) * E, cudaMemcpyDeviceToHost));
+    NGPU_CUDA(cudaMemcpy(h_c_port_.data(), d_c_port_, E, cudaMemcpyDeviceToHost));
+    NGPU_CUDA(cudaMemcpy(h_c_syn_.data(), d_e_syn_, E, cudaMemcpyDeviceToHost));
   }
-  for (uint64_t k = 0; k < nkeys; k++) h_grp_off_[k + 1] += h_grp_off_[k];
-  h_order_.assign(E, 0);
-  // Stable scatter. The edge list is split into T contiguous chunks; each
-  // chunk's edges of a key go after those of the earlier chunks, so the
-  // result keeps insertion order for any T.
-  int nthr = 1;
-#ifdef _OPENMP
-  nthr = omp_get_max_threads();
-  if (E < 4000000) nthr = 1;
-  while (nthr > 1 && (uint64_t)nthr * nkeys > (1ull << 30)) nthr /= 2;
-#endif
-  if (nthr <= 1) {
-    std::vector<uint64_t> fill(h_grp_off_.begin(), h_grp_off_.end() - 1);
-    for (uint64_t k = 0; k < E; k++) {
-      uint64_t key = (uint64_t)e_src_[k] * nd + delay_index_[e_d_[k]];
-      h_order_[fill[key]++] = k;
-    }
-  } else {
-    std::vector<std::vector<uint32_t>> cnt(nthr);
-#pragma omp parallel num_threads(nthr)
-    {
-      int tid = 0;
-#ifdef _OPENMP
-      tid = omp_get_thread_num();
-#endif
-      uint64_t lo = E * tid / nthr, hi = E * (tid + 1) / nthr;
-      std::vector<uint32_t> &c = cnt[tid];
-      c.assign(nkeys, 0);
-      for (uint64_t k = lo; k < hi; k++)
-        c[(uint64_t)e_src_[k] * nd + delay_index_[e_d_[k]]]++;
-#pragma omp barrier
-      // exclusive prefix over chunks, per key (offset inside the group)
-      uint64_t k_lo = nkeys * tid / nthr, k_hi = nkeys * (tid + 1) / nthr;
-      for (uint64_t key = k_lo; key < k_hi; key++) {
-        uint32_t run = 0;
-        for (int t = 0; t < nthr; t++) {
-          uint32_t v = cnt[t][key];
-          cnt[t][key] = run;
-          run += v;
-        }
-      }
-#pragma omp barrier
-      for (uint64_t k = lo; k < hi; k++) {
-        uint64_t key = (uint64_t)e_src_[k] * nd + delay_index_[e_d_[k]];
-        h_order_[h_grp_off_[key] + c[key]++] = k;
-      }
-    }
-  }
-  host_csr_valid_ = true;
+  mirror_valid_ = true;
 }
 
 // ---------------------------------------------------------------------------
@@ -343,7 +366,7 @@ std::vector<ConnectionId> NeuronGPU::GetConnections(const int *src_arr, int i_sr
                                                     int i_tgt0, int n_target,
                                                     int syn_group) {
   const int N = (int)node_group_map_.size();
-  if (!calibrate_flag_) BuildHostCSR();
+  EnsureMirror();
   const int nd = (int)delays_.size();
   if (src_arr == nullptr && n_source <= 0) { i_src0 = 0; n_source = N; }
   if (tgt_arr == nullptr && n_target <= 0) { i_tgt0 = 0; n_target = N; }
@@ -361,12 +384,11 @@ std::vector<ConnectionId> NeuronGPU::GetConnections(const int *src_arr, int i_sr
       uint64_t b = h_grp_off_[(uint64_t)s * nd + di], e = h_grp_off_[(uint64_t)s * nd + di + 1];
       if (b == e) continue;
       for (uint64_t k = b; k < e; k++) {
-        uint64_t o = h_order_[k];
-        int t = (int)e_tgt_[o];
+        int t = (int)h_c_tgt_[k];
         bool ok;
         if (tgt_arr) ok = std::binary_search(tsorted.begin(), tsorted.end(), t);
         else ok = (t >= i_tgt0 && t < i_tgt0 + n_target);
-        if (ok && syn_group >= 0 && e_syn_[o] != syn_group) ok = false;
+        if (ok && syn_group >= 0 && h_c_syn_[k] != syn_group) ok = false;
         if (ok) {
           ConnectionId c;
           c.i_source_ = s; c.i_group_ = ig; c.i_conn_ = (int)(k - b);
@@ -382,27 +404,22 @@ std::vector<ConnectionId> NeuronGPU::GetConnections(const int *src_arr, int i_sr
 long long NeuronGPU::ExportConnections(int *src, int *tgt, int *port, int *syn,
                                        float *delay, float *weight) {
   const long long N = (long long)node_group_map_.size();
-  if (!calibrate_flag_) BuildHostCSR();
+  EnsureMirror();
   const int nd = (int)delays_.size();
-  const long long M = (long long)e_src_.size();
-  std::vector<float> dev_w;
-  if (weight && calibrate_flag_ && M > 0) {
-    dev_w.resize((size_t)M);
-    NGPU_CUDA(cudaMemcpy(dev_w.data(), d_e_w_, sizeof(float) * M, cudaMemcpyDeviceToHost));
-  }
+  const long long M = n_raw_;
+  if (weight && M > 0)
+    NGPU_CUDA(cudaMemcpy(weight, d_e_w_, sizeof(float) * M, cudaMemcpyDeviceToHost));
 #pragma omp parallel for schedule(dynamic, 1024)
   for (long long s = 0; s < N; s++) {
     for (int di = 0; di < nd; di++) {
       const uint64_t b = h_grp_off_[(uint64_t)s * nd + di];
       const uint64_t e = h_grp_off_[(uint64_t)s * nd + di + 1];
       for (uint64_t k = b; k < e; k++) {
-        const uint64_t o = h_order_[k];
         if (src) src[k] = (int)s;
-        if (tgt) tgt[k] = (int)e_tgt_[o];
-        if (port) port[k] = e_port_[o];
-        if (syn) syn[k] = e_syn_[o];
+        if (tgt) tgt[k] = (int)h_c_tgt_[k];
+        if (port) port[k] = h_c_port_[k];
+        if (syn) syn[k] = h_c_syn_[k];
         if (delay) delay[k] = time_resolution_ * (float)delays_[di];
-        if (weight) weight[k] = dev_w.empty() ? e_w_[o] : dev_w[k];
       }
     }
   }
@@ -411,7 +428,7 @@ long long NeuronGPU::ExportConnections(int *src, int *tgt, int *port, int *syn,
 
 ConnectionStatus NeuronGPU::GetConnectionStatus(ConnectionId id) {
   const int N = (int)node_group_map_.size();
-  if (!calibrate_flag_) BuildHostCSR();
+  EnsureMirror();
   const int nd = (int)delays_.size();
   if (id.i_source_ < 0 || id.i_source_ >= N) throw ngpu_exception("Unrecognized source node");
   int ig = 0;
@@ -423,18 +440,14 @@ ConnectionStatus NeuronGPU::GetConnectionStatus(ConnectionId id) {
       if (id.i_conn_ < 0 || (uint64_t)id.i_conn_ >= e - b)
         throw ngpu_exception("Connection index out of range");
       uint64_t k = b + id.i_conn_;
-      uint64_t o = h_order_[k];
       ConnectionStatus st;
       st.i_source = id.i_source_;
-      st.i_target = (int)e_tgt_[o];
-      st.port = e_port_[o];
-      st.syn_group = e_syn_[o];
+      st.i_target = (int)h_c_tgt_[k];
+      st.port = h_c_port_[k];
+      st.syn_group = h_c_syn_[k];
       st.delay = time_resolution_ * (float)delays_[di];
-      st.weight = e_w_[o];
-      if (calibrate_flag_) {
-        // weights may have been changed by plasticity
-        NGPU_CUDA(cudaMemcpy(&st.weight, d_e_w_ + k, sizeof(float), cudaMemcpyDeviceToHost));
-      }
+      // current device weight (plasticity may have changed it)
+      NGPU_CUDA(cudaMemcpy(&st.weight, d_e_w_ + k, sizeof(float), cudaMemcpyDeviceToHost));
       return st;
     }
     ig++;

@@ -79,7 +79,10 @@ void NeuronGPU::FreeDevice() {
   }
   F(d_ctx_); F(d_acc_); F(d_ring_src_); F(d_ring_h_); F(d_ring_cnt_);
   F(d_last_spike_T_); F(d_last_rev_T_); F(d_last_post_T_); F(d_last_spike_h_);
-  F(d_grp_off_); F(d_e_slot_); F(d_e_w_); F(d_e_syn_); F(d_e_stamp_);
+  FreeRaw();
+  F(d_grp_off_); F(d_e_slot_); F(d_e_w_); F(d_e_syn_); F(d_e_stamp_); F(d_c_port_);
+  d_grp_off_ = nullptr; d_e_slot_ = nullptr; d_e_w_ = nullptr; d_e_syn_ = nullptr;
+  d_e_stamp_ = nullptr; d_c_port_ = nullptr;
   F(d_e_post_); F(d_rev_off_); F(d_rev_edge_); F(d_delays_);
   F(d_rev_src_); F(d_rev_cnt_);
   d_rev_src_ = nullptr;
@@ -254,7 +257,7 @@ int NeuronGPU::Create(const std::string &model, int n_node, int n_port) {
   NGPU_CUDA(cudaStreamSynchronize(stream_));
   groups_.push_back(g);
   node_group_map_.insert(node_group_map_.end(), n_node, (int)groups_.size() - 1);
-  host_csr_valid_ = false;
+  csr_valid_ = false;
   return g->i_node_0;
 }
 
@@ -285,7 +288,7 @@ int NeuronGPU::CreatePoissonGenerator(int n_node, float rate) {
   g->poisson_lambda = (float)(rate * time_resolution_ / 1000.0);
   groups_.push_back(g);
   node_group_map_.insert(node_group_map_.end(), n_node, (int)groups_.size() - 1);
-  host_csr_valid_ = false;
+  csr_valid_ = false;
   return g->i_node_0;
 }
 
@@ -1022,9 +1025,11 @@ int NeuronGPU::Calibrate() {
   if (!stream_) NGPU_CUDA(cudaStreamCreate(&stream_));
   if (verbosity_level_ >= 1) printf("Calibrating ...\n");
   neural_time_ = t_min_;
-  BuildHostCSR();
+  BuildCSR();
   BuildDevice();
   calibrate_flag_ = true;
+  // the insertion-order edge store is no longer needed
+  FreeRaw();
   return 0;
 }
 
@@ -1127,77 +1132,63 @@ void NeuronGPU::BuildDevice() {
   if (n_acc_ > 0xFFFFFFFFLL) throw ngpu_exception("Too many (node, port) input slots");
   NGPU_CUDA(cudaMalloc(&d_acc_, sizeof(long long) * (n_acc_ > 0 ? n_acc_ : 1)));
   NGPU_CUDA(cudaMemset(d_acc_, 0, sizeof(long long) * (n_acc_ > 0 ? n_acc_ : 1)));
-  // check ports of every edge and build the slot array
-  const uint64_t E = e_src_.size();
-  std::vector<uint32_t> slot(E);
-  std::vector<float> w(E);
-  std::vector<uint8_t> syn;
-  std::vector<uint32_t> post;
-  plastic_ = false;
-  for (uint64_t k = 0; k < E; k++) {
-    if (e_syn_[h_order_[k]] > 0) { plastic_ = true; break; }
-  }
-  if (plastic_) { syn.resize(E); post.resize(E); }
-  long long bad_port = -1;
-  bool bad_syn = false;
-#pragma omp parallel for schedule(static) if (E > 1000000)
-  for (long long k = 0; k < (long long)E; k++) {
-    uint64_t o = h_order_[k];
-    int t = e_tgt_[o];
-    NodeGroup *g = groups_[node_group_map_[t]];
-    int port = e_port_[o];
-    if (port >= g->n_port) {
-      bad_port = k;
-      continue;
+  // accumulator slot of every CSR edge (device), with the port and
+  // synapse-group checks of src/connect.cu:26-62
+  const uint64_t E = (uint64_t)n_raw_;
+  plastic_ = any_plastic_;
+  {
+    std::vector<long long> acc_base(groups_.size());
+    std::vector<int> n_pad(groups_.size()), i0(groups_.size()), n_port(groups_.size());
+    for (size_t gi = 0; gi < groups_.size(); gi++) {
+      acc_base[gi] = groups_[gi]->acc_base;
+      n_pad[gi] = groups_[gi]->n_pad;
+      i0[gi] = groups_[gi]->i_node_0;
+      n_port[gi] = groups_[gi]->n_port;
     }
-    slot[k] = (uint32_t)(g->acc_base + (long long)port * g->n_pad + (t - g->i_node_0));
-    w[k] = e_w_[o];
-    if (plastic_) {
-      syn[k] = e_syn_[o];
-      post[k] = (uint32_t)t;
-      if (syn[k] > (int)syn_groups_.size()) bad_syn = true;
-    }
+    const size_t G = groups_.size();
+    int *d_map = nullptr, *d_npad = nullptr, *d_i0 = nullptr, *d_nport = nullptr;
+    long long *d_base = nullptr;
+    unsigned *d_err = nullptr;
+    NGPU_CUDA(cudaMalloc(&d_map, sizeof(int) * (N > 0 ? N : 1)));
+    NGPU_CUDA(cudaMalloc(&d_npad, sizeof(int) * G));
+    NGPU_CUDA(cudaMalloc(&d_i0, sizeof(int) * G));
+    NGPU_CUDA(cudaMalloc(&d_nport, sizeof(int) * G));
+    NGPU_CUDA(cudaMalloc(&d_base, sizeof(long long) * G));
+    NGPU_CUDA(cudaMalloc(&d_err, sizeof(unsigned)));
+    NGPU_CUDA(cudaMemcpy(d_map, node_group_map_.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+    NGPU_CUDA(cudaMemcpy(d_npad, n_pad.data(), sizeof(int) * G, cudaMemcpyHostToDevice));
+    NGPU_CUDA(cudaMemcpy(d_i0, i0.data(), sizeof(int) * G, cudaMemcpyHostToDevice));
+    NGPU_CUDA(cudaMemcpy(d_nport, n_port.data(), sizeof(int) * G, cudaMemcpyHostToDevice));
+    NGPU_CUDA(cudaMemcpy(d_base, acc_base.data(), sizeof(long long) * G, cudaMemcpyHostToDevice));
+    NGPU_CUDA(cudaMemset(d_err, 0, sizeof(unsigned)));
+    NGPU_CUDA(cudaMalloc(&d_e_slot_, sizeof(unsigned) * (E > 0 ? E : 1)));
+    SlotTables t;
+    t.node_group = d_map; t.acc_base = d_base; t.n_pad = d_npad; t.i_node_0 = d_i0;
+    t.n_port = d_nport; t.n_syn_groups = (int)syn_groups_.size();
+    DevCsrSlots(d_e_post_, d_c_port_, d_e_syn_, (long long)E, t, d_e_slot_, d_err, stream_);
+    unsigned err = 0;
+    NGPU_CUDA(cudaMemcpyAsync(&err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+    NGPU_CUDA(cudaStreamSynchronize(stream_));
+    cudaFree(d_map); cudaFree(d_npad); cudaFree(d_i0); cudaFree(d_nport); cudaFree(d_base);
+    cudaFree(d_err);
+    if (err & 4u) throw ngpu_exception("Port index out of range for a target node");
+    if (err & 8u) throw ngpu_exception("Unrecognized synapse group");
   }
-  if (bad_port >= 0) {
-    uint64_t o = h_order_[bad_port];
-    throw ngpu_exception("Port index " + std::to_string((int)e_port_[o]) +
-                         " out of range for target node " + std::to_string(e_tgt_[o]));
-  }
-  if (bad_syn) throw ngpu_exception("Unrecognized synapse group");
-  NGPU_CUDA(cudaMalloc(&d_grp_off_, sizeof(unsigned long long) * h_grp_off_.size()));
-  NGPU_CUDA(cudaMemcpy(d_grp_off_, h_grp_off_.data(), sizeof(unsigned long long) * h_grp_off_.size(),
-                       cudaMemcpyHostToDevice));
-  NGPU_CUDA(cudaMalloc(&d_e_slot_, sizeof(unsigned) * (E > 0 ? E : 1)));
-  NGPU_CUDA(cudaMalloc(&d_e_w_, sizeof(float) * (E > 0 ? E : 1)));
-  if (E > 0) {
-    NGPU_CUDA(cudaMemcpy(d_e_slot_, slot.data(), sizeof(unsigned) * E, cudaMemcpyHostToDevice));
-    NGPU_CUDA(cudaMemcpy(d_e_w_, w.data(), sizeof(float) * E, cudaMemcpyHostToDevice));
-  }
-  std::vector<uint32_t>().swap(slot);
   std::vector<int> dl(delays_.begin(), delays_.end());
   NGPU_CUDA(cudaMalloc(&d_delays_, sizeof(int) * (nd > 0 ? nd : 1)));
   if (nd > 0) NGPU_CUDA(cudaMemcpy(d_delays_, dl.data(), sizeof(int) * nd, cudaMemcpyHostToDevice));
   if (nd > NGPU_MAX_DELAYS) throw ngpu_exception("Too many distinct delays");
-  // STDP structures: stamps, target ids and per-target incoming plastic lists
+  // STDP structures: stamps and per-target incoming plastic lists (the CSR
+  // targets d_e_post_ and groups d_e_syn_ are shared with the queries)
   if (plastic_) {
-    if (E >= 0xFFFFFFFFull) throw ngpu_exception("Too many connections for plastic synapses");
-    NGPU_CUDA(cudaMalloc(&d_e_syn_, E));
-    NGPU_CUDA(cudaMemcpy(d_e_syn_, syn.data(), E, cudaMemcpyHostToDevice));
-    NGPU_CUDA(cudaMalloc(&d_e_post_, sizeof(unsigned) * E));
-    NGPU_CUDA(cudaMemcpy(d_e_post_, post.data(), sizeof(unsigned) * E, cudaMemcpyHostToDevice));
-    NGPU_CUDA(cudaMalloc(&d_e_stamp_, sizeof(int) * E));
+    NGPU_CUDA(cudaMalloc(&d_e_stamp_, sizeof(int) * (E > 0 ? E : 1)));
     LaunchFillInt(d_e_stamp_, (long long)E, -(1 << 30), stream_);
-    std::vector<uint64_t> roff(N + 1, 0);
-    for (uint64_t k = 0; k < E; k++) if (syn[k] > 0) roff[post[k] + 1]++;
-    for (long long i = 0; i < N; i++) roff[i + 1] += roff[i];
-    std::vector<uint32_t> redge(roff[N]);
-    std::vector<uint64_t> fill(roff.begin(), roff.end() - 1);
-    for (uint64_t k = 0; k < E; k++) if (syn[k] > 0) redge[fill[post[k]]++] = (uint32_t)k;
     NGPU_CUDA(cudaMalloc(&d_rev_off_, sizeof(unsigned long long) * (N + 1)));
-    NGPU_CUDA(cudaMemcpy(d_rev_off_, roff.data(), sizeof(unsigned long long) * (N + 1), cudaMemcpyHostToDevice));
-    NGPU_CUDA(cudaMalloc(&d_rev_edge_, sizeof(unsigned) * (redge.size() + 1)));
-    if (!redge.empty())
-      NGPU_CUDA(cudaMemcpy(d_rev_edge_, redge.data(), sizeof(unsigned) * redge.size(), cudaMemcpyHostToDevice));
+    long long n_plastic = 0;
+    cudaError_t ce = DevPlasticLists(d_e_post_, d_e_syn_, (long long)E, N, d_rev_off_,
+                                     &d_rev_edge_, &n_plastic, stream_);
+    if (ce != cudaSuccess)
+      throw ngpu_exception(std::string("CUDA error building the plastic lists: ") + cudaGetErrorString(ce));
   }
   // node-level arrays
   NGPU_CUDA(cudaMalloc(&d_last_spike_T_, sizeof(int) * N));
@@ -1240,11 +1231,20 @@ void NeuronGPU::BuildDevice() {
     uint64_t stream = 0;
     for (int gi = 0; gi < n_gen_; gi++) {
       int s = gen_nodes_[gi];
+      const uint64_t b0 = h_grp_off_[(uint64_t)s * nd], e0 = h_grp_off_[(uint64_t)(s + 1) * nd];
+      const size_t m = (size_t)(e0 - b0);
+      std::vector<uint32_t> tg(m);
+      std::vector<uint8_t> pt(m);
+      std::vector<float> wt(m);
+      if (m > 0) {
+        NGPU_CUDA(cudaMemcpy(tg.data(), d_e_post_ + b0, sizeof(uint32_t) * m, cudaMemcpyDeviceToHost));
+        NGPU_CUDA(cudaMemcpy(pt.data(), d_c_port_ + b0, m, cudaMemcpyDeviceToHost));
+        NGPU_CUDA(cudaMemcpy(wt.data(), d_e_w_ + b0, sizeof(float) * m, cudaMemcpyDeviceToHost));
+      }
       for (int di = 0; di < nd; di++) {
         for (uint64_t k = h_grp_off_[(uint64_t)s * nd + di]; k < h_grp_off_[(uint64_t)s * nd + di + 1]; k++) {
-          uint64_t o = h_order_[k];
           DC c;
-          c.tgt = e_tgt_[o]; c.gen = gi; c.port = e_port_[o]; c.w = e_w_[o];
+          c.tgt = tg[k - b0]; c.gen = gi; c.port = pt[k - b0]; c.w = wt[k - b0];
           c.delay = time_resolution_ * (float)delays_[di];
           c.stream = stream++;
           dcs.push_back(c);

@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "ngpu_connect_device.h"
 #include "ngpu_device.h"
 #include "ngpu_kernels.h"
 #include "ngpu_models.h"
@@ -320,7 +321,7 @@ class NeuronGPU {
   int MlpInferHost(const float *x6, int n, const float *params, float *out);
   int SetGraphChunk(int g) { graph_chunk_ = g > 0 ? g : 1; InvalidateGraphs(); return 0; }
   long long NNodes() { return (long long)node_group_map_.size(); }
-  long long NConnections() { return (long long)e_src_.size(); }
+  long long NConnections() { return n_raw_ + (long long)p_src_.size(); }
   // every connection in delivery order (source, delay group, insertion);
   // null outputs are skipped; weights are the device values once calibrated
   long long ExportConnections(int *src, int *tgt, int *port, int *syn,
@@ -378,17 +379,32 @@ class NeuronGPU {
   std::vector<SynGroupHost> syn_groups_;
   std::vector<Record> records_;
 
-  // edges in insertion order (before calibration)
-  std::vector<uint32_t> e_src_, e_tgt_;
-  std::vector<uint8_t> e_port_, e_syn_;
-  std::vector<float> e_w_;
-  std::vector<uint16_t> e_d_;         // delay in steps (>= 1)
-  bool host_csr_valid_ = false;
-  // host CSR (by source, then delay index, insertion order inside)
+  // edges in insertion order: device edge store filled by the rule kernels
+  // (freed at calibration), single connections buffered on the host
+  EdgeStore d_raw_ = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  long long n_raw_ = 0, raw_cap_ = 0;
+  std::vector<uint32_t> p_src_, p_tgt_;
+  std::vector<uint8_t> p_port_, p_syn_;
+  std::vector<float> p_w_;
+  std::vector<uint16_t> p_d_;
+  bool any_plastic_ = false;          // an edge with synapse group > 0 exists
+  bool csr_valid_ = false;
+  // CSR by source, then delay index, insertion order inside (device arrays
+  // d_grp_off_, d_e_post_ = targets, d_c_port_, d_e_syn_, d_e_w_; host copy
+  // of the group offsets; host mirrors of targets, ports and groups for the
+  // connection queries, made on demand)
   std::vector<int> delays_;           // distinct delays (steps), sorted
   std::vector<int> delay_index_;      // D -> di (or -1)
   std::vector<uint64_t> h_grp_off_;   // [n_nodes*nd + 1]
-  std::vector<uint64_t> h_order_;     // csr position -> insertion index
+  unsigned char *d_c_port_ = nullptr;
+  std::vector<uint32_t> h_c_tgt_;
+  std::vector<uint8_t> h_c_port_, h_c_syn_;
+  bool mirror_valid_ = false;
+  void GrowRaw(long long need);
+  void FlushPending();
+  void FreeRaw();
+  void FreeCSR();
+  void EnsureMirror();
 
   // device state
   bool calibrate_flag_ = false;
@@ -470,7 +486,7 @@ class NeuronGPU {
   NodeGroup *GroupOf(int i_node, int n, int &i_local);
   NodeGroup *GroupOfList(const int *nodes, int n, std::vector<int> &local);
   void CheckUncalibrated(const std::string &msg);
-  void BuildHostCSR();
+  void BuildCSR();
   void BuildDevice();
   void UploadGeneratorParams();
   void FlushRecords();

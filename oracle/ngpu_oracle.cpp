@@ -644,6 +644,85 @@ void *orc_create(double dt, unsigned long long seed) {
 
 void orc_free(void *h) { delete (Oracle *)h; }
 
+// Connection rules (src/connect_rules.h:48-400) with the library's random
+// streams: per call index `call`, fixed_total_number draws pair k from
+// Philox(seed, CONNECT, call, k); fixed_indegree / fixed_outdegree draw K
+// distinct pool members for every outer node o from
+// Philox(seed, SOURCE_SET, call, o, draw) by partial Fisher-Yates (pool
+// < 5 K) or rejection of repeats. Writes the source and target list indices
+// of every connection in insertion order; returns their number.
+long long orc_rule_edges(int rule, unsigned long long seed, unsigned long long call,
+                         int n_source, int n_target, int param, int *out_s, int *out_t) {
+  long long m = 0;
+  switch (rule) {
+    case 0:  // one_to_one
+      for (int k = 0; k < n_source; k++) { out_s[m] = k; out_t[m] = k; m++; }
+      break;
+    case 1:  // all_to_all
+      for (int it = 0; it < n_target; it++)
+        for (int is = 0; is < n_source; is++) { out_s[m] = is; out_t[m] = it; m++; }
+      break;
+    case 2:  // fixed_total_number
+      for (long long k = 0; k < param; k++) {
+        ngpu::Philox4 r = ngpu::ng_random_block(seed, ngpu::RNG_TAG_CONNECT, call, (uint64_t)k, 0);
+        out_s[m] = (int)(r.v[0] % (uint32_t)n_source);
+        out_t[m] = (int)(r.v[1] % (uint32_t)n_target);
+        m++;
+      }
+      break;
+    case 3: case 4: {  // fixed_indegree, fixed_outdegree
+      const bool indeg = rule == 3;
+      const int K = param;
+      const long long n_outer = indeg ? n_target : n_source;
+      const long long n_pool = indeg ? n_source : n_target;
+      std::vector<int> pick(K);
+      for (long long o = 0; o < n_outer; o++) {
+        if (n_pool < 5LL * K) {
+          std::vector<int> perm(n_pool);
+          for (long long j = 0; j < n_pool; j++) perm[j] = (int)j;
+          for (int i = 0; i < K; i++) {
+            ngpu::Philox4 r = ngpu::ng_random_block(seed, ngpu::RNG_TAG_SOURCE_SET, call,
+                                                    (uint64_t)o, (uint32_t)i);
+            long long j = i + (long long)(r.v[0] % (uint32_t)(n_pool - i));
+            std::swap(perm[i], perm[j]);
+            pick[i] = perm[i];
+          }
+        } else {
+          int cap = 16;
+          while (cap < 2 * K) cap <<= 1;
+          std::vector<int> table(cap, -1);
+          uint32_t draw = 0;
+          for (int i = 0; i < K; i++) {
+            int j;
+            for (;;) {
+              ngpu::Philox4 r = ngpu::ng_random_block(seed, ngpu::RNG_TAG_SOURCE_SET, call,
+                                                      (uint64_t)o, draw++);
+              j = (int)(r.v[0] % (uint32_t)n_pool);
+              uint32_t h = ((uint32_t)j * 0x9E3779B1u) & (uint32_t)(cap - 1);
+              bool dup = false;
+              while (table[h] >= 0) {
+                if (table[h] == j) { dup = true; break; }
+                h = (h + 1) & (uint32_t)(cap - 1);
+              }
+              if (!dup) { table[h] = j; break; }
+            }
+            pick[i] = j;
+          }
+        }
+        for (int i = 0; i < K; i++) {
+          out_s[m] = indeg ? pick[i] : (int)o;
+          out_t[m] = indeg ? (int)o : pick[i];
+          m++;
+        }
+      }
+      break;
+    }
+    default:
+      return -1;
+  }
+  return m;
+}
+
 // host threads of the parallel node-update and fold loops (results do not
 // depend on it)
 void orc_set_threads(int n) {

@@ -89,6 +89,9 @@ def _load():
     lib.orc_stage_evals.restype = ctypes.c_longlong
     lib.orc_stage_evals.argtypes = (ctypes.c_void_p,)
     lib.orc_set_threads.argtypes = (ctypes.c_int,)
+    lib.orc_rule_edges.restype = ctypes.c_longlong
+    lib.orc_rule_edges.argtypes = (ctypes.c_int, ctypes.c_ulonglong, ctypes.c_ulonglong,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _ip)
     lib.orc_get_threads.restype = ctypes.c_int
     return lib
 
@@ -111,6 +114,27 @@ def set_threads(n):
 
 def get_threads():
     return lib().orc_get_threads()
+
+
+RULES = {"one_to_one": 0, "all_to_all": 1, "fixed_total_number": 2, "fixed_indegree": 3,
+         "fixed_outdegree": 4}
+
+
+def rule_edges(rule, seed, call, n_source, n_target, param=0):
+    """Source and target list indices of a connection rule's connections in
+    insertion order (param: total number, in-degree or out-degree)."""
+    r = RULES[rule]
+    cap = {0: n_source, 1: n_source * n_target}.get(r, 0)
+    if r == 2:
+        cap = param
+    elif r == 3:
+        cap = n_target * param
+    elif r == 4:
+        cap = n_source * param
+    s = np.zeros(max(cap, 1), dtype=np.int32)
+    t = np.zeros(max(cap, 1), dtype=np.int32)
+    m = lib().orc_rule_edges(r, seed, call, n_source, n_target, param, _ptr(s, _ip), _ptr(t, _ip))
+    return s[:m], t[:m]
 
 
 def _ptr(a, t):
