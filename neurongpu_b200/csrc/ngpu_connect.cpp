@@ -1,6 +1,8 @@
-// Connections: specification objects, connection rules, the host CSR that
-// becomes the device delivery graph, connection queries, synapse groups and
-// the host random-array helpers.
+// Connections: specification objects, the connection-rule driver (rules run
+// on the GPU, ngpu_connect_device.cu, appending to a device edge store), the
+// device CSR that becomes the delivery graph, connection queries (served
+// from host copies of the CSR made on demand), synapse groups and the host
+// random-array helpers.
 //
 // Reference behaviour followed (paths within golosio/NeuronGPU):
 //   ConnSpec / SynSpec parameters      src/connect_rules.cpp:14-230, src/connect_spec.h
