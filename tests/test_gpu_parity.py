@@ -245,3 +245,58 @@ def test_connection_queries(ngpu):
     ngpu.Simulate(5.0)
     st2 = ngpu.GetStatus(conns[0])
     assert st2 == st
+
+
+def test_izhikevich_cond_beta_vs_oracle(ngpu):
+    """izhikevich_cond_beta (src/izhikevich_cond_beta_kernel.h) driven by a
+    bias current and excitatory / inhibitory spike trains, 300 ms against the
+    FP64 oracle: the membrane trace up to the first spike (1e-4 relative) and
+    every spike within one step."""
+    from oracle import oracle as orc
+    params = {"I_e": 8.0, "E_rev": [0.0, -85.0], "tau_rise": [0.5, 1.0],
+              "tau_decay": [3.0, 8.0]}
+    times = [10.0, 40.0, 70.0, 100.5, 160.0, 220.0]
+    n = ngpu.Create("izhikevich_cond_beta", 1, 2)
+    ngpu.SetStatus(n, params)
+    sg = ngpu.Create("spike_generator", 2)
+    ngpu.SetStatus([sg[0]], {"spike_times": times})
+    ngpu.SetStatus([sg[1]], {"spike_times": [t + 25.0 for t in times]})
+    ngpu.Connect([sg[0]], n, {"rule": "all_to_all"}, {"weight": 0.8, "delay": 1.0, "receptor": 0})
+    ngpu.Connect([sg[1]], n, {"rule": "all_to_all"}, {"weight": 0.5, "delay": 1.0, "receptor": 1})
+    ngpu.ActivateRecSpikeTimes(n, 100)
+    rec = ngpu.CreateRecord("", ["V_m"], [n[0]], [0])
+    ngpu.Simulate(300.0)
+    v = np.asarray(ngpu.GetRecordData(rec))[1:, 1]
+    net = orc.Network(dt=0.1)
+    on = net.create(orc.IZH_COND_BETA, 1, 2,
+                    params={k: (np.float32(x) if np.isscalar(x) else [np.float32(y) for y in x])
+                            for k, x in params.items()})
+    og = net.create(orc.SPIKE_GENERATOR, 2)
+    net.set_spikes(og, [times, [t + 25.0 for t in times]])
+    net.connect([og.i0], [on.i0], 0, 0.8, 1.0)
+    net.connect([og.i0 + 1], [on.i0], 1, 0.5, 1.0)
+    ov = net.simulate(3000, record=[(on.i0, on.var_index("V_m"))])[:, 0]
+    steps, _ = net.spikes()
+    g_spk = np.rint(np.asarray(ngpu.GetRecSpikeTimes(n[0])) / 0.1).astype(int)
+    assert len(steps) >= 3 and len(g_spk) == len(steps)
+    assert np.max(np.abs(g_spk - (steps + 1))) <= 1
+    first = int(steps.min())
+    assert np.max(np.abs(v[:first] - ov[:first])) / max(1.0, np.max(np.abs(ov))) < 1e-4
+
+
+def test_poisson_generator_nodes_statistics(ngpu):
+    """CreatePoissonGenerator nodes (src/poisson.cu:26-147): every node emits a
+    spike of height n ~ Poisson(rate dt) whenever n > 0; the fraction of
+    steps with a spike matches 1 - exp(-lambda) within 5 sigma."""
+    n, rate, t_ms = 2000, 3000.0, 200.0
+    pg = ngpu.CreatePoissonGenerator(n, rate)
+    ngpu.ActivateSpikeCount(pg)
+    ngpu.Simulate(t_ms)
+    counts = np.asarray(ngpu.GetNeuronIntVarArray(pg.i0, pg.n, "spike_count"), dtype=float)
+    lam = rate * 0.1 / 1000.0
+    steps = t_ms / 0.1
+    p = 1.0 - np.exp(-lam)
+    mean = counts.sum() / (n * steps)
+    sigma = np.sqrt(p * (1.0 - p) / (n * steps))
+    assert abs(mean - p) < 5.0 * sigma, (mean, p, sigma)
+    assert counts.std() > 0
