@@ -276,7 +276,8 @@ def test_izhikevich_cond_beta_vs_oracle(ngpu):
     net.connect([og.i0], [on.i0], 0, 0.8, 1.0)
     net.connect([og.i0 + 1], [on.i0], 1, 0.5, 1.0)
     ov = net.simulate(3000, record=[(on.i0, on.var_index("V_m"))])[:, 0]
-    steps, _ = net.spikes()
+    steps, nodes = net.spikes()
+    steps = steps[nodes == on.i0]
     g_spk = np.rint(np.asarray(ngpu.GetRecSpikeTimes(n[0])) / 0.1).astype(int)
     assert len(steps) >= 3 and len(g_spk) == len(steps)
     assert np.max(np.abs(g_spk - (steps + 1))) <= 1
