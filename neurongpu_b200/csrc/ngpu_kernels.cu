@@ -251,6 +251,9 @@ void LaunchSpikeDetectorUpdate(const GroupArgs &g, const InputArgs &in,
 // CreatePoissonGenerator nodes: one count per node per step pushed as a
 // spike of that height (src/poisson.cu:26-54)
 // ---------------------------------------------------------------------------
+// The reference draws the counts in blocks of ceil(1e5 / n) steps and zeroes
+// counts above 5 lambda in the first step of every block only
+// (src/poisson.cu:45-88: the fix-up kernel covers n_node entries).
 __global__ void k_poisson_nodes(GroupArgs g, PushArgs pa, double lambda,
                                 double explam, unsigned long long seed,
                                 StepCtx *ctx) {
@@ -260,7 +263,8 @@ __global__ void k_poisson_nodes(GroupArgs g, PushArgs pa, double lambda,
   const long long T = T0 + it + 1;
   unsigned n = ng_poisson(lambda, explam, seed, RNG_TAG_POISSON_NODE,
                           (unsigned long long)(g.i_node_0 + i), T);
-  if ((float)n > (float)lambda * 5.0f) n = 0;
+  const long long block_steps = (100000 - 1) / g.n + 1;
+  if ((T - 1) % block_steps == 0 && (float)n > (float)lambda * 5.0f) n = 0;
   if (n > 0) {
     const double t_now = ctx->t0 + (double)g.dt * (double)(it + 1);
     push_spike(pa, ctx, g.i_node_0 + i, i, (float)n, T, t_now, 0);

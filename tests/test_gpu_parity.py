@@ -287,8 +287,10 @@ def test_izhikevich_cond_beta_vs_oracle(ngpu):
 
 def test_poisson_generator_nodes_statistics(ngpu):
     """CreatePoissonGenerator nodes (src/poisson.cu:26-147): every node emits a
-    spike of height n ~ Poisson(rate dt) whenever n > 0; the fraction of
-    steps with a spike matches 1 - exp(-lambda) within 5 sigma."""
+    spike of height n ~ Poisson(rate dt) whenever n > 0, except that counts
+    above 5 lambda are dropped in the first step of every block of
+    ceil(1e5 / n) steps (src/poisson.cu:45-88); the fraction of steps with a
+    spike matches that expectation within 5 sigma."""
     n, rate, t_ms = 2000, 3000.0, 200.0
     pg = ngpu.CreatePoissonGenerator(n, rate)
     ngpu.ActivateSpikeCount(pg)
@@ -296,7 +298,12 @@ def test_poisson_generator_nodes_statistics(ngpu):
     counts = np.asarray(ngpu.GetNeuronIntVarArray(pg.i0, pg.n, "spike_count"), dtype=float)
     lam = rate * 0.1 / 1000.0
     steps = t_ms / 0.1
-    p = 1.0 - np.exp(-lam)
+    from math import exp, factorial, floor
+    p_any = 1.0 - exp(-lam)
+    p_kept = sum(exp(-lam) * lam ** k / factorial(k) for k in range(1, floor(5 * lam) + 1))
+    block = (100000 - 1) // n + 1
+    n_first = len([s for s in range(int(steps)) if s % block == 0])
+    p = (p_kept * n_first + p_any * (steps - n_first)) / steps
     mean = counts.sum() / (n * steps)
     sigma = np.sqrt(p * (1.0 - p) / (n * steps))
     assert abs(mean - p) < 5.0 * sigma, (mean, p, sigma)
