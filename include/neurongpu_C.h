@@ -270,6 +270,15 @@ int NGB200_MlpInfer(const float *x6, int n_rows, const float *params, float *out
  * connections one status call at a time, src/neurongpu_C.h:294-331). */
 long long NGB200_GetAllConnections(int *src, int *tgt, int *port, int *syn,
                                    float *delay, float *weight);
+/* Releases an array returned by one of the entry points that hand the
+ * caller a fresh host array: NeuronGPU_GetNeuronParam / GetNeuronPtParam /
+ * GetArrayParam / GetNeuronIntVar / GetNeuronVar / GetNeuronPtIntVar /
+ * GetNeuronPtVar / GetArrayVar / GetRecSpikeTimes / GetRecordData (the row
+ * table only) / Random* and the Get*Connections lists. The reference's
+ * entry points (src/neurongpu_C.h:54, 109-129, 151-157, 244-255, 284) hand
+ * out such arrays with no way to release them; calling this is optional,
+ * null is ignored. */
+void NGB200_FreeArray(void *p);
 /* Device time (CUDA events on the simulation stream) of the step loop of the
  * last NeuronGPU_Simulate call, in ms. */
 double NGB200_LastSimulateDeviceMs();

@@ -136,7 +136,7 @@ int NeuronGPU_GetRecordDataColumns(int i_record) {
 float **NeuronGPU_GetRecordData(int i_record) {
   return guarded((float **)nullptr, [&](NeuronGPU *n) {
     auto *d = n->GetRecordData(i_record);
-    float **rows = new float *[d->size() > 0 ? d->size() : 1];
+    float **rows = (float **)malloc(sizeof(float *) * (d->size() > 0 ? d->size() : 1));
     for (size_t i = 0; i < d->size(); i++) rows[i] = d->at(i).data();
     return rows;
   });
@@ -471,7 +471,7 @@ int NeuronGPU_GetNRecSpikeTimes(int i_node) {
 float *NeuronGPU_GetRecSpikeTimes(int i_node) {
   return guarded((float *)nullptr, [&](NeuronGPU *n) {
     std::vector<float> v = n->GetRecSpikeTimes(i_node);
-    float *a = new float[v.size() > 0 ? v.size() : 1];
+    float *a = (float *)malloc(sizeof(float) * (v.size() > 0 ? v.size() : 1));
     for (size_t i = 0; i < v.size(); i++) a[i] = v[i];
     return a;
   });
@@ -615,6 +615,7 @@ long long NGB200_GetAllConnections(int *src, int *tgt, int *port, int *syn,
     return n->ExportConnections(src, tgt, port, syn, delay, weight);
   });
 }
+void NGB200_FreeArray(void *p) { free(p); }
 double NGB200_LastSimulateDeviceMs() {
   return guarded(0.0, [&](NeuronGPU *n) { return n->LastSimulateDeviceMs(); });
 }

@@ -516,11 +516,11 @@ int NeuronGPU::SetSynGroupParam(int sg, const std::string &n, float v) {
 }
 
 // ---------------------------------------------------------------------------
-// random arrays: caller owns the returned new[] arrays
+// random arrays: the caller owns the returned malloc'd arrays
 // ---------------------------------------------------------------------------
 unsigned int *NeuronGPU::RandomInt(size_t n) {
   unsigned long long st = NextRngStream();
-  unsigned int *a = new unsigned int[n > 0 ? n : 1];
+  unsigned int *a = (unsigned int *)malloc(sizeof(unsigned int) * (n > 0 ? n : 1));
   for (size_t k = 0; k < n; k++) {
     Philox4 r = ng_random_block(rnd_seed_, RNG_TAG_ARRAY, st, (int64_t)(k >> 2), 0);
     a[k] = r.v[k & 3];
@@ -530,7 +530,7 @@ unsigned int *NeuronGPU::RandomInt(size_t n) {
 
 float *NeuronGPU::RandomUniform(size_t n) {
   unsigned long long st = NextRngStream();
-  float *a = new float[n > 0 ? n : 1];
+  float *a = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
   for (size_t k = 0; k < n; k++) {
     Philox4 r = ng_random_block(rnd_seed_, RNG_TAG_ARRAY, st, (int64_t)(k >> 1), 0);
     int j = (int)(k & 1) * 2;
@@ -554,7 +554,7 @@ static void normal_fill(float *a, size_t n, float mean, float stddev,
 }
 
 float *NeuronGPU::RandomNormal(size_t n, float mean, float stddev) {
-  float *a = new float[n > 0 ? n : 1];
+  float *a = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
   normal_fill(a, n, mean, stddev, rnd_seed_, NextRngStream());
   return a;
 }
@@ -566,7 +566,7 @@ float *NeuronGPU::RandomNormalClipped(size_t n, float mean, float stddev, float 
   const float epsi = 1.0e-6f;
   if (vmax < vmin) throw ngpu_exception("Clipping range is empty");
   size_t n_alloc = (n / 4 + 1) * 4;
-  float *a = new float[n_alloc];
+  float *a = (float *)malloc(sizeof(float) * n_alloc);
   normal_fill(a, n_alloc, mean, stddev, rnd_seed_, NextRngStream());
   std::vector<float> extra;
   size_t ie = 0;
@@ -574,7 +574,10 @@ float *NeuronGPU::RandomNormalClipped(size_t n, float mean, float stddev, float 
   for (size_t k = 0; k < n_alloc; k++) {
     while (a[k] < vmin || a[k] > vmax) {
       if (ie >= extra.size()) {
-        if (++rounds > 100000) throw ngpu_exception("Clipped normal distribution has negligible mass in range");
+        if (++rounds > 100000) {
+          free(a);
+          throw ngpu_exception("Clipped normal distribution has negligible mass in range");
+        }
         extra.assign(std::max<size_t>(n_alloc / 10 + 4, 1024), 0.0f);
         normal_fill(extra.data(), extra.size(), mean, stddev, rnd_seed_, NextRngStream());
         ie = 0;

@@ -332,6 +332,8 @@ void NeuronGPU::SetParamColumn(NodeGroup *g, int col, int i0, int n,
                                int stride) {
   float *base = g->d_param + (size_t)col * g->n_pad;
   bool whole = (nodes == nullptr && i0 == 0 && n == g->n_node);
+  const char old_uniform = g->p_uniform[col];
+  const float old_uval = g->p_uval[col];
   if (vals == nullptr) {
     if (whole) {
       g->p_uniform[col] = 1;
@@ -368,7 +370,11 @@ void NeuronGPU::SetParamColumn(NodeGroup *g, int col, int i0, int n,
     if (d_vals) cudaFree(d_vals);
   }
   NGPU_CUDA(cudaStreamSynchronize(stream_));
-  InvalidateGraphs();
+  // captured step graphs hold the uniform values (and which columns are
+  // per-neuron) as kernel arguments; per-neuron columns are read from device
+  // memory, so the graphs stay valid unless that information changed
+  if (g->p_uniform[col] != old_uniform || (g->p_uniform[col] && g->p_uval[col] != old_uval))
+    InvalidateGraphs();
 }
 
 void NeuronGPU::GetParamColumn(NodeGroup *g, float *col_base, int i0, int n,
@@ -675,8 +681,13 @@ int *NeuronGPU::GetNeuronIntVar(const int *nodes, int n, const std::string &name
   if (j < 0) throw ngpu_exception(std::string("Unrecognized variable ") + name);
   int *base = (g->int_var_names[j] == "spike_count") ? g->d_spike_count : g->d_n_rec;
   int *out = (int *)malloc(sizeof(int) * n);
-  for (int k = 0; k < n; k++)
-    NGPU_CUDA(cudaMemcpy(out + k, base + loc[k], sizeof(int), cudaMemcpyDeviceToHost));
+  if (n == 0) return out;
+  // one copy of the span the list covers, then a host-side pick
+  auto mm = std::minmax_element(loc.begin(), loc.end());
+  std::vector<int> span((size_t)(*mm.second - *mm.first) + 1);
+  NGPU_CUDA(cudaMemcpy(span.data(), base + *mm.first, sizeof(int) * span.size(),
+                       cudaMemcpyDeviceToHost));
+  for (int k = 0; k < n; k++) out[k] = span[loc[k] - *mm.first];
   return out;
 }
 

@@ -241,6 +241,7 @@ _EXT_SIG = {
     "NGB200_NConnections": (ctypes.c_longlong, ()),
     "NGB200_GetAllConnections": (ctypes.c_longlong, (c_int_p, c_int_p, c_int_p, c_int_p,
                                                      c_float_p, c_float_p)),
+    "NGB200_FreeArray": (None, (c_void_p,)),
     "NGB200_SetRk5Batching": (_I, (_I,)),
     "NGB200_Rk5BatchOf": (_I, (_I,)),
     "NGB200_SetStepLog": (_I, (_I, _I)),
@@ -309,6 +310,13 @@ class Binding(object):
         if self._c["GetErrorCode"]() != 0:
             raise ValueError(self.GetErrorMessage())
         return ret
+
+    def _release(self, pt, value):
+        """Frees a host array the library handed out (after its contents
+        were copied into value) and returns value."""
+        if pt:
+            self._c["NGB200_FreeArray"](ctypes.cast(pt, c_void_p))
+        return value
 
     def _names(self, fn, count, *args):
         n = count
@@ -538,30 +546,32 @@ class Binding(object):
 
     def GetNeuronParam(self, i_node, n_node, param_name):
         "Get neuron parameter value"
+        sz = self.GetNeuronParamSize(i_node, param_name)
         pt = self._call("GetNeuronParam", ctypes.c_int(i_node), ctypes.c_int(n_node),
                         _cstr(param_name))
-        return self._rows(pt, n_node, self.GetNeuronParamSize(i_node, param_name))
+        return self._release(pt, self._rows(pt, n_node, sz))
 
     def GetNeuronPtParam(self, nodes, param_name):
         a, p = self._nodes_arr(nodes)
+        sz = self.GetNeuronParamSize(nodes[0], param_name)
         pt = self._call("GetNeuronPtParam", p, ctypes.c_int(len(nodes)), _cstr(param_name))
-        return self._rows(pt, len(nodes), self.GetNeuronParamSize(nodes[0], param_name))
+        return self._release(pt, self._rows(pt, len(nodes), sz))
 
     def GetArrayParam(self, i_node, n_node, param_name):
         "Get neuron array parameter"
         out = []
         for j in range(n_node):
-            pt = self._call("GetArrayParam", ctypes.c_int(i_node + j), _cstr(param_name))
             sz = self.GetNeuronParamSize(i_node + j, param_name)
-            out.append([pt[k] for k in range(sz)])
+            pt = self._call("GetArrayParam", ctypes.c_int(i_node + j), _cstr(param_name))
+            out.append(self._release(pt, [pt[k] for k in range(sz)]))
         return out
 
     def GetNeuronListArrayParam(self, node_list, param_name):
         out = []
         for i in node_list:
-            pt = self._call("GetArrayParam", ctypes.c_int(i), _cstr(param_name))
             sz = self.GetNeuronParamSize(i, param_name)
-            out.append([pt[k] for k in range(sz)])
+            pt = self._call("GetArrayParam", ctypes.c_int(i), _cstr(param_name))
+            out.append(self._release(pt, [pt[k] for k in range(sz)]))
         return out
 
     def GetNeuronGroupParam(self, i_node, param_name):
@@ -576,37 +586,41 @@ class Binding(object):
         import numpy as np
         pt = self._call("GetNeuronIntVar", ctypes.c_int(i_node), ctypes.c_int(n_node),
                         _cstr(var_name))
-        return np.ctypeslib.as_array(pt, shape=(n_node,)).copy()
+        if n_node <= 0:
+            return self._release(pt, np.zeros(0, dtype=np.int32))
+        return self._release(pt, np.ctypeslib.as_array(pt, shape=(n_node,)).copy())
 
     def GetNeuronVar(self, i_node, n_node, var_name):
+        sz = self.GetNeuronVarSize(i_node, var_name)
         pt = self._call("GetNeuronVar", ctypes.c_int(i_node), ctypes.c_int(n_node),
                         _cstr(var_name))
-        return self._rows(pt, n_node, self.GetNeuronVarSize(i_node, var_name))
+        return self._release(pt, self._rows(pt, n_node, sz))
 
     def GetNeuronPtIntVar(self, nodes, var_name):
         a, p = self._nodes_arr(nodes)
         pt = self._call("GetNeuronPtIntVar", p, ctypes.c_int(len(nodes)), _cstr(var_name))
-        return [[pt[i]] for i in range(len(nodes))]
+        return self._release(pt, [[pt[i]] for i in range(len(nodes))])
 
     def GetNeuronPtVar(self, nodes, var_name):
         a, p = self._nodes_arr(nodes)
+        sz = self.GetNeuronVarSize(nodes[0], var_name)
         pt = self._call("GetNeuronPtVar", p, ctypes.c_int(len(nodes)), _cstr(var_name))
-        return self._rows(pt, len(nodes), self.GetNeuronVarSize(nodes[0], var_name))
+        return self._release(pt, self._rows(pt, len(nodes), sz))
 
     def GetArrayVar(self, i_node, n_node, var_name):
         out = []
         for j in range(n_node):
-            pt = self._call("GetArrayVar", ctypes.c_int(i_node + j), _cstr(var_name))
             sz = self.GetNeuronVarSize(i_node + j, var_name)
-            out.append([pt[k] for k in range(sz)])
+            pt = self._call("GetArrayVar", ctypes.c_int(i_node + j), _cstr(var_name))
+            out.append(self._release(pt, [pt[k] for k in range(sz)]))
         return out
 
     def GetNeuronListArrayVar(self, node_list, var_name):
         out = []
         for i in node_list:
-            pt = self._call("GetArrayVar", ctypes.c_int(i), _cstr(var_name))
             sz = self.GetNeuronVarSize(i, var_name)
-            out.append([pt[k] for k in range(sz)])
+            pt = self._call("GetArrayVar", ctypes.c_int(i), _cstr(var_name))
+            out.append(self._release(pt, [pt[k] for k in range(sz)]))
         return out
 
     def GetNeuronStatus(self, nodes, var_name):
@@ -757,10 +771,10 @@ class Binding(object):
 
     def GetRecordData(self, i_record):
         "Get record data"
-        pt = self._call("GetRecordData", ctypes.c_int(i_record))
         nr = self.GetRecordDataRows(i_record)
         nc = self.GetRecordDataColumns(i_record)
-        return [[pt[r][c] for c in range(nc)] for r in range(nr)]
+        pt = self._call("GetRecordData", ctypes.c_int(i_record))
+        return self._release(pt, [[pt[r][c] for c in range(nc)] for r in range(nr)])
 
     def ActivateSpikeCount(self, nodes):
         "Activate spike count for node group"
@@ -780,8 +794,9 @@ class Binding(object):
 
     def GetRecSpikeTimes(self, i_node):
         "Get recorded spike times for node"
+        n = self.GetNRecSpikeTimes(i_node)
         pt = self._call("GetRecSpikeTimes", ctypes.c_int(i_node))
-        return [pt[k] for k in range(self.GetNRecSpikeTimes(i_node))]
+        return self._release(pt, [pt[k] for k in range(n)])
 
     # -- simulation ----------------------------------------------------------
     def Calibrate(self):
@@ -1037,8 +1052,8 @@ class Binding(object):
             else:
                 arr = self._call("GetGroupGroupConnections", sp, len(source), tp, len(target),
                                  syn_group, ctypes.byref(n_conn))
-        return [ConnectionId(arr[3 * i], arr[3 * i + 1], arr[3 * i + 2])
-                for i in range(n_conn.value)]
+        return self._release(arr, [ConnectionId(arr[3 * i], arr[3 * i + 1], arr[3 * i + 2])
+                                   for i in range(n_conn.value)])
 
     def GetConnectionStatus(self, conn_id):
         i_target = ctypes.c_int(0)

@@ -223,6 +223,48 @@ def test_api_status_roundtrip(ngpu):
     assert b[0] == pytest.approx(80.5)
 
 
+def test_param_changes_between_calls(ngpu):
+    """Captured step graphs follow every parameter change made between
+    Simulate calls: group-wide values, per-neuron values, a switch back to a
+    group-wide value and a generator rate; re-setting an unchanged value
+    leaves the results alone."""
+    nrn = ngpu.Create("aeif_cond_beta", 10, 2)
+    pg = ngpu.Create("poisson_generator")
+    ngpu.SetStatus(pg, "rate", 0.0)
+    ngpu.Connect(pg, nrn, {"rule": "all_to_all"}, {"weight": 1.0, "delay": 1.0, "receptor": 0})
+    ngpu.ActivateSpikeCount(nrn)
+
+    def counts():
+        return np.asarray(ngpu.GetNeuronIntVarArray(nrn.i0, nrn.n, "spike_count"))
+
+    ngpu.Simulate(20.0)
+    assert counts().sum() == 0
+    ngpu.SetStatus(nrn, "I_e", 0.0)                    # unchanged
+    ngpu.Simulate(20.0)
+    assert counts().sum() == 0
+    ngpu.SetStatus(nrn, "I_e", 1000.0)                 # new group-wide value
+    ngpu.Simulate(50.0)
+    c1 = counts()
+    assert (c1 > 0).all()
+    ngpu.SetStatus(nrn, "I_e", 0.0)
+    ngpu.SetStatus(nrn[0:3], "I_e", 1000.0)            # per-neuron column
+    ngpu.Simulate(50.0)
+    c2 = counts() - c1
+    assert (c2[0:3] > 0).all() and (c2[3:] == 0).all()
+    ngpu.SetStatus(nrn[3:5], "I_e", 1000.0)            # still per-neuron
+    ngpu.Simulate(50.0)
+    c3 = counts() - c1 - c2
+    assert (c3[0:5] > 0).all() and (c3[5:] == 0).all()
+    ngpu.SetStatus(nrn, "I_e", 0.0)                    # back to group-wide
+    ngpu.Simulate(50.0)                                # adaptation settles
+    c4 = counts()
+    ngpu.Simulate(50.0)
+    assert (counts() == c4).all()
+    ngpu.SetStatus(pg, "rate", 50000.0)                # generator rate
+    ngpu.Simulate(50.0)
+    assert (counts() > c4).all()
+
+
 def test_connection_queries(ngpu):
     a = ngpu.Create("aeif_cond_beta", 20, 2)
     b = ngpu.Create("aeif_cond_beta", 30, 2)
