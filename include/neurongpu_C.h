@@ -282,6 +282,9 @@ void NGB200_FreeArray(void *p);
 /* Device time (CUDA events on the simulation stream) of the step loop of the
  * last NeuronGPU_Simulate call, in ms. */
 double NGB200_LastSimulateDeviceMs();
+/* Kernel launches per time step in the most recently captured step graph
+ * (0 before the first capture). No reference counterpart. */
+double NGB200_KernelsPerStep();
 /* Per-kernel-class timing: on != 0 records CUDA events around every kernel
  * class of every step (resets the totals). Classes: 0 node updates,
  * 1 spike delivery, 2 STDP post rule, 3 recording and step bookkeeping. */

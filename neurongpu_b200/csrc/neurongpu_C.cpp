@@ -616,6 +616,9 @@ long long NGB200_GetAllConnections(int *src, int *tgt, int *port, int *syn,
   });
 }
 void NGB200_FreeArray(void *p) { free(p); }
+double NGB200_KernelsPerStep() {
+  return guarded(0.0, [&](NeuronGPU *n) { return n->KernelsPerStep(); });
+}
 double NGB200_LastSimulateDeviceMs() {
   return guarded(0.0, [&](NeuronGPU *n) { return n->LastSimulateDeviceMs(); });
 }

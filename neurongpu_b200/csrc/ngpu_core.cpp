@@ -70,6 +70,7 @@ void NeuronGPU::FreeDevice() {
     F(g->d_spike_count); F(g->d_rec_times); F(g->d_n_rec);
     F(g->d_sg_off); F(g->d_sg_step); F(g->d_sg_next); F(g->d_sg_height);
     F(g->d_blk_evals);
+    FreeRk5Queue(g->q);
     F(g->d_log_buf); F(g->d_log_count);
     g->d_log_buf = nullptr;
     g->d_log_count = nullptr;
@@ -905,6 +906,7 @@ GroupArgs NeuronGPU::MakeGroupArgs(NodeGroup *g) {
   a.dry = 0;
   a.den_delay_col = g->mi->den_delay_param;
   a.blk_evals = g->d_blk_evals;
+  a.q = g->q;
   a.step_mode = g->step_mode;
   a.mlp_margin = mlp_margin_;
   a.mlp = d_mlp_img_;
@@ -1604,6 +1606,17 @@ void NeuronGPU::LaunchSteps(int n_steps) {
       }
       capturing_ = false;
       NGPU_CUDA(cudaStreamEndCapture(stream_, &graph));
+      size_t n_nodes = 0;
+      NGPU_CUDA(cudaGraphGetNodes(graph, nullptr, &n_nodes));
+      std::vector<cudaGraphNode_t> nodes(n_nodes);
+      if (n_nodes > 0) NGPU_CUDA(cudaGraphGetNodes(graph, nodes.data(), &n_nodes));
+      long long n_kernels = 0;
+      for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType ty;
+        NGPU_CUDA(cudaGraphNodeGetType(nd, &ty));
+        if (ty == cudaGraphNodeTypeKernel) n_kernels++;
+      }
+      kernels_per_step_ = (double)n_kernels / n_steps;
       cudaGraphExec_t exec;
       NGPU_CUDA(cudaGraphInstantiate(&exec, graph, 0));
       cudaGraphDestroy(graph);
@@ -1799,6 +1812,9 @@ void NeuronGPU::BuildRk5Batches() {
     }
     NGPU_CUDA(cudaMemcpy(b.d_blk_seg, map.data(), sizeof(int) * b.n_blocks,
                          cudaMemcpyHostToDevice));
+    long long n_total = 0;
+    for (NodeGroup *g : b.groups) n_total += g->n_node;
+    AllocRk5Queue(b.q, n_total, Rk5RecordFloats(b.model, b.np));
     batches_.push_back(b);
   }
   batch_tables_dirty_ = true;
@@ -1846,6 +1862,7 @@ Rk5Batch NeuronGPU::MakeRk5Batch(const Rk5BatchHost &b) {
   r.segs = b.d_segs;
   r.blk_seg = b.d_blk_seg;
   r.blk_evals = b.d_blk_evals;
+  r.q = b.q;
   return r;
 }
 
@@ -1897,11 +1914,37 @@ void NeuronGPU::TuneRk5Batch(Rk5BatchHost &b) {
   InvalidateGraphs();
 }
 
+void NeuronGPU::AllocRk5Queue(Rk5Queue &q, long long cap, int stride) {
+  FreeRk5Queue(q);
+  const char *env = getenv("NGB200_RK5_QUEUE");
+  if ((env != nullptr && atoi(env) == 0) || cap <= 0 || stride <= 0) return;
+  if (cap > 0x7fffffffLL) cap = 0x7fffffffLL;
+  NGPU_CUDA(cudaMalloc(&q.hdr, sizeof(Rk5QueueHdr)));
+  NGPU_CUDA(cudaMemset(q.hdr, 0, sizeof(Rk5QueueHdr)));
+  NGPU_CUDA(cudaMalloc(&q.rec, sizeof(float) * (size_t)cap * stride));
+  q.cap = (int)cap;
+  q.stride = stride;
+  // finishing launch: up to three 128-thread blocks per SM (its kernel is
+  // compiled for one block per SM's registers), never more blocks than the
+  // update launch has evaluation counters for
+  int dev = 0, n_sm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  q.fin_blocks = (int)std::min<long long>((cap + 127) / 128, 3LL * n_sm);
+}
+
+void NeuronGPU::FreeRk5Queue(Rk5Queue &q) {
+  if (q.hdr) cudaFree(q.hdr);
+  if (q.rec) cudaFree(q.rec);
+  q = Rk5Queue{};
+}
+
 void NeuronGPU::FreeRk5Batches() {
   for (Rk5BatchHost &b : batches_) {
     if (b.d_segs) cudaFree(b.d_segs);
     if (b.d_blk_seg) cudaFree(b.d_blk_seg);
     if (b.d_blk_evals) cudaFree(b.d_blk_evals);
+    FreeRk5Queue(b.q);
   }
   for (NodeGroup *g : groups_) g->batch = -1;
   batches_.clear();
@@ -1928,6 +1971,9 @@ int NeuronGPU::StartSimulation() {
   }
   UploadGeneratorParams();
   if (!batches_built_) BuildRk5Batches();
+  for (NodeGroup *g : groups_)
+    if (g->mi->kind == MK_RK5 && g->batch < 0 && g->q.hdr == nullptr && g->n_node > 0)
+      AllocRk5Queue(g->q, g->n_node, Rk5RecordFloats(g->mi->rk5_model, g->n_port));
   if (batch_tables_dirty_) RefreshRk5BatchTables();
   for (Rk5BatchHost &b : batches_)
     if (!b.tuned) TuneRk5Batch(b);

@@ -126,6 +126,8 @@ struct NodeGroup {
   // per-block RK5 derivative evaluation counters
   unsigned long long *d_blk_evals = nullptr;
   int n_blocks = 0;
+  // straggler queue of the group's own RK5 launch (unbatched groups)
+  Rk5Queue q{};
   // autotuned RK5 kernel variant and the timings it was chosen from
   int rk5_variant = 0;
   bool tuned = false;
@@ -297,6 +299,8 @@ class NeuronGPU {
   unsigned long long TotalSpikes();
   double LastSimulateSeconds() { return last_sim_seconds_; }
   double LastSimulateDeviceMs() { return last_sim_device_ms_; }
+  // kernel launches per time step in the last captured step graph
+  double KernelsPerStep() { return kernels_per_step_; }
   // per-kernel-class device timing (CUDA events around every launch)
   int SetKernelTiming(int on);
   int GetKernelTiming(int kind, double *total_ms, long long *launches);
@@ -360,6 +364,7 @@ class NeuronGPU {
     SegArgs *d_segs = nullptr;
     int *d_blk_seg = nullptr;
     unsigned long long *d_blk_evals = nullptr;
+    Rk5Queue q{};
   };
   std::vector<Rk5BatchHost> batches_;
   bool batches_built_ = false;
@@ -370,6 +375,10 @@ class NeuronGPU {
   void TuneRk5Batch(Rk5BatchHost &b);
   Rk5Batch MakeRk5Batch(const Rk5BatchHost &b);
   void FreeRk5Batches();
+  // straggler queues: capacity cap records of stride floats (cap 0 when the
+  // queue is switched off with NGB200_RK5_QUEUE=0)
+  void AllocRk5Queue(Rk5Queue &q, long long cap, int stride);
+  static void FreeRk5Queue(Rk5Queue &q);
   std::vector<float> mlp_params_;       // FP32 proposer parameters (empty: none)
   MlpImage *d_mlp_img_ = nullptr;
   float mlp_margin_ = 0.25f;
@@ -465,6 +474,7 @@ class NeuronGPU {
   bool input_pending_ = false;
   double last_sim_seconds_ = 0.0;
   double last_sim_device_ms_ = 0.0;
+  double kernels_per_step_ = 0.0;
   cudaEvent_t ev_start_ = nullptr, ev_stop_ = nullptr;
   bool ktime_ = false;
   bool capturing_ = false;

@@ -131,6 +131,25 @@ struct MlpImage {
 // RK5 update modes
 enum StepMode { STEP_PLAIN = 0, STEP_LOG = 1, STEP_LEARNED = 2 };
 
+// Straggler queue of one RK5 update (plain controller). A neuron that is
+// still inside the time step after its first sub-step saves its state to a
+// record and leaves its warp; a second launch finishes the records densely,
+// one neuron per thread, so a warp never carries 31 idle lanes while one
+// neuron near a spike takes many short sub-steps. Resuming from a record
+// repeats exactly the arithmetic of the uninterrupted loop.
+struct Rk5QueueHdr {
+  unsigned tail;                // records reserved (may pass cap: those are not used)
+  unsigned done;                // finishing blocks done (the last one resets the header)
+};
+struct Rk5Queue {
+  Rk5QueueHdr *hdr;
+  float *rec;                   // [cap][stride]: node, segment, sub-steps, h, refractory,
+                                // pad, time (double), state variables
+  int cap;                      // 0: queue off
+  int stride;                   // floats per record, a multiple of 4
+  int fin_blocks;               // grid of the finishing launch
+};
+
 struct GroupArgs {
   int n;                        // nodes
   int n_pad;                    // column length
@@ -151,6 +170,7 @@ struct GroupArgs {
   float eps;                    // RK5 tolerance
   int den_delay_col;            // param column of den_delay or -1
   unsigned long long *blk_evals;  // per-block RK5 derivative evaluations
+  Rk5Queue q;                   // straggler queue of the single-group launch
   // learned step proposer (STEP_LEARNED) and accepted-step logging (STEP_LOG)
   int step_mode;
   float mlp_margin;             // proposal = dt * 2^(output - margin)

@@ -56,8 +56,10 @@ static void launch_rk5(const GroupArgs &g, const InputArgs &in, const PushArgs &
     } else {
       k_rk5_update<M, NP, true, 1, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx);
     }
+    if (g.q.cap > 0) k_rk5_finish<M, NP, true><<<g.q.fin_blocks, block, 0, s>>>(g, in, pa, ctx);
   } else {
     k_rk5_update<M, NP, false, 1, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx);
+    if (g.q.cap > 0) k_rk5_finish<M, NP, false><<<g.q.fin_blocks, block, 0, s>>>(g, in, pa, ctx);
   }
 }
 
@@ -102,6 +104,33 @@ void LaunchRk5Update(int model, int np, const GroupArgs &g,
       launch_rk5_model<IzhCondBeta>(np, g, in, pa, ctx, s); break;
     default: break;
   }
+}
+
+// floats of a straggler record for the kernel instance LaunchRk5Update picks
+template <template <int> class MT>
+static int rk5_nvar(int np) {
+  switch (np) {
+    case 0:
+    case 1: return MT<1>::NVAR;
+    case 2: return MT<2>::NVAR;
+    case 3: return MT<3>::NVAR;
+    case 4: return MT<4>::NVAR;
+    default: return np <= 8 ? MT<8>::NVAR : MT<20>::NVAR;
+  }
+}
+
+int Rk5RecordFloats(int model, int np) {
+  int nv = 0;
+  switch (model) {
+    case RK5_AEIF_COND_BETA: nv = rk5_nvar<AeifCondBeta>(np); break;
+    case RK5_AEIF_COND_ALPHA: nv = rk5_nvar<AeifCondAlpha>(np); break;
+    case RK5_AEIF_PSC_ALPHA: nv = rk5_nvar<AeifPscAlpha>(np); break;
+    case RK5_AEIF_PSC_EXP: nv = rk5_nvar<AeifPscExp>(np); break;
+    case RK5_AEIF_PSC_DELTA: nv = AeifPscDelta<1>::NVAR; break;
+    case RK5_IZHIKEVICH_COND_BETA: nv = rk5_nvar<IzhCondBeta>(np); break;
+    default: return 0;
+  }
+  return (8 + nv + 3) / 4 * 4;
 }
 
 // ---------------------------------------------------------------------------

@@ -18,6 +18,8 @@ void LaunchRk5Update(int model, int np, const GroupArgs &g,
                      StepCtx *ctx, cudaStream_t s);
 // number of RK5 kernel variants (GroupArgs::variant) for a group
 int Rk5VariantCount(int np, int all_uniform);
+// floats per straggler record (Rk5Queue::stride) of an RK5 model / port count
+int Rk5RecordFloats(int model, int np);
 
 // several RK5 groups of one model and port count in one launch: a device
 // segment table (one SegArgs per group) and a block -> segment map
@@ -31,6 +33,7 @@ struct Rk5Batch {
   const SegArgs *segs;
   const int *blk_seg;
   unsigned long long *blk_evals;  // [n_blocks] or null
+  Rk5Queue q;                     // straggler queue of the launch (cap 0: off)
 };
 bool Rk5BatchSupported(int model, int np);
 void LaunchRk5Batch(const Rk5Batch &b, StepCtx *ctx, cudaStream_t s);

@@ -11,8 +11,11 @@
 #include "ngpu_rk5_models.cuh"
 #include "ngpu_rng.h"
 #include "ngpu_step_proposer.cuh"
+#include <cooperative_groups.h>
 
 namespace ngpu {
+
+namespace cg = cooperative_groups;
 
 #define NGPU_BLOCK 128
 
@@ -284,6 +287,143 @@ __device__ __forceinline__ void log_step_sample(const GroupArgs &g, const float 
   }
 }
 
+// Parameters of neuron i when they are not all group-uniform: the per-neuron
+// columns named in pmask, the uniform value otherwise, and the reciprocals
+// formed in registers.
+template <class M, bool UNI>
+__device__ __forceinline__ void rk5_load_params(const GroupArgs &g, int i, bool active,
+                                                float *p_loc, float *q_loc) {
+  if (!UNI) {
+#pragma unroll
+    for (int j = 0; j < (UNI ? 1 : M::NPARAM); j++) {
+      if (j < g.nparam) {
+        p_loc[j] = (active && pbit(g.pmask, j)) ? g.param[(long long)j * g.n_pad + i] : g.puni[j];
+      } else {
+        p_loc[j] = 1.0f;
+      }
+      q_loc[j] = 1.0f / p_loc[j];
+    }
+  }
+}
+
+// One sub-step of the plain controller (src/rk5.h:57-162) followed by the
+// model's spike test; true once the time step is complete.
+template <class M, int NP>
+__device__ __forceinline__ bool rk5_plain_substep(const GroupArgs &g, const PushArgs &pa,
+                                                  StepCtx *ctx, int i, float *y, double &x,
+                                                  float &h, float &refr, int &guard,
+                                                  const float *p, const float *q, int np,
+                                                  float inv_eps, double x1, long long T,
+                                                  int den, bool dry, unsigned &evals) {
+  float h_acc, err_acc;
+  const float hmax = (float)(x1 - x);
+  rk5_step<M, NP>(x, y, h, g.h_min, hmax, p, q, refr, np, inv_eps, evals, h_acc, err_acc);
+  bool end_step = (x >= x1 - (double)g.h_min);
+  if (M::external(y, p, refr, end_step, g.dt)) {
+    if (!dry) push_spike(pa, ctx, g.i_node_0 + i, i, 1.0f, T, x1, den);
+  }
+  if (++guard > NGPU_RK5_MAX_SUBSTEPS) {
+    atomicOr(&ctx->err, (unsigned)DERR_RK5_STUCK);
+    end_step = true;
+  }
+  return end_step;
+}
+
+// end-of-step state of neuron i
+template <class M>
+__device__ __forceinline__ void rk5_store(const GroupArgs &g, int i, const float *y, float h,
+                                          double x, double x1, float refr, bool write_refr) {
+  using Tr = ModelTraits<M>;
+#pragma unroll
+  for (int j = 0; j < M::NVAR; j++) {
+    if (j < g.nvar) g.var[(long long)j * g.n_pad + i] = y[j];
+  }
+  g.h[i] = h;
+  g.dx[i] = (float)(x - x1);
+  if (write_refr) g.param[(long long)Tr::refr * g.n_pad + i] = refr;
+}
+
+// Hands neuron i (segment seg of a batched launch) over to the straggler
+// queue; false if the queue has no room (the caller then carries on). One
+// reservation per group of converged threads.
+template <int NV>
+__device__ __forceinline__ bool rk5_enqueue(const Rk5Queue &qu, int seg, int i, const float *y,
+                                            double x, float h, float refr, int guard) {
+  if (8 + NV > qu.stride) return false;
+  cg::coalesced_group grp = cg::coalesced_threads();
+  unsigned base = 0;
+  if (grp.thread_rank() == 0) base = atomicAdd(&qu.hdr->tail, grp.size());
+  base = grp.shfl(base, 0);
+  const unsigned k = base + grp.thread_rank();
+  if (k >= (unsigned)qu.cap) return false;
+  float *r = qu.rec + (size_t)k * qu.stride;
+  r[0] = __int_as_float(i);
+  r[1] = __int_as_float(seg);
+  r[2] = __int_as_float(guard);
+  r[3] = h;
+  r[4] = refr;
+  *reinterpret_cast<double *>(r + 6) = x;
+#pragma unroll
+  for (int j = 0; j < NV; j++) r[8 + j] = y[j];
+  return true;
+}
+
+// Finishes a straggler record: the rest of the time step of its neuron with
+// the same sub-step sequence as the uninterrupted loop.
+template <class M, int NP, bool UNI>
+__device__ __forceinline__ void rk5_resume(const GroupArgs &g, const PushArgs &pa, StepCtx *ctx,
+                                           const float *p_uni, const float *q_uni, int np,
+                                           const float *r, unsigned &evals, bool dry) {
+  using Tr = ModelTraits<M>;
+  const int i = __float_as_int(r[0]);
+  int guard = __float_as_int(r[2]);
+  float h = r[3];
+  float refr = r[4];
+  double x = *reinterpret_cast<const double *>(r + 6);
+  float y[M::NVAR];
+#pragma unroll
+  for (int j = 0; j < M::NVAR; j++) y[j] = r[8 + j];
+  float p_loc[UNI ? 1 : M::NPARAM];
+  float q_loc[UNI ? 1 : M::NPARAM];
+  rk5_load_params<M, UNI>(g, i, true, p_loc, q_loc);
+  const float *p = UNI ? p_uni : p_loc;
+  const float *q = UNI ? q_uni : q_loc;
+  const long long it = ctx->it;
+  const double x1 = ctx->t0 + (double)g.dt * (double)(it + 1);
+  const long long T = ctx->T0 + it + 1;
+  const float inv_eps = 1.0f / g.eps;
+  const int den = (int)roundf(p[Tr::den] / g.dt);
+  bool end_step = false;
+  while (!end_step) {
+    end_step = rk5_plain_substep<M, NP>(g, pa, ctx, i, y, x, h, refr, guard, p, q, np, inv_eps,
+                                        x1, T, den, dry, evals);
+  }
+  if (!dry) {
+    rk5_store<M>(g, i, y, h, x, x1, refr, true);
+  } else if (y[0] == 1.2345e30f) {
+    g.h[i] = h + (float)x;        // keeps the timing run from being optimised away
+  }
+}
+
+// records of the queue's last update launch
+__device__ __forceinline__ unsigned rk5_queue_count(const Rk5Queue &qu) {
+  const unsigned t = qu.hdr->tail;
+  return t < (unsigned)qu.cap ? t : (unsigned)qu.cap;
+}
+
+// The last block of a finishing launch empties the queue for the next
+// update; every block has read the record count by then.
+__device__ __forceinline__ void rk5_queue_reset(const Rk5Queue &qu) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned prev = atomicAdd(&qu.hdr->done, 1u);
+    if (prev == gridDim.x - 1) {
+      qu.hdr->tail = 0u;
+      qu.hdr->done = 0u;
+    }
+  }
+}
+
 // Integrates neuron i of group g over one time step (one thread per
 // neuron). UNI: every parameter except the refractory counter is
 // group-uniform and is read from p_uni / q_uni (reciprocals); otherwise the
@@ -295,12 +435,15 @@ __device__ __forceinline__ void log_step_sample(const GroupArgs &g, const float 
 // rejects). STEP_LEARNED is called by every thread of the CTA, in lock-step
 // rounds of one accepted sub-step, because each proposal round is one
 // CTA-wide tensor-core MMA; threads past the group end only take part.
+// With a straggler queue (STEP_PLAIN), a neuron still inside the step after
+// its first sub-step is handed over to the queue (segment seg).
 template <class M, int NP, bool UNI, int MODE>
 __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &in,
                                            const PushArgs &pa, StepCtx *ctx, int i,
                                            const float *p_uni, const float *q_uni,
                                            unsigned &evals, bool dry_run,
-                                           ProposerSmem *ps) {
+                                           ProposerSmem *ps, const Rk5Queue *qu = nullptr,
+                                           int seg = 0) {
   using Tr = ModelTraits<M>;
   const bool active = (MODE != STEP_LEARNED) || (i < g.n);
   const bool dry = g.dry || dry_run;
@@ -317,17 +460,7 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
   }
   float p_loc[UNI ? 1 : M::NPARAM];
   float q_loc[UNI ? 1 : M::NPARAM];
-  if (!UNI) {
-#pragma unroll
-    for (int j = 0; j < (UNI ? 1 : M::NPARAM); j++) {
-      if (j < g.nparam) {
-        p_loc[j] = (active && pbit(g.pmask, j)) ? g.param[(long long)j * n_pad + i] : g.puni[j];
-      } else {
-        p_loc[j] = 1.0f;
-      }
-      q_loc[j] = 1.0f / p_loc[j];
-    }
-  }
+  rk5_load_params<M, UNI>(g, i, active, p_loc, q_loc);
   const float *p = UNI ? p_uni : p_loc;
   const float *q = UNI ? q_uni : q_loc;
   float refr = active ? g.param[(long long)Tr::refr * n_pad + i] : 0.0f;
@@ -396,21 +529,17 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
       }
     }
     proposer_teardown(*ps, failed);
-  } else {
+  } else if constexpr (MODE == STEP_LOG) {
     while (!end_step) {
       const float hmax = (float)(x1 - x);
       float f[6];
       bool lg = false;
-      if constexpr (MODE == STEP_LOG) {
-        if (h < hmax && !dry) {
-          ProposerFeatures<M>::get(y, p, h, g.dt, f);
-          lg = true;
-        }
+      if (h < hmax && !dry) {
+        ProposerFeatures<M>::get(y, p, h, g.dt, f);
+        lg = true;
       }
       rk5_step<M, NP>(x, y, h, h_min, hmax, p, q, refr, np, inv_eps, evals, h_acc, err_acc);
-      if constexpr (MODE == STEP_LOG) {
-        if (lg) log_step_sample(g, f, proposer_target(h_acc, err_acc, g.dt));
-      }
+      if (lg) log_step_sample(g, f, proposer_target(h_acc, err_acc, g.dt));
       end_step = (x >= x1 - (double)h_min);
       if (M::external(y, p, refr, end_step, g.dt)) {
         if (!dry) push_spike(pa, ctx, g.i_node_0 + i, i, 1.0f, T, x1, den);
@@ -420,16 +549,18 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
         break;
       }
     }
+  } else {
+    while (!end_step) {
+      end_step = rk5_plain_substep<M, NP>(g, pa, ctx, i, y, x, h, refr, guard, p, q, np,
+                                          inv_eps, x1, T, den, dry, evals);
+      if (!end_step && guard == 1 && qu != nullptr) {
+        if (rk5_enqueue<M::NVAR>(*qu, seg, i, y, x, h, refr, guard)) return;
+      }
+    }
   }
   if (!active) return;
   if (!dry) {
-#pragma unroll
-    for (int j = 0; j < M::NVAR; j++) {
-      if (j < g.nvar) g.var[(long long)j * n_pad + i] = y[j];
-    }
-    g.h[i] = h;
-    g.dx[i] = (float)(x - x1);
-    if (refr != refr0) g.param[(long long)Tr::refr * n_pad + i] = refr;
+    rk5_store<M>(g, i, y, h, x, x1, refr, refr != refr0);
   } else if (y[0] == 1.2345e30f) {
     // keeps the dry run from being optimised away; never true in practice
     g.h[i] = h + (float)x;
@@ -448,10 +579,27 @@ k_rk5_update(const __grid_constant__ GroupArgs g, const __grid_constant__ InputA
     __shared__ ProposerSmem ps;
     rk5_neuron<M, NP, UNI, MODE>(g, in, pa, ctx, i, g.puni, g.pinv, evals, false, &ps);
   } else {
+    const bool queued = (MODE == STEP_PLAIN) && g.q.cap > 0;
     if (i < g.n) rk5_neuron<M, NP, UNI, MODE>(g, in, pa, ctx, i, g.puni, g.pinv, evals, false,
-                                              nullptr);
+                                              nullptr, queued ? &g.q : nullptr, 0);
   }
   if (g.blk_evals != nullptr) block_add_u64(evals, g.blk_evals);
+}
+
+// Second launch of a queued update: one straggler record per thread.
+template <class M, int NP, bool UNI>
+__global__ void __launch_bounds__(NGPU_BLOCK, 1)
+k_rk5_finish(const __grid_constant__ GroupArgs g, const __grid_constant__ InputArgs in,
+             const __grid_constant__ PushArgs pa, StepCtx *ctx) {
+  const unsigned n = rk5_queue_count(g.q);
+  if (n == 0) return;             // the same for every block: nothing to reset
+  unsigned evals = 0;
+  for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    rk5_resume<M, NP, UNI>(g, pa, ctx, g.puni, g.pinv, in.np, g.q.rec + (size_t)k * g.q.stride,
+                           evals, g.dry != 0);
+  }
+  if (g.blk_evals != nullptr) block_add_u64(evals, g.blk_evals);
+  rk5_queue_reset(g.q);
 }
 
 // Many RK5 groups of one model in one launch (independent networks of a
@@ -461,9 +609,11 @@ k_rk5_update(const __grid_constant__ GroupArgs g, const __grid_constant__ InputA
 template <class M, int NP, bool UNI, int MINB, int MODE>
 __global__ void __launch_bounds__(NGPU_BLOCK, MINB)
 k_rk5_update_seg(const SegArgs *__restrict__ segs, const int *__restrict__ blk_seg,
-                 unsigned long long *blk_evals, int dry, StepCtx *ctx) {
+                 unsigned long long *blk_evals, int dry, StepCtx *ctx,
+                 const __grid_constant__ Rk5Queue qu) {
   __shared__ float s_p[M::NPARAM], s_q[M::NPARAM];
-  const SegArgs &S = segs[blk_seg[blockIdx.x]];
+  const int seg = blk_seg[blockIdx.x];
+  const SegArgs &S = segs[seg];
   if (UNI) {
     for (int j = threadIdx.x; j < M::NPARAM; j += blockDim.x) {
       s_p[j] = S.g.puni[j];
@@ -477,10 +627,31 @@ k_rk5_update_seg(const SegArgs *__restrict__ segs, const int *__restrict__ blk_s
     __shared__ ProposerSmem ps;
     rk5_neuron<M, NP, UNI, MODE>(S.g, S.in, S.pa, ctx, i, s_p, s_q, evals, dry != 0, &ps);
   } else {
+    const bool queued = (MODE == STEP_PLAIN) && qu.cap > 0;
     if (i < S.g.n)
-      rk5_neuron<M, NP, UNI, MODE>(S.g, S.in, S.pa, ctx, i, s_p, s_q, evals, dry != 0, nullptr);
+      rk5_neuron<M, NP, UNI, MODE>(S.g, S.in, S.pa, ctx, i, s_p, s_q, evals, dry != 0, nullptr,
+                                   queued ? &qu : nullptr, seg);
   }
   if (blk_evals != nullptr) block_add_u64(evals, blk_evals);
+}
+
+// Second launch of a queued batched update: one straggler record per
+// thread, with the arguments of the record's segment.
+template <class M, int NP, bool UNI>
+__global__ void __launch_bounds__(NGPU_BLOCK, 1)
+k_rk5_finish_seg(const SegArgs *__restrict__ segs, unsigned long long *blk_evals, int dry,
+                 StepCtx *ctx, const __grid_constant__ Rk5Queue qu) {
+  const unsigned n = rk5_queue_count(qu);
+  if (n == 0) return;             // the same for every block: nothing to reset
+  unsigned evals = 0;
+  for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const float *r = qu.rec + (size_t)k * qu.stride;
+    const SegArgs &R = segs[__float_as_int(r[1])];
+    rk5_resume<M, NP, UNI>(R.g, R.pa, ctx, R.g.puni, R.g.pinv, R.in.np, r, evals,
+                           R.g.dry || dry != 0);
+  }
+  if (blk_evals != nullptr) block_add_u64(evals, blk_evals);
+  rk5_queue_reset(qu);
 }
 
 }  // namespace ngpu

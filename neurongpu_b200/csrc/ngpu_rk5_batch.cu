@@ -12,11 +12,11 @@ static void launch_rk5_seg(const Rk5Batch &b, StepCtx *ctx, cudaStream_t s) {
   if (b.mode != STEP_PLAIN) {
     if constexpr (ProposerFeatures<M>::supported && NP <= 2) {
       if (b.mode == STEP_LOG) {
-        if (b.uni) k_rk5_update_seg<M, NP, true, 1, STEP_LOG><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx);
-        else k_rk5_update_seg<M, NP, false, 1, STEP_LOG><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx);
+        if (b.uni) k_rk5_update_seg<M, NP, true, 1, STEP_LOG><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q);
+        else k_rk5_update_seg<M, NP, false, 1, STEP_LOG><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q);
       } else {
-        if (b.uni) k_rk5_update_seg<M, NP, true, 4, STEP_LEARNED><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx);
-        else k_rk5_update_seg<M, NP, false, 4, STEP_LEARNED><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx);
+        if (b.uni) k_rk5_update_seg<M, NP, true, 4, STEP_LEARNED><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q);
+        else k_rk5_update_seg<M, NP, false, 4, STEP_LEARNED><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q);
       }
     }
     return;
@@ -24,13 +24,17 @@ static void launch_rk5_seg(const Rk5Batch &b, StepCtx *ctx, cudaStream_t s) {
   if constexpr (NP <= 4) {
     if (b.uni) {
       switch (b.variant) {
-        case 1: k_rk5_update_seg<M, NP, true, 5, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx); break;
-        case 2: k_rk5_update_seg<M, NP, true, 6, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx); break;
-        case 3: k_rk5_update_seg<M, NP, true, 8, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx); break;
-        default: k_rk5_update_seg<M, NP, true, 1, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx); break;
+        case 1: k_rk5_update_seg<M, NP, true, 5, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q); break;
+        case 2: k_rk5_update_seg<M, NP, true, 6, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q); break;
+        case 3: k_rk5_update_seg<M, NP, true, 8, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q); break;
+        default: k_rk5_update_seg<M, NP, true, 1, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q); break;
       }
     } else {
-      k_rk5_update_seg<M, NP, false, 1, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx);
+      k_rk5_update_seg<M, NP, false, 1, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q);
+    }
+    if (b.q.cap > 0) {
+      if (b.uni) k_rk5_finish_seg<M, NP, true><<<b.q.fin_blocks, block, 0, s>>>(b.segs, b.blk_evals, b.dry, ctx, b.q);
+      else k_rk5_finish_seg<M, NP, false><<<b.q.fin_blocks, block, 0, s>>>(b.segs, b.blk_evals, b.dry, ctx, b.q);
     }
   }
 }

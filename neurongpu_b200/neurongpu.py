@@ -242,6 +242,7 @@ _EXT_SIG = {
     "NGB200_GetAllConnections": (ctypes.c_longlong, (c_int_p, c_int_p, c_int_p, c_int_p,
                                                      c_float_p, c_float_p)),
     "NGB200_FreeArray": (None, (c_void_p,)),
+    "NGB200_KernelsPerStep": (ctypes.c_double, ()),
     "NGB200_SetRk5Batching": (_I, (_I,)),
     "NGB200_Rk5BatchOf": (_I, (_I,)),
     "NGB200_SetStepLog": (_I, (_I, _I)),
@@ -1209,6 +1210,10 @@ class Binding(object):
 
     def LastSimulateDeviceMs(self):
         return self._call("NGB200_LastSimulateDeviceMs")
+
+    def KernelsPerStep(self):
+        "Kernel launches per time step in the last captured step graph"
+        return self._call("NGB200_KernelsPerStep")
 
     def NNodes(self):
         return self._call("NGB200_NNodes")

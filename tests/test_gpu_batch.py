@@ -84,3 +84,31 @@ def test_batched_mixed_models(ngpu):
     assert b1[0] == b1[2] and b1[1] == b1[3] and b1[0] != b1[1] and b1[4] == -1
     assert c1.sum() > 0
     assert np.array_equal(c1, c0)
+
+
+def test_straggler_queue_bit_identical(ngpu):
+    """Neurons still inside the time step after their first sub-step are
+    finished from the straggler queue by other warps; the result equals the
+    uninterrupted loop bit for bit, batched and per group."""
+    grid = sweep.sweep_grid(12, 300, 5000, 50, 150, seed=7)
+    old = os.environ.get("NGB200_RK5_QUEUE")
+    res = {}
+    try:
+        for queue in ("1", "0"):
+            os.environ["NGB200_RK5_QUEUE"] = queue
+            for batching in (True, False):
+                res[(queue, batching)] = _run(ngpu, batching, grid)
+    finally:
+        if old is None:
+            del os.environ["NGB200_RK5_QUEUE"]
+        else:
+            os.environ["NGB200_RK5_QUEUE"] = old
+    c0, v0, w0, e0, _ = res[("0", False)]
+    neuron_steps = sum(p["n"] for p in grid) * 2000
+    assert c0.sum() > 0
+    assert e0 > 6 * neuron_steps          # some neurons took several sub-steps
+    for key, (c, v, w, e, _) in res.items():
+        assert np.array_equal(c, c0), key
+        assert np.array_equal(v.view(np.int32), v0.view(np.int32)), key
+        assert np.array_equal(w.view(np.int32), w0.view(np.int32)), key
+        assert e == e0, key
