@@ -1707,6 +1707,7 @@ void NeuronGPU::TuneRk5(NodeGroup *g) {
   const char *force = getenv("NGB200_RK5_VARIANT");
   GroupArgs a = MakeGroupArgs(g);
   int nv = Rk5VariantCount(g->n_port, a.all_uniform);
+  if (nv <= 1) g->rk5_variant = 0;
   if (force != nullptr) {
     g->rk5_variant = std::max(0, std::min(nv - 1, atoi(force)));
     InvalidateGraphs();
@@ -1748,6 +1749,22 @@ void NeuronGPU::TuneRk5(NodeGroup *g) {
   NGPU_CUDA(cudaGetLastError());
   g->rk5_variant = best;
   InvalidateGraphs();
+}
+
+bool NeuronGPU::TunePending() {
+  for (Rk5BatchHost &b : batches_)
+    if (!b.tuned) return true;
+  for (NodeGroup *g : groups_)
+    if (g->mi->kind == MK_RK5 && g->batch < 0 && !g->tuned) return true;
+  return false;
+}
+
+void NeuronGPU::TuneAll() {
+  if (batch_tables_dirty_) RefreshRk5BatchTables();
+  for (Rk5BatchHost &b : batches_)
+    if (!b.tuned) TuneRk5Batch(b);
+  for (NodeGroup *g : groups_)
+    if (g->mi->kind == MK_RK5 && g->batch < 0 && !g->tuned) TuneRk5(g);
 }
 
 int NeuronGPU::GetRk5Tuning(int i_node, int *variant, float *ms4) {
@@ -1975,10 +1992,8 @@ int NeuronGPU::StartSimulation() {
     if (g->mi->kind == MK_RK5 && g->batch < 0 && g->q.hdr == nullptr && g->n_node > 0)
       AllocRk5Queue(g->q, g->n_node, Rk5RecordFloats(g->mi->rk5_model, g->n_port));
   if (batch_tables_dirty_) RefreshRk5BatchTables();
-  for (Rk5BatchHost &b : batches_)
-    if (!b.tuned) TuneRk5Batch(b);
-  for (NodeGroup *g : groups_)
-    if (g->mi->kind == MK_RK5 && g->batch < 0 && !g->tuned) TuneRk5(g);
+  // a variant forced through NGB200_RK5_VARIANT applies from the first step
+  if (steps_total_ >= kTuneSteps || getenv("NGB200_RK5_VARIANT") != nullptr) TuneAll();
   neur_t0_ = neural_time_;
   it_ = 0;
   Nt_ = (long long)round(sim_time_ / time_resolution_);
@@ -2001,6 +2016,7 @@ int NeuronGPU::SimulationStep() {
   }
   LaunchSteps(1);
   it_++;
+  steps_total_++;
   input_pending_ = true;
   neural_time_ = neur_t0_ + (double)time_resolution_ * (double)it_;
   return 0;
@@ -2032,6 +2048,8 @@ int NeuronGPU::Simulate() {
     done += n;
     it_ = done;
     input_pending_ = true;
+    steps_total_ += n;
+    if (steps_total_ >= kTuneSteps && TunePending()) TuneAll();
   }
   neural_time_ = neur_t0_ + (double)time_resolution_ * (double)Nt_;
   NGPU_CUDA(cudaEventRecord(ev_stop_, stream_));

@@ -129,7 +129,7 @@ struct NodeGroup {
   // straggler queue of the group's own RK5 launch (unbatched groups)
   Rk5Queue q{};
   // autotuned RK5 kernel variant and the timings it was chosen from
-  int rk5_variant = 0;
+  int rk5_variant = 1;
   bool tuned = false;
   float tune_ms[4] = {0, 0, 0, 0};
   // index of the batched RK5 launch this group belongs to, or -1
@@ -307,6 +307,13 @@ class NeuronGPU {
   // RK5 kernel variant chosen for the group of i_node and its timings
   int GetRk5Tuning(int i_node, int *variant, float *ms4);
   void TuneRk5(NodeGroup *g);
+  // the autotuner runs once the network has integrated kTuneSteps steps, so
+  // that it times the kernels on a settled state (the first steps start
+  // from the initial step size and take several sub-steps per neuron)
+  static const long long kTuneSteps = 200;
+  long long steps_total_ = 0;
+  bool TunePending();
+  void TuneAll();
   // RK5 groups of one model and port count are integrated by one launch
   // per step (segment table) unless batching is switched off
   int SetRk5Batching(int on);
@@ -358,7 +365,7 @@ class NeuronGPU {
     int model = 0, np = 0;
     std::vector<NodeGroup *> groups;
     int n_blocks = 0;
-    int variant = 0;
+    int variant = 1;
     bool tuned = false;
     float tune_ms[4] = {0, 0, 0, 0};
     SegArgs *d_segs = nullptr;

@@ -88,21 +88,26 @@ def test_batched_mixed_models(ngpu):
 
 def test_straggler_queue_bit_identical(ngpu):
     """Neurons still inside the time step after their first sub-step are
-    finished from the straggler queue by other warps; the result equals the
-    uninterrupted loop bit for bit, batched and per group."""
+    finished from the straggler queue by a second launch; the result equals
+    the uninterrupted loop bit for bit, batched and per group. The update
+    kernel runs as its one-block-per-SM variant here, the register budget
+    the finishing kernel is compiled for, so both compile the sub-step
+    identically."""
     grid = sweep.sweep_grid(12, 300, 5000, 50, 150, seed=7)
-    old = os.environ.get("NGB200_RK5_QUEUE")
+    old = {k: os.environ.get(k) for k in ("NGB200_RK5_QUEUE", "NGB200_RK5_VARIANT")}
     res = {}
     try:
+        os.environ["NGB200_RK5_VARIANT"] = "0"
         for queue in ("1", "0"):
             os.environ["NGB200_RK5_QUEUE"] = queue
             for batching in (True, False):
                 res[(queue, batching)] = _run(ngpu, batching, grid)
     finally:
-        if old is None:
-            del os.environ["NGB200_RK5_QUEUE"]
-        else:
-            os.environ["NGB200_RK5_QUEUE"] = old
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
     c0, v0, w0, e0, _ = res[("0", False)]
     neuron_steps = sum(p["n"] for p in grid) * 2000
     assert c0.sum() > 0
