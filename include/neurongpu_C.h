@@ -291,12 +291,14 @@ double NGB200_KernelsPerStep();
 int NGB200_SetKernelTiming(int on);
 int NGB200_GetKernelTiming(int kind, double *total_ms, long long *launches);
 /* RK5 kernel variant picked by the autotuner for the group of node i_node
- * (0 = no register cap, 1..3 = caps for 5, 6, 8 resident blocks per SM) and
- * the median device time (ms) of each variant's timing launch. The tuner runs
- * at the first simulation of groups with >= 16384 neurons; the environment
- * variable NGB200_RK5_VARIANT forces a variant, NGB200_AUTOTUNE=0 disables
- * tuning. */
-int NGB200_GetRk5Tuning(int i_node, int *variant, float *ms4);
+ * (0 = no register cap, 1..3 = caps for 5, 6, 8 resident blocks per SM,
+ * 4..5 = persistent kernel with shared-memory prefetch of the state, caps
+ * for 5 and 6 blocks per SM) and, in ms6[0..5], the median device time (ms)
+ * of each variant's timing launch (0 for variants not timed). The tuner runs
+ * once a simulation has integrated 200 steps, for groups with >= 16384
+ * neurons; the environment variable NGB200_RK5_VARIANT forces a variant from
+ * the first step, NGB200_AUTOTUNE=0 disables tuning. */
+int NGB200_GetRk5Tuning(int i_node, int *variant, float *ms6);
 
 /* Standalone synaptic delivery, the simulator's delivery kernel applied to a
  * caller-owned graph and spike batch (all pointers are device memory):

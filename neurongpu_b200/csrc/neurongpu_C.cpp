@@ -631,6 +631,6 @@ int NGB200_GetKernelTiming(int kind, double *total_ms, long long *launches) {
 
 }  // extern "C"
 
-extern "C" int NGB200_GetRk5Tuning(int i_node, int *variant, float *ms4) {
-  return guarded(0, [&](NeuronGPU *n) { return n->GetRk5Tuning(i_node, variant, ms4); });
+extern "C" int NGB200_GetRk5Tuning(int i_node, int *variant, float *ms6) {
+  return guarded(0, [&](NeuronGPU *n) { return n->GetRk5Tuning(i_node, variant, ms6); });
 }

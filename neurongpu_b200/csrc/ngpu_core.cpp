@@ -1683,6 +1683,7 @@ void NeuronGPU::CheckDeviceErrors() {
     if (e & DERR_REC_OVERFLOW) m += " recording buffer overflow;";
     if (e & DERR_PROPOSER_TIMEOUT) m += " a tensor-core wait of the step proposer timed out;";
     if (e & DERR_REV_OVERFLOW) m += " a dendritic delay exceeds the one at calibration (or too many dendritic arrivals in one step);";
+    if (e & DERR_TILE_TIMEOUT) m += " a shared-memory prefetch of the RK5 update timed out;";
     throw ngpu_exception(m);
   }
 }
@@ -1767,17 +1768,17 @@ void NeuronGPU::TuneAll() {
     if (g->mi->kind == MK_RK5 && g->batch < 0 && !g->tuned) TuneRk5(g);
 }
 
-int NeuronGPU::GetRk5Tuning(int i_node, int *variant, float *ms4) {
+int NeuronGPU::GetRk5Tuning(int i_node, int *variant, float *ms6) {
   int il;
   NodeGroup *g = GroupOf(i_node, 1, il);
   if (g->batch >= 0) {
     const Rk5BatchHost &b = batches_[g->batch];
     *variant = b.variant;
-    for (int v = 0; v < 4; v++) ms4[v] = b.tune_ms[v];
+    for (int v = 0; v < 6; v++) ms6[v] = b.tune_ms[v];
     return 0;
   }
   *variant = g->rk5_variant;
-  for (int v = 0; v < 4; v++) ms4[v] = g->tune_ms[v];
+  for (int v = 0; v < 6; v++) ms6[v] = g->tune_ms[v];
   return 0;
 }
 
@@ -1887,7 +1888,8 @@ Rk5Batch NeuronGPU::MakeRk5Batch(const Rk5BatchHost &b) {
 void NeuronGPU::TuneRk5Batch(Rk5BatchHost &b) {
   b.tuned = true;
   Rk5Batch r = MakeRk5Batch(b);
-  const int nv = r.uni ? Rk5VariantCount(b.np, 1) : 1;
+  // the batched kernel has the four register-cap variants (no tile kernel)
+  const int nv = r.uni ? std::min(4, Rk5VariantCount(b.np, 1)) : 1;
   const char *force = getenv("NGB200_RK5_VARIANT");
   if (force != nullptr) {
     b.variant = std::max(0, std::min(nv - 1, atoi(force)));

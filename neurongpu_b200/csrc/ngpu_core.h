@@ -131,7 +131,7 @@ struct NodeGroup {
   // autotuned RK5 kernel variant and the timings it was chosen from
   int rk5_variant = 1;
   bool tuned = false;
-  float tune_ms[4] = {0, 0, 0, 0};
+  float tune_ms[6] = {0, 0, 0, 0, 0, 0};
   // index of the batched RK5 launch this group belongs to, or -1
   int batch = -1;
   // RK5 step mode (StepMode) and the accepted-step log of STEP_LOG
@@ -305,7 +305,7 @@ class NeuronGPU {
   int SetKernelTiming(int on);
   int GetKernelTiming(int kind, double *total_ms, long long *launches);
   // RK5 kernel variant chosen for the group of i_node and its timings
-  int GetRk5Tuning(int i_node, int *variant, float *ms4);
+  int GetRk5Tuning(int i_node, int *variant, float *ms6);
   void TuneRk5(NodeGroup *g);
   // the autotuner runs once the network has integrated kTuneSteps steps, so
   // that it times the kernels on a settled state (the first steps start
@@ -367,7 +367,7 @@ class NeuronGPU {
     int n_blocks = 0;
     int variant = 1;
     bool tuned = false;
-    float tune_ms[4] = {0, 0, 0, 0};
+    float tune_ms[6] = {0, 0, 0, 0, 0, 0};
     SegArgs *d_segs = nullptr;
     int *d_blk_seg = nullptr;
     unsigned long long *d_blk_evals = nullptr;

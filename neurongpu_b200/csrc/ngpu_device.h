@@ -34,7 +34,8 @@ enum DeviceError : unsigned {
   DERR_REC_OVERFLOW = 4u,       // recording buffer overflow
   DERR_NAN_STATE = 8u,
   DERR_PROPOSER_TIMEOUT = 16u,  // a tensor-core completion wait of the step proposer timed out
-  DERR_REV_OVERFLOW = 32u       // dendritic delay above its maximum or too many dendritic arrivals
+  DERR_REV_OVERFLOW = 32u,      // dendritic delay above its maximum or too many dendritic arrivals
+  DERR_TILE_TIMEOUT = 64u       // a shared-memory prefetch of the RK5 update did not complete in time
 };
 
 struct StepCtx {

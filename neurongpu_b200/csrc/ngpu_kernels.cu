@@ -27,6 +27,30 @@
 
 namespace ngpu {
 
+// grid of the persistent tile kernel: as many blocks as are resident at once
+// (at most one per tile)
+template <class M, int NP, int MINB>
+static int tile_grid(int n_tiles) {
+  static int resident = 0;
+  if (resident == 0) {
+    int dev = 0, n_sm = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rk5_update_tiles<M, NP, MINB>,
+                                                  NGPU_BLOCK, 0);
+    resident = (n_sm > 0 ? n_sm : 148) * (per_sm > 0 ? per_sm : 1);
+  }
+  return n_tiles < resident ? n_tiles : resident;
+}
+
+// The tile kernel's bulk copies need 16-byte aligned column and accumulator
+// starts (cudaMalloc bases, columns of n_pad = a multiple of 128 entries).
+static bool tiles_aligned(const GroupArgs &g, const InputArgs &in) {
+  auto al = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
+  return al(g.var) && al(g.param) && al(g.h) && al(g.dx) && al(in.acc + in.acc_base) &&
+         (g.n_pad % NGPU_BLOCK) == 0;
+}
+
 template <class M, int NP>
 static void launch_rk5(const GroupArgs &g, const InputArgs &in, const PushArgs &pa,
                        StepCtx *ctx, cudaStream_t s) {
@@ -47,10 +71,18 @@ static void launch_rk5(const GroupArgs &g, const InputArgs &in, const PushArgs &
   if (g.all_uniform) {
     if constexpr (NP <= 4) {
       // occupancy variants chosen by the autotuner (register cap per thread)
-      switch (g.variant) {
+      const int variant = (g.variant >= 4 && !tiles_aligned(g, in)) ? 1 : g.variant;
+      const int n_tiles = (int)grid.x;
+      switch (variant) {
         case 1: k_rk5_update<M, NP, true, 5, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
         case 2: k_rk5_update<M, NP, true, 6, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
         case 3: k_rk5_update<M, NP, true, 8, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+        case 4:
+          k_rk5_update_tiles<M, NP, 5><<<tile_grid<M, NP, 5>(n_tiles), block, 0, s>>>(g, in, pa, ctx);
+          break;
+        case 5:
+          k_rk5_update_tiles<M, NP, 6><<<tile_grid<M, NP, 6>(n_tiles), block, 0, s>>>(g, in, pa, ctx);
+          break;
         default: k_rk5_update<M, NP, true, 1, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
       }
     } else {
@@ -63,7 +95,7 @@ static void launch_rk5(const GroupArgs &g, const InputArgs &in, const PushArgs &
   }
 }
 
-int Rk5VariantCount(int np, int all_uniform) { return (all_uniform && np <= 4) ? 4 : 1; }
+int Rk5VariantCount(int np, int all_uniform) { return (all_uniform && np <= 4) ? 6 : 1; }
 
 template <template <int> class MT>
 static void launch_rk5_model(int np, const GroupArgs &g, const InputArgs &in,

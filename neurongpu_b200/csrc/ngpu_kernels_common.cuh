@@ -68,19 +68,21 @@ __device__ __forceinline__ void push_spike(const PushArgs &pa, StepCtx *ctx,
 
 // Sum of the pending synaptic input of one node per port (fixed point):
 // accumulator contents (cleared here) plus the Poisson direct connections
-// drawn for the previous step.
+// drawn for the previous step. pre_acc: the accumulator values already
+// fetched (port q at pre_acc[q]), or null.
 template <int NP>
 __device__ __forceinline__ void input_sum(const InputArgs &in, int i,
                                           int n_pad, int np, long long it,
                                           double t0, float dt, int pending,
                                           long long T0, long long *s,
-                                          bool dry = false) {
+                                          bool dry = false,
+                                          const long long *pre_acc = nullptr) {
 #pragma unroll
   for (int q = 0; q < NP; q++) {
     s[q] = 0;
     if (q < np) {
       long long *a = in.acc + in.acc_base + (long long)q * n_pad + i;
-      long long v = *a;
+      long long v = pre_acc ? pre_acc[q] : *a;
       if (v != 0 && !(in.dry || dry)) *a = 0;
       s[q] = v;
     }
@@ -436,14 +438,17 @@ __device__ __forceinline__ void rk5_queue_reset(const Rk5Queue &qu) {
 // rounds of one accepted sub-step, because each proposal round is one
 // CTA-wide tensor-core MMA; threads past the group end only take part.
 // With a straggler queue (STEP_PLAIN), a neuron still inside the step after
-// its first sub-step is handed over to the queue (segment seg).
+// its first sub-step is handed over to the queue (segment seg). pre_col /
+// pre_acc: the neuron's state columns (M::NVAR state variables, refractory
+// counter, step size, time offset) and accumulators already fetched, or null.
 template <class M, int NP, bool UNI, int MODE>
 __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &in,
                                            const PushArgs &pa, StepCtx *ctx, int i,
                                            const float *p_uni, const float *q_uni,
                                            unsigned &evals, bool dry_run,
                                            ProposerSmem *ps, const Rk5Queue *qu = nullptr,
-                                           int seg = 0) {
+                                           int seg = 0, const float *pre_col = nullptr,
+                                           const long long *pre_acc = nullptr) {
   using Tr = ModelTraits<M>;
   const bool active = (MODE != STEP_LEARNED) || (i < g.n);
   const bool dry = g.dry || dry_run;
@@ -456,19 +461,21 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
   float y[M::NVAR];
 #pragma unroll
   for (int j = 0; j < M::NVAR; j++) {
-    y[j] = (active && j < g.nvar) ? g.var[(long long)j * n_pad + i] : 0.0f;
+    y[j] = (active && j < g.nvar) ? (pre_col ? pre_col[j] : g.var[(long long)j * n_pad + i])
+                                  : 0.0f;
   }
   float p_loc[UNI ? 1 : M::NPARAM];
   float q_loc[UNI ? 1 : M::NPARAM];
   rk5_load_params<M, UNI>(g, i, active, p_loc, q_loc);
   const float *p = UNI ? p_uni : p_loc;
   const float *q = UNI ? q_uni : q_loc;
-  float refr = active ? g.param[(long long)Tr::refr * n_pad + i] : 0.0f;
+  float refr = active ? (pre_col ? pre_col[M::NVAR] : g.param[(long long)Tr::refr * n_pad + i])
+                      : 0.0f;
   // fold the previous step's input
   constexpr int NPI = (M::NPV == 0) ? 1 : NP;
   if (active) {
     long long s[NPI];
-    input_sum<NPI>(in, i, n_pad, np, it, t0, g.dt, pending, T0, s, dry);
+    input_sum<NPI>(in, i, n_pad, np, it, t0, g.dt, pending, T0, s, dry, pre_acc);
 #pragma unroll
     for (int qq = 0; qq < NPI; qq++) {
       if (qq < np && s[qq] != 0) {
@@ -480,8 +487,9 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
   }
   const float refr0 = refr;
   const double x1 = t0 + (double)g.dt * (double)(it + 1);
-  double x = t0 + (double)g.dt * (double)it + (active ? (double)g.dx[i] : 0.0);
-  float h = active ? g.h[i] : 0.0f;
+  double x = t0 + (double)g.dt * (double)it +
+             (active ? (double)(pre_col ? pre_col[M::NVAR + 2] : g.dx[i]) : 0.0);
+  float h = active ? (pre_col ? pre_col[M::NVAR + 1] : g.h[i]) : 0.0f;
   const float h_min = g.h_min;
   const float inv_eps = 1.0f / g.eps;
   const long long T = T0 + it + 1;
@@ -582,6 +590,107 @@ k_rk5_update(const __grid_constant__ GroupArgs g, const __grid_constant__ InputA
     const bool queued = (MODE == STEP_PLAIN) && g.q.cap > 0;
     if (i < g.n) rk5_neuron<M, NP, UNI, MODE>(g, in, pa, ctx, i, g.puni, g.pinv, evals, false,
                                               nullptr, queued ? &g.q : nullptr, 0);
+  }
+  if (g.blk_evals != nullptr) block_add_u64(evals, g.blk_evals);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent RK5 update with TMA prefetch of the neuron state. Each block
+// walks the 128-neuron tiles blockIdx.x, blockIdx.x + gridDim.x, ...; the
+// state columns (variables, refractory counter, step size, time offset) and
+// accumulators of the next two tiles are brought into shared memory by 1-D
+// bulk copies (cp.async.bulk, completion counted on an mbarrier) while the
+// block integrates the current tile, so no warp waits for HBM at the start
+// of its neurons. Group-uniform parameters only (they are in the constant
+// bank); the arithmetic is rk5_neuron's.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+               : : "r"(smem_u32(mbar)), "r"(bytes) : "memory");
+}
+
+// global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                         uint64_t *mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      : : "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(mbar)) : "memory");
+}
+
+template <class M, int NP>
+struct Rk5TileStage {
+  enum { NC = M::NVAR + 3, NPI = (M::NPV == 0) ? 1 : NP };
+  float col[NC][NGPU_BLOCK];          // variables, refractory, h, dx
+  long long acc[NPI][NGPU_BLOCK];     // accumulators per port
+};
+
+template <class M, int NP>
+__device__ __forceinline__ void rk5_issue_tile(Rk5TileStage<M, NP> &st, uint64_t *bar,
+                                               const GroupArgs &g, const InputArgs &in,
+                                               int n_acc, int t) {
+  using Tr = ModelTraits<M>;
+  const long long o = (long long)t * NGPU_BLOCK;
+  const uint32_t cb = NGPU_BLOCK * sizeof(float), ab = NGPU_BLOCK * sizeof(long long);
+  const int nv = g.nvar < M::NVAR ? g.nvar : M::NVAR;
+  mbar_expect_tx(bar, (uint32_t)(nv + 3) * cb + (uint32_t)n_acc * ab);
+  for (int j = 0; j < nv; j++) bulk_g2s(st.col[j], g.var + (long long)j * g.n_pad + o, cb, bar);
+  bulk_g2s(st.col[M::NVAR], g.param + (long long)Tr::refr * g.n_pad + o, cb, bar);
+  bulk_g2s(st.col[M::NVAR + 1], g.h + o, cb, bar);
+  bulk_g2s(st.col[M::NVAR + 2], g.dx + o, cb, bar);
+  for (int q = 0; q < n_acc; q++)
+    bulk_g2s(st.acc[q], in.acc + in.acc_base + (long long)q * g.n_pad + o, ab, bar);
+}
+
+template <class M, int NP, int MINB>
+__global__ void __launch_bounds__(NGPU_BLOCK, MINB)
+k_rk5_update_tiles(const __grid_constant__ GroupArgs g, const __grid_constant__ InputArgs in,
+                   const __grid_constant__ PushArgs pa, StepCtx *ctx) {
+  using St = Rk5TileStage<M, NP>;
+  __shared__ alignas(128) St s_st[2];
+  __shared__ alignas(8) uint64_t s_bar[2];
+  const int n_tiles = (g.n + NGPU_BLOCK - 1) / NGPU_BLOCK;
+  const int n_acc = in.np < (int)St::NPI ? in.np : (int)St::NPI;
+  const int G = gridDim.x;
+  if (threadIdx.x == 0) {
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if ((int)blockIdx.x < n_tiles) rk5_issue_tile<M, NP>(s_st[0], &s_bar[0], g, in, n_acc, blockIdx.x);
+    if ((int)blockIdx.x + G < n_tiles)
+      rk5_issue_tile<M, NP>(s_st[1], &s_bar[1], g, in, n_acc, blockIdx.x + G);
+  }
+  const Rk5Queue *qu = g.q.cap > 0 ? &g.q : nullptr;
+  unsigned evals = 0;
+  int k = 0;
+  for (int t = blockIdx.x; t < n_tiles; t += G, k++) {
+    const int s = k & 1;
+    const bool ok = __syncthreads_and(mbar_wait(&s_bar[s], (k >> 1) & 1, 1 << 22));
+    if (!ok) {
+      // a copy did not land: leave this block's remaining tiles untouched,
+      // after giving the copies in flight time to end
+      if (threadIdx.x == 0) {
+        atomicOr(&ctx->err, (unsigned)DERR_TILE_TIMEOUT);
+        mbar_wait(&s_bar[s], (k >> 1) & 1, 1 << 22);
+        if (t + G < n_tiles) mbar_wait(&s_bar[s ^ 1], ((k + 1) >> 1) & 1, 1 << 22);
+      }
+      break;
+    }
+    float pc[St::NC];
+    long long pq[St::NPI];
+#pragma unroll
+    for (int j = 0; j < St::NC; j++) pc[j] = s_st[s].col[j][threadIdx.x];
+#pragma unroll
+    for (int q = 0; q < St::NPI; q++) pq[q] = s_st[s].acc[q][threadIdx.x];
+    __syncthreads();                    // stage s is free again
+    if (threadIdx.x == 0 && t + 2 * G < n_tiles) {
+      proxy_fence_async_smem();         // order the reads above before the copy
+      rk5_issue_tile<M, NP>(s_st[s], &s_bar[s], g, in, n_acc, t + 2 * G);
+    }
+    const int i = t * NGPU_BLOCK + threadIdx.x;
+    if (i < g.n) rk5_neuron<M, NP, true, STEP_PLAIN>(g, in, pa, ctx, i, g.puni, g.pinv, evals,
+                                                     false, nullptr, qu, 0, pc, pq);
   }
   if (g.blk_evals != nullptr) block_add_u64(evals, g.blk_evals);
 }

@@ -1330,9 +1330,9 @@ class Binding(object):
         return t.value, n.value
 
     def GetRk5Tuning(self, i_node):
-        "(chosen RK5 kernel variant, [ms of variants 0..3]) for the group of i_node"
+        "(chosen RK5 kernel variant, [ms of variants 0..5]) for the group of i_node"
         v = ctypes.c_int(0)
-        ms = (ctypes.c_float * 4)()
+        ms = (ctypes.c_float * 6)()
         self._call("NGB200_GetRk5Tuning", ctypes.c_int(i_node), ctypes.byref(v), ms)
         return v.value, list(ms)
 
