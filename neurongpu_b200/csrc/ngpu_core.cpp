@@ -101,6 +101,13 @@ void NeuronGPU::FreeDevice() {
   if (ev_stop_) cudaEventDestroy(ev_stop_);
   ev_start_ = ev_stop_ = nullptr;
   d_ctx_ = nullptr;
+  if (ev_fork_) cudaEventDestroy(ev_fork_);
+  if (ev_join_) cudaEventDestroy(ev_join_);
+  ev_fork_ = ev_join_ = nullptr;
+  if (dstream_) {
+    cudaStreamDestroy(dstream_);
+    dstream_ = nullptr;
+  }
   if (stream_) {
     cudaStreamDestroy(stream_);
     stream_ = nullptr;
@@ -928,6 +935,7 @@ InputArgs NeuronGPU::MakeInputArgs(NodeGroup *g) {
   const ModelInfo *mi = g->mi;
   in.acc = d_acc_;
   in.acc_base = g->acc_base;
+  in.acc_par = n_acc_ > 0 ? n_acc_ : 1;
   in.np = g->n_port;
   if (mi->kind == MK_RK5) {
     in.in_var = mi->in_var - (mi->port_var.empty() ? 0 : 0);
@@ -1006,6 +1014,7 @@ DeliverArgs NeuronGPU::MakeDeliverArgs() {
   d.e_stamp = d_e_stamp_;
   d.e_post = d_e_post_;
   d.acc = d_acc_;
+  d.acc_par = n_acc_ > 0 ? n_acc_ : 1;
   d.ring_src = d_ring_src_;
   d.ring_h = d_ring_h_;
   d.ring_cnt = d_ring_cnt_;
@@ -1143,8 +1152,9 @@ void NeuronGPU::BuildDevice() {
     n_acc_ += (long long)g->n_port * g->n_pad;
   }
   if (n_acc_ > 0xFFFFFFFFLL) throw ngpu_exception("Too many (node, port) input slots");
-  NGPU_CUDA(cudaMalloc(&d_acc_, sizeof(long long) * (n_acc_ > 0 ? n_acc_ : 1)));
-  NGPU_CUDA(cudaMemset(d_acc_, 0, sizeof(long long) * (n_acc_ > 0 ? n_acc_ : 1)));
+  // two parity halves (InputArgs::acc_par)
+  NGPU_CUDA(cudaMalloc(&d_acc_, 2 * sizeof(long long) * (n_acc_ > 0 ? n_acc_ : 1)));
+  NGPU_CUDA(cudaMemset(d_acc_, 0, 2 * sizeof(long long) * (n_acc_ > 0 ? n_acc_ : 1)));
   // accumulator slot of every CSR edge (device), with the port and
   // synapse-group checks of src/connect.cu:26-62
   const uint64_t E = (uint64_t)n_raw_;
@@ -1513,7 +1523,38 @@ int NeuronGPU::GetKernelTiming(int kind, double *total_ms, long long *launches) 
 }
 
 // one time step on stream_ (kernel launches only, no host synchronisation)
+void NeuronGPU::EnsureForkResources() {
+  if (dstream_ != nullptr) return;
+  const char *env = getenv("NGB200_FORK_DELIVERY");
+  if (env != nullptr && atoi(env) == 0) return;
+  // highest priority: when an update block retires, the SM takes a pending
+  // delivery block first, so the (memory-bound) delivery overlaps the
+  // (issue-bound) update instead of waiting for its last wave
+  int least = 0, greatest = 0;
+  NGPU_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  const char *prio = getenv("NGB200_DELIVERY_PRIORITY");
+  NGPU_CUDA(cudaStreamCreateWithPriority(&dstream_, cudaStreamDefault,
+                                         (prio != nullptr && atoi(prio) == 0) ? least : greatest));
+  NGPU_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+  NGPU_CUDA(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
+}
+
 void NeuronGPU::EnqueueStep(int step_in_chunk) {
+  DeliverArgs d = MakeDeliverArgs();
+  const bool has_delivery = d.nd > 0;
+  // The delivery of step T reads the spikes of steps before T and adds into
+  // the accumulator half that the update of T + 1 folds, while the updates
+  // of step T fold the other half: without plastic synapses the two touch
+  // disjoint data, so the delivery runs on its own stream beside the node
+  // updates and the step bookkeeping joins them.
+  const bool fork = has_delivery && !plastic_ && !ktime_ && dstream_ != nullptr;
+  if (fork) {
+    NGPU_CUDA(cudaEventRecord(ev_fork_, stream_));
+    NGPU_CUDA(cudaStreamWaitEvent(dstream_, ev_fork_, 0));
+    d.advance_flags = 0;
+    LaunchDeliver(d, syn_table_, d_ctx_, deliver_blocks_, dstream_);
+    NGPU_CUDA(cudaEventRecord(ev_join_, dstream_));
+  }
   if (ktime_) KEvent(step_in_chunk, 0);
   for (NodeGroup *g : groups_) {
     const ModelInfo *mi = g->mi;
@@ -1559,9 +1600,12 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
     flags |= 2;
   }
   if (ktime_) KEvent(step_in_chunk, 1);
+  if (fork) {
+    NGPU_CUDA(cudaStreamWaitEvent(stream_, ev_join_, 0));
+    LaunchAdvance(d_ring_cnt_, ring_R_, ring_C_, flags, d_ctx_, stream_);
+    return;
+  }
   // the step's last kernel also does the step bookkeeping (finish_step)
-  DeliverArgs d = MakeDeliverArgs();
-  const bool has_delivery = d.nd > 0;
   if (has_delivery && !plastic_) d.advance_flags = flags;
   if (plastic_ && rev_R_ > 1) LaunchRevArrive(d, d_ctx_, stream_);
   LaunchDeliver(d, syn_table_, d_ctx_, deliver_blocks_, stream_);
@@ -1589,6 +1633,7 @@ void NeuronGPU::LaunchSteps(int n_steps) {
       }
     }
   }
+  EnsureForkResources();
   if (!use_graphs_) {
     for (int k = 0; k < n_steps; k++) EnqueueStep(k);
   } else {
@@ -1618,7 +1663,7 @@ void NeuronGPU::LaunchSteps(int n_steps) {
       }
       kernels_per_step_ = (double)n_kernels / n_steps;
       cudaGraphExec_t exec;
-      NGPU_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+      NGPU_CUDA(cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority));
       cudaGraphDestroy(graph);
       it = graphs_.emplace(n_steps, exec).first;
     }

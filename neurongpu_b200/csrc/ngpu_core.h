@@ -426,6 +426,11 @@ class NeuronGPU {
   bool calibrate_flag_ = false;
   bool first_simulation_flag_ = true;
   cudaStream_t stream_ = nullptr;
+  // delivery beside the node updates (non-plastic networks): its stream and
+  // the fork / join events of a step (NGB200_FORK_DELIVERY=0 keeps one stream)
+  cudaStream_t dstream_ = nullptr;
+  cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
+  void EnsureForkResources();
   StepCtx *d_ctx_ = nullptr;
   long long *d_acc_ = nullptr;
   long long n_acc_ = 0;

@@ -73,6 +73,11 @@ struct PushArgs {
 struct InputArgs {
   long long *acc;               // global accumulator array
   long long acc_base;           // this group's first slot
+  // accumulators per parity half (0: one buffer). Deliveries of step T add
+  // into half T & 1 and the update of step T + 1 folds and clears that half,
+  // so the update of a step and the delivery of the same step touch
+  // different halves and may run concurrently.
+  long long acc_par;
   int np;                       // receptor ports
   int in_var;                   // var column of port-0 input
   int in_step;                  // column stride between ports
@@ -209,6 +214,7 @@ struct DeliverArgs {
   int *e_stamp;                        // arrival step of last pre spike
   const unsigned *e_post;              // target node id (plastic networks)
   long long *acc;
+  long long acc_par;                   // accumulators per parity half (0: one buffer)
   const unsigned *ring_src;
   const float *ring_h;
   const int *ring_cnt;

@@ -48,7 +48,7 @@ static int tile_grid(int n_tiles) {
 static bool tiles_aligned(const GroupArgs &g, const InputArgs &in) {
   auto al = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
   return al(g.var) && al(g.param) && al(g.h) && al(g.dx) && al(in.acc + in.acc_base) &&
-         (g.n_pad % NGPU_BLOCK) == 0;
+         ((in.acc_par * sizeof(long long)) & 15u) == 0 && (g.n_pad % NGPU_BLOCK) == 0;
 }
 
 template <class M, int NP>
@@ -364,7 +364,7 @@ __global__ void k_fold_input(GroupArgs g, InputArgs in, StepCtx *ctx) {
   }
   // ports beyond 4 (RK5 groups with many receptors)
   for (int q = 4; q < in.np; q++) {
-    long long *a = in.acc + in.acc_base + (long long)q * g.n_pad + i;
+    long long *a = acc_in(in, ctx->T0, ctx->it) + (long long)q * g.n_pad + i;
     long long sv = *a;
     if (sv == 0) continue;
     *a = 0;
@@ -452,6 +452,7 @@ k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
   __shared__ int s_pref[NGPU_MAX_DELAYS + 1];
   __shared__ int s_slot[NGPU_MAX_DELAYS];
   const long long T = ctx->T0 + ctx->it + 1;
+  long long *const acc = d.acc + ((T & 1) ? d.acc_par : 0);   // folded by the update of T + 1
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int n_warps = (gridDim.x * blockDim.x) >> 5;
@@ -536,7 +537,7 @@ k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
         for (int u = 0; u < 4; u++) {
           const unsigned long long e = e0 + 32 * u;
           if (e < end) {
-            atomicAdd((unsigned long long *)(d.acc + sl[u]),
+            atomicAdd((unsigned long long *)(acc + sl[u]),
                       (unsigned long long)ng_to_fixed(height * wv[u]));
           }
         }
@@ -545,7 +546,7 @@ k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
       for (unsigned long long e = beg + lane; e < end; e += 32) {
         const unsigned slot_t = d.e_slot[e];
         const float w = d.e_w[e];
-        atomicAdd((unsigned long long *)(d.acc + slot_t),
+        atomicAdd((unsigned long long *)(acc + slot_t),
                   (unsigned long long)ng_to_fixed(height * w));
         const int sg = d.e_syn[e];
         if (sg > 0) {

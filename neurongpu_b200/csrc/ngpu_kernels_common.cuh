@@ -66,6 +66,12 @@ __device__ __forceinline__ void push_spike(const PushArgs &pa, StepCtx *ctx,
   }
 }
 
+// This group's accumulators that the update following step T0 + it + 1's
+// predecessor folds: the parity half written by the delivery of step T0 + it.
+__device__ __forceinline__ long long *acc_in(const InputArgs &in, long long T0, long long it) {
+  return in.acc + (((T0 + it) & 1) ? in.acc_par : 0) + in.acc_base;
+}
+
 // Sum of the pending synaptic input of one node per port (fixed point):
 // accumulator contents (cleared here) plus the Poisson direct connections
 // drawn for the previous step. pre_acc: the accumulator values already
@@ -81,7 +87,7 @@ __device__ __forceinline__ void input_sum(const InputArgs &in, int i,
   for (int q = 0; q < NP; q++) {
     s[q] = 0;
     if (q < np) {
-      long long *a = in.acc + in.acc_base + (long long)q * n_pad + i;
+      long long *a = acc_in(in, T0, it) + (long long)q * n_pad + i;
       long long v = pre_acc ? pre_acc[q] : *a;
       if (v != 0 && !(in.dry || dry)) *a = 0;
       s[q] = v;
@@ -626,7 +632,7 @@ struct Rk5TileStage {
 
 template <class M, int NP>
 __device__ __forceinline__ void rk5_issue_tile(Rk5TileStage<M, NP> &st, uint64_t *bar,
-                                               const GroupArgs &g, const InputArgs &in,
+                                               const GroupArgs &g, const long long *acc,
                                                int n_acc, int t) {
   using Tr = ModelTraits<M>;
   const long long o = (long long)t * NGPU_BLOCK;
@@ -637,8 +643,7 @@ __device__ __forceinline__ void rk5_issue_tile(Rk5TileStage<M, NP> &st, uint64_t
   bulk_g2s(st.col[M::NVAR], g.param + (long long)Tr::refr * g.n_pad + o, cb, bar);
   bulk_g2s(st.col[M::NVAR + 1], g.h + o, cb, bar);
   bulk_g2s(st.col[M::NVAR + 2], g.dx + o, cb, bar);
-  for (int q = 0; q < n_acc; q++)
-    bulk_g2s(st.acc[q], in.acc + in.acc_base + (long long)q * g.n_pad + o, ab, bar);
+  for (int q = 0; q < n_acc; q++) bulk_g2s(st.acc[q], acc + (long long)q * g.n_pad + o, ab, bar);
 }
 
 template <class M, int NP, int MINB>
@@ -656,10 +661,12 @@ k_rk5_update_tiles(const __grid_constant__ GroupArgs g, const __grid_constant__ 
     mbar_init(&s_bar[1], 1);
   }
   __syncthreads();
+  // this step's input half (thread 0 issues every copy)
+  const long long *acc = threadIdx.x == 0 ? acc_in(in, ctx->T0, ctx->it) : nullptr;
   if (threadIdx.x == 0) {
-    if ((int)blockIdx.x < n_tiles) rk5_issue_tile<M, NP>(s_st[0], &s_bar[0], g, in, n_acc, blockIdx.x);
+    if ((int)blockIdx.x < n_tiles) rk5_issue_tile<M, NP>(s_st[0], &s_bar[0], g, acc, n_acc, blockIdx.x);
     if ((int)blockIdx.x + G < n_tiles)
-      rk5_issue_tile<M, NP>(s_st[1], &s_bar[1], g, in, n_acc, blockIdx.x + G);
+      rk5_issue_tile<M, NP>(s_st[1], &s_bar[1], g, acc, n_acc, blockIdx.x + G);
   }
   const Rk5Queue *qu = g.q.cap > 0 ? &g.q : nullptr;
   unsigned evals = 0;
@@ -686,7 +693,7 @@ k_rk5_update_tiles(const __grid_constant__ GroupArgs g, const __grid_constant__ 
     __syncthreads();                    // stage s is free again
     if (threadIdx.x == 0 && t + 2 * G < n_tiles) {
       proxy_fence_async_smem();         // order the reads above before the copy
-      rk5_issue_tile<M, NP>(s_st[s], &s_bar[s], g, in, n_acc, t + 2 * G);
+      rk5_issue_tile<M, NP>(s_st[s], &s_bar[s], g, acc, n_acc, t + 2 * G);
     }
     const int i = t * NGPU_BLOCK + threadIdx.x;
     if (i < g.n) rk5_neuron<M, NP, true, STEP_PLAIN>(g, in, pa, ctx, i, g.puni, g.pinv, evals,
