@@ -881,6 +881,57 @@ std::vector<float> NeuronGPU::GetRecSpikeTimes(int i_node) {
 // ---------------------------------------------------------------------------
 // argument builders
 // ---------------------------------------------------------------------------
+// propagator from an exponential current to the membrane potential
+// (src/iaf_psc_exp_g.cu:68-88): the exact expression, or its limit when the
+// two time constants (nearly) coincide
+static double propagator_32(double tau_syn, double tau, double C, double h) {
+  const double P32_linear = 1.0 / (2.0 * C * tau * tau) * h * h * (tau_syn - tau) * exp(-h / tau);
+  const double P32_singular = h / C * exp(-h / tau);
+  const double P32 = -tau / (C * (1.0 - tau / tau_syn)) * exp(-h / tau_syn)
+                     * expm1(h * (1.0 / tau_syn - 1.0 / tau));
+  const double dev = fabs(P32 - P32_singular);
+  if (tau == tau_syn || (fabs(tau - tau_syn) < 0.1 && dev > 2.0 * fabs(P32_linear)))
+    return P32_singular;
+  return P32;
+}
+
+// constants of the non-RK5 models that the reference computes from the group
+// parameters at every update, in the reference's float / double mix
+// (src/iaf_psc_exp_g.cu:143-150, src/izhikevich.cu:140-146,
+// src/izhikevich_psc_exp_2s.cu:145-152)
+static void group_constants(const NodeGroup *g, float dt, float *gc) {
+  const ModelInfo *mi = g->mi;
+  for (int k = 0; k < 8; k++) gc[k] = 0.0f;
+  if (mi->kind == MK_IAF_PSC_EXP_G) {
+    // iaf_psc_exp_hc: iaf_psc_exp_g's defaults at dt = 0.1 ms, whatever the
+    // time resolution (src/iaf_psc_exp_hc_params.h)
+    float h = dt, tau_m = 10.0f, C_m = 250.0f, Theta = 15.0f, V_reset = 0.0f;
+    float tau_syn = 0.5f, t_ref = 2.0f;
+    if (mi->hard_coded) {
+      h = 0.1f;
+    } else {
+      tau_m = g->group_param[0]; C_m = g->group_param[1];
+      Theta = g->group_param[3]; V_reset = g->group_param[4];
+      tau_syn = g->group_param[5]; t_ref = g->group_param[6];
+    }
+    const float P22 = (float)exp((double)(-h / tau_m));
+    gc[0] = (float)exp((double)(-h / tau_syn));
+    gc[1] = P22;
+    gc[2] = (float)propagator_32(tau_syn, tau_m, C_m, h);
+    gc[3] = (float)(tau_m / C_m * (1.0 - (double)P22));
+    gc[4] = Theta;
+    gc[5] = V_reset;
+    gc[6] = (float)(int)round((double)(t_ref / h));
+  } else if (mi->kind == MK_IZHIKEVICH || mi->kind == MK_IZH_PSC_EXP) {
+    const float h = dt / (float)mi->n_sub;
+    for (int k = 0; k < 5; k++) gc[k] = g->group_param[k];   // V_th, a, b, c, d
+    const float t_ref = g->group_param[mi->kind == MK_IZHIKEVICH ? 5 : 6];
+    gc[5] = (float)(int)round((double)(t_ref / h));
+    gc[6] = h;
+    if (mi->kind == MK_IZH_PSC_EXP) gc[7] = (float)exp((double)(-h / g->group_param[5]));
+  }
+}
+
 GroupArgs NeuronGPU::MakeGroupArgs(NodeGroup *g) {
   GroupArgs a;
   memset(&a, 0, sizeof(a));
@@ -909,6 +960,7 @@ GroupArgs NeuronGPU::MakeGroupArgs(NodeGroup *g) {
     a.eps = g->rk5_eps;
   }
   a.dt = time_resolution_;
+  group_constants(g, time_resolution_, a.gc);
   a.variant = g->rk5_variant;
   a.dry = 0;
   a.den_delay_col = g->mi->den_delay_param;
@@ -1571,6 +1623,12 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
         break;
       case MK_IAF_PSC_EXP:
         LaunchIafPscExpUpdate(MakeGroupArgs(g), MakeInputArgs(g), MakePushArgs(g), d_ctx_, stream_);
+        break;
+      case MK_IAF_PSC_EXP_G:
+      case MK_IZHIKEVICH:
+      case MK_IZH_PSC_EXP:
+        LaunchSimpleNeuronUpdate(mi->kind, mi->n_sub, MakeGroupArgs(g), MakeInputArgs(g),
+                                 MakePushArgs(g), d_ctx_, stream_);
         break;
       case MK_SPIKE_GENERATOR:
         if (g->d_sg_off) LaunchSpikeGeneratorUpdate(MakeGroupArgs(g), MakePushArgs(g), d_ctx_, stream_);

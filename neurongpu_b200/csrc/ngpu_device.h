@@ -168,6 +168,8 @@ struct GroupArgs {
   unsigned pmask[NGPU_MAX_PARAM / 32];  // bit j: param j read per neuron
   float puni[NGPU_MAX_PARAM];   // uniform parameter values
   float pinv[NGPU_MAX_PARAM];   // 1 / puni[j] (IEEE division on the host)
+  float gc[8];                  // constants derived from group parameters (propagators,
+                                // thresholds, refractory steps) of the non-RK5 models
   int all_uniform;              // every parameter but refractory_step uniform
   int variant;                  // RK5 kernel variant (occupancy target)
   int dry;                      // timing run: compute everything, store nothing

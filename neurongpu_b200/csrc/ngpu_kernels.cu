@@ -220,6 +220,152 @@ void LaunchIafPscExpUpdate(const GroupArgs &g, const InputArgs &in,
 }
 
 // ---------------------------------------------------------------------------
+// iaf_psc_exp_g and iaf_psc_exp_hc (src/iaf_psc_exp_g.cu:39-66,
+// src/iaf_psc_exp_hc.cu:33-59): one exponential current, exact propagators
+// of the group. gc = P11, P22, P21, P20, Theta_rel, V_reset_rel, refractory
+// steps. Variables I_syn, V_m_rel, refractory_step; parameter I_e.
+// ---------------------------------------------------------------------------
+__global__ void k_iaf_psc_exp_g(GroupArgs g, InputArgs in, PushArgs pa, StepCtx *ctx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.n) return;
+  const long long it = ctx->it, T0 = ctx->T0;
+  const double t0 = ctx->t0;
+  const int n_pad = g.n_pad;
+  float *var = g.var;
+  float I_syn = var[i], V = var[n_pad + i], refr = var[2 * n_pad + i];
+  long long s[1];
+  input_sum<1>(in, i, n_pad, 1, it, t0, g.dt, ctx->poisson_pending, T0, s);
+  if (s[0] != 0) I_syn = fold_value(I_syn, s[0], 1.0f);
+  const float I_e = gparam(g, 0, i);
+  if (refr > 0.0f) {
+    refr -= 1.0f;
+  } else {
+    V = V * g.gc[1] + I_syn * g.gc[2] + I_e * g.gc[3];
+  }
+  I_syn *= g.gc[0];
+  if (V >= g.gc[4]) {
+    const long long T = T0 + it + 1;
+    const double t_now = t0 + (double)g.dt * (double)(it + 1);
+    push_spike(pa, ctx, g.i_node_0 + i, i, 1.0f, T, t_now, 0);
+    V = g.gc[5];
+    refr = g.gc[6];
+  }
+  var[i] = I_syn;
+  var[n_pad + i] = V;
+  var[2 * n_pad + i] = refr;
+}
+
+// ---------------------------------------------------------------------------
+// izhikevich (src/izhikevich.cu:38-72): forward Euler, the input of the
+// previous step added to V_m. The quadratic is evaluated with double
+// constants, i.e. in FP64, as in the reference. gc = V_th, a, b, c, d,
+// refractory steps, h. Variables I_syn, V_m, u, refractory_step; parameters
+// I_e, den_delay.
+// ---------------------------------------------------------------------------
+__global__ void k_izhikevich(GroupArgs g, InputArgs in, PushArgs pa, StepCtx *ctx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.n) return;
+  const long long it = ctx->it, T0 = ctx->T0;
+  const double t0 = ctx->t0;
+  const int n_pad = g.n_pad;
+  float *var = g.var;
+  float I_syn = var[i], V = var[n_pad + i], u = var[2 * n_pad + i];
+  float refr = var[3 * n_pad + i];
+  long long s[1];
+  input_sum<1>(in, i, n_pad, 1, it, t0, g.dt, ctx->poisson_pending, T0, s);
+  if (s[0] != 0) I_syn = fold_value(I_syn, s[0], 1.0f);
+  const float I_e = gparam(g, 0, i);
+  const float h = g.gc[6], a = g.gc[1], b = g.gc[2];
+  if (refr > 0.0f) {
+    refr -= 1.0f;
+  } else {
+    const float v_old = V, u_old = u;
+    V += h * (0.04 * v_old * v_old + 5.0 * v_old + 140.0 - u_old + I_e) + I_syn;
+    u += h * a * (b * v_old - u_old);
+  }
+  I_syn = 0.0f;
+  if (V >= g.gc[0]) {
+    const long long T = T0 + it + 1;
+    const double t_now = t0 + (double)g.dt * (double)(it + 1);
+    const int den = (int)roundf(gparam(g, 1, i) / g.dt);
+    push_spike(pa, ctx, g.i_node_0 + i, i, 1.0f, T, t_now, den);
+    V = g.gc[3];
+    u += g.gc[4];
+    refr = g.gc[5] < 0.0f ? 0.0f : g.gc[5];
+  }
+  var[i] = I_syn;
+  var[n_pad + i] = V;
+  var[2 * n_pad + i] = u;
+  var[3 * n_pad + i] = refr;
+}
+
+// ---------------------------------------------------------------------------
+// izhikevich_psc_exp, _2s, _5s (src/izhikevich_psc_exp.cu:40-76,
+// src/izhikevich_psc_exp_2s.cu:41-83): NSUB forward-Euler sub-steps of
+// dt / NSUB per time step, each followed by the decay of the exponential
+// current; a refractory neuron only decays its current. gc = V_th, a, b, c,
+// d, refractory steps, sub-step h, current decay per sub-step.
+// ---------------------------------------------------------------------------
+template <int NSUB>
+__global__ void k_izh_psc_exp(GroupArgs g, InputArgs in, PushArgs pa, StepCtx *ctx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.n) return;
+  const long long it = ctx->it, T0 = ctx->T0;
+  const double t0 = ctx->t0;
+  const int n_pad = g.n_pad;
+  float *var = g.var;
+  float I_syn = var[i], V = var[n_pad + i], u = var[2 * n_pad + i];
+  float refr = var[3 * n_pad + i];
+  long long s[1];
+  input_sum<1>(in, i, n_pad, 1, it, t0, g.dt, ctx->poisson_pending, T0, s);
+  if (s[0] != 0) I_syn = fold_value(I_syn, s[0], 1.0f);
+  const float I_e = gparam(g, 0, i);
+  const float h = g.gc[6], a = g.gc[1], b = g.gc[2], C_syn = g.gc[7];
+  if (refr > 0.0f) {
+    refr -= 1.0f;
+#pragma unroll
+    for (int k = 0; k < NSUB; k++) I_syn *= C_syn;
+  } else {
+#pragma unroll
+    for (int k = 0; k < NSUB; k++) {
+      const float v_old = V, u_old = u;
+      V += h * (0.04 * v_old * v_old + 5.0 * v_old + 140.0 - u_old + I_syn + I_e);
+      u += h * a * (b * v_old - u_old);
+      I_syn *= C_syn;
+    }
+  }
+  if (V >= g.gc[0]) {
+    const long long T = T0 + it + 1;
+    const double t_now = t0 + (double)g.dt * (double)(it + 1);
+    const int den = (int)roundf(gparam(g, 1, i) / g.dt);
+    push_spike(pa, ctx, g.i_node_0 + i, i, 1.0f, T, t_now, den);
+    V = g.gc[3];
+    u += g.gc[4];
+    refr = g.gc[5] < 0.0f ? 0.0f : g.gc[5];
+  }
+  var[i] = I_syn;
+  var[n_pad + i] = V;
+  var[2 * n_pad + i] = u;
+  var[3 * n_pad + i] = refr;
+}
+
+void LaunchSimpleNeuronUpdate(int kind, int n_sub, const GroupArgs &g, const InputArgs &in,
+                              const PushArgs &pa, StepCtx *ctx, cudaStream_t s) {
+  if (g.n <= 0) return;
+  const dim3 grid((g.n + NGPU_BLOCK - 1) / NGPU_BLOCK), block(NGPU_BLOCK);
+  switch (kind) {
+    case MK_IAF_PSC_EXP_G: k_iaf_psc_exp_g<<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+    case MK_IZHIKEVICH: k_izhikevich<<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+    case MK_IZH_PSC_EXP:
+      if (n_sub == 5) k_izh_psc_exp<5><<<grid, block, 0, s>>>(g, in, pa, ctx);
+      else if (n_sub == 2) k_izh_psc_exp<2><<<grid, block, 0, s>>>(g, in, pa, ctx);
+      else k_izh_psc_exp<1><<<grid, block, 0, s>>>(g, in, pa, ctx);
+      break;
+    default: break;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // spike_generator (src/spike_generator.cu:37-55)
 // ---------------------------------------------------------------------------
 __global__ void k_spike_generator(GroupArgs g, PushArgs pa, StepCtx *ctx) {

@@ -41,6 +41,11 @@ void LaunchRk5Batch(const Rk5Batch &b, StepCtx *ctx, cudaStream_t s);
 bool StepProposerSupported(int model, int np);
 void LaunchIafPscExpUpdate(const GroupArgs &g, const InputArgs &in,
                            const PushArgs &pa, StepCtx *ctx, cudaStream_t s);
+// iaf_psc_exp_g / _hc (MK_IAF_PSC_EXP_G), izhikevich (MK_IZHIKEVICH) and
+// izhikevich_psc_exp with n_sub Euler sub-steps (MK_IZH_PSC_EXP); the group
+// constants are in GroupArgs::gc
+void LaunchSimpleNeuronUpdate(int kind, int n_sub, const GroupArgs &g, const InputArgs &in,
+                              const PushArgs &pa, StepCtx *ctx, cudaStream_t s);
 void LaunchSpikeGeneratorUpdate(const GroupArgs &g, const PushArgs &pa,
                                 StepCtx *ctx, cudaStream_t s);
 void LaunchParrotUpdate(const GroupArgs &g, const InputArgs &in,

@@ -10,6 +10,12 @@
 //   aeif_psc_delta     src/aeif_psc_delta_kernel.h, src/aeif_psc_delta.cu:25-60
 //   izhikevich_cond_beta src/izhikevich_cond_beta_kernel.h, src/izhikevich_cond_beta.cu
 //   iaf_psc_exp        src/iaf_psc_exp.h:20-90, src/iaf_psc_exp.cu:53-180
+//   iaf_psc_exp_g      src/iaf_psc_exp_g.h:30-75, src/iaf_psc_exp_g.cu:39-149
+//   iaf_psc_exp_hc     src/iaf_psc_exp_hc.h:30-50, src/iaf_psc_exp_hc.cu:33-107,
+//                      src/iaf_psc_exp_hc_params.h (iaf_psc_exp_g's defaults at dt 0.1)
+//   izhikevich         src/izhikevich.h:30-72, src/izhikevich.cu:38-136
+//   izhikevich_psc_exp(_2s, _5s) src/izhikevich_psc_exp.h:30-76,
+//                      src/izhikevich_psc_exp.cu:40-148, src/izhikevich_psc_exp_2s.cu:41-155
 //   spike_generator    src/spike_generator.cu:24-60
 //   parrot_neuron      src/parrot_neuron.cu:20-112
 //   spike_detector     src/spike_detector.cu:20-106
@@ -30,7 +36,10 @@ enum ModelKind {
   MK_PARROT,
   MK_SPIKE_DETECTOR,
   MK_POISSON_GENERATOR,   // device Poisson source, delivered by direct connections
-  MK_POISSON_NODES        // CreatePoissonGenerator: nodes that push spike counts
+  MK_POISSON_NODES,       // CreatePoissonGenerator: nodes that push spike counts
+  MK_IAF_PSC_EXP_G,       // iaf_psc_exp_g / iaf_psc_exp_hc: one port, group parameters
+  MK_IZHIKEVICH,          // Euler Izhikevich, input added to V_m
+  MK_IZH_PSC_EXP          // Euler Izhikevich with an exponential current, n_sub Euler steps
 };
 
 enum Rk5Model {
@@ -60,6 +69,8 @@ struct ModelInfo {
   std::vector<float> w_const;   // constant weight per port (w_param false)
   int refr_param;               // param index of refractory_step (-1: none)
   int den_delay_param;          // param index of den_delay (-1: none)
+  int n_sub = 1;                // Euler sub-steps per time step (MK_IZH_PSC_EXP)
+  int hard_coded = 0;           // iaf_psc_exp_hc: constants of iaf_psc_exp_g's defaults
 };
 
 inline const std::vector<ModelInfo> &ModelCatalogue() {
@@ -173,6 +184,58 @@ inline const std::vector<ModelInfo> &ModelCatalogue() {
     m.w_const = {1.0f, 1.0f};
     m.refr_param = -1; m.den_delay_param = 9;
     cat.push_back(m);
+  }
+  {
+    // refractory_step is a state variable here; one input port into I_syn
+    for (int hc = 0; hc < 2; hc++) {
+      ModelInfo m;
+      m.name = hc ? "iaf_psc_exp_hc" : "iaf_psc_exp_g";
+      m.kind = MK_IAF_PSC_EXP_G; m.rk5_model = -1; m.fixed_n_port = 1;
+      m.scal_var = {"I_syn", "V_m_rel", "refractory_step"};
+      m.scal_var_def = {0.0f, 0.0f, 0.0f};
+      m.scal_param = {"I_e"}; m.scal_param_def = {0.0f};
+      if (!hc) {
+        m.group_param = {"tau_m", "C_m", "E_L", "Theta_rel", "V_reset_rel", "tau_syn", "t_ref"};
+        m.group_param_def = {10.0f, 250.0f, -65.0f, 15.0f, 0.0f, 0.5f, 2.0f};
+      }
+      m.hard_coded = hc;
+      m.in_var = 0; m.in_step = 0; m.w_param = false; m.w_param_idx = -1;
+      m.w_const = {1.0f};
+      m.refr_param = -1; m.den_delay_param = -1;
+      cat.push_back(m);
+    }
+  }
+  {
+    ModelInfo m;
+    m.name = "izhikevich"; m.kind = MK_IZHIKEVICH; m.rk5_model = -1; m.fixed_n_port = 1;
+    m.scal_var = {"I_syn", "V_m", "u", "refractory_step"};
+    m.scal_var_def = {0.0f, -70.0f, -70.0f * 0.2f, 0.0f};
+    m.scal_param = {"I_e", "den_delay"}; m.scal_param_def = {0.0f, 0.0f};
+    m.group_param = {"V_th", "a", "b", "c", "d", "t_ref"};
+    m.group_param_def = {30.0f, 0.02f, 0.2f, -65.0f, 8.0f, 0.0f};
+    m.in_var = 0; m.in_step = 0; m.w_param = false; m.w_param_idx = -1;
+    m.w_const = {1.0f};
+    m.refr_param = -1; m.den_delay_param = 1;
+    cat.push_back(m);
+  }
+  {
+    const char *names[3] = {"izhikevich_psc_exp", "izhikevich_psc_exp_2s", "izhikevich_psc_exp_5s"};
+    const int subs[3] = {1, 2, 5};
+    const float tau[3] = {0.5f, 2.0f, 2.0f};
+    for (int k = 0; k < 3; k++) {
+      ModelInfo m;
+      m.name = names[k]; m.kind = MK_IZH_PSC_EXP; m.rk5_model = -1; m.fixed_n_port = 1;
+      m.scal_var = {"I_syn", "V_m", "u", "refractory_step"};
+      m.scal_var_def = {0.0f, -70.0f, -70.0f * 0.2f, 0.0f};
+      m.scal_param = {"I_e", "den_delay"}; m.scal_param_def = {0.0f, 0.0f};
+      m.group_param = {"V_th", "a", "b", "c", "d", "tau_syn", "t_ref"};
+      m.group_param_def = {30.0f, 0.02f, 0.2f, -65.0f, 8.0f, tau[k], 0.0f};
+      m.n_sub = subs[k];
+      m.in_var = 0; m.in_step = 0; m.w_param = false; m.w_param_idx = -1;
+      m.w_const = {1.0f};
+      m.refr_param = -1; m.den_delay_param = 1;
+      cat.push_back(m);
+    }
   }
   {
     ModelInfo m;

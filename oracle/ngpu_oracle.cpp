@@ -13,6 +13,9 @@
 //   conductance normalisation g0 / I0            src/aeif_cond_beta.cu:58-87,
 //                                                src/aeif_cond_alpha.cu:63-68
 //   iaf_psc_exp exact propagators                src/iaf_psc_exp.cu:53-119
+//   iaf_psc_exp_g / _hc (one current, group params) src/iaf_psc_exp_g.cu:39-88,143-150
+//   izhikevich (Euler, input added to V_m)        src/izhikevich.cu:38-72
+//   izhikevich_psc_exp, _2s, _5s (Euler sub-steps) src/izhikevich_psc_exp_2s.cu:41-83
 //   delay handling d_int = round(d/dt)-1 and the
 //   buffer timing (spike of step k reaches the
 //   input after step k+D)                         src/connect.cu:26-62,
@@ -48,8 +51,12 @@ namespace {
 enum OModel {
   O_AEIF_COND_BETA = 0, O_AEIF_COND_ALPHA, O_AEIF_PSC_ALPHA, O_AEIF_PSC_EXP,
   O_AEIF_PSC_DELTA, O_IZH_COND_BETA, O_IAF_PSC_EXP, O_SPIKE_GENERATOR,
-  O_PARROT, O_POISSON_GENERATOR
+  O_PARROT, O_POISSON_GENERATOR, O_IAF_PSC_EXP_G, O_IZHIKEVICH, O_IZH_PSC_EXP
 };
+// simple (non-RK5, non-generator) neuron models updated in the parallel loop
+static inline bool simple_model(int m) {
+  return m == O_IAF_PSC_EXP || m == O_IAF_PSC_EXP_G || m == O_IZHIKEVICH || m == O_IZH_PSC_EXP;
+}
 
 typedef double real;
 
@@ -284,6 +291,7 @@ static int in_var(const Group &g, int q) {
     case O_AEIF_PSC_DELTA: return 0;
     case O_IAF_PSC_EXP: return q;
     case O_PARROT: return q;
+    case O_IAF_PSC_EXP_G: case O_IZHIKEVICH: case O_IZH_PSC_EXP: return 0;
     default: return -1;
   }
 }
@@ -325,6 +333,7 @@ static int den_steps(const Oracle &o, int node) {
     case O_IZH_COND_BETA: d = p[I_den_delay]; break;
     case O_IAF_PSC_EXP: d = p[9]; break;
     case O_PARROT: d = p[1]; break;
+    case O_IZHIKEVICH: case O_IZH_PSC_EXP: d = p[1]; break;
     default: return 0;
   }
   return (int)round((float)d / (float)o.dt);
@@ -463,6 +472,83 @@ static void fold(Oracle &o, long long T_pending, bool poisson) {
   }
 }
 
+// One time step of a simple model; true if the neuron spikes.
+//   iaf_psc_exp:   vars I_ex, I_in, V_m_rel, refr; params as the library
+//   iaf_psc_exp_g: vars I_syn, V_m_rel, refr; params I_e, tau_m, C_m, E_L,
+//                  Theta_rel, V_reset_rel, tau_syn, t_ref, h_prop (the step of
+//                  the propagators: dt, or 0.1 ms for iaf_psc_exp_hc)
+//   izhikevich:    vars I_syn, V_m, u, refr; params I_e, den_delay, V_th, a,
+//                  b, c, d, t_ref
+//   izhikevich_psc_exp: as izhikevich plus tau_syn before t_ref and n_sub
+static bool simple_update(int model, real *y, const real *p, real dt) {
+  if (model == O_IAF_PSC_EXP) {
+    real &I_ex = y[0], &I_in = y[1], &V = y[2], &refr = y[3];
+    if (refr > 0) refr -= 1;
+    else V = V * p[15] + I_ex * p[13] + I_in * p[14] + p[3] * p[10];
+    I_ex *= p[11];
+    I_in *= p[12];
+    if (V >= p[4]) {
+      V = p[5];
+      refr = round(p[8] / dt);
+      return true;
+    }
+    return false;
+  }
+  if (model == O_IAF_PSC_EXP_G) {
+    real &I = y[0], &V = y[1], &refr = y[2];
+    const real h = p[8] > 0 ? p[8] : dt;
+    const real tau_m = p[1], C_m = p[2], tau_syn = p[6];
+    const real P22 = exp(-h / tau_m);
+    if (refr > 0) refr -= 1;
+    else V = V * P22 + I * propagator_32(tau_syn, tau_m, C_m, h) + p[0] * (tau_m / C_m * (1.0 - P22));
+    I *= exp(-h / tau_syn);
+    if (V >= p[4]) {
+      V = p[5];
+      refr = round(p[7] / h);
+      return true;
+    }
+    return false;
+  }
+  // Izhikevich family
+  real &I = y[0], &V = y[1], &u = y[2], &refr = y[3];
+  const real V_th = p[2], a = p[3], b = p[4], c = p[5], d = p[6];
+  real h = dt, t_ref = p[7];
+  if (model == O_IZHIKEVICH) {
+    if (refr > 0) {
+      refr -= 1;
+    } else {
+      const real v = V, w = u;
+      V += h * (0.04 * v * v + 5.0 * v + 140.0 - w + p[0]) + I;
+      u += h * a * (b * v - w);
+    }
+    I = 0;
+  } else {
+    const int n_sub = (int)p[9];
+    h = dt / n_sub;
+    t_ref = p[8];
+    const real C_syn = exp(-h / p[7]);
+    if (refr > 0) {
+      refr -= 1;
+      for (int k = 0; k < n_sub; k++) I *= C_syn;
+    } else {
+      for (int k = 0; k < n_sub; k++) {
+        const real v = V, w = u;
+        V += h * (0.04 * v * v + 5.0 * v + 140.0 - w + I + p[0]);
+        u += h * a * (b * v - w);
+        I *= C_syn;
+      }
+    }
+  }
+  if (V >= V_th) {
+    V = c;
+    u += d;
+    refr = round(t_ref / h);
+    if (refr < 0) refr = 0;
+    return true;
+  }
+  return false;
+}
+
 static void step(Oracle &o, int it_in_session) {
   const long long T = o.T + 1;            // time index after this step
   const double t0 = (double)o.T * (double)(float)o.dt;
@@ -474,7 +560,7 @@ static void step(Oracle &o, int it_in_session) {
     // parallel, each thread collecting its spikes in node order; the lists
     // are merged in thread (= node) order, so the result does not depend on
     // the number of threads
-    if (g.model <= O_IZH_COND_BETA || g.model == O_IAF_PSC_EXP) {
+    if (g.model <= O_IZH_COND_BETA || simple_model(g.model)) {
       int nthr = 1;
 #ifdef _OPENMP
       nthr = omp_get_max_threads();
@@ -506,17 +592,8 @@ static void step(Oracle &o, int it_in_session) {
               end = (x >= x1 - h_min);
               if (external_update(g.model, y, p, end, o.dt)) part[tid].push_back({node, 1.0});
             }
-          } else {
-            real &I_ex = y[0], &I_in = y[1], &V = y[2], &refr = y[3];
-            if (refr > 0) refr -= 1;
-            else V = V * p[15] + I_ex * p[13] + I_in * p[14] + p[3] * p[10];
-            I_ex *= p[11];
-            I_in *= p[12];
-            if (V >= p[4]) {
-              part[tid].push_back({node, 1.0});
-              V = p[5];
-              refr = round(p[8] / o.dt);
-            }
+          } else if (simple_update(g.model, y, p, o.dt)) {
+            part[tid].push_back({node, 1.0});
           }
         }
       }
@@ -543,17 +620,8 @@ static void step(Oracle &o, int it_in_session) {
           end = (x >= x1 - h_min);
           if (external_update(g.model, y, p, end, o.dt)) push(o, node, 1.0, T);
         }
-      } else if (g.model == O_IAF_PSC_EXP) {
-        real &I_ex = y[0], &I_in = y[1], &V = y[2], &refr = y[3];
-        if (refr > 0) refr -= 1;
-        else V = V * p[15] + I_ex * p[13] + I_in * p[14] + p[3] * p[10];
-        I_ex *= p[11];
-        I_in *= p[12];
-        if (V >= p[4]) {
-          push(o, node, 1.0, T);
-          V = p[5];
-          refr = round(p[8] / o.dt);
-        }
+      } else if (simple_model(g.model)) {
+        if (simple_update(g.model, y, p, o.dt)) push(o, node, 1.0, T);
       } else if (g.model == O_SPIKE_GENERATOR) {
         int b = g.sg_next[i];
         if (b < g.sg_off[i + 1] && (long long)g.sg_step[b] == T - 1) {

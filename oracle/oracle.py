@@ -16,7 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "lib", "libngpu_oracle.so")
 
 AEIF_COND_BETA, AEIF_COND_ALPHA, AEIF_PSC_ALPHA, AEIF_PSC_EXP, AEIF_PSC_DELTA, \
-    IZH_COND_BETA, IAF_PSC_EXP, SPIKE_GENERATOR, PARROT, POISSON_GENERATOR = range(10)
+    IZH_COND_BETA, IAF_PSC_EXP, SPIKE_GENERATOR, PARROT, POISSON_GENERATOR, \
+    IAF_PSC_EXP_G, IZHIKEVICH, IZH_PSC_EXP = range(13)
 
 _AEIF_SCAL = ["V_th", "Delta_T", "g_L", "E_L", "C_m", "a", "b", "tau_w", "I_e",
               "V_peak", "V_reset", "t_ref", "refractory_step", "den_delay"]
@@ -51,6 +52,18 @@ MODELS = {
              ["hold_spike_height", "den_delay"], [0.0, 0.0], [], []),
     POISSON_GENERATOR: ([], [], [], [], ["rate", "origin", "start", "stop"],
                         [0.0, 0.0, 0.0, 1.0e30], [], []),
+    # group parameters of the library are per-neuron parameters here;
+    # h_prop = 0.1 reproduces iaf_psc_exp_hc (constants fixed at dt 0.1 ms)
+    IAF_PSC_EXP_G: (["I_syn", "V_m_rel", "refractory_step"], [0.0] * 3, [], [],
+                    ["I_e", "tau_m", "C_m", "E_L", "Theta_rel", "V_reset_rel", "tau_syn",
+                     "t_ref", "h_prop"],
+                    [0.0, 10.0, 250.0, -65.0, 15.0, 0.0, 0.5, 2.0, 0.0], [], []),
+    IZHIKEVICH: (["I_syn", "V_m", "u", "refractory_step"], [0.0, -70.0, -14.0, 0.0], [], [],
+                 ["I_e", "den_delay", "V_th", "a", "b", "c", "d", "t_ref"],
+                 [0.0, 0.0, 30.0, 0.02, 0.2, -65.0, 8.0, 0.0], [], []),
+    IZH_PSC_EXP: (["I_syn", "V_m", "u", "refractory_step"], [0.0, -70.0, -14.0, 0.0], [], [],
+                  ["I_e", "den_delay", "V_th", "a", "b", "c", "d", "tau_syn", "t_ref", "n_sub"],
+                  [0.0, 0.0, 30.0, 0.02, 0.2, -65.0, 8.0, 0.5, 0.0, 1.0], [], []),
 }
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -176,7 +189,7 @@ class Network(object):
                h0_rel=1e-2, eps=1e-6):
         """params / vars: dict name -> scalar, per-port list, or per-neuron array."""
         sv, svd, pv, pvd, sp, spd, pp, ppd = MODELS[model]
-        if model == AEIF_PSC_DELTA:
+        if model in (AEIF_PSC_DELTA, IAF_PSC_EXP_G, IZHIKEVICH, IZH_PSC_EXP):
             n_port = 1
         nvar = len(sv) + len(pv) * n_port
         nparam = len(sp) + len(pp) * n_port

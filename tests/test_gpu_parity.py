@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("name", sorted(netdefs.SINGLE))
 def test_single_neuron_trace(ngpu, name):
     t, v = netdefs.run_single_api(ngpu, name)
-    assert len(v) == 8001
+    assert len(v) == netdefs.n_samples(name)
     rmse = netdefs.nest_rmse(v, name)
     assert rmse <= netdefs.SINGLE[name]["tol"], (name, rmse)
     t_o, v_o, _ = netdefs.run_single_oracle(name)
@@ -350,3 +350,59 @@ def test_poisson_generator_nodes_statistics(ngpu):
     sigma = np.sqrt(p * (1.0 - p) / (n * steps))
     assert abs(mean - p) < 5.0 * sigma, (mean, p, sigma)
     assert counts.std() > 0
+
+
+# model -> (oracle model, extra oracle params, API params, weights of the
+# excitatory / inhibitory spike trains)
+_SIMPLE = {
+    "iaf_psc_exp_g": ("IAF_PSC_EXP_G", {}, {"I_e": 400.0, "tau_syn": 2.0, "t_ref": 1.0},
+                      (60.0, -80.0)),
+    "iaf_psc_exp_hc": ("IAF_PSC_EXP_G", {"h_prop": 0.1}, {"I_e": 400.0}, (60.0, -80.0)),
+    "izhikevich": ("IZHIKEVICH", {}, {"I_e": 10.0, "t_ref": 0.5}, (3.0, -2.0)),
+    "izhikevich_psc_exp": ("IZH_PSC_EXP", {"n_sub": 1.0}, {"I_e": 10.0}, (40.0, -30.0)),
+    "izhikevich_psc_exp_2s": ("IZH_PSC_EXP", {"n_sub": 2.0, "tau_syn": 2.0}, {"I_e": 10.0},
+                              (10.0, -8.0)),
+    "izhikevich_psc_exp_5s": ("IZH_PSC_EXP", {"n_sub": 5.0, "tau_syn": 2.0},
+                              {"I_e": 10.0, "d": 6.0}, (10.0, -8.0)),
+}
+
+
+@pytest.mark.parametrize("model", sorted(_SIMPLE))
+def test_simple_models_vs_oracle(ngpu, model):
+    """iaf_psc_exp_g / _hc (src/iaf_psc_exp_g.cu:39-66) and the Euler
+    Izhikevich family (src/izhikevich.cu:38-72,
+    src/izhikevich_psc_exp_2s.cu:41-83), tonically firing under a bias
+    current with excitatory and inhibitory spike trains on their one port,
+    300 ms against the FP64 oracle: every spike within one step and the
+    membrane trace up to the first spike (1e-4 relative). Group parameters
+    are set through SetStatus where the case lists them."""
+    from oracle import oracle as orc
+    omodel, oextra, params, (w_ex, w_in) = _SIMPLE[model]
+    var = "V_m_rel" if model.startswith("iaf") else "V_m"
+    times = [10.0, 40.0, 70.0, 100.5, 160.0, 220.0]
+    n = ngpu.Create(model, 1)
+    ngpu.SetStatus(n, params)
+    sg = ngpu.Create("spike_generator", 2)
+    ngpu.SetStatus([sg[0]], {"spike_times": times})
+    ngpu.SetStatus([sg[1]], {"spike_times": [t + 25.0 for t in times]})
+    ngpu.Connect([sg[0]], n, {"rule": "all_to_all"}, {"weight": w_ex, "delay": 1.0})
+    ngpu.Connect([sg[1]], n, {"rule": "all_to_all"}, {"weight": w_in, "delay": 1.0})
+    ngpu.ActivateRecSpikeTimes(n, 500)
+    rec = ngpu.CreateRecord("", [var], [n[0]], [0])
+    ngpu.Simulate(300.0)
+    v = np.asarray(ngpu.GetRecordData(rec))[1:, 1]
+    net = orc.Network(dt=0.1)
+    op = {k: np.float32(x) for k, x in dict(params, **oextra).items()}
+    on = net.create(getattr(orc, omodel), 1, 1, params=op)
+    og = net.create(orc.SPIKE_GENERATOR, 2)
+    net.set_spikes(og, [times, [t + 25.0 for t in times]])
+    net.connect([og.i0], [on.i0], 0, w_ex, 1.0)
+    net.connect([og.i0 + 1], [on.i0], 0, w_in, 1.0)
+    ov = net.simulate(3000, record=[(on.i0, on.var_index(var))])[:, 0]
+    steps, nodes = net.spikes()
+    steps = steps[nodes == on.i0]
+    g_spk = np.rint(np.asarray(ngpu.GetRecSpikeTimes(n[0])) / 0.1).astype(int)
+    assert len(steps) >= 3 and len(g_spk) == len(steps), (len(steps), len(g_spk))
+    assert np.max(np.abs(g_spk - (steps + 1))) <= 1
+    first = int(steps.min())
+    assert np.max(np.abs(v[:first] - ov[:first])) / max(1.0, np.max(np.abs(ov))) < 1e-4

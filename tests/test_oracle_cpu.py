@@ -17,7 +17,7 @@ from oracle import oracle as orc
 @pytest.mark.parametrize("name", sorted(netdefs.SINGLE))
 def test_oracle_matches_nest_golden_trace(name):
     t, v, _ = netdefs.run_single_oracle(name)
-    assert len(v) == 8001
+    assert len(v) == netdefs.n_samples(name)
     rmse = netdefs.nest_rmse(v, name)
     assert rmse <= netdefs.SINGLE[name]["tol"], (name, rmse)
 
