@@ -4,6 +4,7 @@
 // The variable/parameter names, their order and their defaults follow the
 // reference models so that scripts that address them by name keep working:
 //   aeif_cond_beta     src/aeif_cond_beta_kernel.h:30-100, src/aeif_cond_beta.cu:25-87
+//                      (also user_m1, user_m2: src/user_m1_kernel.h, src/user_m2_kernel.h)
 //   aeif_cond_alpha    src/aeif_cond_alpha_kernel.h, src/aeif_cond_alpha.cu:25-70
 //   aeif_psc_alpha     src/aeif_psc_alpha_kernel.h, src/aeif_psc_alpha.cu:25-70
 //   aeif_psc_exp       src/aeif_psc_exp_kernel.h, src/aeif_psc_exp.cu:25-60
@@ -97,6 +98,15 @@ inline const std::vector<ModelInfo> &ModelCatalogue() {
     m.in_var = 2 + 1; m.in_step = 2; m.w_param = true; m.w_param_idx = 3;
     m.refr_param = 12; m.den_delay_param = 13;
     cat.push_back(m);
+    // user_m1 / user_m2: the reference ships these user-model templates as
+    // renamed copies of aeif_cond_beta (src/user_m1_kernel.h,
+    // src/user_m2_kernel.h and their .cu files differ from
+    // src/aeif_cond_beta_kernel.h / .cu only in the names)
+    for (const char *alias : {"user_m1", "user_m2"}) {
+      ModelInfo u = m;
+      u.name = alias;
+      cat.push_back(u);
+    }
   }
   {
     ModelInfo m;
