@@ -62,6 +62,10 @@ SINGLE = {
         n_port=1, var="V_m", tol=5e-3, params={}, golden="izh",
         spikes=[10.0, 40.0], sim=80.0, conns=[(0, 1.0, 1.0), (0, -2.0, 10.0)]),
 }
+# user_m1: the reference's user-model template, shipped as a copy of
+# aeif_cond_beta (src/user_m1_kernel.h)
+SINGLE["user_m1"] = dict(SINGLE["aeif_cond_beta"], golden="aeif_cond_beta",
+                         oracle="aeif_cond_beta")
 SPIKE_TIMES = [10.0, 400.0]
 SIM_TIME = 800.0
 
