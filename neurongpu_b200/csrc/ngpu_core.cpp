@@ -78,7 +78,9 @@ void NeuronGPU::FreeDevice() {
     if (g->step_mode == STEP_LOG) g->step_mode = STEP_PLAIN;
     g->d_var = g->d_param = g->d_h = g->d_dx = nullptr;
   }
-  F(d_ctx_); F(d_acc_); F(d_ring_src_); F(d_ring_h_); F(d_ring_cnt_);
+  F(d_ctx_); F(d_ctxs_); F(d_acc_);
+  d_ctxs_ = nullptr;
+  n_ctxs_ = 0; F(d_ring_src_); F(d_ring_h_); F(d_ring_cnt_);
   F(d_last_spike_T_); F(d_last_rev_T_); F(d_last_post_T_); F(d_last_spike_h_);
   FreeRaw();
   F(d_grp_off_); F(d_e_slot_); F(d_e_w_); F(d_e_syn_); F(d_e_stamp_); F(d_c_port_);
@@ -1080,6 +1082,7 @@ DeliverArgs NeuronGPU::MakeDeliverArgs() {
   d.rev_edge = d_rev_edge_;
   d.dt = time_resolution_;
   d.blk_events = d_blk_events_;
+  d.step_book = 1;
   d.advance_flags = 0;
   d.ring_cnt_w = d_ring_cnt_;
   d.done = d_done_;
@@ -1280,7 +1283,9 @@ void NeuronGPU::BuildDevice() {
   // spike ring
   int maxD = 1;
   for (int d : delays_) maxD = std::max(maxD, d);
-  ring_R_ = maxD + 1;
+  // max delay + 2 slots: the slot of step T + 1 is emptied during step T
+  // while the delivery reads the slots of steps T - 1 ... T - max delay
+  ring_R_ = maxD + 2;
   ring_C_ = (int)std::min<long long>(0x7fffffffLL,
                                      (long long)ceil((double)N * std::max(1.0f, max_spike_num_fact_)) + 64);
   NGPU_CUDA(cudaMalloc(&d_ring_src_, sizeof(unsigned) * (size_t)ring_R_ * ring_C_));
@@ -1575,6 +1580,17 @@ int NeuronGPU::GetKernelTiming(int kind, double *total_ms, long long *launches) 
 }
 
 // one time step on stream_ (kernel launches only, no host synchronisation)
+void NeuronGPU::EnsureCtxCopies(int n) {
+  if (n <= n_ctxs_) return;
+  const int want = std::max(n, graph_chunk_);
+  if (d_ctxs_) cudaFree(d_ctxs_);
+  d_ctxs_ = nullptr;
+  n_ctxs_ = 0;
+  NGPU_CUDA(cudaMalloc(&d_ctxs_, sizeof(StepCtx) * want));
+  n_ctxs_ = want;
+  InvalidateGraphs();           // captured graphs hold the old copies
+}
+
 void NeuronGPU::EnsureForkResources() {
   if (dstream_ != nullptr) return;
   const char *env = getenv("NGB200_FORK_DELIVERY");
@@ -1592,19 +1608,21 @@ void NeuronGPU::EnsureForkResources() {
 }
 
 void NeuronGPU::EnqueueStep(int step_in_chunk) {
+  // this step's copy of the step context (k_step_prologue)
+  StepCtx *ctx = d_ctxs_ + step_in_chunk;
   DeliverArgs d = MakeDeliverArgs();
   const bool has_delivery = d.nd > 0;
   // The delivery of step T reads the spikes of steps before T and adds into
   // the accumulator half that the update of T + 1 folds, while the updates
   // of step T fold the other half: without plastic synapses the two touch
   // disjoint data, so the delivery runs on its own stream beside the node
-  // updates and the step bookkeeping joins them.
+  // updates, and the next step (or the chunk's epilogue) waits for both.
   const bool fork = has_delivery && !plastic_ && !ktime_ && dstream_ != nullptr;
   if (fork) {
     NGPU_CUDA(cudaEventRecord(ev_fork_, stream_));
     NGPU_CUDA(cudaStreamWaitEvent(dstream_, ev_fork_, 0));
     d.advance_flags = 0;
-    LaunchDeliver(d, syn_table_, d_ctx_, deliver_blocks_, dstream_);
+    LaunchDeliver(d, syn_table_, ctx, deliver_blocks_, dstream_);
     NGPU_CUDA(cudaEventRecord(ev_join_, dstream_));
   }
   if (ktime_) KEvent(step_in_chunk, 0);
@@ -1615,34 +1633,34 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
         if (g->batch >= 0) {
           // the whole batch is launched once, at its first group
           const Rk5BatchHost &b = batches_[g->batch];
-          if (b.groups[0] == g) LaunchRk5Batch(MakeRk5Batch(b), d_ctx_, stream_);
+          if (b.groups[0] == g) LaunchRk5Batch(MakeRk5Batch(b), ctx, stream_);
         } else {
           LaunchRk5Update(mi->rk5_model, g->n_port, MakeGroupArgs(g), MakeInputArgs(g),
-                          MakePushArgs(g), d_ctx_, stream_);
+                          MakePushArgs(g), ctx, stream_);
         }
         break;
       case MK_IAF_PSC_EXP:
-        LaunchIafPscExpUpdate(MakeGroupArgs(g), MakeInputArgs(g), MakePushArgs(g), d_ctx_, stream_);
+        LaunchIafPscExpUpdate(MakeGroupArgs(g), MakeInputArgs(g), MakePushArgs(g), ctx, stream_);
         break;
       case MK_IAF_PSC_EXP_G:
       case MK_IZHIKEVICH:
       case MK_IZH_PSC_EXP:
         LaunchSimpleNeuronUpdate(mi->kind, mi->n_sub, MakeGroupArgs(g), MakeInputArgs(g),
-                                 MakePushArgs(g), d_ctx_, stream_);
+                                 MakePushArgs(g), ctx, stream_);
         break;
       case MK_SPIKE_GENERATOR:
-        if (g->d_sg_off) LaunchSpikeGeneratorUpdate(MakeGroupArgs(g), MakePushArgs(g), d_ctx_, stream_);
+        if (g->d_sg_off) LaunchSpikeGeneratorUpdate(MakeGroupArgs(g), MakePushArgs(g), ctx, stream_);
         break;
       case MK_PARROT:
-        LaunchParrotUpdate(MakeGroupArgs(g), MakeInputArgs(g), MakePushArgs(g), d_ctx_, stream_);
+        LaunchParrotUpdate(MakeGroupArgs(g), MakeInputArgs(g), MakePushArgs(g), ctx, stream_);
         break;
       case MK_SPIKE_DETECTOR:
-        LaunchSpikeDetectorUpdate(MakeGroupArgs(g), MakeInputArgs(g), d_ctx_, stream_);
+        LaunchSpikeDetectorUpdate(MakeGroupArgs(g), MakeInputArgs(g), ctx, stream_);
         break;
       case MK_POISSON_NODES: {
         double lam = (double)g->poisson_lambda;
         LaunchPoissonNodesUpdate(MakeGroupArgs(g), MakePushArgs(g), lam, exp(-lam), kernel_seed_,
-                                 d_ctx_, stream_);
+                                 ctx, stream_);
         break;
       }
       default:
@@ -1651,34 +1669,31 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
   }
   // multimeter columns: state after the update, before this step's input is
   // delivered (the reference records between the two, src/neurongpu.cu:488)
-  int flags = 1;
   if (n_rec_cols_ > 0) {
     LaunchRecord(d_rec_cols_, n_rec_cols_, d_rec_buf_, rec_cap_rows_, d_last_spike_T_,
-                 d_last_spike_h_, 0, time_resolution_, d_ctx_, stream_);
-    flags |= 2;
+                 d_last_spike_h_, 0, time_resolution_, ctx, stream_);
   }
   if (ktime_) KEvent(step_in_chunk, 1);
   if (fork) {
     NGPU_CUDA(cudaStreamWaitEvent(stream_, ev_join_, 0));
-    LaunchAdvance(d_ring_cnt_, ring_R_, ring_C_, flags, d_ctx_, stream_);
     return;
   }
-  // the step's last kernel also does the step bookkeeping (finish_step)
-  if (has_delivery && !plastic_) d.advance_flags = flags;
-  if (plastic_ && rev_R_ > 1) LaunchRevArrive(d, d_ctx_, stream_);
-  LaunchDeliver(d, syn_table_, d_ctx_, deliver_blocks_, stream_);
+  if (plastic_ && rev_R_ > 1) LaunchRevArrive(d, ctx, stream_);
+  LaunchDeliver(d, syn_table_, ctx, deliver_blocks_, stream_);
   if (ktime_) KEvent(step_in_chunk, 2);
   if (plastic_) {
-    d.advance_flags = flags;
-    LaunchStdpPost(d, syn_table_, d_ctx_, 148 * 2, stream_);
+    d.advance_flags = 1;        // the post rule's last block empties the dendritic slot
+    LaunchStdpPost(d, syn_table_, ctx, 148 * 2, stream_);
   }
   if (ktime_) KEvent(step_in_chunk, 3);
-  if (!has_delivery && !plastic_) LaunchAdvance(d_ring_cnt_, ring_R_, ring_C_, flags, d_ctx_, stream_);
+  if (!has_delivery) LaunchAdvance(d_ring_cnt_, ring_R_, ring_C_, 1, ctx, stream_);
   if (ktime_) KEvent(step_in_chunk, 4);
 }
 
 void NeuronGPU::LaunchSteps(int n_steps) {
   if (n_steps <= 0) return;
+  EnsureForkResources();
+  EnsureCtxCopies(n_steps);
   if (batch_tables_dirty_) RefreshRk5BatchTables();
   if (n_rec_cols_ > 0 && rec_rows_used_ + n_steps > rec_cap_rows_) FlushRecords();
   if (ktime_) {
@@ -1691,9 +1706,11 @@ void NeuronGPU::LaunchSteps(int n_steps) {
       }
     }
   }
-  EnsureForkResources();
+  const int rec = n_rec_cols_ > 0 ? 1 : 0;
   if (!use_graphs_) {
+    LaunchStepPrologue(d_ctx_, d_ctxs_, n_steps, rec, stream_);
     for (int k = 0; k < n_steps; k++) EnqueueStep(k);
+    LaunchStepEpilogue(d_ctx_, d_ctxs_, n_steps, rec, stream_);
   } else {
     auto it = graphs_.find(n_steps);
     if (it == graphs_.end()) {
@@ -1701,7 +1718,9 @@ void NeuronGPU::LaunchSteps(int n_steps) {
       NGPU_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
       capturing_ = true;
       try {
+        LaunchStepPrologue(d_ctx_, d_ctxs_, n_steps, rec, stream_);
         for (int k = 0; k < n_steps; k++) EnqueueStep(k);
+        LaunchStepEpilogue(d_ctx_, d_ctxs_, n_steps, rec, stream_);
       } catch (...) {
         capturing_ = false;
         cudaStreamEndCapture(stream_, &graph);
@@ -2204,7 +2223,17 @@ unsigned long long NeuronGPU::TotalSpikes() {
   if (!d_ctx_) return 0;
   StepCtx c;
   NGPU_CUDA(cudaMemcpy(&c, d_ctx_, sizeof(StepCtx), cudaMemcpyDeviceToHost));
-  return c.n_spikes;
+  // the spikes of the last step are counted by the next step's bookkeeping
+  // (the delivery of step T counts step T - 1): add that ring slot here
+  unsigned long long n = c.n_spikes;
+  if (d_ring_cnt_ != nullptr && ring_R_ > 0) {
+    const long long T_last = c.T0 + c.it;
+    int cnt = 0;
+    NGPU_CUDA(cudaMemcpy(&cnt, d_ring_cnt_ + (int)(T_last % ring_R_), sizeof(int),
+                         cudaMemcpyDeviceToHost));
+    n += (unsigned long long)std::min(cnt, ring_C_);
+  }
+  return n;
 }
 
 }  // namespace ngpu

@@ -431,6 +431,10 @@ class NeuronGPU {
   cudaStream_t dstream_ = nullptr;
   cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
   void EnsureForkResources();
+  // per-step copies of the step context for a chunk of steps
+  StepCtx *d_ctxs_ = nullptr;
+  int n_ctxs_ = 0;
+  void EnsureCtxCopies(int n);
   StepCtx *d_ctx_ = nullptr;
   long long *d_acc_ = nullptr;
   long long n_acc_ = 0;

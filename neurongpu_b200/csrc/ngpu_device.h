@@ -232,8 +232,12 @@ struct DeliverArgs {
   const unsigned *rev_edge;
   float dt;
   unsigned long long *blk_events;      // per-block delivered events
-  // step bookkeeping done by the last block of the step's last kernel:
-  // bit 0 advance the step, bit 1 advance the recording row
+  // step bookkeeping at the start of the delivery (block 0): count the
+  // spikes of step T - 1 and empty the ring slot of step T + 1 (the
+  // simulator sets it; the ring then has max delay + 2 slots)
+  int step_book;
+  // bit 0: the last block clears the dendritic-delay slot of this step
+  // (plastic networks, the step's last kernel)
   int advance_flags;
   int *ring_cnt_w;
   unsigned *done;                      // blocks finished (reset by the last)

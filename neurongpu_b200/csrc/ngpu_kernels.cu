@@ -562,10 +562,11 @@ __device__ __forceinline__ float syn_update(const SynGroupTable &syn, int sg,
   return w;
 }
 
-// Step bookkeeping fused into the step's last kernel: the last block to
-// finish counts the step's spikes, clears the next ring slot and advances the
-// step (and recording row). Every other block has read the step index and
-// finished by then, so nothing reads the context while it changes.
+// End-of-step work of plastic networks, fused into the step's last kernel:
+// the last block to finish empties this step's dendritic-delay slot, which
+// every block of the post rule has read by then. (The step index itself
+// never changes during a chunk of steps: each step reads its own copy of the
+// step context, see k_step_prologue.)
 __device__ __forceinline__ void finish_step(const DeliverArgs &d, StepCtx *ctx) {
   if (d.advance_flags == 0) return;
   __syncthreads();
@@ -574,20 +575,27 @@ __device__ __forceinline__ void finish_step(const DeliverArgs &d, StepCtx *ctx) 
     unsigned prev = atomicAdd(d.done, 1u);
     if (prev == gridDim.x - 1) {
       __threadfence();
-      if (d.advance_flags & 1) {
+      if ((d.advance_flags & 1) && d.rev_cnt != nullptr) {
         const long long T = ctx->T0 + ctx->it + 1;
-        if (d.rev_cnt != nullptr) d.rev_cnt[(int)(T % d.rev_R)] = 0;
-        int c = d.ring_cnt_w[(int)(T % d.ring_R)];
-        ctx->n_spikes += (unsigned long long)(c < d.ring_C ? c : d.ring_C);
-        d.ring_cnt_w[(int)((T + 1) % d.ring_R)] = 0;
-        ctx->it += 1;
-        ctx->poisson_pending = 1;
+        d.rev_cnt[(int)(T % d.rev_R)] = 0;
       }
-      if (d.advance_flags & 2) ctx->rec_row += 1;
       *d.done = 0u;
       __threadfence();
     }
   }
+}
+
+// Spike count of step T - 1 (complete: every kernel of that step has ended)
+// and the emptying of the ring slot that step T + 1 fills. Called once per
+// step, by the step's delivery or by k_advance; the slot of T + 1 is never
+// read in step T (deliveries read T - 1 ... T - max delay of a ring with
+// max delay + 2 slots).
+__device__ __forceinline__ void step_bookkeeping(int *ring_cnt, int ring_R, int ring_C,
+                                                 StepCtx *ctx) {
+  const long long T = ctx->T0 + ctx->it + 1;
+  const int c = ring_cnt[(int)((T - 1) % ring_R)];
+  ctx->n_spikes += (unsigned long long)(c < ring_C ? c : ring_C);
+  ring_cnt[(int)((T + 1) % ring_R)] = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -599,6 +607,8 @@ k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
   __shared__ int s_slot[NGPU_MAX_DELAYS];
   const long long T = ctx->T0 + ctx->it + 1;
   long long *const acc = d.acc + ((T & 1) ? d.acc_par : 0);   // folded by the update of T + 1
+  if (d.step_book && blockIdx.x == 0 && threadIdx.x == 0)
+    step_bookkeeping(d.ring_cnt_w, d.ring_R, d.ring_C, ctx);
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int n_warps = (gridDim.x * blockDim.x) >> 5;
@@ -848,17 +858,63 @@ void LaunchRecord(const RecCol *cols, int n_cols, float *buf, long long cap_rows
                               last_spike_h, initial, dt, ctx);
 }
 
+// bit 0: the step bookkeeping of a network without delivery (see
+// step_bookkeeping); bit 1: advance the recording row of the context
 __global__ void k_advance(int *ring_cnt, int ring_R, int ring_C, int flags,
                           StepCtx *ctx) {
-  if (flags & 1) {
-    const long long T = ctx->T0 + ctx->it + 1;
-    int c = ring_cnt[(int)(T % ring_R)];
-    ctx->n_spikes += (unsigned long long)(c < ring_C ? c : ring_C);
-    ring_cnt[(int)((T + 1) % ring_R)] = 0;
-    ctx->it += 1;
-    ctx->poisson_pending = 1;
-  }
+  if (flags & 1) step_bookkeeping(ring_cnt, ring_R, ring_C, ctx);
   if (flags & 2) ctx->rec_row += 1;
+}
+
+// Per-step copies of the step context for a chunk of n steps: step k of the
+// chunk reads copy k (its step index, recording row, pending Poisson draws),
+// so no kernel has to advance a shared context between the steps of a chunk
+// and each step needs no bookkeeping launch of its own.
+__global__ void k_step_prologue(const StepCtx *base, StepCtx *copies, int n, int rec) {
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    StepCtx c = *base;
+    c.it = base->it + k;
+    if (k > 0) c.poisson_pending = 1;
+    c.rec_row = base->rec_row + (rec ? k : 0);
+    c.err = 0u;
+    c.n_spikes = 0ull;
+    copies[k] = c;
+  }
+}
+
+// Folds the chunk's per-step contexts back into the base context: step
+// index, pending draws, recording row, error bits and spike count.
+__global__ void k_step_epilogue(StepCtx *base, const StepCtx *copies, int n, int rec) {
+  __shared__ unsigned long long s_sp[256];
+  __shared__ unsigned s_err[256];
+  unsigned long long sp = 0;
+  unsigned err = 0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    sp += copies[k].n_spikes;
+    err |= copies[k].err;
+  }
+  s_sp[threadIdx.x] = sp;
+  s_err[threadIdx.x] = err;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int j = 1; j < (int)blockDim.x; j++) {
+      sp += s_sp[j];
+      err |= s_err[j];
+    }
+    base->n_spikes += sp;
+    base->err |= err;
+    base->it += n;
+    if (n > 0) base->poisson_pending = 1;
+    if (rec) base->rec_row += n;
+  }
+}
+
+void LaunchStepPrologue(const StepCtx *base, StepCtx *copies, int n, int rec, cudaStream_t s) {
+  k_step_prologue<<<1, 256, 0, s>>>(base, copies, n, rec);
+}
+
+void LaunchStepEpilogue(StepCtx *base, const StepCtx *copies, int n, int rec, cudaStream_t s) {
+  k_step_epilogue<<<1, 256, 0, s>>>(base, copies, n, rec);
 }
 
 void LaunchAdvance(int *ring_cnt, int ring_R, int ring_C, int flags,

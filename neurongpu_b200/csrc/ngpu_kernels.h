@@ -77,6 +77,9 @@ void LaunchRecord(const RecCol *cols, int n_cols, float *buf, long long cap_rows
                   int initial, float dt, StepCtx *ctx, cudaStream_t s);
 void LaunchAdvance(int *ring_cnt, int ring_R, int ring_C, int flags,
                    StepCtx *ctx, cudaStream_t s);
+// per-step context copies of a chunk of n steps (before / after the steps)
+void LaunchStepPrologue(const StepCtx *base, StepCtx *copies, int n, int rec, cudaStream_t s);
+void LaunchStepEpilogue(StepCtx *base, const StepCtx *copies, int n, int rec, cudaStream_t s);
 
 // calibration
 void LaunchCalibrateRk5(int model, const GroupArgs &g, int np,
