@@ -1952,9 +1952,7 @@ void NeuronGPU::BuildRk5Batches() {
     }
     NGPU_CUDA(cudaMemcpy(b.d_blk_seg, map.data(), sizeof(int) * b.n_blocks,
                          cudaMemcpyHostToDevice));
-    long long n_total = 0;
-    for (NodeGroup *g : b.groups) n_total += g->n_node;
-    AllocRk5Queue(b.q, n_total, Rk5RecordFloats(b.model, b.np));
+    AllocRk5Queue(b.q, b.n_blocks, Rk5RecordFloats(b.model, b.np));
     batches_.push_back(b);
   }
   batch_tables_dirty_ = true;
@@ -2055,15 +2053,20 @@ void NeuronGPU::TuneRk5Batch(Rk5BatchHost &b) {
   InvalidateGraphs();
 }
 
-void NeuronGPU::AllocRk5Queue(Rk5Queue &q, long long cap, int stride) {
+void NeuronGPU::AllocRk5Queue(Rk5Queue &q, long long n_tiles, int stride) {
   FreeRk5Queue(q);
   const char *env = getenv("NGB200_RK5_QUEUE");
-  if ((env != nullptr && atoi(env) == 0) || cap <= 0 || stride <= 0) return;
-  if (cap > 0x7fffffffLL) cap = 0x7fffffffLL;
+  if ((env != nullptr && atoi(env) == 0) || n_tiles <= 0 || stride <= 0) return;
+  // sub-queue j takes the tiles j, j + NGPU_QLANES, ...: at most
+  // ceil(n_tiles / NGPU_QLANES) tiles of 128 neurons, each queued at most once
+  const long long sub_cap = (n_tiles + NGPU_QLANES - 1) / NGPU_QLANES * 128;
+  const long long cap = sub_cap * NGPU_QLANES;
+  if (cap > 0x7fffffffLL) return;
   NGPU_CUDA(cudaMalloc(&q.hdr, sizeof(Rk5QueueHdr)));
   NGPU_CUDA(cudaMemset(q.hdr, 0, sizeof(Rk5QueueHdr)));
   NGPU_CUDA(cudaMalloc(&q.rec, sizeof(float) * (size_t)cap * stride));
   q.cap = (int)cap;
+  q.sub_cap = (int)sub_cap;
   q.stride = stride;
   // finishing launch: up to three 128-thread blocks per SM (its kernel is
   // compiled for one block per SM's registers), never more blocks than the
@@ -2071,7 +2074,7 @@ void NeuronGPU::AllocRk5Queue(Rk5Queue &q, long long cap, int stride) {
   int dev = 0, n_sm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  q.fin_blocks = (int)std::min<long long>((cap + 127) / 128, 3LL * n_sm);
+  q.fin_blocks = (int)std::min<long long>(n_tiles, 3LL * n_sm);
 }
 
 void NeuronGPU::FreeRk5Queue(Rk5Queue &q) {
@@ -2114,7 +2117,7 @@ int NeuronGPU::StartSimulation() {
   if (!batches_built_) BuildRk5Batches();
   for (NodeGroup *g : groups_)
     if (g->mi->kind == MK_RK5 && g->batch < 0 && g->q.hdr == nullptr && g->n_node > 0)
-      AllocRk5Queue(g->q, g->n_node, Rk5RecordFloats(g->mi->rk5_model, g->n_port));
+      AllocRk5Queue(g->q, (g->n_node + 127) / 128, Rk5RecordFloats(g->mi->rk5_model, g->n_port));
   if (batch_tables_dirty_) RefreshRk5BatchTables();
   // a variant forced through NGB200_RK5_VARIANT applies from the first step
   if (steps_total_ >= kTuneSteps || getenv("NGB200_RK5_VARIANT") != nullptr) TuneAll();

@@ -382,9 +382,9 @@ class NeuronGPU {
   void TuneRk5Batch(Rk5BatchHost &b);
   Rk5Batch MakeRk5Batch(const Rk5BatchHost &b);
   void FreeRk5Batches();
-  // straggler queues: capacity cap records of stride floats (cap 0 when the
-  // queue is switched off with NGB200_RK5_QUEUE=0)
-  void AllocRk5Queue(Rk5Queue &q, long long cap, int stride);
+  // straggler queues for a launch of n_tiles 128-neuron tiles, records of
+  // stride floats (none when switched off with NGB200_RK5_QUEUE=0)
+  void AllocRk5Queue(Rk5Queue &q, long long n_tiles, int stride);
   static void FreeRk5Queue(Rk5Queue &q);
   std::vector<float> mlp_params_;       // FP32 proposer parameters (empty: none)
   MlpImage *d_mlp_img_ = nullptr;

@@ -143,15 +143,24 @@ enum StepMode { STEP_PLAIN = 0, STEP_LOG = 1, STEP_LEARNED = 2 };
 // one neuron per thread, so a warp never carries 31 idle lanes while one
 // neuron near a spike takes many short sub-steps. Resuming from a record
 // repeats exactly the arithmetic of the uninterrupted loop.
+// The records are split over NGPU_QLANES sub-queues by tile (128 neurons)
+// index, each with its own counter on its own 128-byte line: reservations of
+// different tiles then do not contend for one address.
+#define NGPU_QLANES 32
 struct Rk5QueueHdr {
-  unsigned tail;                // records reserved (may pass cap: those are not used)
+  struct Lane {
+    unsigned tail;              // records reserved in this sub-queue (may pass sub_cap)
+    unsigned pad_[31];
+  } lane[NGPU_QLANES];
   unsigned done;                // finishing blocks done (the last one resets the header)
+  unsigned pad_[31];
 };
 struct Rk5Queue {
   Rk5QueueHdr *hdr;
-  float *rec;                   // [cap][stride]: node, segment, sub-steps, h, refractory,
-                                // pad, time (double), state variables
-  int cap;                      // 0: queue off
+  float *rec;                   // [NGPU_QLANES][sub_cap][stride]: node, segment, sub-steps,
+                                // h, refractory, pad, time (double), state variables
+  int cap;                      // NGPU_QLANES * sub_cap; 0: queue off
+  int sub_cap;                  // records per sub-queue: 128 x its tiles
   int stride;                   // floats per record, a multiple of 4
   int fin_blocks;               // grid of the finishing launch
 };

@@ -351,20 +351,23 @@ __device__ __forceinline__ void rk5_store(const GroupArgs &g, int i, const float
   if (write_refr) g.param[(long long)Tr::refr * g.n_pad + i] = refr;
 }
 
-// Hands neuron i (segment seg of a batched launch) over to the straggler
-// queue; false if the queue has no room (the caller then carries on). One
-// reservation per group of converged threads.
+// Hands neuron i (segment seg of a batched launch, 128-neuron tile tile)
+// over to the straggler queue; false if the queue has no room (the caller
+// then carries on). One reservation per group of converged threads (a warp
+// lies within one tile, so the group shares the sub-queue).
 template <int NV>
-__device__ __forceinline__ bool rk5_enqueue(const Rk5Queue &qu, int seg, int i, const float *y,
-                                            double x, float h, float refr, int guard) {
+__device__ __forceinline__ bool rk5_enqueue(const Rk5Queue &qu, int seg, int tile, int i,
+                                            const float *y, double x, float h, float refr,
+                                            int guard) {
   if (8 + NV > qu.stride) return false;
+  const int lane_q = tile & (NGPU_QLANES - 1);
   cg::coalesced_group grp = cg::coalesced_threads();
   unsigned base = 0;
-  if (grp.thread_rank() == 0) base = atomicAdd(&qu.hdr->tail, grp.size());
+  if (grp.thread_rank() == 0) base = atomicAdd(&qu.hdr->lane[lane_q].tail, grp.size());
   base = grp.shfl(base, 0);
   const unsigned k = base + grp.thread_rank();
-  if (k >= (unsigned)qu.cap) return false;
-  float *r = qu.rec + (size_t)k * qu.stride;
+  if (k >= (unsigned)qu.sub_cap) return false;
+  float *r = qu.rec + ((size_t)lane_q * qu.sub_cap + k) * qu.stride;
   r[0] = __int_as_float(i);
   r[1] = __int_as_float(seg);
   r[2] = __int_as_float(guard);
@@ -413,10 +416,34 @@ __device__ __forceinline__ void rk5_resume(const GroupArgs &g, const PushArgs &p
   }
 }
 
-// records of the queue's last update launch
-__device__ __forceinline__ unsigned rk5_queue_count(const Rk5Queue &qu) {
-  const unsigned t = qu.hdr->tail;
-  return t < (unsigned)qu.cap ? t : (unsigned)qu.cap;
+// Records of the queue's last update launch: per-sub-queue counts and their
+// prefix in s_pref[0..NGPU_QLANES]; returns the total. Whole blocks call it.
+__device__ __forceinline__ unsigned rk5_queue_prefix(const Rk5Queue &qu, unsigned *s_pref) {
+  if (threadIdx.x < NGPU_QLANES) {
+    unsigned c = qu.hdr->lane[threadIdx.x].tail;
+    c = c < (unsigned)qu.sub_cap ? c : (unsigned)qu.sub_cap;
+    unsigned incl = c;
+#pragma unroll
+    for (int o = 1; o < NGPU_QLANES; o <<= 1) {
+      const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+      if ((int)threadIdx.x >= o) incl += v;
+    }
+    s_pref[threadIdx.x + 1] = incl;
+    if (threadIdx.x == 0) s_pref[0] = 0;
+  }
+  __syncthreads();
+  return s_pref[NGPU_QLANES];
+}
+
+// record number t (< the total) in sub-queue order
+__device__ __forceinline__ const float *rk5_queue_record(const Rk5Queue &qu,
+                                                         const unsigned *s_pref, unsigned t) {
+  int lo = 0, hi = NGPU_QLANES;       // the sub-queue with s_pref[lo] <= t < s_pref[lo + 1]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (s_pref[mid] <= t) lo = mid; else hi = mid;
+  }
+  return qu.rec + ((size_t)lo * qu.sub_cap + (t - s_pref[lo])) * qu.stride;
 }
 
 // The last block of a finishing launch empties the queue for the next
@@ -426,7 +453,7 @@ __device__ __forceinline__ void rk5_queue_reset(const Rk5Queue &qu) {
   if (threadIdx.x == 0) {
     const unsigned prev = atomicAdd(&qu.hdr->done, 1u);
     if (prev == gridDim.x - 1) {
-      qu.hdr->tail = 0u;
+      for (int j = 0; j < NGPU_QLANES; j++) qu.hdr->lane[j].tail = 0u;
       qu.hdr->done = 0u;
     }
   }
@@ -454,7 +481,7 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
                                            unsigned &evals, bool dry_run,
                                            ProposerSmem *ps, const Rk5Queue *qu = nullptr,
                                            int seg = 0, const float *pre_col = nullptr,
-                                           const long long *pre_acc = nullptr) {
+                                           const long long *pre_acc = nullptr, int tile = -1) {
   using Tr = ModelTraits<M>;
   const bool active = (MODE != STEP_LEARNED) || (i < g.n);
   const bool dry = g.dry || dry_run;
@@ -568,7 +595,9 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
       end_step = rk5_plain_substep<M, NP>(g, pa, ctx, i, y, x, h, refr, guard, p, q, np,
                                           inv_eps, x1, T, den, dry, evals);
       if (!end_step && guard == 1 && qu != nullptr) {
-        if (rk5_enqueue<M::NVAR>(*qu, seg, i, y, x, h, refr, guard)) return;
+        if (rk5_enqueue<M::NVAR>(*qu, seg, tile >= 0 ? tile : (i >> 7), i, y, x, h, refr,
+                                 guard))
+          return;
       }
     }
   }
@@ -707,11 +736,12 @@ template <class M, int NP, bool UNI>
 __global__ void __launch_bounds__(NGPU_BLOCK, 1)
 k_rk5_finish(const __grid_constant__ GroupArgs g, const __grid_constant__ InputArgs in,
              const __grid_constant__ PushArgs pa, StepCtx *ctx) {
-  const unsigned n = rk5_queue_count(g.q);
+  __shared__ unsigned s_pref[NGPU_QLANES + 1];
+  const unsigned n = rk5_queue_prefix(g.q, s_pref);
   if (n == 0) return;             // the same for every block: nothing to reset
   unsigned evals = 0;
   for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    rk5_resume<M, NP, UNI>(g, pa, ctx, g.puni, g.pinv, in.np, g.q.rec + (size_t)k * g.q.stride,
+    rk5_resume<M, NP, UNI>(g, pa, ctx, g.puni, g.pinv, in.np, rk5_queue_record(g.q, s_pref, k),
                            evals, g.dry != 0);
   }
   if (g.blk_evals != nullptr) block_add_u64(evals, g.blk_evals);
@@ -746,7 +776,7 @@ k_rk5_update_seg(const SegArgs *__restrict__ segs, const int *__restrict__ blk_s
     const bool queued = (MODE == STEP_PLAIN) && qu.cap > 0;
     if (i < S.g.n)
       rk5_neuron<M, NP, UNI, MODE>(S.g, S.in, S.pa, ctx, i, s_p, s_q, evals, dry != 0, nullptr,
-                                   queued ? &qu : nullptr, seg);
+                                   queued ? &qu : nullptr, seg, nullptr, nullptr, blockIdx.x);
   }
   if (blk_evals != nullptr) block_add_u64(evals, blk_evals);
 }
@@ -757,11 +787,12 @@ template <class M, int NP, bool UNI>
 __global__ void __launch_bounds__(NGPU_BLOCK, 1)
 k_rk5_finish_seg(const SegArgs *__restrict__ segs, unsigned long long *blk_evals, int dry,
                  StepCtx *ctx, const __grid_constant__ Rk5Queue qu) {
-  const unsigned n = rk5_queue_count(qu);
+  __shared__ unsigned s_pref[NGPU_QLANES + 1];
+  const unsigned n = rk5_queue_prefix(qu, s_pref);
   if (n == 0) return;             // the same for every block: nothing to reset
   unsigned evals = 0;
   for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    const float *r = qu.rec + (size_t)k * qu.stride;
+    const float *r = rk5_queue_record(qu, s_pref, k);
     const SegArgs &R = segs[__float_as_int(r[1])];
     rk5_resume<M, NP, UNI>(R.g, R.pa, ctx, R.g.puni, R.g.pinv, R.in.np, r, evals,
                            R.g.dry || dry != 0);
