@@ -222,3 +222,57 @@ def test_stdp_network_full_scale(ngpu):
     print("full-scale STDP: wall s", ngpu.LastSimulateSeconds(), "spikes", ngpu.TotalSpikes(),
           "mean w", w.mean(), "hist", np.round(hist, 4))
     assert ngpu.TotalSpikes() > 0
+
+
+def _chunk_run(ngpu, chunk, fork):
+    import os
+    old = os.environ.get("NGB200_FORK_DELIVERY")
+    if not fork:
+        os.environ["NGB200_FORK_DELIVERY"] = "0"
+    try:
+        b = ngpu.default_binding()
+        b.Reset()
+        b.SetVerbosityLevel(0)
+        ngpu.SetKernelStatus("rnd_seed", 99)
+        pg = ngpu.Create("poisson_generator")
+        ngpu.SetStatus(pg, "rate", 20000.0)
+        nrn = ngpu.Create("aeif_cond_beta", 2000, 2)
+        ngpu.SetStatus(nrn, {"E_rev": [0.0, -85.0], "tau_rise": [0.2, 0.5],
+                             "tau_decay": [2.0, 8.0]})
+        ngpu.Connect(pg, nrn, {"rule": "all_to_all"}, {"weight": 0.5, "delay": 0.1,
+                                                       "receptor": 0})
+        ngpu.Connect(nrn[0:1600], nrn, {"rule": "fixed_indegree", "indegree": 80},
+                     {"weight": 0.05, "delay": 1.5, "receptor": 0})
+        ngpu.Connect(nrn[1600:2000], nrn, {"rule": "fixed_indegree", "indegree": 20},
+                     {"weight": 0.35, "delay": 0.7, "receptor": 1})
+        ngpu.ActivateSpikeCount(nrn)
+        b.SetGraphChunk(chunk)
+        totals = []
+        for t in (33.3, 50.0, 16.7):
+            ngpu.Simulate(t)
+            totals.append(b.TotalSpikes())
+        counts = ngpu.GetNeuronIntVarArray(nrn.i0, nrn.n, "spike_count")
+        v = np.asarray(ngpu.GetNeuronVar(nrn.i0, nrn.n, "V_m"), dtype=np.float32).ravel()
+        return totals, counts, v
+    finally:
+        if old is None:
+            os.environ.pop("NGB200_FORK_DELIVERY", None)
+        else:
+            os.environ["NGB200_FORK_DELIVERY"] = old
+
+
+def test_step_chunks_and_spike_totals(ngpu):
+    """Each step of a captured chunk reads its own copy of the step context
+    and the delivery does the step bookkeeping: graphs of 100, 7 and 1 steps,
+    no graph at all, and the serial (unforked) delivery give bit-identical
+    state, and the running spike total equals the sum of the per-neuron spike
+    counts after every Simulate call."""
+    ref = _chunk_run(ngpu, 100, True)
+    assert ref[1].sum() > 100
+    assert ref[0][-1] == int(ref[1].sum())
+    assert ref[0][0] < ref[0][1] < ref[0][2]
+    for chunk, fork in ((7, True), (1, True), (0, True), (100, False)):
+        totals, counts, v = _chunk_run(ngpu, chunk, fork)
+        assert totals == ref[0], (chunk, fork)
+        assert np.array_equal(counts, ref[1]), (chunk, fork)
+        assert np.array_equal(v.view(np.int32), ref[2].view(np.int32)), (chunk, fork)
