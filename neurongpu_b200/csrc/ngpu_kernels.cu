@@ -74,24 +74,24 @@ static void launch_rk5(const GroupArgs &g, const InputArgs &in, const PushArgs &
       const int variant = (g.variant >= 4 && !tiles_aligned(g, in)) ? 1 : g.variant;
       const int n_tiles = (int)grid.x;
       switch (variant) {
-        case 1: k_rk5_update<M, NP, true, 5, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
-        case 2: k_rk5_update<M, NP, true, 6, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
-        case 3: k_rk5_update<M, NP, true, 8, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+        case 1: launch_pdl(k_rk5_update<M, NP, true, 5, STEP_PLAIN>, grid, block, s, g, in, pa, ctx); break;
+        case 2: launch_pdl(k_rk5_update<M, NP, true, 6, STEP_PLAIN>, grid, block, s, g, in, pa, ctx); break;
+        case 3: launch_pdl(k_rk5_update<M, NP, true, 8, STEP_PLAIN>, grid, block, s, g, in, pa, ctx); break;
         case 4:
-          k_rk5_update_tiles<M, NP, 5><<<tile_grid<M, NP, 5>(n_tiles), block, 0, s>>>(g, in, pa, ctx);
+          launch_pdl(k_rk5_update_tiles<M, NP, 5>, dim3(tile_grid<M, NP, 5>(n_tiles)), block, s, g, in, pa, ctx);
           break;
         case 5:
-          k_rk5_update_tiles<M, NP, 6><<<tile_grid<M, NP, 6>(n_tiles), block, 0, s>>>(g, in, pa, ctx);
+          launch_pdl(k_rk5_update_tiles<M, NP, 6>, dim3(tile_grid<M, NP, 6>(n_tiles)), block, s, g, in, pa, ctx);
           break;
-        default: k_rk5_update<M, NP, true, 1, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx); break;
+        default: launch_pdl(k_rk5_update<M, NP, true, 1, STEP_PLAIN>, grid, block, s, g, in, pa, ctx); break;
       }
     } else {
-      k_rk5_update<M, NP, true, 1, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx);
+      launch_pdl(k_rk5_update<M, NP, true, 1, STEP_PLAIN>, grid, block, s, g, in, pa, ctx);
     }
-    if (g.q.cap > 0) k_rk5_finish<M, NP, true><<<g.q.fin_blocks, block, 0, s>>>(g, in, pa, ctx);
+    if (g.q.cap > 0) launch_pdl(k_rk5_finish<M, NP, true>, dim3(g.q.fin_blocks), block, s, g, in, pa, ctx);
   } else {
-    k_rk5_update<M, NP, false, 1, STEP_PLAIN><<<grid, block, 0, s>>>(g, in, pa, ctx);
-    if (g.q.cap > 0) k_rk5_finish<M, NP, false><<<g.q.fin_blocks, block, 0, s>>>(g, in, pa, ctx);
+    launch_pdl(k_rk5_update<M, NP, false, 1, STEP_PLAIN>, grid, block, s, g, in, pa, ctx);
+    if (g.q.cap > 0) launch_pdl(k_rk5_finish<M, NP, false>, dim3(g.q.fin_blocks), block, s, g, in, pa, ctx);
   }
 }
 

@@ -19,6 +19,50 @@ namespace cg = cooperative_groups;
 
 #define NGPU_BLOCK 128
 
+// Programmatic dependent launch (sm_90+): the RK5 update and its finishing
+// launch are issued with programmatic stream serialization, so the next
+// kernel's blocks may be scheduled before this one has finished. pdl_wait()
+// blocks until the preceding kernel has completed and its memory is
+// visible (a no-op for a kernel launched without the attribute); each block
+// calls pdl_trigger() once it has started, so the dependent kernel's blocks
+// can take the slots that this grid's last wave frees and wait there.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+inline bool PdlEnabled() {
+  static int on = -1;
+  if (on < 0) {
+    const char *e = getenv("NGB200_PDL");
+    on = (e != nullptr && atoi(e) == 0) ? 0 : 1;
+  }
+  return on == 1;
+}
+
+// k<<<grid, block, 0, s>>>(args...) with programmatic stream serialization
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t s,
+                       Args... args) {
+  if (!PdlEnabled()) {
+    k<<<grid, block, 0, s>>>(args...);
+    return;
+  }
+  cudaLaunchConfig_t cfg;
+  memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  memset(at, 0, sizeof(at));
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 __device__ __forceinline__ bool pbit(const unsigned *mask, int j) {
   return (mask[j >> 5] >> (j & 31)) & 1u;
 }
@@ -616,6 +660,8 @@ template <class M, int NP, bool UNI, int MINB, int MODE>
 __global__ void __launch_bounds__(NGPU_BLOCK, MINB)
 k_rk5_update(const __grid_constant__ GroupArgs g, const __grid_constant__ InputArgs in,
              const __grid_constant__ PushArgs pa, StepCtx *ctx) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned evals = 0;
   if constexpr (MODE == STEP_LEARNED) {
@@ -679,6 +725,8 @@ template <class M, int NP, int MINB>
 __global__ void __launch_bounds__(NGPU_BLOCK, MINB)
 k_rk5_update_tiles(const __grid_constant__ GroupArgs g, const __grid_constant__ InputArgs in,
                    const __grid_constant__ PushArgs pa, StepCtx *ctx) {
+  pdl_wait();
+  pdl_trigger();
   using St = Rk5TileStage<M, NP>;
   __shared__ alignas(128) St s_st[2];
   __shared__ alignas(8) uint64_t s_bar[2];
@@ -736,6 +784,8 @@ template <class M, int NP, bool UNI>
 __global__ void __launch_bounds__(NGPU_BLOCK, 1)
 k_rk5_finish(const __grid_constant__ GroupArgs g, const __grid_constant__ InputArgs in,
              const __grid_constant__ PushArgs pa, StepCtx *ctx) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ unsigned s_pref[NGPU_QLANES + 1];
   const unsigned n = rk5_queue_prefix(g.q, s_pref);
   if (n == 0) return;             // the same for every block: nothing to reset
@@ -757,6 +807,8 @@ __global__ void __launch_bounds__(NGPU_BLOCK, MINB)
 k_rk5_update_seg(const SegArgs *__restrict__ segs, const int *__restrict__ blk_seg,
                  unsigned long long *blk_evals, int dry, StepCtx *ctx,
                  const __grid_constant__ Rk5Queue qu) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ float s_p[M::NPARAM], s_q[M::NPARAM];
   const int seg = blk_seg[blockIdx.x];
   const SegArgs &S = segs[seg];
@@ -787,6 +839,8 @@ template <class M, int NP, bool UNI>
 __global__ void __launch_bounds__(NGPU_BLOCK, 1)
 k_rk5_finish_seg(const SegArgs *__restrict__ segs, unsigned long long *blk_evals, int dry,
                  StepCtx *ctx, const __grid_constant__ Rk5Queue qu) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ unsigned s_pref[NGPU_QLANES + 1];
   const unsigned n = rk5_queue_prefix(qu, s_pref);
   if (n == 0) return;             // the same for every block: nothing to reset

@@ -24,17 +24,17 @@ static void launch_rk5_seg(const Rk5Batch &b, StepCtx *ctx, cudaStream_t s) {
   if constexpr (NP <= 4) {
     if (b.uni) {
       switch (b.variant) {
-        case 1: k_rk5_update_seg<M, NP, true, 5, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q); break;
-        case 2: k_rk5_update_seg<M, NP, true, 6, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q); break;
-        case 3: k_rk5_update_seg<M, NP, true, 8, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q); break;
-        default: k_rk5_update_seg<M, NP, true, 1, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q); break;
+        case 1: launch_pdl(k_rk5_update_seg<M, NP, true, 5, STEP_PLAIN>, grid, block, s, b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q); break;
+        case 2: launch_pdl(k_rk5_update_seg<M, NP, true, 6, STEP_PLAIN>, grid, block, s, b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q); break;
+        case 3: launch_pdl(k_rk5_update_seg<M, NP, true, 8, STEP_PLAIN>, grid, block, s, b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q); break;
+        default: launch_pdl(k_rk5_update_seg<M, NP, true, 1, STEP_PLAIN>, grid, block, s, b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q); break;
       }
     } else {
-      k_rk5_update_seg<M, NP, false, 1, STEP_PLAIN><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q);
+      launch_pdl(k_rk5_update_seg<M, NP, false, 1, STEP_PLAIN>, grid, block, s, b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q);
     }
     if (b.q.cap > 0) {
-      if (b.uni) k_rk5_finish_seg<M, NP, true><<<b.q.fin_blocks, block, 0, s>>>(b.segs, b.blk_evals, b.dry, ctx, b.q);
-      else k_rk5_finish_seg<M, NP, false><<<b.q.fin_blocks, block, 0, s>>>(b.segs, b.blk_evals, b.dry, ctx, b.q);
+      if (b.uni) launch_pdl(k_rk5_finish_seg<M, NP, true>, dim3(b.q.fin_blocks), block, s, b.segs, b.blk_evals, b.dry, ctx, b.q);
+      else launch_pdl(k_rk5_finish_seg<M, NP, false>, dim3(b.q.fin_blocks), block, s, b.segs, b.blk_evals, b.dry, ctx, b.q);
     }
   }
 }
