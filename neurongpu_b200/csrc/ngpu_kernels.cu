@@ -537,6 +537,14 @@ void LaunchClearPending(StepCtx *ctx, cudaStream_t s) {
 // ---------------------------------------------------------------------------
 // synapse models (src/stdp.cu:24-51, src/test_syn_model.cu:24-30)
 // ---------------------------------------------------------------------------
+// x^mu; the exponents of additive (0) and multiplicative (1) STDP, the
+// common settings, need no pow (pow(x, 0) is 1 and pow(x, 1) is x exactly)
+__device__ __forceinline__ double pow_mu(double x, double mu) {
+  if (mu == 0.0) return 1.0;
+  if (mu == 1.0) return x;
+  return pow(x, mu);
+}
+
 __device__ __forceinline__ float syn_update(const SynGroupTable &syn, int sg,
                                             float w, float Dt) {
   int type = syn.type[sg - 1];
@@ -548,10 +556,10 @@ __device__ __forceinline__ float syn_update(const SynGroupTable &syn, int sg,
     double w0 = w, w1;
     if (Dt >= 0.0f) {
       double fact = lambda * exp(-(double)Dt / tau_plus);
-      w1 = w0 + fact * Wmax * pow(1.0 - w0 / Wmax, mu_plus);
+      w1 = w0 + fact * Wmax * pow_mu(1.0 - w0 / Wmax, mu_plus);
     } else {
       double fact = -alpha * lambda * exp((double)Dt / tau_minus);
-      w1 = w0 + fact * Wmax * pow(w0 / Wmax, mu_minus);
+      w1 = w0 + fact * Wmax * pow_mu(w0 / Wmax, mu_minus);
     }
     w1 = w1 > 0.0 ? w1 : 0.0;
     w1 = w1 < Wmax ? w1 : Wmax;
@@ -699,18 +707,41 @@ k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
         }
       }
     } else {
-      for (unsigned long long e = beg + lane; e < end; e += 32) {
-        const unsigned slot_t = d.e_slot[e];
-        const float w = d.e_w[e];
-        atomicAdd((unsigned long long *)(acc + slot_t),
-                  (unsigned long long)ng_to_fixed(height * w));
-        const int sg = d.e_syn[e];
-        if (sg > 0) {
-          // pre-spike rule with the last post spike (src/get_spike.cu:73-83)
-          d.e_stamp[e] = (int)T;
-          long long Dt_int = T - (long long)d.last_rev_T[d.e_post[e]];
-          if (Dt_int > 0 && Dt_int < NGPU_MAX_SYN_DT) {
-            d.e_w[e] = syn_update(syn, sg, w, -d.dt * (float)Dt_int);
+      // plastic network: four edges per lane in flight, then the
+      // post-synaptic last-spike gathers of all four, then the updates
+      for (unsigned long long e0 = beg + lane; e0 < end; e0 += 128) {
+        unsigned sl[4], post[4];
+        float wv[4];
+        int sgv[4], lr[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const unsigned long long e = e0 + 32 * u;
+          if (e < end) {
+            sl[u] = d.e_slot[e];
+            wv[u] = d.e_w[e];
+            sgv[u] = d.e_syn[e];
+            post[u] = sgv[u] > 0 ? d.e_post[e] : 0u;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const unsigned long long e = e0 + 32 * u;
+          if (e < end && sgv[u] > 0) lr[u] = d.last_rev_T[post[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const unsigned long long e = e0 + 32 * u;
+          if (e < end) {
+            atomicAdd((unsigned long long *)(acc + sl[u]),
+                      (unsigned long long)ng_to_fixed(height * wv[u]));
+            if (sgv[u] > 0) {
+              // pre-spike rule with the last post spike (src/get_spike.cu:73-83)
+              d.e_stamp[e] = (int)T;
+              const long long Dt_int = T - (long long)lr[u];
+              if (Dt_int > 0 && Dt_int < NGPU_MAX_SYN_DT) {
+                d.e_w[e] = syn_update(syn, sgv[u], wv[u], -d.dt * (float)Dt_int);
+              }
+            }
           }
         }
       }
@@ -752,19 +783,43 @@ void LaunchDeliver(const DeliverArgs &d, const SynGroupTable &syn,
 // every incoming plastic synapse with a pre-synaptic arrival stamp
 // 0 <= T - stamp < 16384 (src/rev_spike.cu:41-55); one warp per node,
 // a node is handled once per step.
+// One block per node, four incoming edges per thread in flight: the edge
+// indices, then the gathers of group, stamp and weight, then the updates.
 __device__ __forceinline__ void post_rule_node(const DeliverArgs &d, const SynGroupTable &syn,
-                                               unsigned node, long long T, int lane) {
-  int first = 0;
-  if (lane == 0) first = (atomicExch(&d.last_post_T[node], (int)T) != (int)T);
-  first = __shfl_sync(0xffffffffu, first, 0);
-  if (!first) return;
+                                               unsigned node, long long T) {
+  __shared__ int s_first;
+  __syncthreads();
+  if (threadIdx.x == 0) s_first = (atomicExch(&d.last_post_T[node], (int)T) != (int)T);
+  __syncthreads();
+  if (!s_first) return;
   const unsigned long long beg = d.rev_off[node], end = d.rev_off[node + 1];
-  for (unsigned long long r = beg + lane; r < end; r += 32) {
-    const unsigned e = d.rev_edge[r];
-    const int sg = d.e_syn[e];
-    long long Dt_int = T - (long long)d.e_stamp[e];
-    if (sg > 0 && Dt_int >= 0 && Dt_int < NGPU_MAX_SYN_DT) {
-      d.e_w[e] = syn_update(syn, sg, d.e_w[e], d.dt * (float)Dt_int);
+  const unsigned B = blockDim.x;
+  for (unsigned long long r0 = beg + threadIdx.x; r0 < end; r0 += 4ull * B) {
+    unsigned e[4];
+    int sg[4], st[4];
+    float w[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const unsigned long long r = r0 + (unsigned long long)u * B;
+      if (r < end) e[u] = d.rev_edge[r];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const unsigned long long r = r0 + (unsigned long long)u * B;
+      if (r < end) {
+        sg[u] = d.e_syn[e[u]];
+        st[u] = d.e_stamp[e[u]];
+        w[u] = d.e_w[e[u]];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const unsigned long long r = r0 + (unsigned long long)u * B;
+      if (r < end) {
+        const long long Dt_int = T - (long long)st[u];
+        if (sg[u] > 0 && Dt_int >= 0 && Dt_int < NGPU_MAX_SYN_DT)
+          d.e_w[e[u]] = syn_update(syn, sg[u], w[u], d.dt * (float)Dt_int);
+      }
     }
   }
 }
@@ -791,22 +846,19 @@ k_stdp_post(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
   const int slot = (int)(T % d.ring_R);
   int cnt = d.ring_cnt[slot];
   cnt = cnt < d.ring_C ? cnt : d.ring_C;
-  const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int n_warps = (gridDim.x * blockDim.x) >> 5;
-  // spikes of this step without dendritic delay
-  for (int item = warp; item < cnt; item += n_warps) {
+  // one block per node: spikes of this step without dendritic delay
+  for (int item = blockIdx.x; item < cnt; item += gridDim.x) {
     const unsigned node = d.ring_src[(long long)slot * d.ring_C + item];
-    if (d.last_rev_T[node] != (int)T) continue;   // dendritic delay > 0
-    post_rule_node(d, syn, node, T, lane);
+    if (d.last_rev_T[node] != (int)T) continue;   // dendritic delay > 0 (block-uniform)
+    post_rule_node(d, syn, node, T);
   }
   // spikes of earlier steps reaching the dendrites now
   if (d.rev_cnt != nullptr) {
     const int rslot = (int)(T % d.rev_R);
     int rcnt = d.rev_cnt[rslot];
     rcnt = rcnt < d.rev_C ? rcnt : d.rev_C;
-    for (int item = warp; item < rcnt; item += n_warps)
-      post_rule_node(d, syn, d.rev_src[(long long)rslot * d.rev_C + item], T, lane);
+    for (int item = blockIdx.x; item < rcnt; item += gridDim.x)
+      post_rule_node(d, syn, d.rev_src[(long long)rslot * d.rev_C + item], T);
   }
   finish_step(d, ctx);
 }
