@@ -1640,13 +1640,20 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
         }
         break;
       case MK_IAF_PSC_EXP:
-        LaunchIafPscExpUpdate(MakeGroupArgs(g), MakeInputArgs(g), MakePushArgs(g), ctx, stream_);
-        break;
       case MK_IAF_PSC_EXP_G:
       case MK_IZHIKEVICH:
       case MK_IZH_PSC_EXP:
-        LaunchSimpleNeuronUpdate(mi->kind, mi->n_sub, MakeGroupArgs(g), MakeInputArgs(g),
-                                 MakePushArgs(g), ctx, stream_);
+        if (g->in_simple_batch) {
+          // the whole batch is launched once, at its first group
+          if (simple_batch_.groups[0] == g)
+            LaunchSimpleBatch(simple_batch_.d_segs, simple_batch_.d_blk_seg,
+                              simple_batch_.n_blocks, ctx, stream_);
+        } else if (mi->kind == MK_IAF_PSC_EXP) {
+          LaunchIafPscExpUpdate(MakeGroupArgs(g), MakeInputArgs(g), MakePushArgs(g), ctx, stream_);
+        } else {
+          LaunchSimpleNeuronUpdate(mi->kind, mi->n_sub, MakeGroupArgs(g), MakeInputArgs(g),
+                                   MakePushArgs(g), ctx, stream_);
+        }
         break;
       case MK_SPIKE_GENERATOR:
         if (g->d_sg_off) LaunchSpikeGeneratorUpdate(MakeGroupArgs(g), MakePushArgs(g), ctx, stream_);
@@ -1930,6 +1937,35 @@ void NeuronGPU::BuildRk5Batches() {
     if (!Rk5BatchSupported(g->mi->rk5_model, g->n_port)) continue;
     by_key[{g->mi->rk5_model, g->n_port}].push_back(g);
   }
+  // simple models: one launch for all their groups
+  {
+    SimpleBatchHost &sb = simple_batch_;
+    for (NodeGroup *g : groups_) {
+      const ModelKind k = g->mi->kind;
+      if (g->n_node > 0 && (k == MK_IAF_PSC_EXP || k == MK_IAF_PSC_EXP_G ||
+                            k == MK_IZHIKEVICH || k == MK_IZH_PSC_EXP))
+        sb.groups.push_back(g);
+    }
+    if (sb.groups.size() >= 2) {
+      for (NodeGroup *g : sb.groups) {
+        g->in_simple_batch = true;
+        sb.n_blocks += (g->n_node + 127) / 128;
+      }
+      std::vector<int> map(sb.n_blocks);
+      int blk = 0;
+      for (size_t si = 0; si < sb.groups.size(); si++) {
+        const int nb = (sb.groups[si]->n_node + 127) / 128;
+        for (int j = 0; j < nb; j++) map[blk + j] = (int)si;
+        blk += nb;
+      }
+      NGPU_CUDA(cudaMalloc(&sb.d_segs, sizeof(SegArgs) * sb.groups.size()));
+      NGPU_CUDA(cudaMalloc(&sb.d_blk_seg, sizeof(int) * sb.n_blocks));
+      NGPU_CUDA(cudaMemcpy(sb.d_blk_seg, map.data(), sizeof(int) * sb.n_blocks,
+                           cudaMemcpyHostToDevice));
+    } else {
+      sb.groups.clear();
+    }
+  }
   for (auto &kv : by_key) {
     if (kv.second.size() < 2) continue;
     Rk5BatchHost b;
@@ -1962,6 +1998,24 @@ void NeuronGPU::BuildRk5Batches() {
 // arguments; captured graphs read the tables at run time, so they stay valid.
 void NeuronGPU::RefreshRk5BatchTables() {
   batch_tables_dirty_ = false;
+  if (!simple_batch_.groups.empty()) {
+    SimpleBatchHost &sb = simple_batch_;
+    std::vector<SegArgs> segs(sb.groups.size());
+    int blk = 0;
+    for (size_t si = 0; si < sb.groups.size(); si++) {
+      NodeGroup *g = sb.groups[si];
+      memset(&segs[si], 0, sizeof(SegArgs));
+      segs[si].g = MakeGroupArgs(g);
+      segs[si].in = MakeInputArgs(g);
+      segs[si].pa = MakePushArgs(g);
+      segs[si].blk0 = blk;
+      segs[si].kind = g->mi->kind;
+      segs[si].n_sub = g->mi->n_sub;
+      blk += (g->n_node + 127) / 128;
+    }
+    NGPU_CUDA(cudaMemcpy(sb.d_segs, segs.data(), sizeof(SegArgs) * segs.size(),
+                         cudaMemcpyHostToDevice));
+  }
   for (Rk5BatchHost &b : batches_) {
     std::vector<SegArgs> segs(b.groups.size());
     int blk = 0;
@@ -2084,6 +2138,10 @@ void NeuronGPU::FreeRk5Queue(Rk5Queue &q) {
 }
 
 void NeuronGPU::FreeRk5Batches() {
+  if (simple_batch_.d_segs) cudaFree(simple_batch_.d_segs);
+  if (simple_batch_.d_blk_seg) cudaFree(simple_batch_.d_blk_seg);
+  for (NodeGroup *g : simple_batch_.groups) g->in_simple_batch = false;
+  simple_batch_ = SimpleBatchHost{};
   for (Rk5BatchHost &b : batches_) {
     if (b.d_segs) cudaFree(b.d_segs);
     if (b.d_blk_seg) cudaFree(b.d_blk_seg);

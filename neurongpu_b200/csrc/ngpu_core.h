@@ -134,6 +134,8 @@ struct NodeGroup {
   float tune_ms[6] = {0, 0, 0, 0, 0, 0};
   // index of the batched RK5 launch this group belongs to, or -1
   int batch = -1;
+  // updated by the batched launch of simple models
+  bool in_simple_batch = false;
   // RK5 step mode (StepMode) and the accepted-step log of STEP_LOG
   int step_mode = 0;
   float *d_log_buf = nullptr;
@@ -374,6 +376,14 @@ class NeuronGPU {
     Rk5Queue q{};
   };
   std::vector<Rk5BatchHost> batches_;
+  // one batched launch for the groups of simple models (iaf_psc_exp,
+  // iaf_psc_exp_g, izhikevich family) when there are at least two
+  struct SimpleBatchHost {
+    std::vector<NodeGroup *> groups;
+    int n_blocks = 0;
+    SegArgs *d_segs = nullptr;
+    int *d_blk_seg = nullptr;
+  } simple_batch_;
   bool batches_built_ = false;
   bool batch_tables_dirty_ = true;
   bool rk5_batching_ = true;

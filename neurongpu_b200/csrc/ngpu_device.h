@@ -208,6 +208,8 @@ struct SegArgs {
   InputArgs in;
   PushArgs pa;
   int blk0;
+  int kind;                     // ModelKind (batched launch of simple models)
+  int n_sub;                    // Euler sub-steps (izhikevich_psc_exp family)
   int pad_;
 };
 

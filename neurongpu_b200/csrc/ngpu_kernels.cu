@@ -172,10 +172,8 @@ __device__ __forceinline__ float gparam(const GroupArgs &g, int j, int i) {
   return pbit(g.pmask, j) ? g.param[(long long)j * g.n_pad + i] : g.puni[j];
 }
 
-__global__ void __launch_bounds__(NGPU_BLOCK)
-k_iaf_psc_exp(GroupArgs g, InputArgs in, PushArgs pa, StepCtx *ctx) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= g.n) return;
+__device__ __forceinline__ void iaf_psc_exp_node(const GroupArgs &g, const InputArgs &in,
+                                                 const PushArgs &pa, StepCtx *ctx, int i) {
   const long long it = ctx->it, T0 = ctx->T0;
   const double t0 = ctx->t0;
   const int n_pad = g.n_pad;
@@ -212,6 +210,12 @@ k_iaf_psc_exp(GroupArgs g, InputArgs in, PushArgs pa, StepCtx *ctx) {
   var[3 * n_pad + i] = refr;
 }
 
+__global__ void __launch_bounds__(NGPU_BLOCK)
+k_iaf_psc_exp(GroupArgs g, InputArgs in, PushArgs pa, StepCtx *ctx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < g.n) iaf_psc_exp_node(g, in, pa, ctx, i);
+}
+
 void LaunchIafPscExpUpdate(const GroupArgs &g, const InputArgs &in,
                            const PushArgs &pa, StepCtx *ctx, cudaStream_t s) {
   if (g.n <= 0) return;
@@ -225,9 +229,8 @@ void LaunchIafPscExpUpdate(const GroupArgs &g, const InputArgs &in,
 // of the group. gc = P11, P22, P21, P20, Theta_rel, V_reset_rel, refractory
 // steps. Variables I_syn, V_m_rel, refractory_step; parameter I_e.
 // ---------------------------------------------------------------------------
-__global__ void k_iaf_psc_exp_g(GroupArgs g, InputArgs in, PushArgs pa, StepCtx *ctx) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= g.n) return;
+__device__ __forceinline__ void iaf_psc_exp_g_node(const GroupArgs &g, const InputArgs &in,
+                                                   const PushArgs &pa, StepCtx *ctx, int i) {
   const long long it = ctx->it, T0 = ctx->T0;
   const double t0 = ctx->t0;
   const int n_pad = g.n_pad;
@@ -262,9 +265,8 @@ __global__ void k_iaf_psc_exp_g(GroupArgs g, InputArgs in, PushArgs pa, StepCtx 
 // refractory steps, h. Variables I_syn, V_m, u, refractory_step; parameters
 // I_e, den_delay.
 // ---------------------------------------------------------------------------
-__global__ void k_izhikevich(GroupArgs g, InputArgs in, PushArgs pa, StepCtx *ctx) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= g.n) return;
+__device__ __forceinline__ void izhikevich_node(const GroupArgs &g, const InputArgs &in,
+                                                const PushArgs &pa, StepCtx *ctx, int i) {
   const long long it = ctx->it, T0 = ctx->T0;
   const double t0 = ctx->t0;
   const int n_pad = g.n_pad;
@@ -307,9 +309,8 @@ __global__ void k_izhikevich(GroupArgs g, InputArgs in, PushArgs pa, StepCtx *ct
 // d, refractory steps, sub-step h, current decay per sub-step.
 // ---------------------------------------------------------------------------
 template <int NSUB>
-__global__ void k_izh_psc_exp(GroupArgs g, InputArgs in, PushArgs pa, StepCtx *ctx) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= g.n) return;
+__device__ __forceinline__ void izh_psc_exp_node(const GroupArgs &g, const InputArgs &in,
+                                                 const PushArgs &pa, StepCtx *ctx, int i) {
   const long long it = ctx->it, T0 = ctx->T0;
   const double t0 = ctx->t0;
   const int n_pad = g.n_pad;
@@ -349,20 +350,51 @@ __global__ void k_izh_psc_exp(GroupArgs g, InputArgs in, PushArgs pa, StepCtx *c
   var[3 * n_pad + i] = refr;
 }
 
+// one node of a simple model (kind: ModelKind; n_sub: Euler sub-steps of
+// the izhikevich_psc_exp family)
+__device__ __forceinline__ void simple_node(int kind, int n_sub, const GroupArgs &g,
+                                            const InputArgs &in, const PushArgs &pa,
+                                            StepCtx *ctx, int i) {
+  switch (kind) {
+    case MK_IAF_PSC_EXP: iaf_psc_exp_node(g, in, pa, ctx, i); break;
+    case MK_IAF_PSC_EXP_G: iaf_psc_exp_g_node(g, in, pa, ctx, i); break;
+    case MK_IZHIKEVICH: izhikevich_node(g, in, pa, ctx, i); break;
+    case MK_IZH_PSC_EXP:
+      if (n_sub == 5) izh_psc_exp_node<5>(g, in, pa, ctx, i);
+      else if (n_sub == 2) izh_psc_exp_node<2>(g, in, pa, ctx, i);
+      else izh_psc_exp_node<1>(g, in, pa, ctx, i);
+      break;
+    default: break;
+  }
+}
+
+__global__ void __launch_bounds__(NGPU_BLOCK)
+k_simple(GroupArgs g, InputArgs in, PushArgs pa, StepCtx *ctx, int kind, int n_sub) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < g.n) simple_node(kind, n_sub, g, in, pa, ctx, i);
+}
+
+// Many groups of simple models in one launch: block b updates 128 nodes of
+// segment blk_seg[b] (the cortical column's eight populations are one
+// launch per step instead of eight).
+__global__ void __launch_bounds__(NGPU_BLOCK)
+k_simple_seg(const SegArgs *__restrict__ segs, const int *__restrict__ blk_seg, StepCtx *ctx) {
+  const SegArgs &S = segs[blk_seg[blockIdx.x]];
+  const int i = (blockIdx.x - S.blk0) * blockDim.x + threadIdx.x;
+  if (i < S.g.n) simple_node(S.kind, S.n_sub, S.g, S.in, S.pa, ctx, i);
+}
+
+void LaunchSimpleBatch(const SegArgs *segs, const int *blk_seg, int n_blocks, StepCtx *ctx,
+                       cudaStream_t s) {
+  if (n_blocks <= 0) return;
+  k_simple_seg<<<n_blocks, NGPU_BLOCK, 0, s>>>(segs, blk_seg, ctx);
+}
+
 void LaunchSimpleNeuronUpdate(int kind, int n_sub, const GroupArgs &g, const InputArgs &in,
                               const PushArgs &pa, StepCtx *ctx, cudaStream_t s) {
   if (g.n <= 0) return;
   const dim3 grid((g.n + NGPU_BLOCK - 1) / NGPU_BLOCK), block(NGPU_BLOCK);
-  switch (kind) {
-    case MK_IAF_PSC_EXP_G: k_iaf_psc_exp_g<<<grid, block, 0, s>>>(g, in, pa, ctx); break;
-    case MK_IZHIKEVICH: k_izhikevich<<<grid, block, 0, s>>>(g, in, pa, ctx); break;
-    case MK_IZH_PSC_EXP:
-      if (n_sub == 5) k_izh_psc_exp<5><<<grid, block, 0, s>>>(g, in, pa, ctx);
-      else if (n_sub == 2) k_izh_psc_exp<2><<<grid, block, 0, s>>>(g, in, pa, ctx);
-      else k_izh_psc_exp<1><<<grid, block, 0, s>>>(g, in, pa, ctx);
-      break;
-    default: break;
-  }
+  k_simple<<<grid, block, 0, s>>>(g, in, pa, ctx, kind, n_sub);
 }
 
 // ---------------------------------------------------------------------------

@@ -46,6 +46,10 @@ void LaunchIafPscExpUpdate(const GroupArgs &g, const InputArgs &in,
 // constants are in GroupArgs::gc
 void LaunchSimpleNeuronUpdate(int kind, int n_sub, const GroupArgs &g, const InputArgs &in,
                               const PushArgs &pa, StepCtx *ctx, cudaStream_t s);
+// groups of iaf_psc_exp / iaf_psc_exp_g / izhikevich / izhikevich_psc_exp in
+// one launch through a segment table (SegArgs::kind, n_sub; block -> segment)
+void LaunchSimpleBatch(const SegArgs *segs, const int *blk_seg, int n_blocks, StepCtx *ctx,
+                       cudaStream_t s);
 void LaunchSpikeGeneratorUpdate(const GroupArgs &g, const PushArgs &pa,
                                 StepCtx *ctx, cudaStream_t s);
 void LaunchParrotUpdate(const GroupArgs &g, const InputArgs &in,

@@ -117,3 +117,34 @@ def test_straggler_queue_bit_identical(ngpu):
         assert np.array_equal(v.view(np.int32), v0.view(np.int32)), key
         assert np.array_equal(w.view(np.int32), w0.view(np.int32)), key
         assert e == e0, key
+
+
+def test_simple_models_batched_equals_per_group(ngpu):
+    """The cortical column's eight iaf_psc_exp populations (10 % scale) plus
+    groups of iaf_psc_exp_g and izhikevich_psc_exp_2s, updated by one batched
+    launch per step, give the same spikes and state as one launch per group."""
+    from tests import cortical_column as cc
+
+    def run(batching):
+        ngpu.Reset()
+        ngpu.SetRk5Batching(batching)
+        pops, gens, d = cc.build(ngpu, n_scaling=0.1, k_scaling=0.1, seed=12349)
+        izh = ngpu.Create("izhikevich_psc_exp_2s", 500)
+        ngpu.SetStatus(izh, {"I_e": 10.0})
+        ig = ngpu.Create("iaf_psc_exp_g", 300)
+        ngpu.SetStatus(ig, {"I_e": 400.0})
+        groups = list(pops) + [izh, ig]
+        for p in groups:
+            ngpu.ActivateSpikeCount(p)
+        ngpu.Simulate(200.0)
+        counts = np.concatenate([ngpu.GetNeuronIntVarArray(p.i0, p.n, "spike_count")
+                                 for p in groups])
+        v = np.concatenate([np.asarray(ngpu.GetNeuronVar(p.i0, p.n, "V_m_rel"),
+                                       dtype=np.float32).ravel() for p in pops])
+        return counts, v
+
+    c1, v1 = run(True)
+    c0, v0 = run(False)
+    assert c1.sum() > 100
+    assert np.array_equal(c1, c0)
+    assert np.array_equal(v1.view(np.int32), v0.view(np.int32))
