@@ -639,8 +639,11 @@ __device__ __forceinline__ void step_bookkeeping(int *ring_cnt, int ring_R, int 
 }
 
 // ---------------------------------------------------------------------------
-// synaptic delivery: one warp per (spike, delay) group
+// synaptic delivery: one warp per (spike, delay) group. PLASTIC: the
+// network has plastic synapses (the STDP pre rule runs on every edge); the
+// static instance does not carry that path's registers.
 // ---------------------------------------------------------------------------
+template <bool PLASTIC>
 __global__ void __launch_bounds__(256)
 k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
   __shared__ int s_pref[NGPU_MAX_DELAYS + 1];
@@ -715,7 +718,7 @@ k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
     const unsigned long long gi = (unsigned long long)src * d.nd + di;
     const unsigned long long beg = d.grp_off[gi], end = d.grp_off[gi + 1];
     if (lane == 0) events += end - beg;
-    if (d.e_syn == nullptr) {
+    if constexpr (!PLASTIC) {
       // four edges per lane in flight; edges are read once per spike, so
       // they are loaded with the streaming (evict-first) hint
       for (unsigned long long e0 = beg + lane; e0 < end; e0 += 128) {
@@ -794,17 +797,21 @@ k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
   finish_step(d, ctx);
 }
 
+// Resident delivery blocks per SM, at most 3: the delivery runs beside the
+// node updates, and a larger grid takes SM slots from them without
+// delivering faster (measured on the silent and the 26 Hz scale networks).
 int DeliverBlocksPerSM() {
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_deliver, 256, 0) != cudaSuccess)
-    return 4;
-  return nb > 0 ? nb : 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_deliver<false>, 256, 0) != cudaSuccess)
+    return 3;
+  return nb > 3 ? 3 : (nb > 0 ? nb : 1);
 }
 
 void LaunchDeliver(const DeliverArgs &d, const SynGroupTable &syn,
                    StepCtx *ctx, int n_blocks, cudaStream_t s) {
   if (d.nd <= 0) return;
-  k_deliver<<<n_blocks, 256, 0, s>>>(d, syn, ctx);
+  if (d.e_syn != nullptr) k_deliver<true><<<n_blocks, 256, 0, s>>>(d, syn, ctx);
+  else k_deliver<false><<<n_blocks, 256, 0, s>>>(d, syn, ctx);
 }
 
 // ---------------------------------------------------------------------------
