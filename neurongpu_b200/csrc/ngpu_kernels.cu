@@ -676,18 +676,44 @@ k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
     }
     total = __shfl_sync(0xffffffffu, my_incl, 31);
   } else {
-    for (int di = threadIdx.x; di < d.nd; di += blockDim.x) {
-      int slot = (int)((T - d.delays[di]) % d.ring_R);
-      if (slot < 0) slot += d.ring_R;
-      s_slot[di] = slot;
-      int c = d.ring_cnt[slot];
-      s_pref[di + 1] = c < d.ring_C ? c : d.ring_C;
+    // block-wide scan, blockDim.x delays per round: warp scans, then a scan
+    // of the warp totals by warp 0, plus the carry of earlier rounds
+    __shared__ int s_wsum[8];
+    const int wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int carry = 0;
+    for (int base = 0; base < d.nd; base += blockDim.x) {
+      const int di = base + threadIdx.x;
+      int c = 0;
+      if (di < d.nd) {
+        int slot = (int)((T - d.delays[di]) % d.ring_R);
+        if (slot < 0) slot += d.ring_R;
+        s_slot[di] = slot;
+        c = d.ring_cnt[slot];
+        c = c < d.ring_C ? c : d.ring_C;
+      }
+      int x = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      if (lane == 31) s_wsum[wid] = x;
+      __syncthreads();
+      if (wid == 0) {
+        int w = lane < nw ? s_wsum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, w, o);
+          if (lane >= o) w += y;
+        }
+        if (lane < nw) s_wsum[lane] = w;
+      }
+      __syncthreads();
+      if (di < d.nd) s_pref[di + 1] = carry + (wid > 0 ? s_wsum[wid - 1] : 0) + x;
+      carry += s_wsum[nw - 1];
+      __syncthreads();
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      s_pref[0] = 0;
-      for (int di = 0; di < d.nd; di++) s_pref[di + 1] += s_pref[di];
-    }
+    if (threadIdx.x == 0) s_pref[0] = 0;
     __syncthreads();
     total = s_pref[d.nd];
   }
@@ -719,13 +745,13 @@ k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
     const unsigned long long beg = d.grp_off[gi], end = d.grp_off[gi + 1];
     if (lane == 0) events += end - beg;
     if constexpr (!PLASTIC) {
-      // four edges per lane in flight; edges are read once per spike, so
+      // eight edges per lane in flight; edges are read once per spike, so
       // they are loaded with the streaming (evict-first) hint
-      for (unsigned long long e0 = beg + lane; e0 < end; e0 += 128) {
-        unsigned sl[4];
-        float wv[4];
+      for (unsigned long long e0 = beg + lane; e0 < end; e0 += 256) {
+        unsigned sl[8];
+        float wv[8];
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
+        for (int u = 0; u < 8; u++) {
           const unsigned long long e = e0 + 32 * u;
           if (e < end) {
             sl[u] = __ldcs(d.e_slot + e);
@@ -733,7 +759,7 @@ k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
           }
         }
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
+        for (int u = 0; u < 8; u++) {
           const unsigned long long e = e0 + 32 * u;
           if (e < end) {
             atomicAdd((unsigned long long *)(acc + sl[u]),
