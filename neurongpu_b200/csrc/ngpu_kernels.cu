@@ -1,21 +1,26 @@
 // Simulation kernels for sm_100a.
 //
-// Per time step the driver launches (optionally captured in a CUDA graph):
-//   1. one update kernel per node group: folds the pending synaptic input of
-//      the previous step into the state (the reference's GetSpikes and
-//      PoissGenSendSpikeKernel, src/get_spike.cu:116-140,
-//      src/poiss_gen.cu:43-74), integrates the step (src/rk5.h:57-195 for
-//      RK5 groups) and appends emitted spikes to this step's ring slot
+// Per time step the driver launches (captured in CUDA graphs of a chunk of
+// steps):
+//   1. the node updates: one launch per RK5 group or batch of RK5 groups
+//      (ngpu_kernels_common.cuh, ngpu_rk5_batch.cu) plus its straggler
+//      finishing launch, and one launch for the groups of simple models; each
+//      folds the pending synaptic input of the previous step into the state
+//      (the reference's GetSpikes and PoissGenSendSpikeKernel,
+//      src/get_spike.cu:116-140, src/poiss_gen.cu:43-74), integrates the step
+//      and appends emitted spikes to this step's ring slot
 //      (src/spike_buffer.cu:143-228);
 //   2. k_deliver: expands the (source, delay) groups that fall due in this
 //      step into fixed-point accumulator additions, with the STDP pre-spike
 //      rule (src/spike_buffer.cu:233-302, src/nested_loop.cu:39-167,
-//      src/get_spike.cu:48-85);
+//      src/get_spike.cu:48-85); without plastic synapses it runs on a second
+//      stream beside the node updates;
 //   3. k_stdp_post: STDP post-spike rule over incoming plastic synapses of the
 //      neurons that spiked (src/rev_spike.cu:41-75);
-//   4. k_record (multimeter columns) and k_advance (step counter).
-// No host synchronisation happens inside a step; every kernel reads the step
-// index from the device-resident StepCtx.
+//   4. k_record (multimeter columns); k_advance only for networks without
+//      delivery.
+// No host synchronisation happens inside a step; each step of a chunk reads
+// its own device-resident copy of the step context (k_step_prologue).
 #include <cuda_runtime.h>
 #include <math.h>
 #include "ngpu_device.h"
