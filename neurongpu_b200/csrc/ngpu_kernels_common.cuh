@@ -430,6 +430,7 @@ __device__ __forceinline__ void rk5_resume(const GroupArgs &g, const PushArgs &p
                                            const float *p_uni, const float *q_uni, int np,
                                            const float *r, unsigned &evals, bool dry) {
   using Tr = ModelTraits<M>;
+  if constexpr (NP >= 2 && NP <= 4) np = NP;   // as in rk5_neuron
   const int i = __float_as_int(r[0]);
   int guard = __float_as_int(r[2]);
   float h = r[3];
@@ -529,7 +530,9 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
   using Tr = ModelTraits<M>;
   const bool active = (MODE != STEP_LEARNED) || (i < g.n);
   const bool dry = g.dry || dry_run;
-  const int np = in.np;
+  // the launchers pick the template port count NP = np for 2..4 ports (1
+  // serves 0 and 1), so there the count is a compile-time constant
+  const int np = (NP >= 2 && NP <= 4) ? NP : in.np;
   const long long it = ctx->it;
   const long long T0 = ctx->T0;
   const double t0 = ctx->t0;
