@@ -382,13 +382,14 @@ __device__ __forceinline__ bool rk5_plain_substep(const GroupArgs &g, const Push
 }
 
 // end-of-step state of neuron i
-template <class M>
+template <class M, int NP>
 __device__ __forceinline__ void rk5_store(const GroupArgs &g, int i, const float *y, float h,
                                           double x, double x1, float refr, bool write_refr) {
   using Tr = ModelTraits<M>;
 #pragma unroll
   for (int j = 0; j < M::NVAR; j++) {
-    if (j < g.nvar) g.var[(long long)j * g.n_pad + i] = y[j];
+    // (every variable column exists for 2-4 ports, see rk5_neuron)
+    if ((NP >= 2 && NP <= 4) || j < g.nvar) g.var[(long long)j * g.n_pad + i] = y[j];
   }
   g.h[i] = h;
   g.dx[i] = (float)(x - x1);
@@ -455,7 +456,7 @@ __device__ __forceinline__ void rk5_resume(const GroupArgs &g, const PushArgs &p
                                         x1, T, den, dry, evals);
   }
   if (!dry) {
-    rk5_store<M>(g, i, y, h, x, x1, refr, true);
+    rk5_store<M, NP>(g, i, y, h, x, x1, refr, true);
   } else if (y[0] == 1.2345e30f) {
     g.h[i] = h + (float)x;        // keeps the timing run from being optimised away
   }
@@ -541,7 +542,8 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
   float y[M::NVAR];
 #pragma unroll
   for (int j = 0; j < M::NVAR; j++) {
-    y[j] = (active && j < g.nvar) ? (pre_col ? pre_col[j] : g.var[(long long)j * n_pad + i])
+    y[j] = (active && ((NP >= 2 && NP <= 4) || j < g.nvar))
+               ? (pre_col ? pre_col[j] : g.var[(long long)j * n_pad + i])
                                   : 0.0f;
   }
   float p_loc[UNI ? 1 : M::NPARAM];
@@ -650,7 +652,7 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
   }
   if (!active) return;
   if (!dry) {
-    rk5_store<M>(g, i, y, h, x, x1, refr, refr != refr0);
+    rk5_store<M, NP>(g, i, y, h, x, x1, refr, refr != refr0);
   } else if (y[0] == 1.2345e30f) {
     // keeps the dry run from being optimised away; never true in practice
     g.h[i] = h + (float)x;
