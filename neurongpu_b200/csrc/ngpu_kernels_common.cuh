@@ -539,6 +539,11 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
   const double t0 = ctx->t0;
   const int pending = ctx->poisson_pending;
   const int n_pad = g.n_pad;
+  // the pending input is summed before the state is loaded, so that the state
+  // is not live across the Poisson draws (fewer registers and spills)
+  constexpr int NPI = (M::NPV == 0) ? 1 : NP;
+  long long s[NPI];
+  if (active) input_sum<NPI>(in, i, n_pad, np, it, t0, g.dt, pending, T0, s, dry, pre_acc);
   float y[M::NVAR];
 #pragma unroll
   for (int j = 0; j < M::NVAR; j++) {
@@ -554,10 +559,7 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
   float refr = active ? (pre_col ? pre_col[M::NVAR] : g.param[(long long)Tr::refr * n_pad + i])
                       : 0.0f;
   // fold the previous step's input
-  constexpr int NPI = (M::NPV == 0) ? 1 : NP;
   if (active) {
-    long long s[NPI];
-    input_sum<NPI>(in, i, n_pad, np, it, t0, g.dt, pending, T0, s, dry, pre_acc);
 #pragma unroll
     for (int qq = 0; qq < NPI; qq++) {
       if (qq < np && s[qq] != 0) {
