@@ -1036,6 +1036,21 @@ InputArgs NeuronGPU::MakeInputArgs(NodeGroup *g) {
   return in;
 }
 
+// Whether Poisson direct connections into group g may draw
+// NGPU_POISSON_INV_MAX or more expected spikes per step; the RK5 update
+// kernels leave those to LaunchPoissonLarge. Generator rates change only
+// between simulation calls and a change re-captures the step graphs, so the
+// answer holds for every step of a captured graph.
+bool NeuronGPU::HasLargePoisson(const NodeGroup *g) const {
+  if (g->ud && g->ud_gen >= 0 && g->ud_gen < (int)gen_lam_h_.size())
+    return gen_lam_h_[g->ud_gen] >= NGPU_POISSON_INV_MAX;
+  if (!g->has_dc) return false;
+  for (double lam : gen_lam_h_) {
+    if (lam >= NGPU_POISSON_INV_MAX) return true;
+  }
+  return false;
+}
+
 PushArgs NeuronGPU::MakePushArgs(NodeGroup *g) {
   PushArgs pa;
   memset(&pa, 0, sizeof(pa));
@@ -1633,8 +1648,15 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
         if (g->batch >= 0) {
           // the whole batch is launched once, at its first group
           const Rk5BatchHost &b = batches_[g->batch];
-          if (b.groups[0] == g) LaunchRk5Batch(MakeRk5Batch(b), ctx, stream_);
+          if (b.groups[0] == g) {
+            for (NodeGroup *bg : b.groups) {
+              if (HasLargePoisson(bg))
+                LaunchPoissonLarge(MakeGroupArgs(bg), MakeInputArgs(bg), ctx, stream_);
+            }
+            LaunchRk5Batch(MakeRk5Batch(b), ctx, stream_);
+          }
         } else {
+          if (HasLargePoisson(g)) LaunchPoissonLarge(MakeGroupArgs(g), MakeInputArgs(g), ctx, stream_);
           LaunchRk5Update(mi->rk5_model, g->n_port, MakeGroupArgs(g), MakeInputArgs(g),
                           MakePushArgs(g), ctx, stream_);
         }

@@ -529,6 +529,7 @@ class NeuronGPU {
   void WriteInitialRecord();
   GroupArgs MakeGroupArgs(NodeGroup *g);
   InputArgs MakeInputArgs(NodeGroup *g);
+  bool HasLargePoisson(const NodeGroup *g) const;
   PushArgs MakePushArgs(NodeGroup *g);
   DeliverArgs MakeDeliverArgs();
   void SetParamColumn(NodeGroup *g, int col, int i0, int n, const int *nodes,

@@ -558,6 +558,43 @@ __global__ void k_fold_input(GroupArgs g, InputArgs in, StepCtx *ctx) {
   }
 }
 
+// Poisson direct connections of NGPU_POISSON_INV_MAX or more expected spikes
+// per step into an RK5 group: drawn here, before the group's update, and
+// added into the accumulator half that the update folds (the update kernels
+// leave these connections out). The draws are the ones the update would make
+// and the accumulators hold fixed-point integers, so the folded input is the
+// same bit for bit. One thread per node, the only writer of its slots at
+// this point of the step (the delivery that filled this half has finished).
+__global__ void k_poisson_large(GroupArgs g, InputArgs in, StepCtx *ctx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.n || !ctx->poisson_pending) return;
+  const long long it = ctx->it, T0 = ctx->T0;
+  const double t = ctx->t0 + (double)g.dt * (double)it;
+  long long *acc = acc_in(in, T0, it) + i;
+  if (in.ud) {
+    const unsigned n = direct_count<false, true>(
+        t - (double)in.ud_origin - (double)in.ud_delay, in.ud_start, in.ud_stop, in.ud_lambda,
+        in.ud_explam, in.ud_cdf, in.seed, in.ud_stream0 + (unsigned long long)i, T0 + it);
+    if (n > 0) acc[(long long)in.ud_port * g.n_pad] += ng_to_fixed(in.ud_w * (float)n);
+  } else if (in.dc_off != nullptr) {
+    const unsigned b = in.dc_off[i], e = in.dc_off[i + 1];
+    for (unsigned c = b; c < e; c++) {
+      const unsigned gen = in.dc_gen[c];
+      const unsigned n = direct_count<false, true>(
+          t - (double)in.gen_origin[gen] - (double)in.dc_delay[c], in.gen_start[gen],
+          in.gen_stop[gen], in.gen_lambda[gen], in.gen_explam[gen], nullptr, in.seed,
+          in.dc_stream[c], T0 + it);
+      if (n > 0) acc[(long long)in.dc_port[c] * g.n_pad] += ng_to_fixed(in.dc_weight[c] * (float)n);
+    }
+  }
+}
+
+void LaunchPoissonLarge(const GroupArgs &g, const InputArgs &in, StepCtx *ctx,
+                        cudaStream_t s) {
+  if (g.n <= 0) return;
+  k_poisson_large<<<(g.n + 127) / 128, 128, 0, s>>>(g, in, ctx);
+}
+
 __global__ void k_clear_pending(StepCtx *ctx) { ctx->poisson_pending = 0; }
 
 void LaunchFoldInput(const GroupArgs &g, const InputArgs &in, StepCtx *ctx,

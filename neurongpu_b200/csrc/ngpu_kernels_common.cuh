@@ -116,11 +116,43 @@ __device__ __forceinline__ long long *acc_in(const InputArgs &in, long long T0, 
   return in.acc + (((T0 + it) & 1) ? in.acc_par : 0) + in.acc_base;
 }
 
+// Poisson count of one direct connection for the step T_prev (the
+// reference's draw for that step); t_rel is the step's time relative to the
+// generator's origin and the connection's delay, and the count is 0 outside
+// the generator's active window. SMALL / LARGE: whether rates below / at or above
+// NGPU_POISSON_INV_MAX per step are drawn; a count that is not drawn is 0.
+// Small rates: inversion against the host-built CDF table (the same counts
+// as ng_poisson_inversion, without device double divisions).
+template <bool SMALL, bool LARGE>
+__device__ __forceinline__ unsigned direct_count(double t_rel, float start, float stop,
+                                                 double lam, double explam, const double *cdf,
+                                                 unsigned long long seed,
+                                                 unsigned long long stream, long long T_prev) {
+  if (!(t_rel >= (double)start && t_rel <= (double)stop)) return 0;
+  unsigned n = 0;
+  if (lam < NGPU_POISSON_INV_MAX) {
+    if constexpr (SMALL) {
+      Philox4 r = ng_random_block(seed, RNG_TAG_POISSON_DIRECT, stream, T_prev, 0);
+      const double u = ng_u01(r.v[0], r.v[1]);
+      if (lam > 0.0) {
+        while (n < NGPU_CDF_LEN - 1 && u > cdf[n]) n++;
+      }
+    }
+  } else {
+    if constexpr (LARGE) n = ng_poisson(lam, explam, seed, RNG_TAG_POISSON_DIRECT, stream, T_prev);
+  }
+  return n;
+}
+
 // Sum of the pending synaptic input of one node per port (fixed point):
 // accumulator contents (cleared here) plus the Poisson direct connections
 // drawn for the previous step. pre_acc: the accumulator values already
-// fetched (port q at pre_acc[q]), or null.
-template <int NP>
+// fetched (port q at pre_acc[q]), or null. LARGE = false leaves out the
+// connections of NGPU_POISSON_INV_MAX or more expected spikes per step:
+// the RK5 update kernels use it, and k_poisson_large adds those draws into
+// the accumulators before them (the large-rate sampler needs many registers,
+// and inlined it raised the update kernels' register count and spills).
+template <int NP, bool LARGE = true>
 __device__ __forceinline__ void input_sum(const InputArgs &in, int i,
                                           int n_pad, int np, long long it,
                                           double t0, float dt, int pending,
@@ -140,27 +172,14 @@ __device__ __forceinline__ void input_sum(const InputArgs &in, int i,
   if (pending && in.ud) {
     const double t = t0 + (double)dt * (double)it;
     const double t_rel = t - (double)in.ud_origin - (double)in.ud_delay;
-    if (t_rel >= (double)in.ud_start && t_rel <= (double)in.ud_stop) {
-      const double lam = in.ud_lambda;
-      unsigned n;
-      if (lam < NGPU_POISSON_INV_MAX) {
-        Philox4 r = ng_random_block(in.seed, RNG_TAG_POISSON_DIRECT,
-                                    in.ud_stream0 + (unsigned long long)i, T0 + it, 0);
-        const double u = ng_u01(r.v[0], r.v[1]);
-        n = 0;
-        if (lam > 0.0) {
-          while (n < NGPU_CDF_LEN - 1 && u > in.ud_cdf[n]) n++;
-        }
-      } else {
-        n = ng_poisson(lam, in.ud_explam, in.seed, RNG_TAG_POISSON_DIRECT,
-                       in.ud_stream0 + (unsigned long long)i, T0 + it);
-      }
-      if (n > 0) {
-        const long long v = ng_to_fixed(in.ud_w * (float)n);
+    const unsigned n = direct_count<true, LARGE>(
+        t_rel, in.ud_start, in.ud_stop, in.ud_lambda, in.ud_explam, in.ud_cdf, in.seed,
+        in.ud_stream0 + (unsigned long long)i, T0 + it);
+    if (n > 0) {
+      const long long v = ng_to_fixed(in.ud_w * (float)n);
 #pragma unroll
-        for (int q = 0; q < NP; q++) {
-          if (q == in.ud_port) s[q] += v;
-        }
+      for (int q = 0; q < NP; q++) {
+        if (q == in.ud_port) s[q] += v;
       }
     }
   } else if (pending && in.dc_off != nullptr) {
@@ -172,32 +191,16 @@ __device__ __forceinline__ void input_sum(const InputArgs &in, int i,
       for (unsigned c = b; c < e; c++) {
         unsigned gen = in.dc_gen[c];
         double t_rel = t - (double)in.gen_origin[gen] - (double)in.dc_delay[c];
-        if (t_rel >= (double)in.gen_start[gen] &&
-            t_rel <= (double)in.gen_stop[gen]) {
-          const double lam = in.gen_lambda[gen];
-          unsigned n;
-          if (lam < NGPU_POISSON_INV_MAX) {
-            // inversion against the host-built CDF table: the same counts as
-            // ng_poisson_inversion, without device double divisions
-            Philox4 r = ng_random_block(in.seed, RNG_TAG_POISSON_DIRECT,
-                                        in.dc_stream[c], T_prev, 0);
-            const double u = ng_u01(r.v[0], r.v[1]);
-            const double *cdf = in.gen_cdf + (size_t)gen * NGPU_CDF_LEN;
-            n = 0;
-            if (lam > 0.0) {
-              while (n < NGPU_CDF_LEN - 1 && u > cdf[n]) n++;
-            }
-          } else {
-            n = ng_poisson(lam, in.gen_explam[gen], in.seed,
-                           RNG_TAG_POISSON_DIRECT, in.dc_stream[c], T_prev);
-          }
-          if (n > 0) {
-            long long v = ng_to_fixed(in.dc_weight[c] * (float)n);
-            int port = in.dc_port[c];
+        const unsigned n = direct_count<true, LARGE>(
+            t_rel, in.gen_start[gen], in.gen_stop[gen], in.gen_lambda[gen],
+            in.gen_explam[gen], in.gen_cdf + (size_t)gen * NGPU_CDF_LEN, in.seed,
+            in.dc_stream[c], T_prev);
+        if (n > 0) {
+          long long v = ng_to_fixed(in.dc_weight[c] * (float)n);
+          int port = in.dc_port[c];
 #pragma unroll
-            for (int q = 0; q < NP; q++) {
-              if (q == port) s[q] += v;
-            }
+          for (int q = 0; q < NP; q++) {
+            if (q == port) s[q] += v;
           }
         }
       }
@@ -543,7 +546,8 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
   // is not live across the Poisson draws (fewer registers and spills)
   constexpr int NPI = (M::NPV == 0) ? 1 : NP;
   long long s[NPI];
-  if (active) input_sum<NPI>(in, i, n_pad, np, it, t0, g.dt, pending, T0, s, dry, pre_acc);
+  if (active)
+    input_sum<NPI, false>(in, i, n_pad, np, it, t0, g.dt, pending, T0, s, dry, pre_acc);
   float y[M::NVAR];
 #pragma unroll
   for (int j = 0; j < M::NVAR; j++) {
