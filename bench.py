@@ -132,9 +132,9 @@ def measured_peaks():
 # of the launch): RK5 update (8-blocks/SM variant) on the silent network at
 # 200,000 neurons in steady state (cold cache; the state's writes stay in L2
 # during the launch), delivery on the active network at 400,000 neurons.
-TRAFFIC_RK5_PER_NEURON_STEP = 52.4       # bytes
+TRAFFIC_RK5_PER_NEURON_STEP = 52.3       # bytes
 TRAFFIC_DELIVER_PER_EVENT = 11.3         # bytes
-INST_RK5_PER_WARP_STEP = 1113.8          # warp instructions per 32 neuron-steps
+INST_RK5_PER_WARP_STEP = 1084.0          # warp instructions per 32 neuron-steps
 SM_COUNT, SMSP_PER_SM = 148, 4
 
 
