@@ -960,8 +960,16 @@ GroupArgs NeuronGPU::MakeGroupArgs(NodeGroup *g) {
   if (g->mi->kind == MK_RK5) {
     a.h_min = g->group_param[0] * time_resolution_;
     a.eps = g->rk5_eps;
+    volatile float one = 1.0f;
+    a.inv_eps = one / g->rk5_eps;
   }
   a.dt = time_resolution_;
+  // the dendritic delay in steps as the update kernels round it, formed once
+  // here for a group-wide value (IEEE float division, then roundf)
+  if (g->mi->den_delay_param >= 0) {
+    volatile float den = g->p_uval[g->mi->den_delay_param];
+    a.den_steps = (int)roundf(den / time_resolution_);
+  }
   group_constants(g, time_resolution_, a.gc);
   a.variant = g->rk5_variant;
   a.dry = 0;

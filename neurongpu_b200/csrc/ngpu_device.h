@@ -185,6 +185,8 @@ struct GroupArgs {
   float h_min;
   float dt;                     // time resolution (ms)
   float eps;                    // RK5 tolerance
+  float inv_eps;                // 1 / eps (IEEE division on the host)
+  int den_steps;                // round(den_delay / dt) of the uniform value
   int den_delay_col;            // param column of den_delay or -1
   unsigned long long *blk_evals;  // per-block RK5 derivative evaluations
   Rk5Queue q;                   // straggler queue of the single-group launch

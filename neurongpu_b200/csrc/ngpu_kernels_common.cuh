@@ -135,7 +135,16 @@ __device__ __forceinline__ unsigned direct_count(double t_rel, float start, floa
       Philox4 r = ng_random_block(seed, RNG_TAG_POISSON_DIRECT, stream, T_prev, 0);
       const double u = ng_u01(r.v[0], r.v[1]);
       if (lam > 0.0) {
-        while (n < NGPU_CDF_LEN - 1 && u > cdf[n]) n++;
+        // the first index k with u <= cdf[k] (NGPU_CDF_LEN - 1 at most). The
+        // table does not decrease, so below 8 that index is the number of
+        // the first 8 entries under u: 8 independent loads and compares
+        // instead of a chain of dependent loads; the search goes on from 8
+        // only in the rare case that all 8 are under u.
+#pragma unroll
+        for (int k = 0; k < 8; k++) n += (u > cdf[k]) ? 1u : 0u;
+        if (n == 8) {
+          while (n < NGPU_CDF_LEN - 1 && u > cdf[n]) n++;
+        }
       }
     }
   } else {
@@ -451,8 +460,10 @@ __device__ __forceinline__ void rk5_resume(const GroupArgs &g, const PushArgs &p
   const long long it = ctx->it;
   const double x1 = ctx->t0 + (double)g.dt * (double)(it + 1);
   const long long T = ctx->T0 + it + 1;
-  const float inv_eps = 1.0f / g.eps;
-  const int den = (int)roundf(p[Tr::den] / g.dt);
+  const float inv_eps = g.inv_eps;
+  // group-wide dendritic delay: the steps formed on the host
+  const int den = (UNI && g.den_delay_col == Tr::den) ? g.den_steps
+                                                       : (int)roundf(p[Tr::den] / g.dt);
   bool end_step = false;
   while (!end_step) {
     end_step = rk5_plain_substep<M, NP>(g, pa, ctx, i, y, x, h, refr, guard, p, q, np, inv_eps,
@@ -579,9 +590,11 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
              (active ? (double)(pre_col ? pre_col[M::NVAR + 2] : g.dx[i]) : 0.0);
   float h = active ? (pre_col ? pre_col[M::NVAR + 1] : g.h[i]) : 0.0f;
   const float h_min = g.h_min;
-  const float inv_eps = 1.0f / g.eps;
+  const float inv_eps = g.inv_eps;
   const long long T = T0 + it + 1;
-  const int den = (int)roundf(p[Tr::den] / g.dt);
+  // group-wide dendritic delay: the steps formed on the host
+  const int den = (UNI && g.den_delay_col == Tr::den) ? g.den_steps
+                                                       : (int)roundf(p[Tr::den] / g.dt);
   bool end_step = !active;
   int guard = 0;
   float h_acc, err_acc;
