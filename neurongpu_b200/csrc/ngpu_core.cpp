@@ -1045,8 +1045,9 @@ InputArgs NeuronGPU::MakeInputArgs(NodeGroup *g) {
 }
 
 // Whether Poisson direct connections into group g may draw
-// NGPU_POISSON_INV_MAX or more expected spikes per step; the RK5 update
-// kernels leave those to LaunchPoissonLarge. Generator rates change only
+// NGPU_POISSON_INV_MAX or more expected spikes per step; the update kernels
+// of RK5 neurons, simple-model neurons and parrots leave those to
+// LaunchPoissonLarge. Generator rates change only
 // between simulation calls and a change re-captures the step graphs, so the
 // answer holds for every step of a captured graph.
 bool NeuronGPU::HasLargePoisson(const NodeGroup *g) const {
@@ -1675,10 +1676,18 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
       case MK_IZH_PSC_EXP:
         if (g->in_simple_batch) {
           // the whole batch is launched once, at its first group
-          if (simple_batch_.groups[0] == g)
+          if (simple_batch_.groups[0] == g) {
+            for (NodeGroup *bg : simple_batch_.groups) {
+              if (HasLargePoisson(bg))
+                LaunchPoissonLarge(MakeGroupArgs(bg), MakeInputArgs(bg), ctx, stream_);
+            }
             LaunchSimpleBatch(simple_batch_.d_segs, simple_batch_.d_blk_seg,
                               simple_batch_.n_blocks, ctx, stream_);
-        } else if (mi->kind == MK_IAF_PSC_EXP) {
+          }
+          break;
+        }
+        if (HasLargePoisson(g)) LaunchPoissonLarge(MakeGroupArgs(g), MakeInputArgs(g), ctx, stream_);
+        if (mi->kind == MK_IAF_PSC_EXP) {
           LaunchIafPscExpUpdate(MakeGroupArgs(g), MakeInputArgs(g), MakePushArgs(g), ctx, stream_);
         } else {
           LaunchSimpleNeuronUpdate(mi->kind, mi->n_sub, MakeGroupArgs(g), MakeInputArgs(g),
@@ -1689,6 +1698,7 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
         if (g->d_sg_off) LaunchSpikeGeneratorUpdate(MakeGroupArgs(g), MakePushArgs(g), ctx, stream_);
         break;
       case MK_PARROT:
+        if (HasLargePoisson(g)) LaunchPoissonLarge(MakeGroupArgs(g), MakeInputArgs(g), ctx, stream_);
         LaunchParrotUpdate(MakeGroupArgs(g), MakeInputArgs(g), MakePushArgs(g), ctx, stream_);
         break;
       case MK_SPIKE_DETECTOR:

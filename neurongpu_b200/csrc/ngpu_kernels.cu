@@ -186,7 +186,7 @@ __device__ __forceinline__ void iaf_psc_exp_node(const GroupArgs &g, const Input
   float I_ex = var[i], I_in = var[n_pad + i];
   float V = var[2 * n_pad + i], refr = var[3 * n_pad + i];
   long long s[2];
-  input_sum<2>(in, i, n_pad, 2, it, t0, g.dt, ctx->poisson_pending, T0, s);
+  input_sum<2, false>(in, i, n_pad, 2, it, t0, g.dt, ctx->poisson_pending, T0, s);
   if (s[0] != 0) I_ex = fold_value(I_ex, s[0], 1.0f);
   if (s[1] != 0) I_in = fold_value(I_in, s[1], 1.0f);
   const float I_e = gparam(g, 3, i), Theta = gparam(g, 4, i);
@@ -242,7 +242,7 @@ __device__ __forceinline__ void iaf_psc_exp_g_node(const GroupArgs &g, const Inp
   float *var = g.var;
   float I_syn = var[i], V = var[n_pad + i], refr = var[2 * n_pad + i];
   long long s[1];
-  input_sum<1>(in, i, n_pad, 1, it, t0, g.dt, ctx->poisson_pending, T0, s);
+  input_sum<1, false>(in, i, n_pad, 1, it, t0, g.dt, ctx->poisson_pending, T0, s);
   if (s[0] != 0) I_syn = fold_value(I_syn, s[0], 1.0f);
   const float I_e = gparam(g, 0, i);
   if (refr > 0.0f) {
@@ -279,7 +279,7 @@ __device__ __forceinline__ void izhikevich_node(const GroupArgs &g, const InputA
   float I_syn = var[i], V = var[n_pad + i], u = var[2 * n_pad + i];
   float refr = var[3 * n_pad + i];
   long long s[1];
-  input_sum<1>(in, i, n_pad, 1, it, t0, g.dt, ctx->poisson_pending, T0, s);
+  input_sum<1, false>(in, i, n_pad, 1, it, t0, g.dt, ctx->poisson_pending, T0, s);
   if (s[0] != 0) I_syn = fold_value(I_syn, s[0], 1.0f);
   const float I_e = gparam(g, 0, i);
   const float h = g.gc[6], a = g.gc[1], b = g.gc[2];
@@ -323,7 +323,7 @@ __device__ __forceinline__ void izh_psc_exp_node(const GroupArgs &g, const Input
   float I_syn = var[i], V = var[n_pad + i], u = var[2 * n_pad + i];
   float refr = var[3 * n_pad + i];
   long long s[1];
-  input_sum<1>(in, i, n_pad, 1, it, t0, g.dt, ctx->poisson_pending, T0, s);
+  input_sum<1, false>(in, i, n_pad, 1, it, t0, g.dt, ctx->poisson_pending, T0, s);
   if (s[0] != 0) I_syn = fold_value(I_syn, s[0], 1.0f);
   const float I_e = gparam(g, 0, i);
   const float h = g.gc[6], a = g.gc[1], b = g.gc[2], C_syn = g.gc[7];
@@ -438,7 +438,7 @@ __global__ void k_parrot(GroupArgs g, InputArgs in, PushArgs pa,
   const int n_pad = g.n_pad;
   float *var = g.var;
   long long s[2];
-  input_sum<2>(in, i, n_pad, 2, it, t0, g.dt, ctx->poisson_pending, T0, s);
+  input_sum<2, false>(in, i, n_pad, 2, it, t0, g.dt, ctx->poisson_pending, T0, s);
   float sh = var[i];
   if (s[0] != 0) sh = fold_value(sh, s[0], 1.0f);
   if (s[1] != 0) var[n_pad + i] = fold_value(var[n_pad + i], s[1], 0.0f);
@@ -559,9 +559,9 @@ __global__ void k_fold_input(GroupArgs g, InputArgs in, StepCtx *ctx) {
 }
 
 // Poisson direct connections of NGPU_POISSON_INV_MAX or more expected spikes
-// per step into an RK5 group: drawn here, before the group's update, and
-// added into the accumulator half that the update folds (the update kernels
-// leave these connections out). The draws are the ones the update would make
+// per step into a group of RK5 neurons, simple-model neurons or parrots:
+// drawn here, before the group's update, and added into the accumulator half
+// that the update folds (those update kernels leave these connections out). The draws are the ones the update would make
 // and the accumulators hold fixed-point integers, so the folded input is the
 // same bit for bit. One thread per node, the only writer of its slots at
 // this point of the step (the delivery that filled this half has finished).

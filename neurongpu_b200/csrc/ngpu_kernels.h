@@ -64,9 +64,9 @@ void LaunchPoissonNodesUpdate(const GroupArgs &g, const PushArgs &pa,
 void LaunchFoldInput(const GroupArgs &g, const InputArgs &in, StepCtx *ctx,
                      cudaStream_t s);
 void LaunchClearPending(StepCtx *ctx, cudaStream_t s);
-// draws an RK5 group's Poisson direct connections of NGPU_POISSON_INV_MAX or
-// more expected spikes per step into its accumulators (before its update,
-// which leaves them out)
+// draws a group's Poisson direct connections of NGPU_POISSON_INV_MAX or more
+// expected spikes per step into its accumulators (before the update of RK5
+// neurons, simple-model neurons or parrots, which leaves them out)
 void LaunchPoissonLarge(const GroupArgs &g, const InputArgs &in, StepCtx *ctx,
                         cudaStream_t s);
 

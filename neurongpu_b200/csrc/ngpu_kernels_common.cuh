@@ -158,9 +158,10 @@ __device__ __forceinline__ unsigned direct_count(double t_rel, float start, floa
 // drawn for the previous step. pre_acc: the accumulator values already
 // fetched (port q at pre_acc[q]), or null. LARGE = false leaves out the
 // connections of NGPU_POISSON_INV_MAX or more expected spikes per step:
-// the RK5 update kernels use it, and k_poisson_large adds those draws into
-// the accumulators before them (the large-rate sampler needs many registers,
-// and inlined it raised the update kernels' register count and spills).
+// the update kernels of RK5 neurons, simple-model neurons and parrots use it,
+// and k_poisson_large adds those draws into the accumulators before them
+// (the large-rate sampler needs many registers, and inlined it raised the
+// update kernels' register count and spills).
 template <int NP, bool LARGE = true>
 __device__ __forceinline__ void input_sum(const InputArgs &in, int i,
                                           int n_pad, int np, long long it,
