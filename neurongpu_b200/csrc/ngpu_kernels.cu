@@ -688,8 +688,6 @@ __device__ __forceinline__ void step_bookkeeping(int *ring_cnt, int ring_R, int 
 template <bool PLASTIC>
 __global__ void __launch_bounds__(256)
 k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
-  __shared__ int s_pref[NGPU_MAX_DELAYS + 1];
-  __shared__ int s_slot[NGPU_MAX_DELAYS];
   const long long T = ctx->T0 + ctx->it + 1;
   long long *const acc = d.acc + ((T & 1) ? d.acc_par : 0);   // folded by the update of T + 1
   if (d.step_book && blockIdx.x == 0 && threadIdx.x == 0)
@@ -698,89 +696,11 @@ k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int n_warps = (gridDim.x * blockDim.x) >> 5;
   const bool warp_scan = d.nd <= 32;
-  // per-delay spike counts and their prefix: in registers of every warp when
-  // there are at most 32 distinct delays, else in shared memory
-  int my_slot = 0, my_incl = 0, total;
-  if (warp_scan) {
-    int c = 0;
-    if (lane < d.nd) {
-      int slot = (int)((T - d.delays[lane]) % d.ring_R);
-      if (slot < 0) slot += d.ring_R;
-      my_slot = slot;
-      c = d.ring_cnt[slot];
-      c = c < d.ring_C ? c : d.ring_C;
-    }
-    my_incl = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int v = __shfl_up_sync(0xffffffffu, my_incl, o);
-      if (lane >= o) my_incl += v;
-    }
-    total = __shfl_sync(0xffffffffu, my_incl, 31);
-  } else {
-    // block-wide scan, blockDim.x delays per round: warp scans, then a scan
-    // of the warp totals by warp 0, plus the carry of earlier rounds
-    __shared__ int s_wsum[8];
-    const int wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    int carry = 0;
-    for (int base = 0; base < d.nd; base += blockDim.x) {
-      const int di = base + threadIdx.x;
-      int c = 0;
-      if (di < d.nd) {
-        int slot = (int)((T - d.delays[di]) % d.ring_R);
-        if (slot < 0) slot += d.ring_R;
-        s_slot[di] = slot;
-        c = d.ring_cnt[slot];
-        c = c < d.ring_C ? c : d.ring_C;
-      }
-      int x = c;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-      }
-      if (lane == 31) s_wsum[wid] = x;
-      __syncthreads();
-      if (wid == 0) {
-        int w = lane < nw ? s_wsum[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int y = __shfl_up_sync(0xffffffffu, w, o);
-          if (lane >= o) w += y;
-        }
-        if (lane < nw) s_wsum[lane] = w;
-      }
-      __syncthreads();
-      if (di < d.nd) s_pref[di + 1] = carry + (wid > 0 ? s_wsum[wid - 1] : 0) + x;
-      carry += s_wsum[nw - 1];
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) s_pref[0] = 0;
-    __syncthreads();
-    total = s_pref[d.nd];
-  }
   unsigned long long events = 0;
-  for (int item = warp; item < total; item += n_warps) {
-    int di, slot, base;
-    if (warp_scan) {
-      // first delay whose inclusive prefix exceeds the item
-      // (item < total, so some lane's inclusive prefix exceeds it)
-      unsigned m = __ballot_sync(0xffffffffu, my_incl > item);
-      di = __ffs(m) - 1;
-      slot = __shfl_sync(0xffffffffu, my_slot, di);
-      const int prev = __shfl_sync(0xffffffffu, my_incl, di > 0 ? di - 1 : 0);
-      base = di > 0 ? prev : 0;
-    } else {
-      int lo = 0, hi = d.nd;          // find di with s_pref[di] <= item
-      while (hi - lo > 1) {
-        int mid = (lo + hi) >> 1;
-        if (s_pref[mid] <= item) lo = mid; else hi = mid;
-      }
-      di = lo;
-      slot = s_slot[di];
-      base = s_pref[di];
-    }
-    const long long k = (long long)slot * d.ring_C + (item - base);
+  // the edges of one (spike, delay) item: spike j of ring slot `slot` at
+  // distinct-delay index di; called by whole warps
+  auto deliver_item = [&](int di, int slot, int j) {
+    const long long k = (long long)slot * d.ring_C + j;
     const unsigned src = d.ring_src[k];
     const float height = d.ring_h[k];
     const unsigned long long gi = (unsigned long long)src * d.nd + di;
@@ -847,6 +767,50 @@ k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
             }
           }
         }
+      }
+    }
+  };
+  if (warp_scan) {
+    // per-delay spike counts and their prefix in registers of every warp
+    int my_slot = 0, my_incl = 0, total;
+    int c = 0;
+    if (lane < d.nd) {
+      int slot = (int)((T - d.delays[lane]) % d.ring_R);
+      if (slot < 0) slot += d.ring_R;
+      my_slot = slot;
+      c = d.ring_cnt[slot];
+      c = c < d.ring_C ? c : d.ring_C;
+    }
+    my_incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int v = __shfl_up_sync(0xffffffffu, my_incl, o);
+      if (lane >= o) my_incl += v;
+    }
+    total = __shfl_sync(0xffffffffu, my_incl, 31);
+    for (int item = warp; item < total; item += n_warps) {
+      // first delay whose inclusive prefix exceeds the item
+      // (item < total, so some lane's inclusive prefix exceeds it)
+      const unsigned m = __ballot_sync(0xffffffffu, my_incl > item);
+      const int di = __ffs(m) - 1;
+      const int slot = __shfl_sync(0xffffffffu, my_slot, di);
+      const int prev = __shfl_sync(0xffffffffu, my_incl, di > 0 ? di - 1 : 0);
+      deliver_item(di, slot, item - (di > 0 ? prev : 0));
+    }
+  } else {
+    // more than 32 distinct delays: every delay has a fixed set of G warps,
+    // which read its spike count themselves and take its spikes in turn (no
+    // prefix over the delays, no search); with fewer warps than delays each
+    // warp takes every n_warps-th delay
+    const bool per_delay = n_warps >= d.nd;
+    const int G = per_delay ? n_warps / d.nd : 1;
+    if (!per_delay || warp < G * d.nd) {
+      for (int di = per_delay ? warp % d.nd : warp; di < d.nd; di += per_delay ? d.nd : n_warps) {
+        int slot = (int)((T - d.delays[di]) % d.ring_R);
+        if (slot < 0) slot += d.ring_R;
+        int c = d.ring_cnt[slot];
+        c = c < d.ring_C ? c : d.ring_C;
+        for (int j = per_delay ? warp / d.nd : 0; j < c; j += G) deliver_item(di, slot, j);
       }
     }
   }
