@@ -13,6 +13,7 @@
 #include <stdio.h>
 #include <string.h>
 #include <algorithm>
+#include <functional>
 #include <chrono>
 #include <cstdlib>
 
@@ -976,6 +977,7 @@ GroupArgs NeuronGPU::MakeGroupArgs(NodeGroup *g) {
   a.den_delay_col = g->mi->den_delay_param;
   a.blk_evals = g->d_blk_evals;
   a.q = g->q;
+  if (g->queue_off) a.q.cap = 0;
   a.step_mode = g->step_mode;
   a.mlp_margin = mlp_margin_;
   a.mlp = d_mlp_img_;
@@ -1872,6 +1874,37 @@ int NeuronGPU::FlushInput() {
 // RK5 autotuner: times every kernel variant of a group on the live state in
 // dry mode (full computation, no stores) and keeps the fastest. The variants
 // differ only in their register cap (occupancy), not in arithmetic.
+// sum of a device array of per-block counters
+static unsigned long long sum_counters(const unsigned long long *d, int n) {
+  if (d == nullptr || n <= 0) return 0;
+  std::vector<unsigned long long> v(n);
+  NGPU_CUDA(cudaMemcpy(v.data(), d, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost));
+  unsigned long long t = 0;
+  for (auto x : v) t += x;
+  return t;
+}
+
+// median of three timed launches of f on stream s, after one untimed
+static float median_launch_ms(cudaStream_t s, const std::function<void()> &f) {
+  cudaEvent_t e0, e1;
+  NGPU_CUDA(cudaEventCreate(&e0));
+  NGPU_CUDA(cudaEventCreate(&e1));
+  f();
+  float t[3];
+  for (int r = 0; r < 3; r++) {
+    NGPU_CUDA(cudaEventRecord(e0, s));
+    f();
+    NGPU_CUDA(cudaEventRecord(e1, s));
+    NGPU_CUDA(cudaEventSynchronize(e1));
+    NGPU_CUDA(cudaEventElapsedTime(&t[r], e0, e1));
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  NGPU_CUDA(cudaGetLastError());
+  std::sort(t, t + 3);
+  return t[1];
+}
+
 void NeuronGPU::TuneRk5(NodeGroup *g) {
   g->tuned = true;
   const char *force = getenv("NGB200_RK5_VARIANT");
@@ -1891,34 +1924,85 @@ void NeuronGPU::TuneRk5(NodeGroup *g) {
   in.dry = 1;
   a.blk_evals = nullptr;
   a.step_mode = STEP_PLAIN;       // the variants exist for the plain controller
-  cudaEvent_t e0, e1;
-  NGPU_CUDA(cudaEventCreate(&e0));
-  NGPU_CUDA(cudaEventCreate(&e1));
-  int best = 0;
-  float best_ms = 1e30f;
+  // every variant with and without the straggler queue (four dry steps back
+  // to back, so that the queue's extra launch in the chain shows); the
+  // queue goes off only if the best variant without it is at least 3 %
+  // faster than the best with it
+  const Rk5Queue q_on = g->q;
+  auto run = [&] {
+    for (int k = 0; k < 4; k++)
+      LaunchRk5Update(g->mi->rk5_model, g->n_port, a, in, pa, d_ctx_, stream_);
+  };
+  int best_on = 0, best_off = -1;
+  float ms_on = 1e30f, ms_off = 1e30f;
   for (int v = 0; v < nv; v++) {
     a.variant = v;
-    LaunchRk5Update(g->mi->rk5_model, g->n_port, a, in, pa, d_ctx_, stream_);
-    float t[3];
-    for (int r = 0; r < 3; r++) {
-      NGPU_CUDA(cudaEventRecord(e0, stream_));
-      LaunchRk5Update(g->mi->rk5_model, g->n_port, a, in, pa, d_ctx_, stream_);
-      NGPU_CUDA(cudaEventRecord(e1, stream_));
-      NGPU_CUDA(cudaEventSynchronize(e1));
-      NGPU_CUDA(cudaEventElapsedTime(&t[r], e0, e1));
+    a.q = q_on;
+    const float t_on = median_launch_ms(stream_, run) / 4.0f;
+    g->tune_ms[v] = t_on;
+    if (t_on < ms_on) {
+      ms_on = t_on;
+      best_on = v;
     }
-    std::sort(t, t + 3);
-    g->tune_ms[v] = t[1];
-    if (t[1] < best_ms) {
-      best_ms = t[1];
-      best = v;
+    if (q_on.cap > 0 && !g->queue_keep) {
+      a.q.cap = 0;
+      const float t_off = median_launch_ms(stream_, run) / 4.0f;
+      if (t_off < ms_off) {
+        ms_off = t_off;
+        best_off = v;
+      }
     }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  NGPU_CUDA(cudaGetLastError());
-  g->rk5_variant = best;
+  g->queue_off = best_off >= 0 && ms_off < 0.97f * ms_on;
+  g->rk5_variant = g->queue_off ? best_off : best_on;
+  g->queue_checked = steps_total_;
+  g->evals_mark = sum_counters(g->d_blk_evals, g->n_blocks);
   InvalidateGraphs();
+}
+
+
+
+// The straggler queue adds a launch (the finishing grid) to every step's
+// chain of launches, which pays only while some neurons take extra
+// sub-steps; the autotuner switches it off for a group or batch that runs
+// at least 3 % faster without it (the network was quiet when it was timed).
+// Every kQueueRecheckSteps steps such a group's stage evaluations per
+// neuron-step are read from its per-block counters: one RK5 attempt per
+// step is 6 evaluations, and above 6.06 (neurons have begun to take extra
+// sub-steps) the queue goes back on for good and the group's variant is
+// tuned again. The results are the same with and without the queue.
+void NeuronGPU::RecheckRk5Queues() {
+  const double kEvalsQuiet = 6.06;
+  for (Rk5BatchHost &b : batches_) {
+    const long long ds = steps_total_ - b.queue_checked;
+    if (!b.tuned || !b.queue_off || ds < kQueueRecheckSteps) continue;
+    long long n = 0;
+    for (NodeGroup *g : b.groups) n += g->n_node;
+    const unsigned long long e = sum_counters(b.d_blk_evals, b.n_blocks);
+    if ((double)(e - b.evals_mark) > kEvalsQuiet * (double)n * (double)ds) {
+      b.queue_off = false;
+      b.queue_keep = true;
+      b.tuned = false;
+      InvalidateGraphs();
+    }
+    b.evals_mark = e;
+    b.queue_checked = steps_total_;
+  }
+  for (NodeGroup *g : groups_) {
+    const long long ds = steps_total_ - g->queue_checked;
+    if (g->mi->kind != MK_RK5 || g->batch >= 0 || !g->tuned || !g->queue_off ||
+        ds < kQueueRecheckSteps)
+      continue;
+    const unsigned long long e = sum_counters(g->d_blk_evals, g->n_blocks);
+    if ((double)(e - g->evals_mark) > kEvalsQuiet * (double)g->n_node * (double)ds) {
+      g->queue_off = false;
+      g->queue_keep = true;
+      g->tuned = false;
+      InvalidateGraphs();
+    }
+    g->evals_mark = e;
+    g->queue_checked = steps_total_;
+  }
 }
 
 bool NeuronGPU::TunePending() {
@@ -2095,6 +2179,7 @@ Rk5Batch NeuronGPU::MakeRk5Batch(const Rk5BatchHost &b) {
   r.blk_seg = b.d_blk_seg;
   r.blk_evals = b.d_blk_evals;
   r.q = b.q;
+  if (b.queue_off) r.q.cap = 0;
   return r;
 }
 
@@ -2117,33 +2202,35 @@ void NeuronGPU::TuneRk5Batch(Rk5BatchHost &b) {
   r.dry = 1;
   r.blk_evals = nullptr;
   r.mode = STEP_PLAIN;
-  cudaEvent_t e0, e1;
-  NGPU_CUDA(cudaEventCreate(&e0));
-  NGPU_CUDA(cudaEventCreate(&e1));
-  int best = 0;
-  float best_ms = 1e30f;
+  // every variant with and without the straggler queue, as TuneRk5
+  const Rk5Queue q_on = b.q;
+  auto run = [&] {
+    for (int k = 0; k < 4; k++) LaunchRk5Batch(r, d_ctx_, stream_);
+  };
+  int best_on = 0, best_off = -1;
+  float ms_on = 1e30f, ms_off = 1e30f;
   for (int v = 0; v < nv; v++) {
     r.variant = v;
-    LaunchRk5Batch(r, d_ctx_, stream_);
-    float t[3];
-    for (int k = 0; k < 3; k++) {
-      NGPU_CUDA(cudaEventRecord(e0, stream_));
-      LaunchRk5Batch(r, d_ctx_, stream_);
-      NGPU_CUDA(cudaEventRecord(e1, stream_));
-      NGPU_CUDA(cudaEventSynchronize(e1));
-      NGPU_CUDA(cudaEventElapsedTime(&t[k], e0, e1));
+    r.q = q_on;
+    const float t_on = median_launch_ms(stream_, run) / 4.0f;
+    b.tune_ms[v] = t_on;
+    if (t_on < ms_on) {
+      ms_on = t_on;
+      best_on = v;
     }
-    std::sort(t, t + 3);
-    b.tune_ms[v] = t[1];
-    if (t[1] < best_ms) {
-      best_ms = t[1];
-      best = v;
+    if (q_on.cap > 0 && !b.queue_keep) {
+      r.q.cap = 0;
+      const float t_off = median_launch_ms(stream_, run) / 4.0f;
+      if (t_off < ms_off) {
+        ms_off = t_off;
+        best_off = v;
+      }
     }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  NGPU_CUDA(cudaGetLastError());
-  b.variant = best;
+  b.queue_off = best_off >= 0 && ms_off < 0.97f * ms_on;
+  b.variant = b.queue_off ? best_off : best_on;
+  b.queue_checked = steps_total_;
+  b.evals_mark = sum_counters(b.d_blk_evals, b.n_blocks);
   InvalidateGraphs();
 }
 
@@ -2275,6 +2362,7 @@ int NeuronGPU::Simulate() {
     input_pending_ = true;
     steps_total_ += n;
     if (steps_total_ >= kTuneSteps && TunePending()) TuneAll();
+    RecheckRk5Queues();
   }
   neural_time_ = neur_t0_ + (double)time_resolution_ * (double)Nt_;
   NGPU_CUDA(cudaEventRecord(ev_stop_, stream_));

@@ -132,6 +132,10 @@ struct NodeGroup {
   int rk5_variant = 1;
   bool tuned = false;
   float tune_ms[6] = {0, 0, 0, 0, 0, 0};
+  bool queue_off = false;       // the autotuner switched the straggler queue off
+  long long queue_checked = 0;  // steps_total_ at the last choice or check
+  unsigned long long evals_mark = 0;  // stage evaluations counted by then
+  bool queue_keep = false;      // the queue came back on: later tunings keep it
   // index of the batched RK5 launch this group belongs to, or -1
   int batch = -1;
   // updated by the batched launch of simple models
@@ -316,6 +320,11 @@ class NeuronGPU {
   long long steps_total_ = 0;
   bool TunePending();
   void TuneAll();
+  // the autotuner chooses the variant and whether the straggler queue is
+  // used together; groups and batches without the queue are checked every
+  // kQueueRecheckSteps steps (RecheckRk5Queues)
+  static const long long kQueueRecheckSteps = 1000;
+  void RecheckRk5Queues();
   // RK5 groups of one model and port count are integrated by one launch
   // per step (segment table) unless batching is switched off
   int SetRk5Batching(int on);
@@ -370,6 +379,10 @@ class NeuronGPU {
     int variant = 1;
     bool tuned = false;
     float tune_ms[6] = {0, 0, 0, 0, 0, 0};
+    bool queue_off = false;
+    long long queue_checked = 0;
+    unsigned long long evals_mark = 0;
+    bool queue_keep = false;
     SegArgs *d_segs = nullptr;
     int *d_blk_seg = nullptr;
     unsigned long long *d_blk_evals = nullptr;

@@ -809,8 +809,10 @@ template <class M, int NP, bool UNI>
 __global__ void __launch_bounds__(NGPU_BLOCK, 1)
 k_rk5_finish(const __grid_constant__ GroupArgs g, const __grid_constant__ InputArgs in,
              const __grid_constant__ PushArgs pa, StepCtx *ctx) {
-  pdl_wait();
+  // the next launch may be scheduled at once (its own wait still holds it
+  // until this grid has completed); then wait for the update's records
   pdl_trigger();
+  pdl_wait();
   __shared__ unsigned s_pref[NGPU_QLANES + 1];
   const unsigned n = rk5_queue_prefix(g.q, s_pref);
   if (n == 0) return;             // the same for every block: nothing to reset
@@ -864,8 +866,10 @@ template <class M, int NP, bool UNI>
 __global__ void __launch_bounds__(NGPU_BLOCK, 1)
 k_rk5_finish_seg(const SegArgs *__restrict__ segs, unsigned long long *blk_evals, int dry,
                  StepCtx *ctx, const __grid_constant__ Rk5Queue qu) {
-  pdl_wait();
+  // the next launch may be scheduled at once (its own wait still holds it
+  // until this grid has completed); then wait for the update's records
   pdl_trigger();
+  pdl_wait();
   __shared__ unsigned s_pref[NGPU_QLANES + 1];
   const unsigned n = rk5_queue_prefix(qu, s_pref);
   if (n == 0) return;             // the same for every block: nothing to reset
