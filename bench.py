@@ -129,12 +129,12 @@ def measured_peaks():
 # DRAM traffic and executed instructions per unit, from ncu captures of the
 # same kernels (dram__bytes_read.sum + dram__bytes_write.sum and
 # smsp__inst_executed.sum per launch, divided by the neurons / warps / events
-# of the launch): RK5 update (6-blocks/SM variant) on the silent network at
+# of the launch): RK5 update (8-blocks/SM variant) on the silent network at
 # 200,000 neurons in steady state (cold cache; the state's writes stay in L2
 # during the launch), delivery on the active network at 400,000 neurons.
 TRAFFIC_RK5_PER_NEURON_STEP = 52.4       # bytes
 TRAFFIC_DELIVER_PER_EVENT = 11.3         # bytes
-INST_RK5_PER_WARP_STEP = 974.2           # warp instructions per 32 neuron-steps
+INST_RK5_PER_WARP_STEP = 995.2           # warp instructions per 32 neuron-steps
 SM_COUNT, SMSP_PER_SM = 148, 4
 
 
