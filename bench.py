@@ -37,18 +37,21 @@ BYTES_PER_NEURON_STEP = 72     # algorithmic: state r+w, h r+w, port inputs
 BYTES_PER_EVENT = 8            # algorithmic: 4 B target slot + 4 B weight
 
 
-def build_network(ngpu, cfg, seed=1234):
+def build_network(ngpu, cfg, seed=1234, eps_param=True):
     """The scale network through the drop-in API. Delays are drawn per
     connection group: for every delay value d in 1..5 ms each neuron gets
     k_exc/5 excitatory and k_inh/5 inhibitory inputs, i.e. the integer
-    delays are uniform over the 5 values."""
+    delays are uniform over the 5 values. eps_param: set the RK5 tolerance
+    as the group parameter rk5_eps (a library whose tolerance is a fixed
+    constant, as the reference's, is given it otherwise)."""
     ngpu.SetKernelStatus("rnd_seed", seed)
     pg = ngpu.Create("poisson_generator")
     ngpu.SetStatus(pg, "rate", cfg["rate"])
     n = cfg["n"]
     nrn = ngpu.Create("aeif_cond_beta", n, 2)
     ngpu.SetStatus(nrn, NEURON_PARAMS)
-    ngpu.SetNeuronGroupParam(nrn, "rk5_eps", cfg["eps"])
+    if eps_param:
+        ngpu.SetNeuronGroupParam(nrn, "rk5_eps", cfg["eps"])
     ne = int(0.8 * n)
     exc, inh = nrn[0:ne], nrn[ne:n]
     nd = len(cfg["delays"])

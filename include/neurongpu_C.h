@@ -290,15 +290,33 @@ double NGB200_KernelsPerStep();
  * 1 spike delivery, 2 STDP post rule, 3 recording and step bookkeeping. */
 int NGB200_SetKernelTiming(int on);
 int NGB200_GetKernelTiming(int kind, double *total_ms, long long *launches);
+/* RK5 sub-steps one neuron may take in one time step (default 200,000)
+ * before its update gives up on the step and Simulate fails with "RK5
+ * integration exceeded the substep limit" (the reference has no limit). */
+int NGB200_SetRk5MaxSubsteps(int n_substeps);
+/* Test hook for the time-out paths of the bounded device waits: mask bit 0
+ * makes the shared-memory prefetch wait of the persistent RK5 update and the
+ * first tensor-core wait of each step-proposer round give up after one
+ * non-blocking test, bit 1 the second tensor-core wait of a round; 0 (the
+ * default) restores normal waits. A wait that gives up sets its error bit,
+ * which the next Simulate reports; the kernels still wait (bounded) for
+ * their outstanding copies and tensor-core work before they exit. */
+int NGB200_SetWaitTest(int mask);
+/* Parity bookkeeping of a step-proposer round's completion barrier (host
+ * copy of the device function): the parity kept after a round that started
+ * at phase_in, whose first / second completion wait succeeded (ok1 / ok2). */
+unsigned NGB200_ProposerPhaseAfter(unsigned phase_in, int ok1, int ok2);
 /* RK5 kernel variant picked by the autotuner for the group of node i_node
  * (0 = no register cap, 1..3 = caps for 5, 6, 8 resident blocks per SM,
  * 4..5 = persistent kernel with shared-memory prefetch of the state, caps
- * for 5 and 6 blocks per SM) and, in ms6[0..5], the median device time (ms)
- * of each variant's timing launch (0 for variants not timed). The tuner runs
+ * for 5 and 6 blocks per SM, 6 = cap for 4 blocks per SM, 7..8 = persistent
+ * kernel with caps for 4 and 3 blocks per SM) and, in ms[0..8], the median
+ * device time (ms) of each variant's timing launch (0 for variants not
+ * timed). The tuner runs
  * once a simulation has integrated 200 steps, for groups with >= 16384
  * neurons; the environment variable NGB200_RK5_VARIANT forces a variant from
  * the first step, NGB200_AUTOTUNE=0 disables tuning. */
-int NGB200_GetRk5Tuning(int i_node, int *variant, float *ms6);
+int NGB200_GetRk5Tuning(int i_node, int *variant, float *ms);
 
 /* Standalone synaptic delivery, the simulator's delivery kernel applied to a
  * caller-owned graph and spike batch (all pointers are device memory):

@@ -20,8 +20,10 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["ngpu_kernels.cu", "ngpu_rk5_batch.cu", "ngpu_step_proposer.cu", "ngpu_connect_device.cu",
-              "ngpu_deliver_api.cu", "ngpu_deliver_static.cu"]
+CU_SOURCES = ["ngpu_kernels.cu", "ngpu_rk5_aeif_cond_beta.cu", "ngpu_rk5_aeif_cond_alpha.cu",
+              "ngpu_rk5_aeif_psc.cu", "ngpu_rk5_izh_cond_beta.cu", "ngpu_rk5_batch.cu",
+              "ngpu_step_proposer.cu", "ngpu_connect_device.cu", "ngpu_deliver_api.cu",
+              "ngpu_deliver_static.cu"]
 CPP_SOURCES = ["ngpu_core.cpp", "ngpu_connect.cpp", "neurongpu_C.cpp"]
 
 
@@ -60,7 +62,7 @@ def build(force=False, verbose=False):
     """Compiles every source and links the shared library; returns its path."""
     os.makedirs(OBJDIR, exist_ok=True)
     srcs = CU_SOURCES + CPP_SOURCES
-    with ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
+    with ThreadPoolExecutor(max_workers=min(max(os.cpu_count() or 1, 1), len(srcs))) as ex:
         objs = list(ex.map(lambda s: _compile(s, force, verbose), srcs))
     if (force or not os.path.exists(LIB)
             or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs)):

@@ -628,9 +628,18 @@ int NGB200_SetKernelTiming(int on) {
 int NGB200_GetKernelTiming(int kind, double *total_ms, long long *launches) {
   return guarded(0, [&](NeuronGPU *n) { return n->GetKernelTiming(kind, total_ms, launches); });
 }
+int NGB200_SetRk5MaxSubsteps(int n_substeps) {
+  return guarded(0, [&](NeuronGPU *n) { return n->SetRk5MaxSubsteps(n_substeps); });
+}
+int NGB200_SetWaitTest(int mask) {
+  return guarded(0, [&](NeuronGPU *n) { return n->SetWaitTest(mask); });
+}
+unsigned NGB200_ProposerPhaseAfter(unsigned phase_in, int ok1, int ok2) {
+  return ngpu::proposer_phase_after(phase_in, ok1 != 0, ok2 != 0);
+}
 
 }  // extern "C"
 
-extern "C" int NGB200_GetRk5Tuning(int i_node, int *variant, float *ms6) {
-  return guarded(0, [&](NeuronGPU *n) { return n->GetRk5Tuning(i_node, variant, ms6); });
+extern "C" int NGB200_GetRk5Tuning(int i_node, int *variant, float *ms) {
+  return guarded(0, [&](NeuronGPU *n) { return n->GetRk5Tuning(i_node, variant, ms); });
 }

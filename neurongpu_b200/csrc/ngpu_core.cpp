@@ -94,7 +94,7 @@ void NeuronGPU::FreeDevice() {
   rev_R_ = rev_C_ = 0;
   F(d_dc_off_); F(d_dc_gen_); F(d_dc_port_); F(d_dc_w_); F(d_dc_delay_);
   F(d_dc_stream_); F(d_gen_rate_); F(d_gen_origin_); F(d_gen_start_);
-  F(d_gen_stop_); F(d_gen_lambda_); F(d_gen_explam_); F(d_gen_cdf_); F(d_blk_events_); F(d_done_);
+  F(d_gen_stop_); F(d_gen_lambda_); F(d_gen_explam_); F(d_gen_thr_); F(d_blk_events_); F(d_done_);
   F(d_rec_cols_); F(d_rec_buf_);
   F(d_mlp_img_);
   d_mlp_img_ = nullptr;
@@ -960,11 +960,22 @@ GroupArgs NeuronGPU::MakeGroupArgs(NodeGroup *g) {
   }
   if (g->mi->kind == MK_RK5) {
     a.h_min = g->group_param[0] * time_resolution_;
+    {
+      // the reference's escape test h <= h_min * (1.0 + 1.0e-5) is a double
+      // comparison of the float h: the same as h <= the largest float that
+      // does not exceed the double threshold
+      const double thr = (double)a.h_min * (1.0 + 1.0e-5);
+      float f = (float)thr;
+      if ((double)f > thr) f = nextafterf(f, 0.0f);
+      a.h_min_thr = f;
+    }
     a.eps = g->rk5_eps;
     volatile float one = 1.0f;
     a.inv_eps = one / g->rk5_eps;
   }
   a.dt = time_resolution_;
+  a.max_substeps = rk5_max_substeps_;
+  a.wait_test = wait_test_;
   // the dendritic delay in steps as the update kernels round it, formed once
   // here for a group-wide value (IEEE float division, then roundf)
   if (g->mi->den_delay_param >= 0) {
@@ -1026,7 +1037,7 @@ InputArgs NeuronGPU::MakeInputArgs(NodeGroup *g) {
     in.gen_stop = d_gen_stop_;
     in.gen_lambda = d_gen_lambda_;
     in.gen_explam = d_gen_explam_;
-    in.gen_cdf = d_gen_cdf_;
+    in.gen_thr = d_gen_thr_;
   }
   if (g->ud && g->ud_gen < (int)gen_lam_h_.size()) {
     const int k = g->ud_gen;
@@ -1039,7 +1050,8 @@ InputArgs NeuronGPU::MakeInputArgs(NodeGroup *g) {
     in.ud_stop = gen_stop_h_[k];
     in.ud_lambda = gen_lam_h_[k];
     in.ud_explam = gen_explam_h_[k];
-    in.ud_cdf = d_gen_cdf_ + (size_t)k * NGPU_CDF_LEN;
+    in.ud_thr = d_gen_thr_ + (size_t)k * NGPU_CDF_LEN;
+    for (int j = 0; j < 8; j++) in.ud_thr8[j] = gen_thr_h_[(size_t)k * NGPU_CDF_LEN + j];
     in.ud_stream0 = g->ud_stream0;
   }
   in.seed = kernel_seed_;
@@ -1312,8 +1324,17 @@ void NeuronGPU::BuildDevice() {
   // max delay + 2 slots: the slot of step T + 1 is emptied during step T
   // while the delivery reads the slots of steps T - 1 ... T - max delay
   ring_R_ = maxD + 2;
-  ring_C_ = (int)std::min<long long>(0x7fffffffLL,
-                                     (long long)ceil((double)N * std::max(1.0f, max_spike_num_fact_)) + 64);
+  // spike-list capacity per step: nodes x max_spike_num_fact (with a margin
+  // of 64 for a node spiking twice in one step at the default factor 1); a
+  // factor below 1 is honoured as set, as the reference sizes its spike
+  // array from it (src/neurongpu.cu:294), and a step with more spikes sets
+  // DERR_RING_OVERFLOW
+  {
+    const double want = (double)N * (double)max_spike_num_fact_;
+    const long long c = max_spike_num_fact_ >= 1.0f ? (long long)ceil(want) + 64
+                                                    : std::max(1LL, (long long)ceil(want));
+    ring_C_ = (int)std::min<long long>(0x7fffffffLL, c);
+  }
   NGPU_CUDA(cudaMalloc(&d_ring_src_, sizeof(unsigned) * (size_t)ring_R_ * ring_C_));
   NGPU_CUDA(cudaMalloc(&d_ring_h_, sizeof(float) * (size_t)ring_R_ * ring_C_));
   NGPU_CUDA(cudaMalloc(&d_ring_cnt_, sizeof(int) * ring_R_));
@@ -1414,7 +1435,7 @@ void NeuronGPU::BuildDevice() {
     NGPU_CUDA(cudaMalloc(&d_gen_stop_, sizeof(float) * n_gen_));
     NGPU_CUDA(cudaMalloc(&d_gen_lambda_, sizeof(double) * n_gen_));
     NGPU_CUDA(cudaMalloc(&d_gen_explam_, sizeof(double) * n_gen_));
-    NGPU_CUDA(cudaMalloc(&d_gen_cdf_, sizeof(double) * n_gen_ * NGPU_CDF_LEN));
+    NGPU_CUDA(cudaMalloc(&d_gen_thr_, sizeof(unsigned) * n_gen_ * NGPU_CDF_LEN));
   }
   // counters, per-group device extras and calibration
   // one full wave of resident delivery blocks (grid-stride over the items)
@@ -1517,7 +1538,7 @@ void NeuronGPU::UploadGeneratorParams() {
   if (n_gen_ == 0) return;
   std::vector<float> rate(n_gen_), origin(n_gen_), start(n_gen_), stop(n_gen_);
   std::vector<double> lam(n_gen_), explam(n_gen_);
-  std::vector<double> cdf((size_t)n_gen_ * NGPU_CDF_LEN);
+  std::vector<unsigned> thr((size_t)n_gen_ * NGPU_CDF_LEN);
   const float time_step = (float)(time_resolution_ / 1000.0);
   for (int k = 0; k < n_gen_; k++) {
     int node = gen_nodes_[k];
@@ -1531,20 +1552,15 @@ void NeuronGPU::UploadGeneratorParams() {
     float lf = time_step * rate[k];      // float product, as in src/poiss_gen.cu:62
     lam[k] = (double)lf;
     explam[k] = exp(-(double)lf);
-    // CDF by the recurrence of ng_poisson_inversion (same double operations)
-    double pk = explam[k], F = pk;
-    cdf[(size_t)k * NGPU_CDF_LEN] = F;
-    for (int n = 1; n < NGPU_CDF_LEN; n++) {
-      pk = (pk * lam[k]) / (double)n;
-      F = F + pk;
-      cdf[(size_t)k * NGPU_CDF_LEN + n] = F;
-    }
+    // inversion thresholds of the direct-connection sampler
+    ng_poisson_thresholds(lam[k], explam[k], thr.data() + (size_t)k * NGPU_CDF_LEN);
   }
   // unchanged generator parameters keep the captured step graphs valid
   if (gen_lam_h_ == lam && gen_origin_h_ == origin && gen_start_h_ == start &&
       gen_stop_h_ == stop)
     return;
-  NGPU_CUDA(cudaMemcpy(d_gen_cdf_, cdf.data(), sizeof(double) * cdf.size(), cudaMemcpyHostToDevice));
+  NGPU_CUDA(cudaMemcpy(d_gen_thr_, thr.data(), sizeof(unsigned) * thr.size(), cudaMemcpyHostToDevice));
+  gen_thr_h_ = thr;
   gen_origin_h_ = origin;
   gen_start_h_ = start;
   gen_stop_h_ = stop;
@@ -1591,6 +1607,21 @@ void NeuronGPU::AccumulateKernelTiming(int n_steps) {
   }
 }
 
+int NeuronGPU::SetRk5MaxSubsteps(int n) {
+  if (n < 1) throw ngpu_exception("the RK5 sub-step limit must be >= 1");
+  rk5_max_substeps_ = n;
+  InvalidateGraphs();           // the limit is a launch argument of the captured updates
+  return 0;
+}
+
+int NeuronGPU::SetWaitTest(int mask) {
+  if (mask < 0 || mask > (WAIT_TEST_FIRST | WAIT_TEST_SECOND))
+    throw ngpu_exception("unknown wait-test bits");
+  wait_test_ = mask;
+  InvalidateGraphs();
+  return 0;
+}
+
 int NeuronGPU::SetKernelTiming(int on) {
   ktime_ = on != 0;
   for (int j = 0; j < 4; j++) { ktime_ms_[j] = 0; klaunch_[j] = 0; }
@@ -1633,6 +1664,35 @@ void NeuronGPU::EnsureForkResources() {
   NGPU_CUDA(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
 }
 
+// The RK5 group whose update grid carries the step's delivery: the first
+// single-group RK5 update with the plain controller and a variant that can
+// carry it (null: none, or switched off with NGB200_FUSE_DELIVERY=0).
+NodeGroup *NeuronGPU::FusedDeliveryGroup() {
+  const char *e = getenv("NGB200_FUSE_DELIVERY");
+  if (e != nullptr && atoi(e) == 0) return nullptr;
+  if (delivery_busy_) return nullptr;
+  for (NodeGroup *g : groups_) {
+    if (g->mi->kind != MK_RK5 || g->batch >= 0 || g->n_node <= 0) continue;
+    if (g->step_mode != STEP_PLAIN || g->n_port < 1 || g->n_port > 4) continue;
+    const GroupArgs a = MakeGroupArgs(g);
+    if (!a.all_uniform || !Rk5FusesDelivery(g->rk5_variant)) continue;
+    return g;
+  }
+  return nullptr;
+}
+
+// Delivery blocks (128 threads) in a fused update grid: two per SM, or
+// NGB200_FUSED_DELIVERY_BLOCKS per SM.
+int NeuronGPU::FusedDeliveryBlocks() {
+  const char *e = getenv("NGB200_FUSED_DELIVERY_BLOCKS");
+  const int per_sm = (e != nullptr && atoi(e) > 0) ? atoi(e) : 2;
+  int dev = 0, n_sm = 0;
+  NGPU_CUDA(cudaGetDevice(&dev));
+  NGPU_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+  // at most the delivery grid's size: the per-block event counters hold that many
+  return std::min(std::max(1, n_sm) * per_sm, std::max(1, deliver_blocks_));
+}
+
 void NeuronGPU::EnqueueStep(int step_in_chunk) {
   // this step's copy of the step context (k_step_prologue)
   StepCtx *ctx = d_ctxs_ + step_in_chunk;
@@ -1643,7 +1703,12 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
   // of step T fold the other half: without plastic synapses the two touch
   // disjoint data, so the delivery runs on its own stream beside the node
   // updates, and the next step (or the chunk's epilogue) waits for both.
-  const bool fork = has_delivery && !plastic_ && !ktime_ && dstream_ != nullptr;
+  // Preferably the delivery runs inside the grid of one RK5 group's update
+  // (k_rk5_update_deliver): no second stream, no join, and consecutive
+  // steps' updates keep their programmatic launch overlap.
+  NodeGroup *fuse_g = (has_delivery && !plastic_ && !ktime_) ? FusedDeliveryGroup() : nullptr;
+  const bool fork = has_delivery && !plastic_ && !ktime_ && dstream_ != nullptr && fuse_g == nullptr;
+  if (fuse_g != nullptr) d.advance_flags = 0;
   if (fork) {
     NGPU_CUDA(cudaEventRecord(ev_fork_, stream_));
     NGPU_CUDA(cudaStreamWaitEvent(dstream_, ev_fork_, 0));
@@ -1668,8 +1733,14 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
           }
         } else {
           if (HasLargePoisson(g)) LaunchPoissonLarge(MakeGroupArgs(g), MakeInputArgs(g), ctx, stream_);
-          LaunchRk5Update(mi->rk5_model, g->n_port, MakeGroupArgs(g), MakeInputArgs(g),
-                          MakePushArgs(g), ctx, stream_);
+          if (g == fuse_g) {
+            if (!LaunchRk5Update(mi->rk5_model, g->n_port, MakeGroupArgs(g), MakeInputArgs(g),
+                                 MakePushArgs(g), ctx, stream_, &d, FusedDeliveryBlocks()))
+              throw ngpu_exception("internal error: the delivery could not be fused into the update");
+          } else {
+            LaunchRk5Update(mi->rk5_model, g->n_port, MakeGroupArgs(g), MakeInputArgs(g),
+                            MakePushArgs(g), ctx, stream_);
+          }
         }
         break;
       case MK_IAF_PSC_EXP:
@@ -1727,6 +1798,7 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
     NGPU_CUDA(cudaStreamWaitEvent(stream_, ev_join_, 0));
     return;
   }
+  if (fuse_g != nullptr) return;
   if (plastic_ && rev_R_ > 1) LaunchRevArrive(d, ctx, stream_);
   LaunchDeliver(d, syn_table_, ctx, deliver_blocks_, stream_);
   if (ktime_) KEvent(step_in_chunk, 2);
@@ -1855,6 +1927,12 @@ void NeuronGPU::CheckDeviceErrors() {
     if (e & DERR_PROPOSER_TIMEOUT) m += " a tensor-core wait of the step proposer timed out;";
     if (e & DERR_REV_OVERFLOW) m += " a dendritic delay exceeds the one at calibration (or too many dendritic arrivals in one step);";
     if (e & DERR_TILE_TIMEOUT) m += " a shared-memory prefetch of the RK5 update timed out;";
+    if (e & DERR_TILE_DRAIN) {
+      // a bulk copy may still have landed in the shared memory of a block
+      // that had exited: nothing computed on this device is trusted after it
+      device_lost_ = true;
+      m += " a timed-out prefetch did not drain (device state lost; reset the simulator);";
+    }
     throw ngpu_exception(m);
   }
 }
@@ -1971,6 +2049,30 @@ void NeuronGPU::TuneRk5(NodeGroup *g) {
 // step is 6 evaluations, and above 6.06 (neurons have begun to take extra
 // sub-steps) the queue goes back on for good and the group's variant is
 // tuned again. The results are the same with and without the queue.
+// The delivery inside an update grid saves the launch and the join of a
+// separate delivery (about 1 us per step on a quiet network) but has fewer
+// warps than the forked delivery on its own high-priority stream, which is
+// faster once there is much to deliver (26 Hz on the 1e9-synapse network:
+// 94 vs 111 us per step). Every kQueueRecheckSteps steps the delivered
+// events per step are read from the delivery's per-block counters; above
+// kFusedDeliveryMaxEvents the step graphs are rebuilt with the forked
+// delivery, and back with the fused one when the rate falls below half of
+// it. Both give the same results.
+void NeuronGPU::RecheckDeliveryMode() {
+  const long long ds = steps_total_ - deliver_checked_;
+  if (ds < kQueueRecheckSteps || d_blk_events_ == nullptr) return;
+  const unsigned long long e = DeliveredEvents();
+  const double per_step = (double)(e - events_mark_) / (double)ds;
+  const bool busy = delivery_busy_ ? per_step > 0.5 * kFusedDeliveryMaxEvents
+                                   : per_step > kFusedDeliveryMaxEvents;
+  if (busy != delivery_busy_) {
+    delivery_busy_ = busy;
+    InvalidateGraphs();
+  }
+  events_mark_ = e;
+  deliver_checked_ = steps_total_;
+}
+
 void NeuronGPU::RecheckRk5Queues() {
   const double kEvalsQuiet = 6.06;
   for (Rk5BatchHost &b : batches_) {
@@ -2021,17 +2123,17 @@ void NeuronGPU::TuneAll() {
     if (g->mi->kind == MK_RK5 && g->batch < 0 && !g->tuned) TuneRk5(g);
 }
 
-int NeuronGPU::GetRk5Tuning(int i_node, int *variant, float *ms6) {
+int NeuronGPU::GetRk5Tuning(int i_node, int *variant, float *ms) {
   int il;
   NodeGroup *g = GroupOf(i_node, 1, il);
   if (g->batch >= 0) {
     const Rk5BatchHost &b = batches_[g->batch];
     *variant = b.variant;
-    for (int v = 0; v < 6; v++) ms6[v] = b.tune_ms[v];
+    for (int v = 0; v < NGPU_RK5_VARIANTS; v++) ms[v] = b.tune_ms[v];
     return 0;
   }
   *variant = g->rk5_variant;
-  for (int v = 0; v < 6; v++) ms6[v] = g->tune_ms[v];
+  for (int v = 0; v < NGPU_RK5_VARIANTS; v++) ms[v] = g->tune_ms[v];
   return 0;
 }
 
@@ -2281,6 +2383,9 @@ void NeuronGPU::FreeRk5Batches() {
 }
 
 int NeuronGPU::StartSimulation() {
+  if (device_lost_)
+    throw ngpu_exception("the device state was lost in an earlier step (DERR_TILE_DRAIN); "
+                         "reset the simulator");
   if (!calibrate_flag_) Calibrate();
   FlushInput();
   if (first_simulation_flag_) {
@@ -2363,6 +2468,7 @@ int NeuronGPU::Simulate() {
     steps_total_ += n;
     if (steps_total_ >= kTuneSteps && TunePending()) TuneAll();
     RecheckRk5Queues();
+    RecheckDeliveryMode();
   }
   neural_time_ = neur_t0_ + (double)time_resolution_ * (double)Nt_;
   NGPU_CUDA(cudaEventRecord(ev_stop_, stream_));

@@ -131,7 +131,7 @@ struct NodeGroup {
   // autotuned RK5 kernel variant and the timings it was chosen from
   int rk5_variant = 1;
   bool tuned = false;
-  float tune_ms[6] = {0, 0, 0, 0, 0, 0};
+  float tune_ms[NGPU_RK5_VARIANTS] = {0};
   bool queue_off = false;       // the autotuner switched the straggler queue off
   long long queue_checked = 0;  // steps_total_ at the last choice or check
   unsigned long long evals_mark = 0;  // stage evaluations counted by then
@@ -309,9 +309,18 @@ class NeuronGPU {
   double KernelsPerStep() { return kernels_per_step_; }
   // per-kernel-class device timing (CUDA events around every launch)
   int SetKernelTiming(int on);
+  NodeGroup *FusedDeliveryGroup();
+  int FusedDeliveryBlocks();
+  // RK5 sub-steps a neuron may take in one time step before the update
+  // gives up on it and reports DERR_RK5_STUCK (default NGPU_RK5_MAX_SUBSTEPS)
+  int SetRk5MaxSubsteps(int n);
+  int Rk5MaxSubsteps() const { return rk5_max_substeps_; }
+  // test hook: WaitTest bits; the marked bounded waits of the RK5 kernels
+  // give up after a single non-blocking test (0: normal waits)
+  int SetWaitTest(int mask);
   int GetKernelTiming(int kind, double *total_ms, long long *launches);
   // RK5 kernel variant chosen for the group of i_node and its timings
-  int GetRk5Tuning(int i_node, int *variant, float *ms6);
+  int GetRk5Tuning(int i_node, int *variant, float *ms);
   void TuneRk5(NodeGroup *g);
   // the autotuner runs once the network has integrated kTuneSteps steps, so
   // that it times the kernels on a settled state (the first steps start
@@ -325,6 +334,12 @@ class NeuronGPU {
   // kQueueRecheckSteps steps (RecheckRk5Queues)
   static const long long kQueueRecheckSteps = 1000;
   void RecheckRk5Queues();
+  // delivery in the update grid or on its own stream, by the delivered rate
+  static constexpr double kFusedDeliveryMaxEvents = 65536.0;
+  void RecheckDeliveryMode();
+  bool delivery_busy_ = false;
+  long long deliver_checked_ = 0;
+  unsigned long long events_mark_ = 0;
   // RK5 groups of one model and port count are integrated by one launch
   // per step (segment table) unless batching is switched off
   int SetRk5Batching(int on);
@@ -378,7 +393,7 @@ class NeuronGPU {
     int n_blocks = 0;
     int variant = 1;
     bool tuned = false;
-    float tune_ms[6] = {0, 0, 0, 0, 0, 0};
+    float tune_ms[NGPU_RK5_VARIANTS] = {0};
     bool queue_off = false;
     long long queue_checked = 0;
     unsigned long long evals_mark = 0;
@@ -412,6 +427,9 @@ class NeuronGPU {
   std::vector<float> mlp_params_;       // FP32 proposer parameters (empty: none)
   MlpImage *d_mlp_img_ = nullptr;
   float mlp_margin_ = 0.25f;
+  int rk5_max_substeps_ = NGPU_RK5_MAX_SUBSTEPS;
+  int wait_test_ = 0;
+  bool device_lost_ = false;    // set by DERR_TILE_DRAIN; every later simulation call fails
   void UploadMlpImage();
   std::vector<NodeGroup *> ProposerGroups(int i_node);
   std::vector<int> node_group_map_;
@@ -492,7 +510,9 @@ class NeuronGPU {
   std::vector<int> gen_nodes_;        // generator index -> node
   float *d_gen_rate_ = nullptr, *d_gen_origin_ = nullptr;
   float *d_gen_start_ = nullptr, *d_gen_stop_ = nullptr;
-  double *d_gen_lambda_ = nullptr, *d_gen_explam_ = nullptr, *d_gen_cdf_ = nullptr;
+  double *d_gen_lambda_ = nullptr, *d_gen_explam_ = nullptr;
+  unsigned *d_gen_thr_ = nullptr;       // [gen][NGPU_CDF_LEN] inversion thresholds
+  std::vector<unsigned> gen_thr_h_;
   std::vector<float> gen_origin_h_, gen_start_h_, gen_stop_h_;
   std::vector<double> gen_lam_h_, gen_explam_h_;
   // delivery counters

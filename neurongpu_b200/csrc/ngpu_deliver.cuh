@@ -1,0 +1,228 @@
+// Synaptic delivery (the reference's SpikeBufferUpdate / NestedLoop /
+// NestedLoopFunction0, src/spike_buffer.cu:233-302, src/nested_loop.cu:39-167,
+// src/get_spike.cu:48-85) and the synapse-model updates of the STDP rules.
+// Included by ngpu_kernels.cu (the delivery and STDP kernels) and by the RK5
+// launch header (delivery blocks fused into the update grid).
+#pragma once
+#include "ngpu_kernels_common.cuh"
+
+namespace ngpu {
+
+// ---------------------------------------------------------------------------
+// synapse models (src/stdp.cu:24-51, src/test_syn_model.cu:24-30)
+// ---------------------------------------------------------------------------
+// x^mu; the exponents of additive (0) and multiplicative (1) STDP, the
+// common settings, need no pow (pow(x, 0) is 1 and pow(x, 1) is x exactly)
+__device__ __forceinline__ double pow_mu(double x, double mu) {
+  if (mu == 0.0) return 1.0;
+  if (mu == 1.0) return x;
+  return pow(x, mu);
+}
+
+__device__ __forceinline__ float syn_update(const SynGroupTable &syn, int sg,
+                                            float w, float Dt) {
+  int type = syn.type[sg - 1];
+  const float *prm = syn.param[sg - 1];
+  if (type == 2) {
+    double tau_plus = prm[0], tau_minus = prm[1], lambda = prm[2];
+    double alpha = prm[3], mu_plus = prm[4], mu_minus = prm[5];
+    double Wmax = prm[6];
+    double w0 = w, w1;
+    if (Dt >= 0.0f) {
+      double fact = lambda * exp(-(double)Dt / tau_plus);
+      w1 = w0 + fact * Wmax * pow_mu(1.0 - w0 / Wmax, mu_plus);
+    } else {
+      double fact = -alpha * lambda * exp((double)Dt / tau_minus);
+      w1 = w0 + fact * Wmax * pow_mu(w0 / Wmax, mu_minus);
+    }
+    w1 = w1 > 0.0 ? w1 : 0.0;
+    w1 = w1 < Wmax ? w1 : Wmax;
+    return (float)w1;
+  } else if (type == 1) {
+    return w + (prm[1] + prm[0] * Dt);
+  }
+  return w;
+}
+
+// End-of-step work of plastic networks, fused into the step's last kernel:
+// the last block to finish empties this step's dendritic-delay slot, which
+// every block of the post rule has read by then. (The step index itself
+// never changes during a chunk of steps: each step reads its own copy of the
+// step context, see k_step_prologue.)
+__device__ __forceinline__ void finish_step(const DeliverArgs &d, StepCtx *ctx, int nblk) {
+  if (d.advance_flags == 0) return;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned prev = atomicAdd(d.done, 1u);
+    if (prev == (unsigned)nblk - 1) {
+      __threadfence();
+      if ((d.advance_flags & 1) && d.rev_cnt != nullptr) {
+        const long long T = ctx->T0 + ctx->it + 1;
+        d.rev_cnt[(int)(T % d.rev_R)] = 0;
+      }
+      *d.done = 0u;
+      __threadfence();
+    }
+  }
+}
+
+// Spike count of step T - 1 (complete: every kernel of that step has ended)
+// and the emptying of the ring slot that step T + 1 fills. Called once per
+// step, by the step's delivery or by k_advance; the slot of T + 1 is never
+// read in step T (deliveries read T - 1 ... T - max delay of a ring with
+// max delay + 2 slots).
+__device__ __forceinline__ void step_bookkeeping(int *ring_cnt, int ring_R, int ring_C,
+                                                 StepCtx *ctx) {
+  const long long T = ctx->T0 + ctx->it + 1;
+  const int c = ring_cnt[(int)((T - 1) % ring_R)];
+  ctx->n_spikes += (unsigned long long)(c < ring_C ? c : ring_C);
+  ring_cnt[(int)((T + 1) % ring_R)] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// synaptic delivery: one warp per (spike, delay) group. PLASTIC: the
+// network has plastic synapses (the STDP pre rule runs on every edge); the
+// static instance does not carry that path's registers.
+// ---------------------------------------------------------------------------
+// Delivery work of block blk of nblk delivery blocks (any block size that
+// is a multiple of 32, at most 256 threads): the whole grid of k_deliver, or
+// the first blocks of a fused RK5 update (k_rk5_update_deliver).
+template <bool PLASTIC>
+__device__ __forceinline__ void deliver_blocks(const DeliverArgs &d, const SynGroupTable &syn,
+                                               StepCtx *ctx, int blk, int nblk) {
+  const long long T = ctx->T0 + ctx->it + 1;
+  long long *const acc = d.acc + ((T & 1) ? d.acc_par : 0);   // folded by the update of T + 1
+  if (d.step_book && blk == 0 && threadIdx.x == 0)
+    step_bookkeeping(d.ring_cnt_w, d.ring_R, d.ring_C, ctx);
+  const int lane = threadIdx.x & 31;
+  const int warp = (blk * (int)blockDim.x + (int)threadIdx.x) >> 5;
+  const int n_warps = (nblk * (int)blockDim.x) >> 5;
+  const bool warp_scan = d.nd <= 32;
+  unsigned long long events = 0;
+  // the edges of one (spike, delay) item: spike j of ring slot `slot` at
+  // distinct-delay index di; called by whole warps
+  auto deliver_item = [&](int di, int slot, int j) {
+    const long long k = (long long)slot * d.ring_C + j;
+    const unsigned src = d.ring_src[k];
+    const float height = d.ring_h[k];
+    const unsigned long long gi = (unsigned long long)src * d.nd + di;
+    const unsigned long long beg = d.grp_off[gi], end = d.grp_off[gi + 1];
+    if (lane == 0) events += end - beg;
+    if constexpr (!PLASTIC) {
+      // eight edges per lane in flight; edges are read once per spike, so
+      // they are loaded with the streaming (evict-first) hint
+      for (unsigned long long e0 = beg + lane; e0 < end; e0 += 256) {
+        unsigned sl[8];
+        float wv[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const unsigned long long e = e0 + 32 * u;
+          if (e < end) {
+            sl[u] = __ldcs(d.e_slot + e);
+            wv[u] = __ldcs(d.e_w + e);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const unsigned long long e = e0 + 32 * u;
+          if (e < end) {
+            atomicAdd((unsigned long long *)(acc + sl[u]),
+                      (unsigned long long)ng_to_fixed(height * wv[u]));
+          }
+        }
+      }
+    } else {
+      // plastic network: four edges per lane in flight, then the
+      // post-synaptic last-spike gathers of all four, then the updates
+      for (unsigned long long e0 = beg + lane; e0 < end; e0 += 128) {
+        unsigned sl[4], post[4];
+        float wv[4];
+        int sgv[4], lr[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const unsigned long long e = e0 + 32 * u;
+          if (e < end) {
+            sl[u] = d.e_slot[e];
+            wv[u] = d.e_w[e];
+            sgv[u] = d.e_syn[e];
+            post[u] = sgv[u] > 0 ? d.e_post[e] : 0u;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const unsigned long long e = e0 + 32 * u;
+          if (e < end && sgv[u] > 0) lr[u] = d.last_rev_T[post[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const unsigned long long e = e0 + 32 * u;
+          if (e < end) {
+            atomicAdd((unsigned long long *)(acc + sl[u]),
+                      (unsigned long long)ng_to_fixed(height * wv[u]));
+            if (sgv[u] > 0) {
+              // pre-spike rule with the last post spike (src/get_spike.cu:73-83)
+              d.e_stamp[e] = (int)T;
+              const long long Dt_int = T - (long long)lr[u];
+              if (Dt_int > 0 && Dt_int < NGPU_MAX_SYN_DT) {
+                d.e_w[e] = syn_update(syn, sgv[u], wv[u], -d.dt * (float)Dt_int);
+              }
+            }
+          }
+        }
+      }
+    }
+  };
+  if (warp_scan) {
+    // per-delay spike counts and their prefix in registers of every warp
+    int my_slot = 0, my_incl = 0, total;
+    int c = 0;
+    if (lane < d.nd) {
+      int slot = (int)((T - d.delays[lane]) % d.ring_R);
+      if (slot < 0) slot += d.ring_R;
+      my_slot = slot;
+      c = d.ring_cnt[slot];
+      c = c < d.ring_C ? c : d.ring_C;
+    }
+    my_incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int v = __shfl_up_sync(0xffffffffu, my_incl, o);
+      if (lane >= o) my_incl += v;
+    }
+    total = __shfl_sync(0xffffffffu, my_incl, 31);
+    for (int item = warp; item < total; item += n_warps) {
+      // first delay whose inclusive prefix exceeds the item
+      // (item < total, so some lane's inclusive prefix exceeds it)
+      const unsigned m = __ballot_sync(0xffffffffu, my_incl > item);
+      const int di = __ffs(m) - 1;
+      const int slot = __shfl_sync(0xffffffffu, my_slot, di);
+      const int prev = __shfl_sync(0xffffffffu, my_incl, di > 0 ? di - 1 : 0);
+      deliver_item(di, slot, item - (di > 0 ? prev : 0));
+    }
+  } else {
+    // more than 32 distinct delays: every delay has a fixed set of G warps,
+    // which read its spike count themselves and take its spikes in turn (no
+    // prefix over the delays, no search); with fewer warps than delays each
+    // warp takes every n_warps-th delay
+    const bool per_delay = n_warps >= d.nd;
+    const int G = per_delay ? n_warps / d.nd : 1;
+    if (!per_delay || warp < G * d.nd) {
+      for (int di = per_delay ? warp % d.nd : warp; di < d.nd; di += per_delay ? d.nd : n_warps) {
+        int slot = (int)((T - d.delays[di]) % d.ring_R);
+        if (slot < 0) slot += d.ring_R;
+        int c = d.ring_cnt[slot];
+        c = c < d.ring_C ? c : d.ring_C;
+        for (int j = per_delay ? warp / d.nd : 0; j < c; j += G) deliver_item(di, slot, j);
+      }
+    }
+  }
+  if (d.blk_events != nullptr) {
+    // per warp, a reduction whose result is not waited for (see block_add_u64)
+    for (int o = 16; o > 0; o >>= 1) events += __shfl_down_sync(0xffffffffu, events, o);
+    if (lane == 0 && events != 0) atomicAdd(d.blk_events + blk, events);
+  }
+  finish_step(d, ctx, nblk);
+}
+
+}  // namespace ngpu

@@ -48,6 +48,23 @@ __global__ void k_prepare_batch(StepCtx *ctx, int *delays, int *ring_cnt, int nd
   for (int k = t; k < nd + 1; k += blockDim.x) ring_cnt[k] = 0;
 }
 
+// Grid of a standalone delivery: every SM of the current device with as
+// many delivery blocks as fit (nothing else runs beside it here, unlike the
+// simulator's delivery), cached per device.
+static int StandaloneDeliverBlocks() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return 148 * 8;
+  if (dev < 64 && cached[dev] > 0) return cached[dev];
+  int n_sm = 0, per_sm = 0;
+  if (cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n_sm <= 0)
+    n_sm = 148;
+  per_sm = DeliverOccupancy();
+  const int blocks = n_sm * (per_sm > 0 ? per_sm : 1);
+  if (dev < 64) cached[dev] = blocks;
+  return blocks;
+}
+
 int DeliverBatch(const unsigned long long *grp_off, const unsigned *e_slot, const float *e_w,
                  int nd, const unsigned *spike_src, const float *spike_h, const int *spike_di,
                  int n_spikes, long long *acc, cudaStream_t stream, unsigned *ring_src,
@@ -73,7 +90,7 @@ int DeliverBatch(const unsigned long long *grp_off, const unsigned *e_slot, cons
   d.delays = delays;
   SynGroupTable syn;
   memset(&syn, 0, sizeof(syn));
-  LaunchDeliver(d, syn, ctx, 148 * 8, stream);
+  LaunchDeliver(d, syn, ctx, StandaloneDeliverBlocks(), stream);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -16,6 +16,7 @@
 //     per-source shift queues of src/spike_buffer.cu:143-302.
 #pragma once
 #include <stdint.h>
+#include "ngpu_rng.h"
 
 namespace ngpu {
 
@@ -35,8 +36,47 @@ enum DeviceError : unsigned {
   DERR_NAN_STATE = 8u,
   DERR_PROPOSER_TIMEOUT = 16u,  // a tensor-core completion wait of the step proposer timed out
   DERR_REV_OVERFLOW = 32u,      // dendritic delay above its maximum or too many dendritic arrivals
-  DERR_TILE_TIMEOUT = 64u       // a shared-memory prefetch of the RK5 update did not complete in time
+  // a shared-memory prefetch of the RK5 update did not complete in time: the
+  // block leaves its remaining tiles untouched (their neurons skip the step)
+  DERR_TILE_TIMEOUT = 64u,
+  // after DERR_TILE_TIMEOUT the block's wait for its copies still in flight
+  // also ran out, so a copy may land in shared memory after the block has
+  // exited: the host treats the device state as lost (Simulate fails and
+  // every later call is refused until the simulator is reset)
+  DERR_TILE_DRAIN = 128u
 };
+
+// Bits of GroupArgs::wait_test (test hook, 0 in normal runs): the marked
+// bounded waits make a single non-blocking test instead of waiting, so that
+// their time-out paths can be exercised without a fault or a hang.
+enum WaitTest : int {
+  WAIT_TEST_FIRST = 1,          // the tile prefetch wait; the first MMA wait of a proposal round
+  WAIT_TEST_SECOND = 2          // the second MMA wait of a proposal round
+};
+
+#if defined(__CUDACC__)
+#define NGPU_HD __host__ __device__ __forceinline__
+#else
+#define NGPU_HD inline
+#endif
+
+// Parity bookkeeping of a proposal round's completion barrier. A round
+// commits two tensor-core completions (layer 1, then layer 2) and waits for
+// them in order; phase_in is the parity of the first. Returns the parity
+// to keep in ProposerSmem::phase: after a complete round the parity of the
+// next round's first completion (two phases later: phase_in again); after a
+// failed wait the parity of the completion still pending, which the
+// teardown waits for before the tensor memory is released (ok1: the first
+// wait succeeded, ok2: the second).
+NGPU_HD uint32_t proposer_phase_after(uint32_t phase_in, bool ok1, bool ok2) {
+  if (!ok1) return phase_in;            // layer 1 still pending
+  if (!ok2) return phase_in ^ 1u;       // layer 2 still pending
+  return phase_in;                      // both completed
+}
+
+// Iterations of a bounded mbarrier wait (each try_wait may also suspend the
+// thread for a hardware-defined time)
+#define NGPU_WAIT_ITERS (1 << 22)
 
 struct StepCtx {
   long long it;                 // iteration index within the current session
@@ -98,7 +138,7 @@ struct InputArgs {
   const float *gen_stop;
   const double *gen_lambda;     // rate*dt/1000 as the reference computes it
   const double *gen_explam;     // exp(-lambda)
-  const double *gen_cdf;        // [gen * NGPU_CDF_LEN + k] Poisson CDF F(k)
+  const unsigned *gen_thr;      // [gen * NGPU_CDF_LEN + k] inversion thresholds (ng_poisson_thresholds)
   unsigned long long seed;
   int dry;                      // timing run: leave the accumulators as they are
   // Uniform drive: every node of the group has exactly one direct connection,
@@ -109,14 +149,11 @@ struct InputArgs {
   int ud_port;
   float ud_w, ud_delay, ud_origin, ud_start, ud_stop;
   double ud_lambda, ud_explam;
-  const double *ud_cdf;
+  const unsigned *ud_thr;       // the generator's thresholds
+  unsigned ud_thr8[8];          // its first 8 thresholds (kernel parameters)
   unsigned long long ud_stream0;
 };
 
-// Poisson CDF table entries per generator: F(0..200), built on the host by
-// the recurrence of ng_poisson_inversion so that searching it returns the
-// same counts as the sequential-search sampler
-#define NGPU_CDF_LEN 201
 
 // Inference image of the learned RK5 step proposer (6 -> 32 -> 32 -> 1 MLP):
 // BF16 weight tiles already in the UMMA K-major layout of the kernels' shared
@@ -183,9 +220,12 @@ struct GroupArgs {
   int variant;                  // RK5 kernel variant (occupancy target)
   int dry;                      // timing run: compute everything, store nothing
   float h_min;
+  float h_min_thr;              // largest float <= h_min * (1 + 1e-5) in double (RK5 escape)
   float dt;                     // time resolution (ms)
   float eps;                    // RK5 tolerance
   float inv_eps;                // 1 / eps (IEEE division on the host)
+  int max_substeps;             // RK5 sub-steps per neuron and step before DERR_RK5_STUCK
+  int wait_test;                // WaitTest bits (0 in normal runs)
   int den_steps;                // round(den_delay / dt) of the uniform value
   int den_delay_col;            // param column of den_delay or -1
   unsigned long long *blk_evals;  // per-block RK5 derivative evaluations

@@ -29,117 +29,25 @@
 #include "ngpu_rk5_models.cuh"
 #include "ngpu_rng.h"
 #include "ngpu_kernels_common.cuh"
+#include "ngpu_deliver.cuh"
 
 namespace ngpu {
 
-// grid of the persistent tile kernel: as many blocks as are resident at once
-// (at most one per tile)
-template <class M, int NP, int MINB>
-static int tile_grid(int n_tiles) {
-  static int resident = 0;
-  if (resident == 0) {
-    int dev = 0, n_sm = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rk5_update_tiles<M, NP, MINB>,
-                                                  NGPU_BLOCK, 0);
-    resident = (n_sm > 0 ? n_sm : 148) * (per_sm > 0 ? per_sm : 1);
-  }
-  return n_tiles < resident ? n_tiles : resident;
-}
+int Rk5VariantCount(int np, int all_uniform) { return (all_uniform && np <= 4) ? NGPU_RK5_VARIANTS : 1; }
 
-// The tile kernel's bulk copies need 16-byte aligned column and accumulator
-// starts (cudaMalloc bases, columns of n_pad = a multiple of 128 entries).
-static bool tiles_aligned(const GroupArgs &g, const InputArgs &in) {
-  auto al = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
-  return al(g.var) && al(g.param) && al(g.h) && al(g.dx) && al(in.acc + in.acc_base) &&
-         ((in.acc_par * sizeof(long long)) & 15u) == 0 && (g.n_pad % NGPU_BLOCK) == 0;
-}
-
-template <class M, int NP>
-static void launch_rk5(const GroupArgs &g, const InputArgs &in, const PushArgs &pa,
-                       StepCtx *ctx, cudaStream_t s) {
-  dim3 grid((g.n + NGPU_BLOCK - 1) / NGPU_BLOCK), block(NGPU_BLOCK);
-  if (g.step_mode != STEP_PLAIN) {
-    // step logging and the learned proposer: conductance AdEx, <= 2 ports
-    if constexpr (ProposerFeatures<M>::supported && NP <= 2) {
-      if (g.step_mode == STEP_LOG) {
-        if (g.all_uniform) k_rk5_update<M, NP, true, 1, STEP_LOG><<<grid, block, 0, s>>>(g, in, pa, ctx);
-        else k_rk5_update<M, NP, false, 1, STEP_LOG><<<grid, block, 0, s>>>(g, in, pa, ctx);
-      } else {
-        if (g.all_uniform) k_rk5_update<M, NP, true, 4, STEP_LEARNED><<<grid, block, 0, s>>>(g, in, pa, ctx);
-        else k_rk5_update<M, NP, false, 4, STEP_LEARNED><<<grid, block, 0, s>>>(g, in, pa, ctx);
-      }
-    }
-    return;
-  }
-  if (g.all_uniform) {
-    if constexpr (NP <= 4) {
-      // occupancy variants chosen by the autotuner (register cap per thread)
-      const int variant = (g.variant >= 4 && !tiles_aligned(g, in)) ? 1 : g.variant;
-      const int n_tiles = (int)grid.x;
-      switch (variant) {
-        case 1: launch_pdl(k_rk5_update<M, NP, true, 5, STEP_PLAIN>, grid, block, s, g, in, pa, ctx); break;
-        case 2: launch_pdl(k_rk5_update<M, NP, true, 6, STEP_PLAIN>, grid, block, s, g, in, pa, ctx); break;
-        case 3: launch_pdl(k_rk5_update<M, NP, true, 8, STEP_PLAIN>, grid, block, s, g, in, pa, ctx); break;
-        case 4:
-          launch_pdl(k_rk5_update_tiles<M, NP, 5>, dim3(tile_grid<M, NP, 5>(n_tiles)), block, s, g, in, pa, ctx);
-          break;
-        case 5:
-          launch_pdl(k_rk5_update_tiles<M, NP, 6>, dim3(tile_grid<M, NP, 6>(n_tiles)), block, s, g, in, pa, ctx);
-          break;
-        default: launch_pdl(k_rk5_update<M, NP, true, 1, STEP_PLAIN>, grid, block, s, g, in, pa, ctx); break;
-      }
-    } else {
-      launch_pdl(k_rk5_update<M, NP, true, 1, STEP_PLAIN>, grid, block, s, g, in, pa, ctx);
-    }
-    if (g.q.cap > 0) launch_pdl(k_rk5_finish<M, NP, true>, dim3(g.q.fin_blocks), block, s, g, in, pa, ctx);
-  } else {
-    launch_pdl(k_rk5_update<M, NP, false, 1, STEP_PLAIN>, grid, block, s, g, in, pa, ctx);
-    if (g.q.cap > 0) launch_pdl(k_rk5_finish<M, NP, false>, dim3(g.q.fin_blocks), block, s, g, in, pa, ctx);
-  }
-}
-
-int Rk5VariantCount(int np, int all_uniform) { return (all_uniform && np <= 4) ? 6 : 1; }
-
-template <template <int> class MT>
-static void launch_rk5_model(int np, const GroupArgs &g, const InputArgs &in,
-                             const PushArgs &pa, StepCtx *ctx,
-                             cudaStream_t s) {
-  switch (np) {
-    case 0:
-    case 1: launch_rk5<MT<1>, 1>(g, in, pa, ctx, s); break;
-    case 2: launch_rk5<MT<2>, 2>(g, in, pa, ctx, s); break;
-    case 3: launch_rk5<MT<3>, 3>(g, in, pa, ctx, s); break;
-    case 4: launch_rk5<MT<4>, 4>(g, in, pa, ctx, s); break;
-    default:
-      if (np <= 8) {
-        launch_rk5<MT<8>, 8>(g, in, pa, ctx, s);
-      } else {
-        launch_rk5<MT<20>, 20>(g, in, pa, ctx, s);
-      }
-  }
-}
-
-void LaunchRk5Update(int model, int np, const GroupArgs &g,
+bool LaunchRk5Update(int model, int np, const GroupArgs &g,
                      const InputArgs &in, const PushArgs &pa, StepCtx *ctx,
-                     cudaStream_t s) {
-  if (g.n <= 0) return;
+                     cudaStream_t s, const DeliverArgs *del, int n_del) {
+  if (g.n <= 0) return false;
+  if (del != nullptr && (del->nd <= 0 || del->e_syn != nullptr || n_del <= 0)) del = nullptr;
   switch (model) {
-    case RK5_AEIF_COND_BETA:
-      launch_rk5_model<AeifCondBeta>(np, g, in, pa, ctx, s); break;
-    case RK5_AEIF_COND_ALPHA:
-      launch_rk5_model<AeifCondAlpha>(np, g, in, pa, ctx, s); break;
+    case RK5_AEIF_COND_BETA: return LaunchRk5AeifCondBeta(np, g, in, pa, ctx, s, del, n_del);
+    case RK5_AEIF_COND_ALPHA: return LaunchRk5AeifCondAlpha(np, g, in, pa, ctx, s, del, n_del);
     case RK5_AEIF_PSC_ALPHA:
-      launch_rk5_model<AeifPscAlpha>(np, g, in, pa, ctx, s); break;
     case RK5_AEIF_PSC_EXP:
-      launch_rk5_model<AeifPscExp>(np, g, in, pa, ctx, s); break;
-    case RK5_AEIF_PSC_DELTA:
-      launch_rk5<AeifPscDelta<1>, 1>(g, in, pa, ctx, s);
-      break;
-    case RK5_IZHIKEVICH_COND_BETA:
-      launch_rk5_model<IzhCondBeta>(np, g, in, pa, ctx, s); break;
-    default: break;
+    case RK5_AEIF_PSC_DELTA: return LaunchRk5AeifPsc(model, np, g, in, pa, ctx, s, del, n_del);
+    case RK5_IZHIKEVICH_COND_BETA: return LaunchRk5IzhCondBeta(np, g, in, pa, ctx, s, del, n_del);
+    default: return false;
   }
 }
 
@@ -574,7 +482,7 @@ __global__ void k_poisson_large(GroupArgs g, InputArgs in, StepCtx *ctx) {
   if (in.ud) {
     const unsigned n = direct_count<false, true>(
         t - (double)in.ud_origin - (double)in.ud_delay, in.ud_start, in.ud_stop, in.ud_lambda,
-        in.ud_explam, in.ud_cdf, in.seed, in.ud_stream0 + (unsigned long long)i, T0 + it);
+        nullptr, nullptr, in.seed, in.ud_stream0 + (unsigned long long)i, T0 + it);
     if (n > 0) acc[(long long)in.ud_port * g.n_pad] += ng_to_fixed(in.ud_w * (float)n);
   } else if (in.dc_off != nullptr) {
     const unsigned b = in.dc_off[i], e = in.dc_off[i + 1];
@@ -582,7 +490,7 @@ __global__ void k_poisson_large(GroupArgs g, InputArgs in, StepCtx *ctx) {
       const unsigned gen = in.dc_gen[c];
       const unsigned n = direct_count<false, true>(
           t - (double)in.gen_origin[gen] - (double)in.dc_delay[c], in.gen_start[gen],
-          in.gen_stop[gen], in.gen_lambda[gen], in.gen_explam[gen], nullptr, in.seed,
+          in.gen_stop[gen], in.gen_lambda[gen], nullptr, nullptr, in.seed,
           in.dc_stream[c], T0 + it);
       if (n > 0) acc[(long long)in.dc_port[c] * g.n_pad] += ng_to_fixed(in.dc_weight[c] * (float)n);
     }
@@ -608,225 +516,10 @@ void LaunchClearPending(StepCtx *ctx, cudaStream_t s) {
   k_clear_pending<<<1, 1, 0, s>>>(ctx);
 }
 
-// ---------------------------------------------------------------------------
-// synapse models (src/stdp.cu:24-51, src/test_syn_model.cu:24-30)
-// ---------------------------------------------------------------------------
-// x^mu; the exponents of additive (0) and multiplicative (1) STDP, the
-// common settings, need no pow (pow(x, 0) is 1 and pow(x, 1) is x exactly)
-__device__ __forceinline__ double pow_mu(double x, double mu) {
-  if (mu == 0.0) return 1.0;
-  if (mu == 1.0) return x;
-  return pow(x, mu);
-}
-
-__device__ __forceinline__ float syn_update(const SynGroupTable &syn, int sg,
-                                            float w, float Dt) {
-  int type = syn.type[sg - 1];
-  const float *prm = syn.param[sg - 1];
-  if (type == 2) {
-    double tau_plus = prm[0], tau_minus = prm[1], lambda = prm[2];
-    double alpha = prm[3], mu_plus = prm[4], mu_minus = prm[5];
-    double Wmax = prm[6];
-    double w0 = w, w1;
-    if (Dt >= 0.0f) {
-      double fact = lambda * exp(-(double)Dt / tau_plus);
-      w1 = w0 + fact * Wmax * pow_mu(1.0 - w0 / Wmax, mu_plus);
-    } else {
-      double fact = -alpha * lambda * exp((double)Dt / tau_minus);
-      w1 = w0 + fact * Wmax * pow_mu(w0 / Wmax, mu_minus);
-    }
-    w1 = w1 > 0.0 ? w1 : 0.0;
-    w1 = w1 < Wmax ? w1 : Wmax;
-    return (float)w1;
-  } else if (type == 1) {
-    return w + (prm[1] + prm[0] * Dt);
-  }
-  return w;
-}
-
-// End-of-step work of plastic networks, fused into the step's last kernel:
-// the last block to finish empties this step's dendritic-delay slot, which
-// every block of the post rule has read by then. (The step index itself
-// never changes during a chunk of steps: each step reads its own copy of the
-// step context, see k_step_prologue.)
-__device__ __forceinline__ void finish_step(const DeliverArgs &d, StepCtx *ctx) {
-  if (d.advance_flags == 0) return;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    unsigned prev = atomicAdd(d.done, 1u);
-    if (prev == gridDim.x - 1) {
-      __threadfence();
-      if ((d.advance_flags & 1) && d.rev_cnt != nullptr) {
-        const long long T = ctx->T0 + ctx->it + 1;
-        d.rev_cnt[(int)(T % d.rev_R)] = 0;
-      }
-      *d.done = 0u;
-      __threadfence();
-    }
-  }
-}
-
-// Spike count of step T - 1 (complete: every kernel of that step has ended)
-// and the emptying of the ring slot that step T + 1 fills. Called once per
-// step, by the step's delivery or by k_advance; the slot of T + 1 is never
-// read in step T (deliveries read T - 1 ... T - max delay of a ring with
-// max delay + 2 slots).
-__device__ __forceinline__ void step_bookkeeping(int *ring_cnt, int ring_R, int ring_C,
-                                                 StepCtx *ctx) {
-  const long long T = ctx->T0 + ctx->it + 1;
-  const int c = ring_cnt[(int)((T - 1) % ring_R)];
-  ctx->n_spikes += (unsigned long long)(c < ring_C ? c : ring_C);
-  ring_cnt[(int)((T + 1) % ring_R)] = 0;
-}
-
-// ---------------------------------------------------------------------------
-// synaptic delivery: one warp per (spike, delay) group. PLASTIC: the
-// network has plastic synapses (the STDP pre rule runs on every edge); the
-// static instance does not carry that path's registers.
-// ---------------------------------------------------------------------------
 template <bool PLASTIC>
 __global__ void __launch_bounds__(256)
 k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
-  const long long T = ctx->T0 + ctx->it + 1;
-  long long *const acc = d.acc + ((T & 1) ? d.acc_par : 0);   // folded by the update of T + 1
-  if (d.step_book && blockIdx.x == 0 && threadIdx.x == 0)
-    step_bookkeeping(d.ring_cnt_w, d.ring_R, d.ring_C, ctx);
-  const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int n_warps = (gridDim.x * blockDim.x) >> 5;
-  const bool warp_scan = d.nd <= 32;
-  unsigned long long events = 0;
-  // the edges of one (spike, delay) item: spike j of ring slot `slot` at
-  // distinct-delay index di; called by whole warps
-  auto deliver_item = [&](int di, int slot, int j) {
-    const long long k = (long long)slot * d.ring_C + j;
-    const unsigned src = d.ring_src[k];
-    const float height = d.ring_h[k];
-    const unsigned long long gi = (unsigned long long)src * d.nd + di;
-    const unsigned long long beg = d.grp_off[gi], end = d.grp_off[gi + 1];
-    if (lane == 0) events += end - beg;
-    if constexpr (!PLASTIC) {
-      // eight edges per lane in flight; edges are read once per spike, so
-      // they are loaded with the streaming (evict-first) hint
-      for (unsigned long long e0 = beg + lane; e0 < end; e0 += 256) {
-        unsigned sl[8];
-        float wv[8];
-#pragma unroll
-        for (int u = 0; u < 8; u++) {
-          const unsigned long long e = e0 + 32 * u;
-          if (e < end) {
-            sl[u] = __ldcs(d.e_slot + e);
-            wv[u] = __ldcs(d.e_w + e);
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < 8; u++) {
-          const unsigned long long e = e0 + 32 * u;
-          if (e < end) {
-            atomicAdd((unsigned long long *)(acc + sl[u]),
-                      (unsigned long long)ng_to_fixed(height * wv[u]));
-          }
-        }
-      }
-    } else {
-      // plastic network: four edges per lane in flight, then the
-      // post-synaptic last-spike gathers of all four, then the updates
-      for (unsigned long long e0 = beg + lane; e0 < end; e0 += 128) {
-        unsigned sl[4], post[4];
-        float wv[4];
-        int sgv[4], lr[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          const unsigned long long e = e0 + 32 * u;
-          if (e < end) {
-            sl[u] = d.e_slot[e];
-            wv[u] = d.e_w[e];
-            sgv[u] = d.e_syn[e];
-            post[u] = sgv[u] > 0 ? d.e_post[e] : 0u;
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          const unsigned long long e = e0 + 32 * u;
-          if (e < end && sgv[u] > 0) lr[u] = d.last_rev_T[post[u]];
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          const unsigned long long e = e0 + 32 * u;
-          if (e < end) {
-            atomicAdd((unsigned long long *)(acc + sl[u]),
-                      (unsigned long long)ng_to_fixed(height * wv[u]));
-            if (sgv[u] > 0) {
-              // pre-spike rule with the last post spike (src/get_spike.cu:73-83)
-              d.e_stamp[e] = (int)T;
-              const long long Dt_int = T - (long long)lr[u];
-              if (Dt_int > 0 && Dt_int < NGPU_MAX_SYN_DT) {
-                d.e_w[e] = syn_update(syn, sgv[u], wv[u], -d.dt * (float)Dt_int);
-              }
-            }
-          }
-        }
-      }
-    }
-  };
-  if (warp_scan) {
-    // per-delay spike counts and their prefix in registers of every warp
-    int my_slot = 0, my_incl = 0, total;
-    int c = 0;
-    if (lane < d.nd) {
-      int slot = (int)((T - d.delays[lane]) % d.ring_R);
-      if (slot < 0) slot += d.ring_R;
-      my_slot = slot;
-      c = d.ring_cnt[slot];
-      c = c < d.ring_C ? c : d.ring_C;
-    }
-    my_incl = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int v = __shfl_up_sync(0xffffffffu, my_incl, o);
-      if (lane >= o) my_incl += v;
-    }
-    total = __shfl_sync(0xffffffffu, my_incl, 31);
-    for (int item = warp; item < total; item += n_warps) {
-      // first delay whose inclusive prefix exceeds the item
-      // (item < total, so some lane's inclusive prefix exceeds it)
-      const unsigned m = __ballot_sync(0xffffffffu, my_incl > item);
-      const int di = __ffs(m) - 1;
-      const int slot = __shfl_sync(0xffffffffu, my_slot, di);
-      const int prev = __shfl_sync(0xffffffffu, my_incl, di > 0 ? di - 1 : 0);
-      deliver_item(di, slot, item - (di > 0 ? prev : 0));
-    }
-  } else {
-    // more than 32 distinct delays: every delay has a fixed set of G warps,
-    // which read its spike count themselves and take its spikes in turn (no
-    // prefix over the delays, no search); with fewer warps than delays each
-    // warp takes every n_warps-th delay
-    const bool per_delay = n_warps >= d.nd;
-    const int G = per_delay ? n_warps / d.nd : 1;
-    if (!per_delay || warp < G * d.nd) {
-      for (int di = per_delay ? warp % d.nd : warp; di < d.nd; di += per_delay ? d.nd : n_warps) {
-        int slot = (int)((T - d.delays[di]) % d.ring_R);
-        if (slot < 0) slot += d.ring_R;
-        int c = d.ring_cnt[slot];
-        c = c < d.ring_C ? c : d.ring_C;
-        for (int j = per_delay ? warp / d.nd : 0; j < c; j += G) deliver_item(di, slot, j);
-      }
-    }
-  }
-  if (d.blk_events != nullptr) {
-    __shared__ unsigned long long s_ev[8];
-    for (int o = 16; o > 0; o >>= 1)
-      events += __shfl_down_sync(0xffffffffu, events, o);
-    if (lane == 0) s_ev[threadIdx.x >> 5] = events;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      unsigned long long t = 0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += s_ev[w];
-      d.blk_events[blockIdx.x] += t;
-    }
-  }
-  finish_step(d, ctx);
+  deliver_blocks<PLASTIC>(d, syn, ctx, blockIdx.x, gridDim.x);
 }
 
 // Resident delivery blocks per SM, at most 3: the delivery runs beside the
@@ -837,6 +530,14 @@ int DeliverBlocksPerSM() {
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_deliver<false>, 256, 0) != cudaSuccess)
     return 3;
   return nb > 3 ? 3 : (nb > 0 ? nb : 1);
+}
+
+// Resident blocks per SM of the static delivery kernel (no cap).
+int DeliverOccupancy() {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_deliver<false>, 256, 0) != cudaSuccess)
+    return 8;
+  return nb > 0 ? nb : 1;
 }
 
 void LaunchDeliver(const DeliverArgs &d, const SynGroupTable &syn,
@@ -931,7 +632,7 @@ k_stdp_post(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
     for (int item = blockIdx.x; item < rcnt; item += gridDim.x)
       post_rule_node(d, syn, d.rev_src[(long long)rslot * d.rev_C + item], T);
   }
-  finish_step(d, ctx);
+  finish_step(d, ctx, gridDim.x);
 }
 
 void LaunchStdpPost(const DeliverArgs &d, const SynGroupTable &syn,

@@ -13,11 +13,34 @@ struct RecCol {
 };
 
 // per-step node updates
-void LaunchRk5Update(int model, int np, const GroupArgs &g,
-                     const InputArgs &in, const PushArgs &pa,
-                     StepCtx *ctx, cudaStream_t s);
+bool LaunchRk5Update(int model, int np, const GroupArgs &g,
+                     const InputArgs &in, const PushArgs &pa, StepCtx *ctx,
+                     cudaStream_t s, const DeliverArgs *del = nullptr, int n_del = 0);
 // number of RK5 kernel variants (GroupArgs::variant) for a group
 int Rk5VariantCount(int np, int all_uniform);
+// RK5 kernel variants of a group with uniform parameters (2-4 ports):
+// 0 no register cap; 1, 2, 3: caps for 5, 6, 8 resident blocks per SM;
+// 4, 5: persistent kernel with shared-memory prefetch of the state, caps for
+// 5 and 6 blocks per SM; 6: cap for 4 blocks per SM; 7, 8: persistent
+// kernel with caps for 4 and 3 blocks per SM
+#define NGPU_RK5_VARIANTS 9
+// per-model launchers (one translation unit each); with del != nullptr the
+// step's delivery (n_del blocks) runs in the update's grid when the chosen
+// variant allows it (returns true then)
+bool LaunchRk5AeifCondBeta(int np, const GroupArgs &g, const InputArgs &in, const PushArgs &pa,
+                           StepCtx *ctx, cudaStream_t s, const DeliverArgs *del, int n_del);
+bool LaunchRk5AeifCondAlpha(int np, const GroupArgs &g, const InputArgs &in, const PushArgs &pa,
+                            StepCtx *ctx, cudaStream_t s, const DeliverArgs *del, int n_del);
+bool LaunchRk5AeifPsc(int model, int np, const GroupArgs &g, const InputArgs &in,
+                      const PushArgs &pa, StepCtx *ctx, cudaStream_t s, const DeliverArgs *del,
+                      int n_del);
+bool LaunchRk5IzhCondBeta(int np, const GroupArgs &g, const InputArgs &in, const PushArgs &pa,
+                          StepCtx *ctx, cudaStream_t s, const DeliverArgs *del, int n_del);
+// whether the variant's update grid can carry the delivery blocks (the
+// register-capped one-block-per-tile variants; not the persistent ones)
+inline bool Rk5FusesDelivery(int variant) {
+  return variant == 0 || variant == 1 || variant == 2 || variant == 3 || variant == 6;
+}
 // floats per straggler record (Rk5Queue::stride) of an RK5 model / port count
 int Rk5RecordFloats(int model, int np);
 
@@ -75,6 +98,7 @@ void LaunchDeliver(const DeliverArgs &d, const SynGroupTable &syn,
                    StepCtx *ctx, int n_blocks, cudaStream_t s);
 // resident 256-thread delivery blocks per SM (grid = SMs x this)
 int DeliverBlocksPerSM();
+int DeliverOccupancy();
 // dendritic-delay arrivals of this step (before the delivery kernel)
 void LaunchRevArrive(const DeliverArgs &d, StepCtx *ctx, cudaStream_t s);
 void LaunchStdpPost(const DeliverArgs &d, const SynGroupTable &syn,

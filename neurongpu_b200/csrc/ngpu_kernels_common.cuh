@@ -10,6 +10,7 @@
 #include "ngpu_models.h"
 #include "ngpu_rk5_models.cuh"
 #include "ngpu_rng.h"
+#include "ngpu_f32x2.cuh"
 #include "ngpu_step_proposer.cuh"
 #include <cooperative_groups.h>
 
@@ -121,34 +122,33 @@ __device__ __forceinline__ long long *acc_in(const InputArgs &in, long long T0, 
 // generator's origin and the connection's delay, and the count is 0 outside
 // the generator's active window. SMALL / LARGE: whether rates below / at or above
 // NGPU_POISSON_INV_MAX per step are drawn; a count that is not drawn is 0.
-// Small rates: inversion against the host-built CDF table (the same counts
-// as ng_poisson_inversion, without device double divisions).
+// Small rates: the 32-bit uniform against the generator's inversion
+// thresholds (ng_poisson_count_thr): the thresholds do not decrease, so
+// the count below 8 is the number of the first 8 thresholds at or under u
+// (8 independent integer compares; t8 holds them, in the kernel parameters
+// for a uniform drive), and the search goes on in the table only in the
+// rare case that all 8 are.
 template <bool SMALL, bool LARGE>
 __device__ __forceinline__ unsigned direct_count(double t_rel, float start, float stop,
-                                                 double lam, double explam, const double *cdf,
+                                                 double lam, const unsigned *thr,
+                                                 const unsigned *t8,
                                                  unsigned long long seed,
                                                  unsigned long long stream, long long T_prev) {
   if (!(t_rel >= (double)start && t_rel <= (double)stop)) return 0;
   unsigned n = 0;
   if (lam < NGPU_POISSON_INV_MAX) {
     if constexpr (SMALL) {
-      Philox4 r = ng_random_block(seed, RNG_TAG_POISSON_DIRECT, stream, T_prev, 0);
-      const double u = ng_u01(r.v[0], r.v[1]);
       if (lam > 0.0) {
-        // the first index k with u <= cdf[k] (NGPU_CDF_LEN - 1 at most). The
-        // table does not decrease, so below 8 that index is the number of
-        // the first 8 entries under u: 8 independent loads and compares
-        // instead of a chain of dependent loads; the search goes on from 8
-        // only in the rare case that all 8 are under u.
+        const unsigned u = ng_random_block(seed, RNG_TAG_POISSON_DIRECT, stream, T_prev, 0).v[0];
 #pragma unroll
-        for (int k = 0; k < 8; k++) n += (u > cdf[k]) ? 1u : 0u;
+        for (int k = 0; k < 8; k++) n += (u >= t8[k]) ? 1u : 0u;
         if (n == 8) {
-          while (n < NGPU_CDF_LEN - 1 && u > cdf[n]) n++;
+          while (n < NGPU_CDF_LEN - 1 && u >= thr[n]) n++;
         }
       }
     }
   } else {
-    if constexpr (LARGE) n = ng_poisson(lam, explam, seed, RNG_TAG_POISSON_DIRECT, stream, T_prev);
+    if constexpr (LARGE) n = ng_poisson_ptrs(lam, seed, RNG_TAG_POISSON_DIRECT, stream, T_prev);
   }
   return n;
 }
@@ -183,7 +183,7 @@ __device__ __forceinline__ void input_sum(const InputArgs &in, int i,
     const double t = t0 + (double)dt * (double)it;
     const double t_rel = t - (double)in.ud_origin - (double)in.ud_delay;
     const unsigned n = direct_count<true, LARGE>(
-        t_rel, in.ud_start, in.ud_stop, in.ud_lambda, in.ud_explam, in.ud_cdf, in.seed,
+        t_rel, in.ud_start, in.ud_stop, in.ud_lambda, in.ud_thr, in.ud_thr8, in.seed,
         in.ud_stream0 + (unsigned long long)i, T0 + it);
     if (n > 0) {
       const long long v = ng_to_fixed(in.ud_w * (float)n);
@@ -201,9 +201,9 @@ __device__ __forceinline__ void input_sum(const InputArgs &in, int i,
       for (unsigned c = b; c < e; c++) {
         unsigned gen = in.dc_gen[c];
         double t_rel = t - (double)in.gen_origin[gen] - (double)in.dc_delay[c];
+        const unsigned *thr = in.gen_thr + (size_t)gen * NGPU_CDF_LEN;
         const unsigned n = direct_count<true, LARGE>(
-            t_rel, in.gen_start[gen], in.gen_stop[gen], in.gen_lambda[gen],
-            in.gen_explam[gen], in.gen_cdf + (size_t)gen * NGPU_CDF_LEN, in.seed,
+            t_rel, in.gen_start[gen], in.gen_stop[gen], in.gen_lambda[gen], thr, thr, in.seed,
             in.dc_stream[c], T_prev);
         if (n > 0) {
           long long v = ng_to_fixed(in.dc_weight[c] * (float)n);
@@ -225,68 +225,182 @@ __device__ __forceinline__ float fold_value(float var, long long s, float w) {
 // ---------------------------------------------------------------------------
 // RK5 (Cash-Karp) step and update, following src/rk5.h:57-162
 // ---------------------------------------------------------------------------
-// err^e for err > 0 with e = -0.2 or -0.25 (step-size controller)
+// err^e for err > 0 with e = -0.2 or -0.25 (step-size controller): the
+// special-function unit's base-2 logarithm and power
 __device__ __forceinline__ float ctrl_pow(float err, float e) {
-  return exp2f(e * log2f(err));
+  return ex2_approx(e * lg2_approx(err));
 }
 
+// Cash-Karp coefficients as pairs (c, c): one operand of the packed stage
+// arithmetic, read from the constant bank.
+struct Rk5PairConsts {
+  float2 a21, a31, a32, a41, a42, a43, a51, a52, a53, a54, a61, a62, a63, a64, a65;
+  float2 a71, a73, a74, a76, e1, e3, e4, e5, e6;
+};
+#define NGPU_PAIR(c) {rk5c::c, rk5c::c}
+static __constant__ Rk5PairConsts c_rk5[1] = {{
+    NGPU_PAIR(a21), NGPU_PAIR(a31), NGPU_PAIR(a32), NGPU_PAIR(a41), NGPU_PAIR(a42),
+    NGPU_PAIR(a43), NGPU_PAIR(a51), NGPU_PAIR(a52), NGPU_PAIR(a53), NGPU_PAIR(a54),
+    NGPU_PAIR(a61), NGPU_PAIR(a62), NGPU_PAIR(a63), NGPU_PAIR(a64), NGPU_PAIR(a65),
+    NGPU_PAIR(a71), NGPU_PAIR(a73), NGPU_PAIR(a74), NGPU_PAIR(a76), NGPU_PAIR(e1),
+    NGPU_PAIR(e3), NGPU_PAIR(e4), NGPU_PAIR(e5), NGPU_PAIR(e6)}};
+#undef NGPU_PAIR
+#define NGPU_C2(name) (c_rk5[cz].name)
+
+// error scale |y| + |h k1| + scal_min of one pair of variables
+__device__ __forceinline__ void rk5_err_scale(f2 y, f2 k1, float h, float &s0, float &s1) {
+  float y0, y1, k0, k1s;
+  f2_unpack(y, y0, y1);
+  f2_unpack(k1, k0, k1s);
+  s0 = fabsf(y0) + fabsf(k0 * h) + rk5c::scal_min;
+  s1 = fabsf(y1) + fabsf(k1s * h) + rk5c::scal_min;
+}
+
+// One RK5 step (src/rk5.h:57-147): Cash-Karp stages, error estimate and
+// step-size control, retried with a smaller step until accepted. The state
+// variables are processed as pairs (y[2j], y[2j+1]) with packed FP32x2
+// arithmetic, which rounds every half as the scalar operation would; an odd
+// variable count is padded with a zero variable. Kept from the reference:
+// the error scale |y| + |h k1| + 0.1 with the step size before clamping, the
+// clamp to [h_min, h_max], the escape at h <= h_min (1 + 1e-5) (h_min_thr:
+// the largest float at or below that double), the reduction to at least
+// 0.1 h (in double) and the growth rules. The scaled errors |e_i| / ys_i
+// are products with the reciprocal of ys_i; when their maximum, times
+// 1 / eps, lies within 1e-5 of 1 the norm is recomputed in FP64 (IEEE
+// quotients) so that the accept / reject decision is the exact one.
 template <class M, int NP>
 __device__ __forceinline__ void rk5_step(double &x, float *y, float &h,
-                                         float h_min, float h_max,
+                                         float h_min, float h_min_thr, float h_max,
                                          const float *p, const float *q,
                                          float refr, int np, float inv_eps,
                                          unsigned &evals, float &h_acc, float &err_acc) {
   using namespace rk5c;
   constexpr int NV = M::NVAR;
-  float k1[NV], k2[NV], k3[NV], k4[NV], k5[NV], k6[NV], yn[NV], ys[NV];
-  M::deriv(y, k1, p, q, refr, np);
+  constexpr int NH = (NV + 1) / 2;
+  constexpr int NVP = 2 * NH;
+  // K1: the derivative at the start (kept across retries); K2..K4 while
+  // stages need them; S6 / P5 / PE: running sums of the sixth stage's
+  // input, the fifth-order solution and the error estimate, formed in the
+  // reference's order of terms as soon as their terms exist, so that K2..K5
+  // are not live at the same time
+  f2 Y[NH], K1[NH], K2[NH], K3[NH], K4[NH], YN[NH];
+  float d[NVP], yn[NVP];
+#pragma unroll
+  for (int j = 0; j < NVP; j++) d[j] = 0.0f;
+#pragma unroll
+  for (int j = 0; j < NH; j++) Y[j] = f2_pack(y[2 * j], (2 * j + 1 < NV) ? y[2 * j + 1] : 0.0f);
+  M::deriv(y, d, p, q, refr, np);
   evals++;
 #pragma unroll
-  for (int i = 0; i < NV; i++) ys[i] = fabsf(y[i]) + fabsf(k1[i] * h) + scal_min;
+  for (int j = 0; j < NH; j++) K1[j] = f2_pack(d[2 * j], d[2 * j + 1]);
+  // the error scale |y| + |h k1| + scal_min uses the step size the call
+  // starts with; it is formed where the error is (fewer live registers)
+  const float h_in = h;
   float err = 0.0f;
   for (int guard = 0;; guard++) {
-    if (h > h_max) h = h_max;
-    if (h < h_min) h = h_min;
+    // an index the compiler cannot see is 0: the coefficient pairs are read
+    // from the constant bank in every attempt instead of being hoisted out
+    // of the retry loop into registers (24 pairs = 48 registers)
+    int cz;
+    asm volatile("mov.u32 %0, 0;" : "=r"(cz));
+    h = fmaxf(fminf(h, h_max), h_min);
+    const f2 HH = f2_pack(h, h);
+    // stage 2
+    const f2 HA21 = f2_mul(HH, NGPU_C2(a21));
 #pragma unroll
-    for (int i = 0; i < NV; i++) yn[i] = y[i] + h * a21 * k1[i];
-    M::deriv(yn, k2, p, q, refr, np);
+    for (int j = 0; j < NH; j++) {
+      YN[j] = f2_fma(HA21, K1[j], Y[j]);
+      f2_unpack(YN[j], yn[2 * j], yn[2 * j + 1]);
+    }
+    M::deriv(yn, d, p, q, refr, np);
 #pragma unroll
-    for (int i = 0; i < NV; i++) yn[i] = y[i] + h * (a31 * k1[i] + a32 * k2[i]);
-    M::deriv(yn, k3, p, q, refr, np);
+    for (int j = 0; j < NH; j++) K2[j] = f2_pack(d[2 * j], d[2 * j + 1]);
+    // stage 3
 #pragma unroll
-    for (int i = 0; i < NV; i++)
-      yn[i] = y[i] + h * (a41 * k1[i] + a42 * k2[i] + a43 * k3[i]);
-    M::deriv(yn, k4, p, q, refr, np);
+    for (int j = 0; j < NH; j++) {
+      f2 t = f2_mul(NGPU_C2(a31), K1[j]);
+      t = f2_fma(NGPU_C2(a32), K2[j], t);
+      YN[j] = f2_fma(HH, t, Y[j]);
+      f2_unpack(YN[j], yn[2 * j], yn[2 * j + 1]);
+    }
+    M::deriv(yn, d, p, q, refr, np);
 #pragma unroll
-    for (int i = 0; i < NV; i++)
-      yn[i] = y[i] + h * (a51 * k1[i] + a52 * k2[i] + a53 * k3[i]
-                          + a54 * k4[i]);
-    M::deriv(yn, k5, p, q, refr, np);
+    for (int j = 0; j < NH; j++) K3[j] = f2_pack(d[2 * j], d[2 * j + 1]);
+    // stage 4
 #pragma unroll
-    for (int i = 0; i < NV; i++)
-      yn[i] = y[i] + h * (a61 * k1[i] + a62 * k2[i] + a63 * k3[i]
-                          + a64 * k4[i] + a65 * k5[i]);
-    M::deriv(yn, k6, p, q, refr, np);
+    for (int j = 0; j < NH; j++) {
+      f2 t = f2_mul(NGPU_C2(a41), K1[j]);
+      t = f2_fma(NGPU_C2(a42), K2[j], t);
+      t = f2_fma(NGPU_C2(a43), K3[j], t);
+      YN[j] = f2_fma(HH, t, Y[j]);
+      f2_unpack(YN[j], yn[2 * j], yn[2 * j + 1]);
+    }
+    M::deriv(yn, d, p, q, refr, np);
 #pragma unroll
-    for (int i = 0; i < NV; i++)
-      yn[i] = y[i] + h * (a71 * k1[i] + a73 * k3[i] + a74 * k4[i]
-                          + a76 * k6[i]);
+    for (int j = 0; j < NH; j++) K4[j] = f2_pack(d[2 * j], d[2 * j + 1]);
+    // stage 5 input; the terms of K2..K4 in the later sums
+    f2 S6[NH], P5[NH], PE[NH];
+#pragma unroll
+    for (int j = 0; j < NH; j++) {
+      f2 t = f2_mul(NGPU_C2(a51), K1[j]);
+      t = f2_fma(NGPU_C2(a52), K2[j], t);
+      t = f2_fma(NGPU_C2(a53), K3[j], t);
+      t = f2_fma(NGPU_C2(a54), K4[j], t);
+      YN[j] = f2_fma(HH, t, Y[j]);
+      f2_unpack(YN[j], yn[2 * j], yn[2 * j + 1]);
+      f2 u = f2_mul(NGPU_C2(a61), K1[j]);
+      u = f2_fma(NGPU_C2(a62), K2[j], u);
+      u = f2_fma(NGPU_C2(a63), K3[j], u);
+      S6[j] = f2_fma(NGPU_C2(a64), K4[j], u);
+      f2 v = f2_mul(NGPU_C2(a71), K1[j]);
+      v = f2_fma(NGPU_C2(a73), K3[j], v);
+      P5[j] = f2_fma(NGPU_C2(a74), K4[j], v);
+      f2 e = f2_mul(NGPU_C2(e1), K1[j]);
+      e = f2_fma(NGPU_C2(e3), K3[j], e);
+      PE[j] = f2_fma(NGPU_C2(e4), K4[j], e);
+    }
+    M::deriv(yn, d, p, q, refr, np);
+    // stage 6 input (K5 = d)
+#pragma unroll
+    for (int j = 0; j < NH; j++) {
+      const f2 k5 = f2_pack(d[2 * j], d[2 * j + 1]);
+      YN[j] = f2_fma(HH, f2_fma(NGPU_C2(a65), k5, S6[j]), Y[j]);
+      f2_unpack(YN[j], yn[2 * j], yn[2 * j + 1]);
+      PE[j] = f2_fma(NGPU_C2(e5), k5, PE[j]);
+    }
+    M::deriv(yn, d, p, q, refr, np);
     evals += 5;
+    // fifth-order solution and the scaled error of the embedded estimate (K6 = d)
     err = 0.0f;
 #pragma unroll
-    for (int i = 0; i < NV; i++) {
-      float val = h * (e1 * k1[i] + e3 * k3[i] + e4 * k4[i] + e5 * k5[i]
-                       + e6 * k6[i]);
-      // scaled error |val| / ys: an approximate quotient (2 ulp) instead of
-      // the IEEE division, which costs a dozen instructions per variable
-      float av = fabsf(__fdividef(val, ys[i]));
-      err = (err > av) ? err : av;
+    for (int j = 0; j < NH; j++) {
+      const f2 k6 = f2_pack(d[2 * j], d[2 * j + 1]);
+      YN[j] = f2_fma(HH, f2_fma(NGPU_C2(a76), k6, P5[j]), Y[j]);
+      PE[j] = f2_mul(HH, f2_fma(NGPU_C2(e6), k6, PE[j]));
+      float v0, v1, s0, s1;
+      f2_unpack(PE[j], v0, v1);
+      rk5_err_scale(Y[j], K1[j], h_in, s0, s1);
+      err = fmaxf(err, fmaxf(fabsf(v0) * rcp_approx(s0), fabsf(v1) * rcp_approx(s1)));
     }
     err *= inv_eps;
-    if (err <= 1.0f || (double)h <= (double)h_min * (1.0 + 1.0e-5)) break;
+    bool accept = err <= 1.0f;
+    if (fabsf(err - 1.0f) < 1.0e-5f) {
+      // borderline: the norm in FP64 with IEEE quotients decides
+      double e64 = 0.0;
+#pragma unroll
+      for (int j = 0; j < NH; j++) {
+        float v0, v1, s0, s1;
+        f2_unpack(PE[j], v0, v1);
+        rk5_err_scale(Y[j], K1[j], h_in, s0, s1);
+        e64 = fmax(e64, fabs((double)v0 / (double)s0));
+        e64 = fmax(e64, fabs((double)v1 / (double)s1));
+      }
+      accept = e64 * (double)inv_eps <= 1.0;
+    }
+    if (accept || h <= h_min_thr) break;
     if (guard >= 256) break;
-    float h_new = h * coeff * ctrl_pow(err, exp_dec);
-    double h01 = 0.1 * (double)h;
+    const float h_new = h * coeff * ctrl_pow(err, exp_dec);
+    const double h01 = 0.1 * (double)h;
     h = (float)(((double)h_new > h01) ? (double)h_new : h01);
   }
   x += h;
@@ -298,8 +412,14 @@ __device__ __forceinline__ void rk5_step(double &x, float *y, float &h,
     h = (float)(5.0 * (double)h);
   }
 #pragma unroll
-  for (int i = 0; i < NV; i++) y[i] = yn[i];
+  for (int j = 0; j < NH; j++) {
+    float a, b;
+    f2_unpack(YN[j], a, b);
+    y[2 * j] = a;
+    if (2 * j + 1 < NV) y[2 * j + 1] = b;
+  }
 }
+#undef NGPU_C2
 
 template <class M>
 struct ModelTraits;
@@ -320,17 +440,13 @@ NGPU_TRAITS(AeifPscDelta, 0, 0, -1, 0, A_refr, A_den_delay)
 NGPU_TRAITS(IzhCondBeta, 3, 2, I_NSP + 3, 4, I_refr, I_den_delay)
 
 __device__ __forceinline__ void block_add_u64(unsigned long long v,
-                                              unsigned long long *dst) {
-  __shared__ unsigned long long s_part[NGPU_BLOCK / 32];
+                                              unsigned long long *dst, int blk = -1) {
+  // per warp: a shuffle sum, then one reduction into the block's counter
+  // whose result is not waited for (red.global.add), so a finished block
+  // frees its SM slot at once (a barrier and a load-add-store of the
+  // counter by one thread held every block for an L2 round trip)
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0) s_part[wid] = v;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned long long t = 0;
-    for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += s_part[k];
-    dst[blockIdx.x] += t;
-  }
+  if ((threadIdx.x & 31) == 0 && v != 0) atomicAdd(dst + (blk >= 0 ? blk : (int)blockIdx.x), v);
 }
 
 // Appends one accepted sub-step (features at its start, training target) to
@@ -382,12 +498,13 @@ __device__ __forceinline__ bool rk5_plain_substep(const GroupArgs &g, const Push
                                                   int den, bool dry, unsigned &evals) {
   float h_acc, err_acc;
   const float hmax = (float)(x1 - x);
-  rk5_step<M, NP>(x, y, h, g.h_min, hmax, p, q, refr, np, inv_eps, evals, h_acc, err_acc);
+  rk5_step<M, NP>(x, y, h, g.h_min, g.h_min_thr, hmax, p, q, refr, np, inv_eps, evals, h_acc,
+                  err_acc);
   bool end_step = (x >= x1 - (double)g.h_min);
   if (M::external(y, p, refr, end_step, g.dt)) {
     if (!dry) push_spike(pa, ctx, g.i_node_0 + i, i, 1.0f, T, x1, den);
   }
-  if (++guard > NGPU_RK5_MAX_SUBSTEPS) {
+  if (++guard > g.max_substeps) {
     atomicOr(&ctx->err, (unsigned)DERR_RK5_STUCK);
     end_step = true;
   }
@@ -613,7 +730,7 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
         float f[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
         if (want) ProposerFeatures<M>::get(y, p, h, g.dt, f);
         float o = 0.0f;
-        if (proposer_round(*ps, want, f, o, &ctx->err)) {
+        if (proposer_round(*ps, want, f, o, &ctx->err, g.wait_test)) {
           if (want) {
             // the proposal may shrink the controller's guess by at most 4x
             // (after a low-error step it then still grows, >= 1.25x) and
@@ -627,12 +744,13 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
         }
       }
       if (!end_step) {
-        rk5_step<M, NP>(x, y, h, h_min, hmax, p, q, refr, np, inv_eps, evals, h_acc, err_acc);
+        rk5_step<M, NP>(x, y, h, h_min, g.h_min_thr, hmax, p, q, refr, np, inv_eps, evals, h_acc,
+                        err_acc);
         end_step = (x >= x1 - (double)h_min);
         if (M::external(y, p, refr, end_step, g.dt)) {
           if (!dry) push_spike(pa, ctx, g.i_node_0 + i, i, 1.0f, T, x1, den);
         }
-        if (++guard > NGPU_RK5_MAX_SUBSTEPS) {
+        if (++guard > g.max_substeps) {
           atomicOr(&ctx->err, (unsigned)DERR_RK5_STUCK);
           end_step = true;
         }
@@ -648,13 +766,14 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
         ProposerFeatures<M>::get(y, p, h, g.dt, f);
         lg = true;
       }
-      rk5_step<M, NP>(x, y, h, h_min, hmax, p, q, refr, np, inv_eps, evals, h_acc, err_acc);
+      rk5_step<M, NP>(x, y, h, h_min, g.h_min_thr, hmax, p, q, refr, np, inv_eps, evals, h_acc,
+                      err_acc);
       if (lg) log_step_sample(g, f, proposer_target(h_acc, err_acc, g.dt));
       end_step = (x >= x1 - (double)h_min);
       if (M::external(y, p, refr, end_step, g.dt)) {
         if (!dry) push_spike(pa, ctx, g.i_node_0 + i, i, 1.0f, T, x1, den);
       }
-      if (++guard > NGPU_RK5_MAX_SUBSTEPS) {
+      if (++guard > g.max_substeps) {
         atomicOr(&ctx->err, (unsigned)DERR_RK5_STUCK);
         break;
       }
@@ -775,15 +894,21 @@ k_rk5_update_tiles(const __grid_constant__ GroupArgs g, const __grid_constant__ 
   int k = 0;
   for (int t = blockIdx.x; t < n_tiles; t += G, k++) {
     const int s = k & 1;
-    const bool ok = __syncthreads_and(mbar_wait(&s_bar[s], (k >> 1) & 1, 1 << 22));
+    const bool ok = __syncthreads_and(
+        mbar_wait(&s_bar[s], (k >> 1) & 1, NGPU_WAIT_ITERS, (g.wait_test & WAIT_TEST_FIRST) != 0));
     if (!ok) {
       // a copy did not land: leave this block's remaining tiles untouched,
-      // after giving the copies in flight time to end
+      // after waiting (bounded) for the copies in flight, which write into
+      // this block's shared memory; if that wait runs out too, the host is
+      // told that the device state is lost
       if (threadIdx.x == 0) {
         atomicOr(&ctx->err, (unsigned)DERR_TILE_TIMEOUT);
-        mbar_wait(&s_bar[s], (k >> 1) & 1, 1 << 22);
-        if (t + G < n_tiles) mbar_wait(&s_bar[s ^ 1], ((k + 1) >> 1) & 1, 1 << 22);
+        bool drained = mbar_wait(&s_bar[s], (k >> 1) & 1, NGPU_WAIT_ITERS);
+        if (t + G < n_tiles)
+          drained = mbar_wait(&s_bar[s ^ 1], ((k + 1) >> 1) & 1, NGPU_WAIT_ITERS) && drained;
+        if (!drained) atomicOr(&ctx->err, (unsigned)DERR_TILE_DRAIN);
       }
+      __syncthreads();
       break;
     }
     float pc[St::NC];

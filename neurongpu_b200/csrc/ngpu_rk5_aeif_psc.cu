@@ -1,0 +1,18 @@
+// Single-group RK5 update launches of the current-based AdEx models (aeif_psc_alpha, aeif_psc_exp, aeif_psc_delta) (template instances of
+// ngpu_rk5_launch.cuh, compiled in their own translation unit).
+#include "ngpu_rk5_launch.cuh"
+
+namespace ngpu {
+
+bool LaunchRk5AeifPsc(int model, int np, const GroupArgs &g, const InputArgs &in,
+                      const PushArgs &pa, StepCtx *ctx, cudaStream_t s, const DeliverArgs *del,
+                      int n_del) {
+  switch (model) {
+    case RK5_AEIF_PSC_ALPHA: return launch_rk5_model<AeifPscAlpha>(np, g, in, pa, ctx, s, del, n_del);
+    case RK5_AEIF_PSC_EXP: return launch_rk5_model<AeifPscExp>(np, g, in, pa, ctx, s, del, n_del);
+    case RK5_AEIF_PSC_DELTA: return launch_rk5<AeifPscDelta<1>, 1>(g, in, pa, ctx, s, del, n_del);
+    default: return false;
+  }
+}
+
+}  // namespace ngpu

@@ -17,6 +17,7 @@
 // src/aeif_cond_beta_kernel.h:153-214 and the other *_kernel.h files.
 #pragma once
 #include <math.h>
+#include "ngpu_f32x2.cuh"
 
 namespace ngpu {
 
@@ -93,7 +94,8 @@ __device__ __forceinline__ void aeif_vw(const float *y, float *dydx,
   if (exp_guard && p[A_Delta_T] == 0.0f) {
     V_spike = 0.0f;
   } else {
-    V_spike = p[A_Delta_T] * expf((V - p[A_V_th]) * q[A_Delta_T]);
+    // Delta_T e^((V - V_th) / Delta_T) as Delta_T 2^((V - V_th) log2(e) / Delta_T)
+    V_spike = p[A_Delta_T] * ex2_approx((V - p[A_V_th]) * (q[A_Delta_T] * kLog2e));
   }
   dydx[0] = (refr > 0.0f) ? 0.0f
       : (-p[A_g_L] * (V - p[A_E_L] - V_spike) + I_in - y[1] + p[A_I_e])

@@ -156,6 +156,49 @@ NG_HD uint32_t ng_poisson(double lambda, double exp_neg_lambda, uint64_t seed,
   return ng_poisson_ptrs(lambda, seed, tag, stream, step);
 }
 
+// Poisson CDF table entries per generator (inversion thresholds)
+#define NGPU_CDF_LEN 201
+
+// Inversion thresholds of the direct-connection sampler: thr[k] = F(k) 2^32
+// rounded to the nearest integer and saturated at 2^32 - 1, where F(k) is
+// the Poisson CDF formed by the recurrence of ng_poisson_inversion (same
+// double operations on every host). A count for a 32-bit uniform u is the
+// number of leading thresholds with u >= thr[k], so P(count > k) =
+// 1 - thr[k] / 2^32, the CDF to 2^-32. Integer compares make the device
+// search cheap and identical on the host.
+NG_HD void ng_poisson_thresholds(double lambda, double exp_neg_lambda, uint32_t *thr) {
+  double p = exp_neg_lambda;
+  double F = p;
+  for (int n = 0; n < NGPU_CDF_LEN; n++) {
+    if (n > 0) {
+      p = NG_DDIV(NG_DMUL(p, lambda), (double)n);
+      F = NG_DADD(F, p);
+    }
+    const double v = floor(NG_DADD(NG_DMUL(F, 4294967296.0), 0.5));
+    thr[n] = v >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)v;
+  }
+}
+
+// Count of the direct-connection sampler for lambda < NGPU_POISSON_INV_MAX:
+// u is word 0 of the Philox block of (seed, POISSON_DIRECT, stream, step).
+NG_HD uint32_t ng_poisson_count_thr(uint32_t u, const uint32_t *thr) {
+  uint32_t n = 0;
+  while (n < NGPU_CDF_LEN - 1 && u >= thr[n]) n++;
+  return n;
+}
+
+// Direct-connection Poisson count for one (stream, step): inversion against
+// the thresholds below NGPU_POISSON_INV_MAX, PTRS above.
+NG_HD uint32_t ng_poisson_direct(double lambda, const uint32_t *thr, uint64_t seed,
+                                 uint64_t stream, int64_t step) {
+  if (!(lambda > 0.0)) return 0;
+  if (lambda < NGPU_POISSON_INV_MAX) {
+    Philox4 r = ng_random_block(seed, RNG_TAG_POISSON_DIRECT, stream, step, 0);
+    return ng_poisson_count_thr(r.v[0], thr);
+  }
+  return ng_poisson_ptrs(lambda, seed, RNG_TAG_POISSON_DIRECT, stream, step);
+}
+
 // fixed-point accumulation of synaptic input: 32 fractional bits
 #define NGPU_ACC_SCALE 4294967296.0
 #define NGPU_ACC_INV_SCALE (1.0 / 4294967296.0)

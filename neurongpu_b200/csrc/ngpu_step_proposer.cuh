@@ -124,8 +124,23 @@ __device__ __forceinline__ void mbar_init(uint64_t *mbar, uint32_t count) {
 }
 
 // bounded wait for the phase with the given parity; false on time-out
-__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, int max_iter) {
+// Bounded wait for the completion of the barrier phase with the given
+// parity; false if it did not complete within max_iter tries. test_once: a
+// single non-blocking test instead (the wait-test hook of GroupArgs).
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, int max_iter,
+                                          bool test_once = false) {
   const uint32_t a = smem_u32(mbar);
+  if (test_once) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return done != 0;
+  }
   for (int k = 0; k < max_iter; k++) {
     uint32_t done;
     asm volatile(
@@ -254,8 +269,10 @@ __device__ __forceinline__ void proposer_stage_weights(ProposerSmem &s, const Ml
 // its features f[0..5]; out receives the network output (log2 of the
 // proposed step over dt) for this thread's row. Must be called by all
 // threads; returns false (CTA-uniformly) if a completion wait timed out.
+// wait_test: WaitTest bits of the test hook (0 in normal runs).
 __device__ __forceinline__ bool proposer_round(ProposerSmem &s, bool want, const float *f,
-                                               float &out, unsigned *err_flags) {
+                                               float &out, unsigned *err_flags,
+                                               int wait_test = 0) {
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
   if (want) {
@@ -276,9 +293,9 @@ __device__ __forceinline__ bool proposer_round(ProposerSmem &s, bool want, const
               umma_desc_kmajor(smem_u32(s.w1), 128, 256), kMlpIdesc, 0u);
     umma_commit(&s.mbar);
   }
-  uint32_t ph = s.phase;
-  bool ok = __all_sync(0xffffffffu, mbar_wait(&s.mbar, ph, 1 << 22));
-  ph ^= 1u;
+  const uint32_t ph0 = s.phase;
+  bool ok = __all_sync(0xffffffffu, mbar_wait(&s.mbar, ph0, NGPU_WAIT_ITERS,
+                                             (wait_test & WAIT_TEST_FIRST) != 0));
   tc_fence_after();
   float r[32];
   const uint32_t lane_addr = taddr + ((uint32_t)(warp * 32) << 16);
@@ -298,7 +315,10 @@ __device__ __forceinline__ bool proposer_round(ProposerSmem &s, bool want, const
   tc_fence_before();
   const int ok1 = __syncthreads_and(ok);
   if (!ok1) {
-    if (tid == 0) atomicOr(err_flags, (unsigned)DERR_PROPOSER_TIMEOUT);
+    if (tid == 0) {
+      atomicOr(err_flags, (unsigned)DERR_PROPOSER_TIMEOUT);
+      s.phase = proposer_phase_after(ph0, false, false);
+    }
     __syncthreads();
     return false;
   }
@@ -310,8 +330,8 @@ __device__ __forceinline__ bool proposer_round(ProposerSmem &s, bool want, const
               umma_desc_kmajor(smem_u32(s.w2) + 256, 128, 512), kMlpIdesc, 1u);
     umma_commit(&s.mbar);
   }
-  ok = __all_sync(0xffffffffu, mbar_wait(&s.mbar, ph, 1 << 22));
-  ph ^= 1u;
+  ok = __all_sync(0xffffffffu, mbar_wait(&s.mbar, ph0 ^ 1u, NGPU_WAIT_ITERS,
+                                        (wait_test & WAIT_TEST_SECOND) != 0));
   tc_fence_after();
   float o = s.b3;
   if (ok) {
@@ -321,7 +341,7 @@ __device__ __forceinline__ bool proposer_round(ProposerSmem &s, bool want, const
   }
   tc_fence_before();
   const int ok2 = __syncthreads_and(ok);
-  if (tid == 0) s.phase = ph;
+  if (tid == 0) s.phase = proposer_phase_after(ph0, true, ok2 != 0);
   if (!ok2) {
     if (tid == 0) atomicOr(err_flags, (unsigned)DERR_PROPOSER_TIMEOUT);
     __syncthreads();
@@ -335,7 +355,7 @@ __device__ __forceinline__ bool proposer_round(ProposerSmem &s, bool want, const
 // a timed-out wait the tensor-core work may still be in flight: wait for the
 // outstanding completion (bounded) before the columns are released.
 __device__ __forceinline__ void proposer_teardown(ProposerSmem &s, bool failed) {
-  if (failed) mbar_wait(&s.mbar, s.phase, 1 << 22);
+  if (failed) mbar_wait(&s.mbar, s.phase, NGPU_WAIT_ITERS);
   tc_fence_before();
   __syncthreads();
   if ((threadIdx.x >> 5) == 0) {

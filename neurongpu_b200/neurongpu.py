@@ -256,6 +256,9 @@ _EXT_SIG = {
     "NGB200_MlpGradients": (_F, (c_float_p, _I, c_float_p, c_float_p)),
     "NGB200_MlpInfer": (_I, (c_float_p, _I, c_float_p, c_float_p)),
     "NGB200_LastSimulateDeviceMs": (ctypes.c_double, ()),
+    "NGB200_SetRk5MaxSubsteps": (_I, (_I,)),
+    "NGB200_SetWaitTest": (_I, (_I,)),
+    "NGB200_ProposerPhaseAfter": (ctypes.c_uint, (ctypes.c_uint, _I, _I)),
     "NGB200_SetKernelTiming": (_I, (_I,)),
     "NGB200_GetKernelTiming": (_I, (_I, ctypes.POINTER(ctypes.c_double),
                                     ctypes.POINTER(ctypes.c_longlong))),
@@ -315,7 +318,9 @@ class Binding(object):
     def _release(self, pt, value):
         """Frees a host array the library handed out (after its contents
         were copied into value) and returns value."""
-        if pt:
+        # a library without the extensions (the reference's own build) hands
+        # out arrays that its callers never free (src/base_neuron.cu:459)
+        if pt and self.has_extensions:
             self._c["NGB200_FreeArray"](ctypes.cast(pt, c_void_p))
         return value
 
@@ -1208,6 +1213,24 @@ class Binding(object):
     def SetGraphChunk(self, n_steps):
         return self._call("NGB200_SetGraphChunk", ctypes.c_int(n_steps))
 
+    def SetRk5MaxSubsteps(self, n_substeps):
+        """RK5 sub-steps one neuron may take in one time step before
+        Simulate fails with "RK5 integration exceeded the substep limit"
+        (extension; default 200,000)."""
+        return self._call("NGB200_SetRk5MaxSubsteps", ctypes.c_int(n_substeps))
+
+    def SetWaitTest(self, mask):
+        """Test hook (extension): bit 0 / bit 1 make the marked bounded
+        device waits give up after one non-blocking test, so their time-out
+        paths can be exercised; 0 restores normal waits."""
+        return self._call("NGB200_SetWaitTest", ctypes.c_int(mask))
+
+    def ProposerPhaseAfter(self, phase_in, ok1, ok2):
+        """Host copy of the step proposer's barrier-parity bookkeeping
+        (extension, for tests)."""
+        return self._c["NGB200_ProposerPhaseAfter"](ctypes.c_uint(phase_in), ctypes.c_int(int(ok1)),
+                                                    ctypes.c_int(int(ok2)))
+
     def LastSimulateDeviceMs(self):
         return self._call("NGB200_LastSimulateDeviceMs")
 
@@ -1330,9 +1353,9 @@ class Binding(object):
         return t.value, n.value
 
     def GetRk5Tuning(self, i_node):
-        "(chosen RK5 kernel variant, [ms of variants 0..5]) for the group of i_node"
+        "(chosen RK5 kernel variant, [ms of variants 0..8]) for the group of i_node"
         v = ctypes.c_int(0)
-        ms = (ctypes.c_float * 6)()
+        ms = (ctypes.c_float * 9)()
         self._call("NGB200_GetRk5Tuning", ctypes.c_int(i_node), ctypes.byref(v), ms)
         return v.value, list(ms)
 

@@ -92,6 +92,10 @@ struct Oracle {
   struct DC { int gen_node, port; real w, delay; uint64_t stream; };
   std::vector<std::vector<DC>> dc_of;
   std::vector<real> gen_rate, gen_origin, gen_start, gen_stop;  // per node
+  // direct-connection sampler thresholds per generator node and the rate
+  // per step they were formed for
+  std::vector<std::vector<uint32_t>> gen_thr;
+  std::vector<double> gen_thr_lam;
   std::vector<real> acc;          // [node*maxport + port]
   int maxport = 1;
   std::vector<std::vector<std::pair<int, real>>> spikes_at;  // per step: (node, height)
@@ -445,6 +449,23 @@ static void prepare(Oracle &o) {
 static void fold(Oracle &o, long long T_pending, bool poisson) {
   const int N = (int)o.node_group.size();
   double t = (double)T_pending * (double)(float)o.dt;
+  // inversion thresholds per generator node (kept while its rate is unchanged)
+  if (poisson) {
+    if (o.gen_thr.size() != o.gen_rate.size()) {
+      o.gen_thr.assign(o.gen_rate.size(), std::vector<uint32_t>());
+      o.gen_thr_lam.assign(o.gen_rate.size(), -1.0);
+    }
+    for (size_t k = 0; k < o.gen_rate.size(); k++) {
+      if (o.gen_rate[k] == 0) continue;
+      float lf = (float)((double)(float)o.dt / 1000.0) * (float)o.gen_rate[k];
+      double lam = (double)lf;
+      if (o.gen_thr_lam[k] != lam) {
+        o.gen_thr[k].resize(NGPU_CDF_LEN);
+        ngpu::ng_poisson_thresholds(lam, exp(-lam), o.gen_thr[k].data());
+        o.gen_thr_lam[k] = lam;
+      }
+    }
+  }
   // every node folds only its own accumulators and state
 #pragma omp parallel for schedule(static)
   for (int n = 0; n < N; n++) {
@@ -456,8 +477,8 @@ static void fold(Oracle &o, long long T_pending, bool poisson) {
         if (t_rel >= o.gen_start[c.gen_node] && t_rel <= o.gen_stop[c.gen_node]) {
           float lf = (float)((double)(float)o.dt / 1000.0) * (float)o.gen_rate[c.gen_node];
           double lam = (double)lf;
-          unsigned cnt = ngpu::ng_poisson(lam, exp(-lam), o.seed + 12345ULL,
-                                          ngpu::RNG_TAG_POISSON_DIRECT, c.stream, T_pending);
+          unsigned cnt = ngpu::ng_poisson_direct(lam, o.gen_thr[c.gen_node].data(),
+                                                 o.seed + 12345ULL, c.stream, T_pending);
           if (cnt > 0) o.acc[(size_t)n * o.maxport + c.port] += (double)((float)c.w * (float)cnt);
         }
       }

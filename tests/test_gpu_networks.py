@@ -224,11 +224,18 @@ def test_stdp_network_full_scale(ngpu):
     assert ngpu.TotalSpikes() > 0
 
 
-def _chunk_run(ngpu, chunk, fork):
+# delivery modes: in the update's grid (default), on a forked stream, serial
+DELIVERY_ENV = {"fused": {}, "fork": {"NGB200_FUSE_DELIVERY": "0"},
+                "serial": {"NGB200_FUSE_DELIVERY": "0", "NGB200_FORK_DELIVERY": "0"}}
+
+
+def _chunk_run(ngpu, chunk, mode):
     import os
-    old = os.environ.get("NGB200_FORK_DELIVERY")
-    if not fork:
-        os.environ["NGB200_FORK_DELIVERY"] = "0"
+    keys = ("NGB200_FUSE_DELIVERY", "NGB200_FORK_DELIVERY")
+    old = {k: os.environ.get(k) for k in keys}
+    for k in keys:
+        os.environ.pop(k, None)
+    os.environ.update(DELIVERY_ENV[mode])
     try:
         b = ngpu.default_binding()
         b.Reset()
@@ -255,24 +262,27 @@ def _chunk_run(ngpu, chunk, fork):
         v = np.asarray(ngpu.GetNeuronVar(nrn.i0, nrn.n, "V_m"), dtype=np.float32).ravel()
         return totals, counts, v
     finally:
-        if old is None:
-            os.environ.pop("NGB200_FORK_DELIVERY", None)
-        else:
-            os.environ["NGB200_FORK_DELIVERY"] = old
+        for k in keys:
+            if old[k] is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = old[k]
 
 
 def test_step_chunks_and_spike_totals(ngpu):
     """Each step of a captured chunk reads its own copy of the step context
     and the delivery does the step bookkeeping: graphs of 100, 7 and 1 steps,
-    no graph at all, and the serial (unforked) delivery give bit-identical
-    state, and the running spike total equals the sum of the per-neuron spike
-    counts after every Simulate call."""
-    ref = _chunk_run(ngpu, 100, True)
+    no graph at all, and the delivery in the update's grid, on a forked
+    stream or serial give bit-identical state, and the running spike total
+    equals the sum of the per-neuron spike counts after every Simulate
+    call."""
+    ref = _chunk_run(ngpu, 100, "fused")
     assert ref[1].sum() > 100
     assert ref[0][-1] == int(ref[1].sum())
     assert ref[0][0] < ref[0][1] < ref[0][2]
-    for chunk, fork in ((7, True), (1, True), (0, True), (100, False)):
-        totals, counts, v = _chunk_run(ngpu, chunk, fork)
-        assert totals == ref[0], (chunk, fork)
-        assert np.array_equal(counts, ref[1]), (chunk, fork)
-        assert np.array_equal(v.view(np.int32), ref[2].view(np.int32)), (chunk, fork)
+    for chunk, mode in ((7, "fused"), (1, "fused"), (0, "fused"), (100, "fork"), (7, "fork"),
+                        (100, "serial")):
+        totals, counts, v = _chunk_run(ngpu, chunk, mode)
+        assert totals == ref[0], (chunk, mode)
+        assert np.array_equal(counts, ref[1]), (chunk, mode)
+        assert np.array_equal(v.view(np.int32), ref[2].view(np.int32)), (chunk, mode)
