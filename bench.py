@@ -132,28 +132,88 @@ def measured_peaks():
 # DRAM traffic and executed instructions per unit, from ncu captures of the
 # same kernels (dram__bytes_read.sum + dram__bytes_write.sum and
 # smsp__inst_executed.sum per launch, divided by the neurons / warps / events
-# of the launch): RK5 update (8-blocks/SM variant) on the silent network at
-# 200,000 neurons in steady state (cold cache; the state's writes stay in L2
-# during the launch), delivery on the active network at 400,000 neurons.
-TRAFFIC_RK5_PER_NEURON_STEP = 52.4       # bytes
+# of the launch): the RK5 update (6-blocks/SM variant with the fused
+# delivery) on the silent 1e6-neuron network in steady state, caches kept
+# between launches (profiles/rk5_update_steady_1m.md); the delivery on the
+# active network at 400,000 neurons (profiles/deliver_active_400k.md).
+TRAFFIC_RK5_PER_NEURON_STEP = 6.2        # bytes (the state stays L2-resident)
 TRAFFIC_DELIVER_PER_EVENT = 11.3         # bytes
-INST_RK5_PER_WARP_STEP = 995.2           # warp instructions per 32 neuron-steps
+INST_RK5_PER_WARP_STEP = 821.9           # warp instructions per 32 neuron-steps
 SM_COUNT, SMSP_PER_SM = 148, 4
 
 
-def issue_roofline(kname, n, avg_ms, clocks):
-    """Instruction-issue view of the RK5 update (it is issue and latency
-    bound, not HBM bound): warp instructions per launch from the ncu count
+def issue_roofline(n, avg_ms, clocks):
+    """Instruction-issue roofline of the RK5 update (the binding one: the
+    kernel issues 821 warp instructions per 32 neuron-steps and reads its
+    state mostly from L2): warp instructions per launch from the ncu count
     per warp-step, against one instruction per cycle per SM sub-partition at
     the median SM clock sampled during the timed region."""
-    if kname != "rk5_update" or avg_ms <= 0:
-        return None
     mhz = (clocks or {}).get("sm_mhz") or 1965.0
     inst = INST_RK5_PER_WARP_STEP * ((n + 31) // 32)
     achieved = inst / (avg_ms / 1000.0) / 1e9
     peak = SM_COUNT * SMSP_PER_SM * mhz * 1e6 / 1e9
-    return {"unit": "Ginst/s", "achieved": achieved, "peak": peak, "frac": achieved / peak,
+    return {"achieved": achieved, "peak": peak, "unit": "Ginst/s", "frac": achieved / peak,
             "inst_per_launch": inst, "sm_mhz": mhz}
+
+
+SAMPLE_VARS = ("V_m", "w", "g", "g1")
+
+
+def sample_state(ngpu, nrn, idx):
+    """State of the sampled neurons (group-local indices idx): V_m, w and
+    per port g, g1."""
+    import numpy as np
+    nodes = [nrn[int(i)] for i in idx]
+    out = {}
+    for v in SAMPLE_VARS:
+        out[v] = np.asarray(ngpu.GetNeuronPtVar(nodes, v), dtype=np.float64).reshape(len(idx), -1)
+    return out
+
+
+def oracle_replay(cfg, idx, n_steps, gpu_state, threads=0):
+    """Error of the GPU run against the FP64 oracle: the sampled neurons of
+    the silent network (checked by the caller: no spike in the whole run, so
+    each neuron saw only its own Poisson drive) replayed for the same number
+    of steps with the same random streams; returns the largest deviations
+    of the final state."""
+    import numpy as np
+    from oracle import oracle as orc
+    orc.set_threads(threads if threads > 0 else (os.cpu_count() or 1))
+    n = len(idx)
+    net = orc.Network(dt=0.1, seed=1234)
+    net.create(orc.POISSON_GENERATOR, 1, params={"rate": cfg["rate"]})
+    p = {k: (np.float32(v) if np.isscalar(v) else [np.float32(x) for x in v])
+         for k, v in NEURON_PARAMS.items()}
+    grp = net.create(orc.AEIF_COND_BETA, n, 2, params=p, eps=cfg["eps"])
+    net.connect(np.zeros(n, dtype=np.int32), np.arange(n) + 1, 0, cfg["w_pg"], 0.1)
+    net.set_direct_streams(np.asarray(idx, dtype=np.uint64))
+    t0 = time.perf_counter()
+    left = n_steps
+    while left > 0:
+        k = min(left, 10000)
+        net.simulate(k)
+        left -= k
+    wall = time.perf_counter() - t0
+    # the GPU's variable getters fold the last step's pending input first
+    net.flush()
+    nv = len(grp.var_names)
+    err = {"V_m_max_abs_mV": 0.0, "V_m_max_rel": 0.0, "w_max_abs_pA": 0.0,
+           "g_max_rel": 0.0}
+    for k in range(n):
+        v, _ = net.state(1 + k, nv)
+        dv = abs(v[grp.var_index("V_m")] - gpu_state["V_m"][k, 0])
+        err["V_m_max_abs_mV"] = max(err["V_m_max_abs_mV"], dv)
+        err["V_m_max_rel"] = max(err["V_m_max_rel"], dv / 70.0)
+        err["w_max_abs_pA"] = max(err["w_max_abs_pA"],
+                                  abs(v[grp.var_index("w")] - gpu_state["w"][k, 0]))
+        for q in range(2):
+            for name in ("g", "g1"):
+                o = v[grp.var_index(name, q)]
+                g = gpu_state[name][k, q]
+                err["g_max_rel"] = max(err["g_max_rel"], abs(o - g) / max(abs(o), 1e-3))
+    err.update({"neurons": n, "steps": n_steps, "replay_wall_s": wall,
+                "against": "FP64 oracle, same Poisson streams, final state of the run"})
+    return err
 
 
 def cpu_baseline(cfg, n_sample=2000, sim_ms=20.0, threads=0):
@@ -230,12 +290,7 @@ def run_reference(args, world, rank):
     cfg = SCALE if args.config == "scale" else SMALL
     if rank != 0:
         return 0
-    ref_lib = os.path.join(ROOT, "oracle", "_ref", "libneurongpu_ref.so")
     metric = "bio_s_per_wall_s"
-    if os.path.exists(ref_lib) and args.ref_gpu:
-        line = {"impl": "reference", "unavailable": "reference GPU arm not enabled"}
-        print(json.dumps(line))
-        return 0
     vals = []
     for _ in range(max(1, args.warmup)):
         cpu_baseline(cfg, n_sample=args.cpu_sample, sim_ms=5.0)
@@ -252,9 +307,30 @@ def run_reference(args, world, rank):
                                    "dt 0.1 ms, RK5 eps 1e-3", "sample": cb["sample"]},
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "bio_s/wall_s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "reference_gpu": reference_gpu(cfg, args)}
     print(json.dumps(line))
     return 0
+
+
+def reference_gpu(cfg, args):
+    """The reference's own CUDA build (oracle/_ref, compiled from its sources
+    for sm_100a) on the same workload and GPU, driven through its C ABI in a
+    separate process (oracle/ref_gpu.py): wall time of Simulate at the
+    workload's RK5 tolerance 1e-3 and at the reference's built-in 1e-6."""
+    ref_lib = os.path.join(ROOT, "oracle", "_ref", "libneurongpu_ref.so")
+    if not os.path.exists(ref_lib):
+        return {"unavailable": "oracle/_ref/libneurongpu_ref.so was not built"}
+    if args.no_ref_gpu:
+        return {"unavailable": "skipped (--no-ref-gpu)"}
+    cmd = [sys.executable, os.path.join(ROOT, "oracle", "ref_gpu.py"), "--n", str(cfg["n"]),
+           "--steps", "3", "--warmup", "1", "--step-ms", "100", "--eps", "1e-3,1e-6",
+           "--w-pg", str(cfg["w_pg"])]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+        return json.loads(r.stdout.strip().split("\n")[-1])
+    except Exception as e:
+        return {"unavailable": "reference GPU run failed: %s" % str(e)[:200]}
 
 
 def run_sweep(args, world, rank):
@@ -318,6 +394,48 @@ def run_sweep(args, world, rank):
     return 0
 
 
+def run_network(ngpu, b, cfg, args, world, step_ms, steps, warmup):
+    """Builds the network of cfg, warms up, then measures: the timed region
+    (device time of the step loops, no instrumentation), a second run of the
+    same length with CUDA events around every kernel class (per-kernel
+    launch durations), and the counters. Returns a dict."""
+    t_build = time.perf_counter()
+    pg, nrn = build_network(ngpu, cfg)
+    ngpu.ActivateSpikeCount(nrn)
+    connect_s = time.perf_counter() - t_build
+    ngpu.Calibrate()
+    build_s = time.perf_counter() - t_build
+    for _ in range(warmup):
+        ngpu.Simulate(step_ms)
+    ev0, evals0, spikes0 = b.DeliveredEvents(), b.StageEvaluations(), b.TotalSpikes()
+    barrier(world)
+    sampler = ClockSampler(0)
+    sampler.start()
+    dev_ms = 0.0
+    for _ in range(steps):
+        ngpu.Simulate(step_ms)
+        dev_ms += b.LastSimulateDeviceMs()
+    clocks = sampler.stop()
+    barrier(world)
+    dev_ms_max = reduce_max(dev_ms, world)
+    r = {"pg": pg, "nrn": nrn, "build_s": build_s, "connect_s": connect_s, "clocks": clocks,
+         "dev_ms": dev_ms_max, "kernels_per_step": b.KernelsPerStep(),
+         "events": b.DeliveredEvents() - ev0, "evals": b.StageEvaluations() - evals0,
+         "spikes": b.TotalSpikes() - spikes0, "steps_run": warmup + steps}
+    # the same steps with events around every kernel class (serial delivery)
+    b.SetKernelTiming(True)
+    ev1 = b.DeliveredEvents()
+    for _ in range(steps):
+        ngpu.Simulate(step_ms)
+    r["events_instr"] = b.DeliveredEvents() - ev1
+    r["ktime"] = {k: b.GetKernelTiming(i) for i, k in
+                  enumerate(("update", "deliver", "stdp", "bookkeeping"))}
+    b.SetKernelTiming(False)
+    r["steps_run"] += steps
+    r["tuning"] = b.GetRk5Tuning(nrn.i0)
+    return r
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -334,13 +452,24 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=16000)
     ap.add_argument("--cpu-ms", type=float, default=100.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--ref-gpu", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="reference arm: skip the reference's CUDA build")
+    ap.add_argument("--no-active", action="store_true",
+                    help="skip the active (26 Hz) variant of the workload")
+    ap.add_argument("--active-w-pg", type=float, default=0.5,
+                    help="Poisson weight (nS) of the active variant")
     ap.add_argument("--n", type=int, default=0, help="override the number of neurons")
+    ap.add_argument("--k-in", type=int, default=0,
+                    help="override the in-degree (80 %% exc / 20 %% inh; profiling captures "
+                         "of the update kernel at a small device footprint)")
     ap.add_argument("--w-pg", type=float, default=0.0,
                     help="override the Poisson drive weight (nS) for an active network")
     args = ap.parse_args()
     if args.n > 0:
         SCALE["n"] = SMALL["n"] = args.n
+    if args.k_in > 0:
+        for c in (SCALE, SMALL):
+            c["k_exc"], c["k_inh"] = (4 * args.k_in) // 5, args.k_in // 5
     if args.w_pg > 0:
         SCALE["w_pg"] = SMALL["w_pg"] = args.w_pg
     world, rank, local = dist_setup(args)
@@ -349,107 +478,67 @@ def main():
     os.environ.setdefault("CUDA_VISIBLE_DEVICES", str(local))
     if args.config == "sweep":
         return run_sweep(args, world, rank)
+    import numpy as np
     cfg = SCALE if args.config == "scale" else SMALL
     from neurongpu_b200 import neurongpu as ngpu
     b = ngpu.default_binding()
     b.SetVerbosityLevel(0)
-    t_build = time.perf_counter()
-    pg, nrn = build_network(ngpu, cfg)
-    ngpu.ActivateSpikeCount(nrn)
-    connect_s = time.perf_counter() - t_build
-    ngpu.Calibrate()
-    build_s = time.perf_counter() - t_build
     step_ms = args.step_ms
-    # warm-up
-    for _ in range(args.warmup):
-        ngpu.Simulate(step_ms)
-    # timed region (device time of the step loops), per-kernel events on
-    # timed region: device time of the step loops (CUDA events on the
-    # simulation stream), no per-kernel instrumentation
-    ev0 = b.DeliveredEvents()
-    evals0 = b.StageEvaluations()
-    spikes0 = b.TotalSpikes()
-    barrier(world)
-    sampler = ClockSampler(0)
-    sampler.start()
-    dev_ms = 0.0
-    for _ in range(args.steps):
-        ngpu.Simulate(step_ms)
-        dev_ms += b.LastSimulateDeviceMs()
-    clocks = sampler.stop()
-    barrier(world)
-    dev_ms_max = reduce_max(dev_ms, world)
-    kernels_per_step = b.KernelsPerStep()
-    events = b.DeliveredEvents() - ev0
-    evals = b.StageEvaluations() - evals0
-    spikes = b.TotalSpikes() - spikes0
-    # same number of steps again with CUDA events around every kernel class
-    # of every step, for the per-kernel launch durations of the roofline
-    b.SetKernelTiming(True)
-    ev1 = b.DeliveredEvents()
-    for _ in range(args.steps):
-        ngpu.Simulate(step_ms)
-    events_instr = b.DeliveredEvents() - ev1
-    upd_ms, upd_n = b.GetKernelTiming(0)
-    del_ms, del_n = b.GetKernelTiming(1)
-    stdp_ms, stdp_n = b.GetKernelTiming(2)
-    oth_ms, oth_n = b.GetKernelTiming(3)
-    b.SetKernelTiming(False)
+    r = run_network(ngpu, b, cfg, args, world, step_ms, args.steps, args.warmup)
+    pg, nrn = r["pg"], r["nrn"]
     bio_s = args.steps * step_ms / 1000.0
+    dev_ms_max = r["dev_ms"]
     value = world * bio_s / (dev_ms_max / 1000.0)
-    events_per_s = world * events / (dev_ms_max / 1000.0)
     n_steps = int(round(args.steps * step_ms / 0.1))
-    # roofline of the dominant kernel
+    step_launch_ms = dev_ms_max / n_steps
+    upd_ms, upd_n = r["ktime"]["update"]
+    # Roofline of the RK5 update from the uninstrumented timed run: with
+    # about one launch per step (the update with the delivery in its grid,
+    # 1.02 launches per step with the chunk prologue and epilogue) the
+    # launch lasts at most the device time per step; with the delivery on
+    # its own stream the update's own duration comes from the instrumented
+    # run, capped by the step time.
+    one_launch = r["kernels_per_step"] <= 1.1
+    avg_ms = step_launch_ms if one_launch else min(upd_ms / max(upd_n, 1), step_launch_ms)
     peak, peak_kind = measured_peaks()
-    if upd_ms >= del_ms:
-        kname = "rk5_update"
-        bytes_launch = BYTES_PER_NEURON_STEP * cfg["n"]
-        avg_ms = upd_ms / max(upd_n, 1)
-        traffic = TRAFFIC_RK5_PER_NEURON_STEP * cfg["n"]
-    else:
-        kname = "deliver"
-        ev_launch = events_instr / max(del_n, 1)
-        bytes_launch = BYTES_PER_EVENT * ev_launch
-        avg_ms = del_ms / max(del_n, 1)
-        traffic = TRAFFIC_DELIVER_PER_EVENT * ev_launch
-    achieved = bytes_launch / (avg_ms / 1000.0) / 1e9
-    roof = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
-            "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+    bytes_launch = BYTES_PER_NEURON_STEP * cfg["n"]
+    hbm_achieved = bytes_launch / (avg_ms / 1000.0) / 1e9
+    iss = issue_roofline(cfg["n"], avg_ms, r["clocks"])
+    traffic = TRAFFIC_RK5_PER_NEURON_STEP * cfg["n"]
+    roof = {"kernel": "rk5_update", "bound": "issue", "achieved": iss["achieved"],
+            "peak": iss["peak"], "unit": "Ginst/s", "frac": iss["frac"],
+            "inst_per_launch": iss["inst_per_launch"], "sm_mhz": iss["sm_mhz"],
             "traffic": traffic, "avg_launch_ms": avg_ms,
-            "issue": issue_roofline(kname, cfg["n"], avg_ms, clocks),
-            "kernel_ms": {"update": upd_ms, "deliver": del_ms, "stdp": stdp_ms,
-                          "bookkeeping": oth_ms},
-            "launches": {"update": upd_n, "deliver": del_n, "stdp": stdp_n,
-                         "bookkeeping": oth_n},
-            "timing": "kernel events over a second run of the timed steps"}
+            "timing": ("device time per integration step of the uninstrumented timed run "
+                       "(%.2f launches per step)" % r["kernels_per_step"]) if one_launch else
+                      "update launch events of a second run, capped by the step time",
+            "hbm": {"achieved": hbm_achieved, "peak": peak, "peak_source": peak_kind,
+                    "unit": "GB/s", "frac": hbm_achieved / peak, "traffic": traffic,
+                    "bytes_per_launch": bytes_launch},
+            "kernel_ms": {k: v[0] for k, v in r["ktime"].items()},
+            "launches": {k: v[1] for k, v in r["ktime"].items()}}
     # end-to-end through the public API: H2D of the generator parameters,
     # the simulation call, D2H of the per-neuron spike counts
-    # (untimed warm-up first: switching the kernel events off above dropped
-    # the captured step graphs)
     def e2e_step():
         ngpu.SetStatus(pg, "rate", cfg["rate"])
         ngpu.Simulate(step_ms)
         return ngpu.GetNeuronIntVarArray(nrn.i0, nrn.n, "spike_count")
     for _ in range(args.warmup):
         e2e_step()
-    e2e_steps = args.steps
     barrier(world)
     t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        counts = e2e_step()
+    for _ in range(args.steps):
+        e2e_step()
     e2e_wall = reduce_max(time.perf_counter() - t0, world)
-    e2e = {"value": world * e2e_steps * step_ms / 1000.0 / e2e_wall, "unit": "bio_s/wall_s",
+    steps_run = r["steps_run"] + args.warmup + args.steps
+    e2e = {"value": world * args.steps * step_ms / 1000.0 / e2e_wall, "unit": "bio_s/wall_s",
            "h2d_bytes_per_step": 48, "d2h_bytes_per_step": 4 * cfg["n"]}
-    rate_hz = spikes / (cfg["n"] * bio_s)
-    if rank != 0:
-        barrier(world)
-        return 0
-    cpu = None
-    if not args.no_cpu:
-        try:
-            cpu = cpu_baseline(cfg, n_sample=args.cpu_sample, sim_ms=args.cpu_ms)
-        except Exception as e:
-            cpu = {"error": str(e)}
+    rate_hz = r["spikes"] / (cfg["n"] * bio_s)
+    # final state of a sample of neurons for the error against the oracle
+    # (meaningful while the whole run stayed silent)
+    silent_run = b.TotalSpikes() == 0
+    idx = np.linspace(0, cfg["n"] - 1, min(256, cfg["n"])).astype(np.int64)
+    gpu_state = sample_state(ngpu, nrn, idx) if silent_run else None
     line = {
         "metric": "bio_s_per_wall_s", "value": value, "unit": "bio_s/wall_s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -460,20 +549,74 @@ def main():
                    "RK5 eps %g" % (cfg["n"], cfg["k_exc"] + cfg["k_inh"], cfg["rate"],
                                    cfg["w_pg"], cfg["eps"]),
                    "step_bio_ms": step_ms, "integration_steps": n_steps,
-                   "l2": "inputs larger than L2 (1e9 synapses, 8 GB)",
+                   "l2": ("no flush: the synapse tables (%.1f GB) exceed L2; the neuron state "
+                          "(%d MB) stays L2-resident across the integration steps of a bench "
+                          "step, as in any run of the simulator"
+                          % (cfg["n"] * (cfg["k_exc"] + cfg["k_inh"]) * 8 / 1e9,
+                             cfg["n"] * 72 // 1000000)),
                    "parallelism": "replicas" if world > 1 else "single"},
-        "syn_events_per_s": events_per_s,
+        "syn_events_per_s": world * r["events"] / (dev_ms_max / 1000.0),
         "mean_rate_hz": rate_hz,
-        "rk5_stage_evals_per_neuron_step": evals / (cfg["n"] * n_steps),
+        "rk5_stage_evals_per_neuron_step": r["evals"] / (cfg["n"] * n_steps),
         "wall_per_bio_s": (dev_ms_max / 1000.0) / bio_s,
-        "rk5_tuning": b.GetRk5Tuning(nrn.i0),
-        "build_s": build_s, "connect_s": connect_s, "calibrate_s": build_s - connect_s,
-        "gpu_launches": int(round(kernels_per_step * n_steps)),
+        "rk5_tuning": r["tuning"],
+        "build_s": r["build_s"], "connect_s": r["connect_s"],
+        "calibrate_s": r["build_s"] - r["connect_s"],
+        "gpu_launches": int(round(r["kernels_per_step"] * n_steps)),
         "roofline": roof,
-        "cpu_baseline": cpu,
         "e2e": e2e,
-        "clocks": clocks,
+        "clocks": r["clocks"],
     }
+    # the same network at a drive that makes it fire (delivery measured)
+    if not args.no_active and args.config == "scale":
+        acfg = dict(cfg)
+        acfg["w_pg"] = args.active_w_pg
+        b.Reset()
+        b.SetVerbosityLevel(0)
+        a_steps = max(1, min(args.steps, 3))
+        ar = run_network(ngpu, b, acfg, args, world, step_ms, a_steps, max(1, min(args.warmup, 3)))
+        a_bio = a_steps * step_ms / 1000.0
+        a_nst = int(round(a_steps * step_ms / 0.1))
+        d_ms, d_n = ar["ktime"]["deliver"]
+        ev_launch = ar["events_instr"] / max(d_n, 1)
+        d_avg = d_ms / max(d_n, 1)
+        d_ach = BYTES_PER_EVENT * ev_launch / (d_avg / 1000.0) / 1e9 if d_avg > 0 else 0.0
+        line["active"] = {
+            "workload": "the same network with Poisson w %g nS" % acfg["w_pg"],
+            "value": world * a_bio / (ar["dev_ms"] / 1000.0), "unit": "bio_s/wall_s",
+            "ms_per_step": ar["dev_ms"] / a_steps, "steps": a_steps,
+            "syn_events_per_s": world * ar["events"] / (ar["dev_ms"] / 1000.0),
+            "mean_rate_hz": ar["spikes"] / (acfg["n"] * a_bio),
+            "rk5_stage_evals_per_neuron_step": ar["evals"] / (acfg["n"] * a_nst),
+            "kernels_per_step": ar["kernels_per_step"],
+            "deliver_roofline": {"kernel": "deliver", "bound": "hbm", "achieved": d_ach,
+                                 "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+                                 "frac": d_ach / peak, "events_per_launch": ev_launch,
+                                 "traffic": TRAFFIC_DELIVER_PER_EVENT * ev_launch,
+                                 "avg_launch_ms": d_avg,
+                                 "timing": "delivery launch events of the instrumented run "
+                                           "(serial delivery)"},
+            "kernel_ms": {k: v[0] for k, v in ar["ktime"].items()},
+            "rk5_tuning": ar["tuning"], "clocks": ar["clocks"]}
+    if rank != 0:
+        barrier(world)
+        return 0
+    cpu = None
+    if not args.no_cpu:
+        try:
+            cpu = cpu_baseline(cfg, n_sample=args.cpu_sample, sim_ms=args.cpu_ms)
+        except Exception as e:
+            cpu = {"error": str(e)}
+        if gpu_state is not None:
+            try:
+                line["oracle_err"] = oracle_replay(cfg, idx, steps_run * int(round(step_ms / 0.1)),
+                                                   gpu_state)
+            except Exception as e:
+                line["oracle_err"] = {"error": str(e)[:300]}
+        else:
+            line["oracle_err"] = {"unavailable": "the network spiked; sampled neurons are not "
+                                                 "independent of the rest"}
+    line["cpu_baseline"] = cpu
     print(json.dumps(line))
     sys.stdout.flush()
     barrier(world)

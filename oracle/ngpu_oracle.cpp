@@ -95,6 +95,10 @@ struct Oracle {
   // direct-connection sampler thresholds per generator node and the rate
   // per step they were formed for
   std::vector<std::vector<uint32_t>> gen_thr;
+  // explicit random streams of the direct connections, in their (source,
+  // delay, insertion) order; empty: the order index (test hook: a sample of
+  // a larger network keeps that network's streams)
+  std::vector<uint64_t> dc_stream_set;
   std::vector<double> gen_thr_lam;
   std::vector<real> acc;          // [node*maxport + port]
   int maxport = 1;
@@ -388,7 +392,8 @@ static void prepare(Oracle &o) {
       Oracle::DC c;
       c.gen_node = s; c.port = e.port; c.w = e.w;
       c.delay = (real)((float)o.dt * (float)e.d);
-      c.stream = stream++;
+      c.stream = stream < o.dc_stream_set.size() ? o.dc_stream_set[stream] : stream;
+      stream++;
       o.dc_of[e.tgt].push_back(c);
     }
   }
@@ -883,6 +888,12 @@ int orc_add_syn_group(void *h, int type, const double *p, int np) {
 }
 
 // delays in ms, converted like src/connect.cu:37 (d_int + 1 steps)
+void orc_set_direct_streams(void *h, long long n, const unsigned long long *streams) {
+  Oracle *o = (Oracle *)h;
+  o->dc_stream_set.assign(streams, streams + n);
+  o->prepared = false;
+}
+
 int orc_connect(void *h, long long n, const int *src, const int *tgt, const int *port,
                 const int *syn, const float *w, const float *delay) {
   Oracle *o = (Oracle *)h;

@@ -106,6 +106,7 @@ def _load():
     lib.orc_rule_edges.argtypes = (ctypes.c_int, ctypes.c_ulonglong, ctypes.c_ulonglong,
                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _ip)
     lib.orc_get_threads.restype = ctypes.c_int
+    lib.orc_set_direct_streams.argtypes = (ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p)
     return lib
 
 
@@ -270,6 +271,13 @@ class Network(object):
         d = np.ascontiguousarray(np.broadcast_to(delay, (n,)), dtype=np.float32)
         lib().orc_connect(self.h, n, _ptr(src, _ip), _ptr(tgt, _ip), _ptr(port, _ip),
                           _ptr(syn, _ip), _ptr(w, _fp), _ptr(d, _fp))
+
+    def set_direct_streams(self, streams):
+        """Random streams of the Poisson direct connections in their (source,
+        delay, insertion) order, e.g. those a sample of neurons has in a
+        larger network (the GPU numbers them the same way)."""
+        st = np.ascontiguousarray(streams, dtype=np.uint64)
+        lib().orc_set_direct_streams(self.h, len(st), st.ctypes.data_as(ctypes.c_void_p))
 
     def simulate(self, n_steps, record=()):
         """record: list of (node, var_index). Returns array [n_steps, len(record)]."""
