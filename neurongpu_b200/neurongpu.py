@@ -105,6 +105,11 @@ def _cstr(s):
     return ctypes.create_string_buffer(b, len(b) + 1)
 
 
+def waitenter(val):
+    "Print val and wait for the Enter key (as the reference's module does)"
+    return input(val)
+
+
 def _is_seq(x):
     return isinstance(x, (list, tuple, NodeSeq))
 

@@ -69,6 +69,7 @@ struct Group {
   std::vector<int> sg_off, sg_step, sg_next;
   std::vector<real> sg_height;
   long long evals = 0;
+  bool step_search = false;     // exact step search instead of the controller (bound)
 };
 
 struct Edge {
@@ -277,6 +278,68 @@ static void rk5_step(int model, int np, int nv, real &x, real *y, real &h, real 
   if (err > c_err_min) h = h * c_coeff * pow(err, c_exp_inc);
   else h = 5.0 * h;
   for (int i = 0; i < nv; i++) y[i] = yn[i];
+}
+
+// Scaled error of one Cash-Karp attempt with step h from y (no state
+// change): the quantity the controller compares with 1 (the error scale
+// formed with this h). Used by the exact step search.
+static real rk5_trial_err(int model, int np, int nv, const real *y, const real *k1, real h,
+                          const real *p, real eps, real *yout) {
+  real k2[64], k3[64], k4[64], k5[64], k6[64], yn[64];
+  for (int i = 0; i < nv; i++) yn[i] = y[i] + h * c_a21 * k1[i];
+  deriv(model, np, yn, k2, p);
+  for (int i = 0; i < nv; i++) yn[i] = y[i] + h * (c_a31 * k1[i] + c_a32 * k2[i]);
+  deriv(model, np, yn, k3, p);
+  for (int i = 0; i < nv; i++) yn[i] = y[i] + h * (c_a41 * k1[i] + c_a42 * k2[i] + c_a43 * k3[i]);
+  deriv(model, np, yn, k4, p);
+  for (int i = 0; i < nv; i++)
+    yn[i] = y[i] + h * (c_a51 * k1[i] + c_a52 * k2[i] + c_a53 * k3[i] + c_a54 * k4[i]);
+  deriv(model, np, yn, k5, p);
+  for (int i = 0; i < nv; i++)
+    yn[i] = y[i] + h * (c_a61 * k1[i] + c_a62 * k2[i] + c_a63 * k3[i] + c_a64 * k4[i]
+                        + c_a65 * k5[i]);
+  deriv(model, np, yn, k6, p);
+  real err = 0;
+  for (int i = 0; i < nv; i++) {
+    yout[i] = y[i] + h * (c_a71 * k1[i] + c_a73 * k3[i] + c_a74 * k4[i] + c_a76 * k6[i]);
+    real val = h * (c_e1 * k1[i] + c_e3 * k3[i] + c_e4 * k4[i] + c_e5 * k5[i] + c_e6 * k6[i]);
+    real ys = fabs(y[i]) + fabs(k1[i] * h) + c_scal_min;
+    err = std::max(err, fabs(val / ys));
+  }
+  return err / eps;
+}
+
+// One sub-step with the largest step in [h_min, h_max] that the error test
+// accepts, found by bisection over log h (a proposer that knew the answer):
+// only the accepted attempt's 6 evaluations are counted, so the group's
+// evaluation count is a lower bound for any step-size proposer that keeps
+// the same acceptance test.
+static void rk5_step_search(int model, int np, int nv, real &x, real *y, real &h, real h_min,
+                            real h_max, const real *p, real eps, long long &evals) {
+  real k1[64], yn[64], yb[64];
+  deriv(model, np, y, k1, p);
+  real hs = h_max;
+  if (rk5_trial_err(model, np, nv, y, k1, h_max, p, eps, yb) > 1.0) {
+    real lo = log(h_min), hi = log(h_max);
+    real best = h_min;
+    rk5_trial_err(model, np, nv, y, k1, h_min, p, eps, yb);
+    for (int it = 0; it < 40; it++) {
+      const real mid = 0.5 * (lo + hi);
+      const real hm = exp(mid);
+      if (rk5_trial_err(model, np, nv, y, k1, hm, p, eps, yn) <= 1.0) {
+        lo = mid;
+        best = hm;
+        for (int i = 0; i < nv; i++) yb[i] = yn[i];
+      } else {
+        hi = mid;
+      }
+    }
+    hs = best;
+  }
+  evals += 6;
+  x += hs;
+  h = hs;
+  for (int i = 0; i < nv; i++) y[i] = yb[i];
 }
 
 static double propagator_32(double tau_syn, double tau, double C, double h) {
@@ -613,8 +676,12 @@ static void step(Oracle &o, int it_in_session) {
             int guard = 0;
             while (!end && guard++ < 200000) {
               real hmax = x1 - x;
-              rk5_step(g.model, g.model == O_AEIF_PSC_DELTA ? 0 : g.np, g.nvar, x, y, h, h_min,
-                       hmax, p, g.eps, evals[tid]);
+              if (g.step_search)
+                rk5_step_search(g.model, g.model == O_AEIF_PSC_DELTA ? 0 : g.np, g.nvar, x, y, h,
+                                h_min, hmax, p, g.eps, evals[tid]);
+              else
+                rk5_step(g.model, g.model == O_AEIF_PSC_DELTA ? 0 : g.np, g.nvar, x, y, h, h_min,
+                         hmax, p, g.eps, evals[tid]);
               end = (x >= x1 - h_min);
               if (external_update(g.model, y, p, end, o.dt)) part[tid].push_back({node, 1.0});
             }
@@ -641,8 +708,12 @@ static void step(Oracle &o, int it_in_session) {
         int guard = 0;
         while (!end && guard++ < 200000) {
           real hmax = x1 - x;
-          rk5_step(g.model, g.model == O_AEIF_PSC_DELTA ? 0 : g.np, g.nvar, x, y, h, h_min, hmax,
-                   p, g.eps, g.evals);
+          if (g.step_search)
+            rk5_step_search(g.model, g.model == O_AEIF_PSC_DELTA ? 0 : g.np, g.nvar, x, y, h,
+                            h_min, hmax, p, g.eps, g.evals);
+          else
+            rk5_step(g.model, g.model == O_AEIF_PSC_DELTA ? 0 : g.np, g.nvar, x, y, h, h_min,
+                     hmax, p, g.eps, g.evals);
           end = (x >= x1 - h_min);
           if (external_update(g.model, y, p, end, o.dt)) push(o, node, 1.0, T);
         }
@@ -888,6 +959,13 @@ int orc_add_syn_group(void *h, int type, const double *p, int np) {
 }
 
 // delays in ms, converted like src/connect.cu:37 (d_int + 1 steps)
+void orc_set_step_search(void *h, int group, int on) {
+  Oracle *o = (Oracle *)h;
+  o->groups[group].step_search = on != 0;
+}
+
+long long orc_group_evals(void *h, int group) { return ((Oracle *)h)->groups[group].evals; }
+
 void orc_set_direct_streams(void *h, long long n, const unsigned long long *streams) {
   Oracle *o = (Oracle *)h;
   o->dc_stream_set.assign(streams, streams + n);

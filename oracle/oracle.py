@@ -107,6 +107,9 @@ def _load():
                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _ip)
     lib.orc_get_threads.restype = ctypes.c_int
     lib.orc_set_direct_streams.argtypes = (ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p)
+    lib.orc_set_step_search.argtypes = (ctypes.c_void_p, ctypes.c_int, ctypes.c_int)
+    lib.orc_group_evals.restype = ctypes.c_longlong
+    lib.orc_group_evals.argtypes = (ctypes.c_void_p, ctypes.c_int)
     return lib
 
 
@@ -271,6 +274,15 @@ class Network(object):
         d = np.ascontiguousarray(np.broadcast_to(delay, (n,)), dtype=np.float32)
         lib().orc_connect(self.h, n, _ptr(src, _ip), _ptr(tgt, _ip), _ptr(port, _ip),
                           _ptr(syn, _ip), _ptr(w, _fp), _ptr(d, _fp))
+
+    def set_step_search(self, group, on=True):
+        """Exact step search for an RK5 group: every sub-step takes the
+        largest step the error test accepts (a lower bound on the stage
+        evaluations of any step proposer)."""
+        lib().orc_set_step_search(self.h, group.gid, 1 if on else 0)
+
+    def group_evals(self, group):
+        return lib().orc_group_evals(self.h, group.gid)
 
     def set_direct_streams(self, streams):
         """Random streams of the Poisson direct connections in their (source,
