@@ -333,10 +333,45 @@ def reference_gpu(cfg, args):
         return {"unavailable": "reference GPU run failed: %s" % str(e)[:200]}
 
 
+def shard_networks(sizes, world):
+    """Independent networks to ranks, greedily by neuron count: the largest
+    unassigned network goes to the rank with the fewest neurons so far
+    (ties to the lower rank). Returns the network indices of every rank."""
+    order = sorted(range(len(sizes)), key=lambda i: (-sizes[i], i))
+    load = [0] * world
+    out = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += sizes[i]
+    return [sorted(x) for x in out]
+
+
+def reduce_sum(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def sweep_phase_totals(local, world):
+    """Whole-sweep figures of one phase from every rank's own: device time is
+    the slowest rank's, counts are summed."""
+    out = {"device_ms": reduce_max(local["device_ms"], world)}
+    for k in ("evals", "spikes", "neuron_steps", "neurons"):
+        out[k] = reduce_sum(local[k], world)
+    return out
+
+
 def run_sweep(args, world, rank):
     """Batched + learned workload: 256 independent AdEx networks (sizes
     log-uniform in 1k-50k, in-degree 100-500, a, b and Poisson rate on a
-    seeded grid), all RK5 groups integrated by one batched launch per step.
+    seeded grid), all RK5 groups of a rank integrated by one batched launch
+    per step. With N ranks the networks are sharded by size (no exchange:
+    they are independent); the device time is the slowest rank's.
     Phases: plain controller with accepted-step logging, GPU training of the
     step proposer, then the same networks continued with the plain and with
     the learned controller; prints one JSON line comparing them."""
@@ -347,28 +382,36 @@ def run_sweep(args, world, rank):
     if args.no_batch:
         b.SetRk5Batching(False)
     grid = sweep.sweep_grid(args.nets, 1000, 50000, 100, 500, seed=2024)
+    mine = shard_networks([p["n"] for p in grid], world)[rank]
+    my_grid = [grid[i] for i in mine]
     t0 = time.perf_counter()
-    nets = sweep.build_sweep(b, grid, w_pg=args.sweep_w_pg)
+    nets = sweep.build_sweep(b, my_grid, w_pg=args.sweep_w_pg)
     ngpu.Calibrate()
-    build_s = time.perf_counter() - t0
+    build_s = reduce_max(time.perf_counter() - t0, world)
+    n_mine = sum(p["n"] for p in my_grid)
     n_tot = sum(p["n"] for p in grid)
     b.SetStepLog(None, args.log_cap)
     b.Simulate(args.step_ms)
-    logged = b.GetStepLogCount(None)
+    logged = reduce_sum(b.GetStepLogCount(None), world)
     t1 = time.perf_counter()
     rows, l0, l1 = b.TrainStepProposer(steps=args.train_steps, blocks=64, lr=3e-3, seed=5)
-    train_s = time.perf_counter() - t1
+    train_s = reduce_max(time.perf_counter() - t1, world)
 
     def phase():
         e0, s0, ms = b.StageEvaluations(), b.TotalSpikes(), 0.0
+        barrier(world)
         for _ in range(args.steps):
             b.Simulate(args.step_ms)
             ms += b.LastSimulateDeviceMs()
-        steps = n_tot * args.steps * args.step_ms / 0.1
+        steps = args.steps * args.step_ms / 0.1
+        tot = sweep_phase_totals({"device_ms": ms, "evals": b.StageEvaluations() - e0,
+                                  "spikes": b.TotalSpikes() - s0,
+                                  "neuron_steps": n_mine * steps, "neurons": n_mine}, world)
         bio = args.steps * args.step_ms / 1000.0
-        return {"bio_s_per_wall_s": bio / (ms / 1000.0), "device_ms": ms,
-                "stage_evals_per_neuron_step": (b.StageEvaluations() - e0) / steps,
-                "mean_rate_hz": (b.TotalSpikes() - s0) / (n_tot * bio)}
+        return {"bio_s_per_wall_s": bio / (tot["device_ms"] / 1000.0),
+                "device_ms": tot["device_ms"],
+                "stage_evals_per_neuron_step": tot["evals"] / tot["neuron_steps"],
+                "mean_rate_hz": tot["spikes"] / (tot["neurons"] * bio)}
     for _ in range(args.warmup):
         b.Simulate(args.step_ms)
     plain = phase()
@@ -376,14 +419,19 @@ def run_sweep(args, world, rank):
     for _ in range(args.warmup):
         b.Simulate(args.step_ms)
     learned = phase()
+    if rank != 0:
+        return 0
     line = {"metric": "sweep_bio_s_per_wall_s", "value": plain["bio_s_per_wall_s"],
-            "unit": "bio_s/wall_s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "unit": "bio_s/wall_s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "strong" if world > 1 else "weak",
+            "dtype": "f32", "data": "synthetic",
             "config": {"workload": "sweep: %d aeif_cond_beta networks, %d neurons, sizes "
                                    "log-uniform 1k-50k, in-degree 100-500, a 0-8 nS, b 0-150 pA, "
                                    "Poisson 10-30 kHz w %g nS, dt 0.1 ms, RK5 eps 1e-3"
                                    % (len(grid), n_tot, args.sweep_w_pg),
-                       "batched_launch": not args.no_batch, "step_bio_ms": args.step_ms},
+                       "batched_launch": not args.no_batch, "step_bio_ms": args.step_ms,
+                       "parallelism": ("networks sharded by size over %d ranks, no exchange"
+                                       % world) if world > 1 else "single"},
             "build_s": build_s, "logged_substeps": logged, "train_rows": rows,
             "train_loss_first": l0, "train_loss_last": l1, "train_s": train_s,
             "plain": plain, "learned": learned,
