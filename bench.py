@@ -139,17 +139,28 @@ def measured_peaks():
 TRAFFIC_RK5_PER_NEURON_STEP = 6.2        # bytes (the state stays L2-resident)
 TRAFFIC_DELIVER_PER_EVENT = 11.3         # bytes
 INST_RK5_PER_WARP_STEP = 821.9           # warp instructions per 32 neuron-steps
+# the window kernel (several steps per launch; register cap for 6 blocks per
+# SM), 200,000 neurons of the silent network, windows of 10 steps
+# (profiles/rk5_window_200k.md)
+TRAFFIC_RK5_WINDOW_PER_NEURON_STEP = 3.69
+INST_RK5_WINDOW_PER_WARP_STEP = 634.6
+# algorithmic bytes of a window launch per neuron: the state (variables,
+# step size, time offset, refractory counter) read and written once per
+# window, the port inputs read and cleared every step
+BYTES_WINDOW_STATE_PER_NEURON = 56
+BYTES_WINDOW_INPUT_PER_NEURON_STEP = 16
 SM_COUNT, SMSP_PER_SM = 148, 4
 
 
-def issue_roofline(n, avg_ms, clocks):
+def issue_roofline(n, avg_ms, clocks, steps_per_launch=1, inst_per_warp_step=None):
     """Instruction-issue roofline of the RK5 update (the binding one: the
-    kernel issues 821 warp instructions per 32 neuron-steps and reads its
-    state mostly from L2): warp instructions per launch from the ncu count
-    per warp-step, against one instruction per cycle per SM sub-partition at
-    the median SM clock sampled during the timed region."""
+    kernel issues 650-820 warp instructions per 32 neuron-steps and reads
+    its state mostly from L2): warp instructions per launch from the ncu
+    count per warp-step, against one instruction per cycle per SM
+    sub-partition at the median SM clock sampled during the timed region."""
     mhz = (clocks or {}).get("sm_mhz") or 1965.0
-    inst = INST_RK5_PER_WARP_STEP * ((n + 31) // 32)
+    per = INST_RK5_PER_WARP_STEP if inst_per_warp_step is None else inst_per_warp_step
+    inst = per * ((n + 31) // 32) * steps_per_launch
     achieved = inst / (avg_ms / 1000.0) / 1e9
     peak = SM_COUNT * SMSP_PER_SM * mhz * 1e6 / 1e9
     return {"achieved": achieved, "peak": peak, "unit": "Ginst/s", "frac": achieved / peak,
@@ -546,20 +557,39 @@ def main():
     # launch lasts at most the device time per step; with the delivery on
     # its own stream the update's own duration comes from the instrumented
     # run, capped by the step time.
+    # With several steps per launch (a quiet network whose delays allow
+    # windows) the update launch integrates W steps; its duration comes from
+    # the instrumented run's events around it (nothing runs beside it).
+    spl = n_steps / max(upd_n, 1)
+    window = spl > 1.5
     one_launch = r["kernels_per_step"] <= 1.1
-    avg_ms = step_launch_ms if one_launch else min(upd_ms / max(upd_n, 1), step_launch_ms)
     peak, peak_kind = measured_peaks()
-    bytes_launch = BYTES_PER_NEURON_STEP * cfg["n"]
+    if window:
+        W = int(round(spl))
+        avg_ms = upd_ms / max(upd_n, 1)
+        bytes_launch = cfg["n"] * (BYTES_WINDOW_STATE_PER_NEURON +
+                                   BYTES_WINDOW_INPUT_PER_NEURON_STEP * W)
+        iss = issue_roofline(cfg["n"], avg_ms, r["clocks"], W, INST_RK5_WINDOW_PER_WARP_STEP)
+        traffic = TRAFFIC_RK5_WINDOW_PER_NEURON_STEP * cfg["n"] * W
+        kernel = "rk5_window"
+        timing = ("window launch events of the instrumented run (%d integration steps per "
+                  "launch)" % W)
+    else:
+        W = 1
+        avg_ms = step_launch_ms if one_launch else min(upd_ms / max(upd_n, 1), step_launch_ms)
+        bytes_launch = BYTES_PER_NEURON_STEP * cfg["n"]
+        iss = issue_roofline(cfg["n"], avg_ms, r["clocks"])
+        traffic = TRAFFIC_RK5_PER_NEURON_STEP * cfg["n"]
+        kernel = "rk5_update"
+        timing = ("device time per integration step of the uninstrumented timed run "
+                  "(%.2f launches per step)" % r["kernels_per_step"]) if one_launch else \
+                 "update launch events of a second run, capped by the step time"
     hbm_achieved = bytes_launch / (avg_ms / 1000.0) / 1e9
-    iss = issue_roofline(cfg["n"], avg_ms, r["clocks"])
-    traffic = TRAFFIC_RK5_PER_NEURON_STEP * cfg["n"]
-    roof = {"kernel": "rk5_update", "bound": "issue", "achieved": iss["achieved"],
+    roof = {"kernel": kernel, "bound": "issue", "achieved": iss["achieved"],
             "peak": iss["peak"], "unit": "Ginst/s", "frac": iss["frac"],
             "inst_per_launch": iss["inst_per_launch"], "sm_mhz": iss["sm_mhz"],
-            "traffic": traffic, "avg_launch_ms": avg_ms,
-            "timing": ("device time per integration step of the uninstrumented timed run "
-                       "(%.2f launches per step)" % r["kernels_per_step"]) if one_launch else
-                      "update launch events of a second run, capped by the step time",
+            "traffic": traffic, "avg_launch_ms": avg_ms, "steps_per_launch": W,
+            "timing": timing,
             "hbm": {"achieved": hbm_achieved, "peak": peak, "peak_source": peak_kind,
                     "unit": "GB/s", "frac": hbm_achieved / peak, "traffic": traffic,
                     "bytes_per_launch": bytes_launch},

@@ -213,6 +213,42 @@ unsigned long long NGB200_StageEvaluations();
 unsigned long long NGB200_DeliveredEvents();
 /* Spikes emitted so far (all nodes). */
 unsigned long long NGB200_TotalSpikes();
+
+/* Networks partitioned over hosts, one GPU per host process. These replace
+ * the reference's MPI transport (src/spike_mpi.cu:284-486, the per-step
+ * exchange of src/neurongpu.cu:490-521); NeuronGPU_ConnectMpiInit takes the
+ * host index and count from the job launcher's environment, and the remote
+ * entry points above make image nodes on the target host and mark exported
+ * nodes on the source host. The caller moves the spikes between hosts with
+ * its own collective, every NGB200_RemoteExchangeSteps() steps:
+ *   NGB200_SimulateSteps(E); count = NGB200_PackRemoteSpikes(E, buf, cap);
+ *   all-gather the lists; NGB200_UnpackRemoteSpikes(h, E, list_h, count_h)
+ *   for every other host h.
+ * The Python layer's Simulate does this with torch.distributed. */
+/* Sets this instance's host index and host count. */
+int NGB200_SetHost(int id, int n_hosts);
+/* Runs n_steps steps of a started simulation (NeuronGPU_StartSimulation). */
+int NGB200_SimulateSteps(long long n_steps);
+/* The longest exchange interval (steps) this host allows: the shortest delay
+ * of a connection from an image node, and on a host that exports spikes the
+ * steps its spike ring keeps (at least 32); 0 if it neither receives nor
+ * sends remote spikes. The hosts exchange at the minimum over all hosts. */
+int NGB200_RemoteExchangeSteps();
+/* Packs the spikes of exported nodes emitted in the last n_steps steps into
+ * the device buffer buf of 4 + 3 * cap 32-bit words: [count, overflow, 0, 0]
+ * then (step offset, node, height bits) per spike. Returns the count; when
+ * it exceeds cap only cap spikes were written: pack again into a larger
+ * buffer (the spikes stay in the ring). Synchronises the simulation stream. */
+long long NGB200_PackRemoteSpikes(int n_steps, void *buf, long long cap);
+/* Pushes the spikes of host src_host's packed list (device buffer, count
+ * entries) whose nodes have images here into the spike ring, at the steps
+ * they were emitted; n_steps as in the matching pack. Queued on the
+ * simulation stream. */
+int NGB200_UnpackRemoteSpikes(int src_host, int n_steps, const void *buf, long long count);
+/* Selects simulation instance k (0 <= k < 16; created on first use): every
+ * later call of this interface acts on it. Instance 0 is the default. */
+int NGB200_SetInstance(int k);
+int NGB200_GetInstance();
 /* Host wall time of the last NeuronGPU_Simulate call, in seconds. */
 double NGB200_LastSimulateSeconds();
 /* Steps per captured CUDA graph (default 100); 0 launches without graphs. */
@@ -349,7 +385,9 @@ int NGB200_DeliverSpikes(const unsigned long long *grp_off,
  * (nd + 1) * n_spikes <= 1048576 spike-list entries, larger batches are
  * rejected with return code 5 before any work is queued. The first call on a
  * device looks up the array's device address with that device current; make
- * that first call before any stream capture. All calls share the array:
+ * that first call before any stream capture. The address is kept for the
+ * life of the process: do not call this entry point after cudaDeviceReset
+ * (the reset ends the context the address belongs to). All calls share the array:
  * each call clears its counters and error word first, and calls that
  * overlap on the GPU race on it. Returns after the stream is drained. */
 int NGB200_DeliverSpikesNoAlloc(const unsigned long long *grp_off,

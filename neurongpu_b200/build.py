@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["ngpu_kernels.cu", "ngpu_rk5_aeif_cond_beta.cu", "ngpu_rk5_aeif_cond_alpha.cu",
               "ngpu_rk5_aeif_psc.cu", "ngpu_rk5_izh_cond_beta.cu", "ngpu_rk5_batch.cu",
               "ngpu_step_proposer.cu", "ngpu_connect_device.cu", "ngpu_deliver_api.cu",
-              "ngpu_deliver_static.cu"]
+              "ngpu_deliver_static.cu", "ngpu_remote.cu"]
 CPP_SOURCES = ["ngpu_core.cpp", "ngpu_connect.cpp", "neurongpu_C.cpp"]
 
 

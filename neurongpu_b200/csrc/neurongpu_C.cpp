@@ -18,11 +18,35 @@ using ngpu::ConnectionId;
 using ngpu::ConnectionStatus;
 using ngpu::NeuronGPU;
 
-static NeuronGPU *g_ngpu = nullptr;
+// Instances: one by default, as in the reference; NGB200_SetInstance selects
+// another (several simulators in one process, e.g. the hosts of a
+// partitioned network driven from one process).
+static const int kMaxInstances = 16;
+static NeuronGPU *g_inst[kMaxInstances] = {nullptr};
+static int g_cur = 0;
 
 static NeuronGPU *inst() {
-  if (g_ngpu == nullptr) g_ngpu = new NeuronGPU();
-  return g_ngpu;
+  if (g_inst[g_cur] == nullptr) g_inst[g_cur] = new NeuronGPU();
+  return g_inst[g_cur];
+}
+
+// host index and count of this process in a job launched one process per
+// GPU: the launcher's environment (torchrun RANK / WORLD_SIZE, Open MPI,
+// PMI), 0 of 1 without one
+static void host_from_env(int *id, int *n) {
+  const char *pairs[][2] = {{"RANK", "WORLD_SIZE"},
+                            {"OMPI_COMM_WORLD_RANK", "OMPI_COMM_WORLD_SIZE"},
+                            {"PMI_RANK", "PMI_SIZE"}};
+  *id = 0;
+  *n = 1;
+  for (auto &p : pairs) {
+    const char *r = getenv(p[0]), *s = getenv(p[1]);
+    if (r != nullptr && s != nullptr) {
+      *id = atoi(r);
+      *n = atoi(s);
+      return;
+    }
+  }
 }
 
 template <class R, class F>
@@ -76,10 +100,6 @@ static int *conn_ids_to_c(const std::vector<ConnectionId> &v, int *n_conn) {
     a[3 * i + 2] = v[i].i_conn_;
   }
   return a;
-}
-
-static int no_mpi() {
-  throw ngpu::ngpu_exception("MPI is not available in this build (single-GPU core)");
 }
 
 extern "C" {
@@ -254,11 +274,21 @@ int NeuronGPU_SimulationStep() {
 int NeuronGPU_EndSimulation() {
   return guarded(0, [&](NeuronGPU *n) { return n->EndSimulation(); });
 }
-int NeuronGPU_ConnectMpiInit(int, char *[]) { return guarded(0, [&](NeuronGPU *) { return no_mpi(); }); }
-int NeuronGPU_MpiId() { return guarded(0, [&](NeuronGPU *) { return no_mpi(); }); }
-int NeuronGPU_MpiNp() { return guarded(0, [&](NeuronGPU *) { return no_mpi(); }); }
-int NeuronGPU_ProcMaster() { return guarded(0, [&](NeuronGPU *) { return no_mpi(); }); }
-int NeuronGPU_MpiFinalize() { return guarded(0, [&](NeuronGPU *) { return no_mpi(); }); }
+// Without MPI: the host index and count come from the job launcher's
+// environment; the spike exchange is driven by the caller's collective
+// (NGB200_PackRemoteSpikes / NGB200_UnpackRemoteSpikes, the Python layer's
+// Simulate uses torch.distributed).
+int NeuronGPU_ConnectMpiInit(int, char *[]) {
+  return guarded(0, [&](NeuronGPU *n) {
+    int id = 0, np = 1;
+    host_from_env(&id, &np);
+    return n->SetHost(id, np);
+  });
+}
+int NeuronGPU_MpiId() { return guarded(0, [&](NeuronGPU *n) { return n->HostId(); }); }
+int NeuronGPU_MpiNp() { return guarded(0, [&](NeuronGPU *n) { return n->NHosts(); }); }
+int NeuronGPU_ProcMaster() { return guarded(0, [&](NeuronGPU *n) { return n->HostId() == 0 ? 1 : 0; }); }
+int NeuronGPU_MpiFinalize() { return guarded(0, [&](NeuronGPU *) { return 0; }); }
 unsigned int *NeuronGPU_RandomInt(size_t n_) {
   return guarded((unsigned int *)nullptr, [&](NeuronGPU *n) { return n->RandomInt(n_); });
 }
@@ -335,17 +365,33 @@ int NeuronGPU_ConnectGroupGroup(int *i_source, int n_source, int *i_target, int 
     return n->Connect(i_source, 0, n_source, i_target, 0, n_target, n->conn_spec_, n->syn_spec_);
   });
 }
-int NeuronGPU_RemoteConnectSeqSeq(int, int, int, int, int, int) {
-  return guarded(0, [&](NeuronGPU *) { return no_mpi(); });
+int NeuronGPU_RemoteConnectSeqSeq(int i_source_host, int i_source, int n_source,
+                                  int i_target_host, int i_target, int n_target) {
+  return guarded(0, [&](NeuronGPU *n) {
+    return n->RemoteConnect(i_source_host, nullptr, i_source, n_source, i_target_host, nullptr,
+                            i_target, n_target, n->conn_spec_, n->syn_spec_);
+  });
 }
-int NeuronGPU_RemoteConnectSeqGroup(int, int, int, int, int *, int) {
-  return guarded(0, [&](NeuronGPU *) { return no_mpi(); });
+int NeuronGPU_RemoteConnectSeqGroup(int i_source_host, int i_source, int n_source,
+                                    int i_target_host, int *i_target, int n_target) {
+  return guarded(0, [&](NeuronGPU *n) {
+    return n->RemoteConnect(i_source_host, nullptr, i_source, n_source, i_target_host, i_target,
+                            0, n_target, n->conn_spec_, n->syn_spec_);
+  });
 }
-int NeuronGPU_RemoteConnectGroupSeq(int, int *, int, int, int, int) {
-  return guarded(0, [&](NeuronGPU *) { return no_mpi(); });
+int NeuronGPU_RemoteConnectGroupSeq(int i_source_host, int *i_source, int n_source,
+                                    int i_target_host, int i_target, int n_target) {
+  return guarded(0, [&](NeuronGPU *n) {
+    return n->RemoteConnect(i_source_host, i_source, 0, n_source, i_target_host, nullptr,
+                            i_target, n_target, n->conn_spec_, n->syn_spec_);
+  });
 }
-int NeuronGPU_RemoteConnectGroupGroup(int, int *, int, int, int *, int) {
-  return guarded(0, [&](NeuronGPU *) { return no_mpi(); });
+int NeuronGPU_RemoteConnectGroupGroup(int i_source_host, int *i_source, int n_source,
+                                      int i_target_host, int *i_target, int n_target) {
+  return guarded(0, [&](NeuronGPU *n) {
+    return n->RemoteConnect(i_source_host, i_source, 0, n_source, i_target_host, i_target, 0,
+                            n_target, n->conn_spec_, n->syn_spec_);
+  });
 }
 char **NeuronGPU_GetIntVarNames(int i) {
   return guarded((char **)nullptr, [&](NeuronGPU *n) { return names_to_c(n->GetIntVarNames(i)); });
@@ -529,18 +575,46 @@ int NeuronGPU_GetIntParam(char *p) {
 int NeuronGPU_SetIntParam(char *p, int val) {
   return guarded(0, [&](NeuronGPU *n) { return n->SetIntParam(p, val); });
 }
-int NeuronGPU_RemoteCreate(int, char *, int, int) {
-  return guarded(0, [&](NeuronGPU *) { return no_mpi(); });
+int NeuronGPU_RemoteCreate(int i_host, char *model_name, int n_neuron, int n_port) {
+  return guarded(0, [&](NeuronGPU *n) {
+    return n->RemoteCreate(i_host, std::string(model_name), n_neuron, n_port);
+  });
 }
 
 // ---- extensions ----
 int NGB200_Reset() {
   return guarded(0, [&](NeuronGPU *n) {
     int on_exc = n->OnException();
-    delete g_ngpu;
-    g_ngpu = new NeuronGPU();
-    g_ngpu->SetOnException(on_exc);
+    delete g_inst[g_cur];
+    g_inst[g_cur] = new NeuronGPU();
+    g_inst[g_cur]->SetOnException(on_exc);
     return 0;
+  });
+}
+int NGB200_SetInstance(int k) {
+  if (k < 0 || k >= kMaxInstances) return -1;
+  g_cur = k;
+  inst();
+  return 0;
+}
+int NGB200_GetInstance() { return g_cur; }
+int NGB200_SetHost(int id, int n_hosts) {
+  return guarded(0, [&](NeuronGPU *n) { return n->SetHost(id, n_hosts); });
+}
+int NGB200_SimulateSteps(long long n_steps) {
+  return guarded(0, [&](NeuronGPU *n) { return n->SimulateSteps(n_steps); });
+}
+int NGB200_RemoteExchangeSteps() {
+  return guarded(0, [&](NeuronGPU *n) { return n->RemoteExchangeSteps(); });
+}
+long long NGB200_PackRemoteSpikes(int n_steps, void *buf, long long cap) {
+  return guarded(-1LL, [&](NeuronGPU *n) {
+    return n->PackRemoteSpikes(n_steps, (unsigned *)buf, cap);
+  });
+}
+int NGB200_UnpackRemoteSpikes(int src_host, int n_steps, const void *buf, long long count) {
+  return guarded(0, [&](NeuronGPU *n) {
+    return n->UnpackRemoteSpikes(src_host, n_steps, (const unsigned *)buf, count);
   });
 }
 unsigned long long NGB200_StageEvaluations() {

@@ -79,7 +79,12 @@ void NeuronGPU::FreeDevice() {
     if (g->step_mode == STEP_LOG) g->step_mode = STEP_PLAIN;
     g->d_var = g->d_param = g->d_h = g->d_dx = nullptr;
   }
-  F(d_ctx_); F(d_ctxs_); F(d_acc_);
+  F(d_ctx_); F(d_ctxs_); F(d_acc_); F(d_acc_stamp_);
+  d_acc_stamp_ = nullptr;
+  F(d_exported_);
+  d_exported_ = nullptr;
+  for (int *p : d_image_lut_) F(p);
+  d_image_lut_.clear();
   d_ctxs_ = nullptr;
   n_ctxs_ = 0; F(d_ring_src_); F(d_ring_h_); F(d_ring_cnt_);
   F(d_last_spike_T_); F(d_last_rev_T_); F(d_last_post_T_); F(d_last_spike_h_);
@@ -988,7 +993,8 @@ GroupArgs NeuronGPU::MakeGroupArgs(NodeGroup *g) {
   a.den_delay_col = g->mi->den_delay_param;
   a.blk_evals = g->d_blk_evals;
   a.q = g->q;
-  if (g->queue_off) a.q.cap = 0;
+  // the learned proposer runs in the queue's finishing launch: queue kept on
+  if (g->queue_off && g->step_mode != STEP_LEARNED) a.q.cap = 0;
   a.step_mode = g->step_mode;
   a.mlp_margin = mlp_margin_;
   a.mlp = d_mlp_img_;
@@ -1011,6 +1017,8 @@ InputArgs NeuronGPU::MakeInputArgs(NodeGroup *g) {
   in.acc = d_acc_;
   in.acc_base = g->acc_base;
   in.acc_par = n_acc_ > 0 ? n_acc_ : 1;
+  in.acc_slots = acc_slots_;
+  in.acc_stamp = d_acc_stamp_;
   in.np = g->n_port;
   if (mi->kind == MK_RK5) {
     in.in_var = mi->in_var - (mi->port_var.empty() ? 0 : 0);
@@ -1107,6 +1115,8 @@ DeliverArgs NeuronGPU::MakeDeliverArgs() {
   d.e_post = d_e_post_;
   d.acc = d_acc_;
   d.acc_par = n_acc_ > 0 ? n_acc_ : 1;
+  d.acc_slots = acc_slots_;
+  d.acc_stamp = d_acc_stamp_;
   d.ring_src = d_ring_src_;
   d.ring_h = d_ring_h_;
   d.ring_cnt = d_ring_cnt_;
@@ -1245,9 +1255,25 @@ void NeuronGPU::BuildDevice() {
     n_acc_ += (long long)g->n_port * g->n_pad;
   }
   if (n_acc_ > 0xFFFFFFFFLL) throw ngpu_exception("Too many (node, port) input slots");
-  // two parity halves (InputArgs::acc_par)
-  NGPU_CUDA(cudaMalloc(&d_acc_, 2 * sizeof(long long) * (n_acc_ > 0 ? n_acc_ : 1)));
-  NGPU_CUDA(cudaMemset(d_acc_, 0, 2 * sizeof(long long) * (n_acc_ > 0 ? n_acc_ : 1)));
+  // accumulator ring (InputArgs::acc_par, acc_slots): two slots, or, for a
+  // network that can run several steps per launch (RK5 neurons and Poisson
+  // generators only, no plastic synapse), one slot per step up to the
+  // longest delay + 2, so that the delivery after a window can fill the
+  // slots of every later step at once; at most kWindowAccBytes
+  {
+    int maxD_acc = 1;
+    for (int dly : delays_) maxD_acc = std::max(maxD_acc, dly);
+    bool capable = !any_plastic_;
+    for (NodeGroup *g : groups_)
+      if (g->mi->kind != MK_RK5 && g->mi->kind != MK_POISSON_GENERATOR) capable = false;
+    const double bytes = (double)(maxD_acc + 2) * 8.0 * (double)(n_acc_ > 0 ? n_acc_ : 1);
+    acc_slots_ = (capable && bytes <= kWindowAccBytes) ? maxD_acc + 2 : 2;
+  }
+  const size_t acc_bytes = (size_t)acc_slots_ * sizeof(long long) * (n_acc_ > 0 ? n_acc_ : 1);
+  NGPU_CUDA(cudaMalloc(&d_acc_, acc_bytes));
+  NGPU_CUDA(cudaMemset(d_acc_, 0, acc_bytes));
+  NGPU_CUDA(cudaMalloc(&d_acc_stamp_, sizeof(long long) * acc_slots_));
+  NGPU_CUDA(cudaMemset(d_acc_stamp_, 0xFF, sizeof(long long) * acc_slots_));   // -1: no step
   // accumulator slot of every CSR edge (device), with the port and
   // synapse-group checks of src/connect.cu:26-62
   const uint64_t E = (uint64_t)n_raw_;
@@ -1318,9 +1344,33 @@ void NeuronGPU::BuildDevice() {
   has_out_.assign(N, 0);
   for (long long s = 0; s < N; s++)
     has_out_[s] = (h_grp_off_[(s + 1) * nd] > h_grp_off_[s * nd]) ? 1 : 0;
+  // shortest delay of a connection whose source can spike (Poisson
+  // generators reach their targets through the direct connections, not
+  // through the spike ring): the bound of a window of steps
+  {
+    std::vector<unsigned char> is_gen(N, 0);
+    for (NodeGroup *g : groups_)
+      if (g->mi->kind == MK_POISSON_GENERATOR)
+        for (int k = 0; k < g->n_node; k++) is_gen[g->i_node_0 + k] = 1;
+    min_ring_delay_ = 0;
+    for (int di = 0; di < nd && min_ring_delay_ == 0; di++) {
+      for (long long s2 = 0; s2 < N; s2++) {
+        if (!is_gen[s2] && h_grp_off_[s2 * nd + di + 1] > h_grp_off_[s2 * nd + di]) {
+          min_ring_delay_ = delays_[di];      // delays_ is sorted
+          break;
+        }
+      }
+    }
+  }
+  BuildRemoteTables();
   // spike ring
   int maxD = 1;
   for (int d : delays_) maxD = std::max(maxD, d);
+  // a host that exports spikes keeps them for an exchange interval at least
+  if (n_exported_ > 0) maxD = std::max(maxD, kExchangeRingSteps);
+  // a network that can run several steps per launch keeps every step of a
+  // window (up to 16) in its own ring slot, also where its delays are short
+  if (acc_slots_ > 2) maxD = std::max(maxD, 15);
   // max delay + 2 slots: the slot of step T + 1 is emptied during step T
   // while the delivery reads the slots of steps T - 1 ... T - max delay
   ring_R_ = maxD + 2;
@@ -1446,10 +1496,13 @@ void NeuronGPU::BuildDevice() {
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
   }
   deliver_blocks_ = n_sm * DeliverBlocksPerSM();
+  // the delivery after a window runs alone: every resident block
+  window_blocks_ = n_sm * DeliverOccupancy();
+  n_evt_blocks_ = std::max(deliver_blocks_, window_blocks_);
   NGPU_CUDA(cudaMalloc(&d_done_, sizeof(unsigned)));
   NGPU_CUDA(cudaMemset(d_done_, 0, sizeof(unsigned)));
-  NGPU_CUDA(cudaMalloc(&d_blk_events_, sizeof(unsigned long long) * deliver_blocks_));
-  NGPU_CUDA(cudaMemset(d_blk_events_, 0, sizeof(unsigned long long) * deliver_blocks_));
+  NGPU_CUDA(cudaMalloc(&d_blk_events_, sizeof(unsigned long long) * n_evt_blocks_));
+  NGPU_CUDA(cudaMemset(d_blk_events_, 0, sizeof(unsigned long long) * n_evt_blocks_));
   int max_den_steps = 0;
   for (NodeGroup *g : groups_) {
     if (g->mi->kind == MK_RK5) {
@@ -1529,6 +1582,9 @@ void NeuronGPU::BuildDevice() {
   NGPU_CUDA(cudaMalloc(&d_ctx_, sizeof(StepCtx)));
   StepCtx c;
   memset(&c, 0, sizeof(c));
+  c.acc_slots = acc_slots_;
+  c.ring_R = ring_R_;
+  ctx_set_slots(c);
   NGPU_CUDA(cudaMemcpy(d_ctx_, &c, sizeof(StepCtx), cudaMemcpyHostToDevice));
   NGPU_CUDA(cudaStreamSynchronize(stream_));
   NGPU_CUDA(cudaDeviceSynchronize());
@@ -1595,9 +1651,11 @@ void NeuronGPU::KEvent(int step_in_chunk, int j) {
                                      capturing_ ? cudaEventRecordExternal : cudaEventRecordDefault));
 }
 
-void NeuronGPU::AccumulateKernelTiming(int n_steps) {
+// class times of the event groups k0 ... k0 + n - 1 (one group per step, or
+// one per window at the window's first step)
+void NeuronGPU::AccumulateKernelTiming(int k0, int n) {
   NGPU_CUDA(cudaStreamSynchronize(stream_));
-  for (int k = 0; k < n_steps; k++) {
+  for (int k = k0; k < k0 + n; k++) {
     for (int j = 0; j < 4; j++) {
       float ms = 0.0f;
       NGPU_CUDA(cudaEventElapsedTime(&ms, kev_[(size_t)k * 5 + j], kev_[(size_t)k * 5 + j + 1]));
@@ -1811,6 +1869,87 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
   if (ktime_) KEvent(step_in_chunk, 4);
 }
 
+// Steps per launch. A spike emitted in step s with a delay of D steps is
+// folded by the update of step s + D + 1, so with W <= shortest delay + 1 no
+// spike of a window of W steps arrives inside it, and one launch per RK5
+// group can integrate its neurons through all W steps before one delivery
+// of the window's spikes (k_rk5_window, k_deliver_window, k_window_book).
+// Windows need: every node group an RK5 group with its own launch and the
+// plain controller, or a Poisson generator; no plastic synapse, multimeter
+// record or large-rate Poisson pre-pass; the accumulator ring of the
+// longest delay + 2 slots; and a quiet network (below kFusedDeliveryMaxEvents
+// delivered events per step, checked every kQueueRecheckSteps steps): the
+// delivery after a window adds into the slots of up to W + max delay later
+// steps at once, a working set that leaves L2 when many events arrive,
+// where one step's delivery adds into one slot. W is at most 16 and
+// preferably divides the graph chunk; NGB200_WINDOW caps it (0: one step
+// per launch). 0: no windows.
+int NeuronGPU::WindowSteps() {
+  const char *env = getenv("NGB200_WINDOW");
+  int cap = 16;
+  if (env != nullptr) cap = std::max(0, std::min(16, atoi(env)));
+  if (cap < 2 || acc_slots_ <= 2 || d_acc_stamp_ == nullptr || plastic_ || n_rec_cols_ > 0 ||
+      delivery_busy_ || n_exported_ > 0 || has_images_)
+    return 0;
+  for (NodeGroup *g : groups_) {
+    if (g->mi->kind == MK_POISSON_GENERATOR) continue;
+    if (g->mi->kind != MK_RK5 || g->batch >= 0 || g->step_mode != STEP_PLAIN || g->n_port > 4 ||
+        HasLargePoisson(g))
+      return 0;
+  }
+  // no connection through the spike ring: any W; every step of a window
+  // has its own ring slot
+  const int minD = min_ring_delay_ > 0 ? min_ring_delay_ : 15;
+  int W = std::min(std::min(cap, minD + 1), ring_R_ - 1);
+  if (W < 2) return 0;
+  // prefer a divisor of the chunk (equal windows in every chunk) if one of
+  // at least W / 2 exists
+  for (int w = W; 2 * w >= W; w--) {
+    if (graph_chunk_ % w == 0) return w;
+  }
+  return W;
+}
+
+// The steps k0 ... k0 + w - 1 of the chunk as one window: each RK5 group's
+// window launch, the delivery of the window's spikes at all their delays,
+// the window's spike count and the emptying of its ring slots.
+void NeuronGPU::EnqueueWindow(int k0, int w) {
+  StepCtx *ctxs = d_ctxs_ + k0;
+  if (ktime_) KEvent(k0, 0);
+  for (NodeGroup *g : groups_) {
+    if (g->mi->kind != MK_RK5) continue;
+    if (!LaunchRk5Window(g->mi->rk5_model, g->n_port, MakeGroupArgs(g), MakeInputArgs(g),
+                         MakePushArgs(g), ctxs, w, stream_))
+      throw ngpu_exception("internal error: no window kernel for this node group");
+  }
+  if (ktime_) KEvent(k0, 1);
+  const DeliverArgs d = MakeDeliverArgs();
+  LaunchDeliverWindow(d, ctxs, 0, w, 0, min_ring_delay_, window_blocks_, stream_);
+  if (ktime_) {
+    KEvent(k0, 2);
+    KEvent(k0, 3);
+  }
+  LaunchWindowBook(d_ring_cnt_, ring_R_, ring_C_, ctxs, 0, w, 0, w, stream_);
+  if (ktime_) KEvent(k0, 4);
+}
+
+// Hand-over from one step per launch to windows, before the first window
+// (T_b = its first step): the spikes of the last max-delay steps are
+// delivered for their arrivals from T_b on (the one-step deliveries made
+// the earlier ones), the spikes of step T_b - 1 (which the next step's
+// bookkeeping would count) are counted, and every ring slot is emptied, as
+// the windows expect. From windows back to one step per launch needs
+// nothing: every window leaves its ring slots empty and its spikes
+// delivered.
+void NeuronGPU::EnqueueWindowCatchUp() {
+  const int maxD = ring_R_ - 2;
+  const DeliverArgs d = MakeDeliverArgs();
+  LaunchDeliverWindow(d, d_ctx_, -(long long)maxD, maxD, 0, min_ring_delay_, window_blocks_,
+                      stream_);
+  LaunchWindowBook(d_ring_cnt_, ring_R_, ring_C_, d_ctx_, -(long long)(ring_R_ - 1), ring_R_,
+                   -1, 0, stream_);
+}
+
 void NeuronGPU::LaunchSteps(int n_steps) {
   if (n_steps <= 0) return;
   EnsureForkResources();
@@ -1828,10 +1967,26 @@ void NeuronGPU::LaunchSteps(int n_steps) {
     }
   }
   const int rec = n_rec_cols_ > 0 ? 1 : 0;
-  if (!use_graphs_) {
+  const int W = WindowSteps();
+  if (W != window_w_) {
+    InvalidateGraphs();
+    window_w_ = W;
+  }
+  // the hand-over to windows depends on the mode of the previous chunk, so
+  // it runs before the chunk's graph, not in it
+  if (W > 0 && !windowed_) EnqueueWindowCatchUp();
+  windowed_ = W > 0;
+  auto enqueue_chunk = [&]() {
     LaunchStepPrologue(d_ctx_, d_ctxs_, n_steps, rec, stream_);
-    for (int k = 0; k < n_steps; k++) EnqueueStep(k);
+    if (W > 0) {
+      for (int k = 0; k < n_steps; k += W) EnqueueWindow(k, std::min(W, n_steps - k));
+    } else {
+      for (int k = 0; k < n_steps; k++) EnqueueStep(k);
+    }
     LaunchStepEpilogue(d_ctx_, d_ctxs_, n_steps, rec, stream_);
+  };
+  if (!use_graphs_) {
+    enqueue_chunk();
   } else {
     auto it = graphs_.find(n_steps);
     if (it == graphs_.end()) {
@@ -1839,9 +1994,7 @@ void NeuronGPU::LaunchSteps(int n_steps) {
       NGPU_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
       capturing_ = true;
       try {
-        LaunchStepPrologue(d_ctx_, d_ctxs_, n_steps, rec, stream_);
-        for (int k = 0; k < n_steps; k++) EnqueueStep(k);
-        LaunchStepEpilogue(d_ctx_, d_ctxs_, n_steps, rec, stream_);
+        enqueue_chunk();
       } catch (...) {
         capturing_ = false;
         cudaStreamEndCapture(stream_, &graph);
@@ -1869,7 +2022,13 @@ void NeuronGPU::LaunchSteps(int n_steps) {
   }
   if (n_rec_cols_ > 0) rec_rows_used_ += n_steps;
   NGPU_CUDA(cudaGetLastError());
-  if (ktime_) AccumulateKernelTiming(n_steps);
+  if (ktime_) {
+    if (W > 0) {
+      for (int k = 0; k < n_steps; k += W) AccumulateKernelTiming(k, 1);
+    } else {
+      AccumulateKernelTiming(0, n_steps);
+    }
+  }
 }
 
 void NeuronGPU::WriteInitialRecord() {
@@ -2281,7 +2440,8 @@ Rk5Batch NeuronGPU::MakeRk5Batch(const Rk5BatchHost &b) {
   r.blk_seg = b.d_blk_seg;
   r.blk_evals = b.d_blk_evals;
   r.q = b.q;
-  if (b.queue_off) r.q.cap = 0;
+  if (b.queue_off && r.mode != STEP_LEARNED) r.q.cap = 0;
+  r.first = MakeGroupArgs(b.groups[0]);
   return r;
 }
 
@@ -2395,6 +2555,7 @@ int NeuronGPU::StartSimulation() {
     c.it = 0;
     c.t0 = neural_time_;
     c.T0 = (long long)round(neural_time_ / time_resolution_);
+    ctx_set_slots(c);
     NGPU_CUDA(cudaMemcpy(d_ctx_, &c, sizeof(StepCtx), cudaMemcpyHostToDevice));
     WriteInitialRecord();
     first_simulation_flag_ = false;
@@ -2421,6 +2582,7 @@ int NeuronGPU::StartSimulation() {
   c.t0 = neur_t0_;
   c.T0 = (long long)round(neur_t0_ / time_resolution_);
   c.poisson_pending = 0;
+  ctx_set_slots(c);
   NGPU_CUDA(cudaMemcpy(d_ctx_, &c, sizeof(StepCtx), cudaMemcpyHostToDevice));
   return 0;
 }
@@ -2448,6 +2610,12 @@ int NeuronGPU::EndSimulation() {
 }
 
 int NeuronGPU::Simulate() {
+  // the spikes of a partitioned network cross hosts between runs of steps,
+  // through the caller's collective: a plain Simulate would drop them
+  if (n_hosts_ > 1 && (has_images_ || n_exported_ > 0))
+    throw ngpu_exception("a network partitioned over hosts is simulated by the Python "
+                         "layer's Simulate, or by NGB200_SimulateSteps with the spike "
+                         "exchange (NGB200_PackRemoteSpikes / NGB200_UnpackRemoteSpikes)");
   StartSimulation();
   auto t_start = std::chrono::steady_clock::now();
   if (!ev_start_) {
@@ -2481,6 +2649,178 @@ int NeuronGPU::Simulate() {
   return 0;
 }
 
+int NeuronGPU::SimulateSteps(long long n) {
+  if (n < 0) throw ngpu_exception("the number of steps must be >= 0");
+  if (first_simulation_flag_) StartSimulation();
+  long long done = 0;
+  while (done < n) {
+    const long long k = std::min<long long>(graph_chunk_, n - done);
+    LaunchSteps((int)k);
+    done += k;
+    it_ += k;
+    steps_total_ += k;
+    input_pending_ = true;
+    if (steps_total_ >= kTuneSteps && TunePending()) TuneAll();
+    RecheckRk5Queues();
+    RecheckDeliveryMode();
+  }
+  neural_time_ = neur_t0_ + (double)time_resolution_ * (double)it_;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// networks partitioned over hosts
+// ---------------------------------------------------------------------------
+int NeuronGPU::SetHost(int id, int n_hosts) {
+  if (n_hosts < 1 || id < 0 || id >= n_hosts) throw ngpu_exception("Invalid host index or count");
+  if (has_images_ || n_exported_ > 0)
+    throw ngpu_exception("the host cannot change after remote connections were made");
+  host_id_ = id;
+  n_hosts_ = n_hosts;
+  image_of_.assign(n_hosts, std::map<int, int>());
+  return 0;
+}
+
+int NeuronGPU::RemoteCreate(int i_host, const std::string &model, int n_node, int n_port) {
+  if (i_host < 0 || i_host >= n_hosts_) throw ngpu_exception("Invalid host index in RemoteCreate");
+  if (i_host == host_id_) return Create(model, n_node, n_port);
+  return -1;
+}
+
+int NeuronGPU::RemoteConnect(int i_source_host, const int *src_arr, int i_src0, int n_source,
+                             int i_target_host, const int *tgt_arr, int i_tgt0, int n_target,
+                             ConnSpec &cs, SynSpec &ss) {
+  if (i_source_host < 0 || i_source_host >= n_hosts_ || i_target_host < 0 ||
+      i_target_host >= n_hosts_)
+    throw ngpu_exception("Invalid host index in RemoteConnect");
+  CheckUncalibrated("Connections cannot be created after calibration");
+  if (n_source <= 0 || n_target <= 0) throw ngpu_exception("Empty source or target in RemoteConnect");
+  auto src_of = [&](int k) { return src_arr != nullptr ? src_arr[k] : i_src0 + k; };
+  if (i_source_host == i_target_host) {
+    // both ends on one host: an ordinary connection there
+    if (host_id_ != i_source_host) return 0;
+    return Connect(src_arr, i_src0, n_source, tgt_arr, i_tgt0, n_target, cs, ss);
+  }
+  if (host_id_ == i_source_host) {
+    // the sources send their spikes to the other hosts
+    const long long N = (long long)node_group_map_.size();
+    if ((long long)exported_.size() < N) exported_.resize(N, 0);
+    for (int k = 0; k < n_source; k++) {
+      const int s = src_of(k);
+      if (s < 0 || s >= N) throw ngpu_exception("Source node index out of range in RemoteConnect");
+      if (!exported_[s]) {
+        exported_[s] = 1;
+        n_exported_++;
+      }
+    }
+    return 0;
+  }
+  if (host_id_ != i_target_host) return 0;
+  // target host: image nodes of the remote sources, made in order of first
+  // appearance, then the connection from the images with the given rule
+  if ((int)image_of_.size() < n_hosts_) image_of_.resize(n_hosts_);
+  std::map<int, int> &img_of = image_of_[i_source_host];
+  std::vector<int> fresh;
+  std::map<int, int> fresh_index;
+  for (int k = 0; k < n_source; k++) {
+    const int s = src_of(k);
+    if (s < 0) throw ngpu_exception("Source node index out of range in RemoteConnect");
+    if (img_of.count(s) == 0 && fresh_index.count(s) == 0) {
+      fresh_index[s] = (int)fresh.size();
+      fresh.push_back(s);
+    }
+  }
+  if (!fresh.empty()) {
+    const int i0 = Create("remote_image", (int)fresh.size(), 0);
+    for (size_t j = 0; j < fresh.size(); j++) img_of[fresh[j]] = i0 + (int)j;
+  }
+  std::vector<int> img(n_source);
+  for (int k = 0; k < n_source; k++) img[k] = img_of[src_of(k)];
+  has_images_ = true;
+  return Connect(img.data(), 0, n_source, tgt_arr, i_tgt0, n_target, cs, ss);
+}
+
+// device tables of the exchange, built at calibration
+void NeuronGPU::BuildRemoteTables() {
+  const long long N = (long long)node_group_map_.size();
+  const int nd = (int)delays_.size();
+  if (n_exported_ > 0) {
+    exported_.resize(N, 0);
+    NGPU_CUDA(cudaMalloc(&d_exported_, N));
+    NGPU_CUDA(cudaMemcpy(d_exported_, exported_.data(), N, cudaMemcpyHostToDevice));
+  }
+  d_image_lut_.assign(n_hosts_, nullptr);
+  image_lut_n_.assign(n_hosts_, 0);
+  for (int h = 0; h < (int)image_of_.size() && h < n_hosts_; h++) {
+    if (image_of_[h].empty()) continue;
+    const int n = image_of_[h].rbegin()->first + 1;
+    std::vector<int> lut(n, -1);
+    for (const auto &kv : image_of_[h]) lut[kv.first] = kv.second;
+    NGPU_CUDA(cudaMalloc(&d_image_lut_[h], sizeof(int) * n));
+    NGPU_CUDA(cudaMemcpy(d_image_lut_[h], lut.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    image_lut_n_[h] = n;
+  }
+  // the exchange interval: the shortest delay of a connection from an image
+  min_image_delay_ = 0;
+  for (NodeGroup *g : groups_) {
+    if (g->mi->kind != MK_IMAGE) continue;
+    for (int di = 0; di < nd; di++) {
+      if (min_image_delay_ > 0 && delays_[di] >= min_image_delay_) break;
+      for (int k = 0; k < g->n_node; k++) {
+        const long long s = g->i_node_0 + k;
+        if (h_grp_off_[s * nd + di + 1] > h_grp_off_[s * nd + di]) {
+          min_image_delay_ = delays_[di];
+          break;
+        }
+      }
+    }
+  }
+}
+
+// The longest exchange interval this host allows: the shortest delay of a
+// connection from an image node (no remote spike may be due before it
+// arrives), and on an exporting host the steps its spike ring keeps; 0 if
+// the host neither receives nor sends remote spikes.
+int NeuronGPU::RemoteExchangeSteps() {
+  if (!calibrate_flag_) Calibrate();
+  int e = min_image_delay_;
+  if (n_exported_ > 0) e = e > 0 ? std::min(e, ring_R_ - 2) : ring_R_ - 2;
+  return e;
+}
+
+long long NeuronGPU::PackRemoteSpikes(int n_steps, unsigned *buf, long long cap) {
+  if (n_steps < 0 || n_steps > ring_R_ - 2)
+    throw ngpu_exception("the exchange interval must lie within the longest delay");
+  if (buf == nullptr) throw ngpu_exception("null exchange buffer");
+  if (d_exported_ == nullptr || n_steps == 0) {
+    NGPU_CUDA(cudaMemsetAsync(buf, 0, 4 * sizeof(unsigned), stream_));
+    NGPU_CUDA(cudaStreamSynchronize(stream_));
+    return 0;
+  }
+  LaunchPackRemote(d_ring_cnt_, d_ring_src_, d_ring_h_, ring_R_, ring_C_, d_ctx_, n_steps,
+                   d_exported_, buf, cap, stream_);
+  // the count of every exported spike; above cap only cap were written and
+  // the caller packs again into a larger buffer (the ring is unchanged)
+  unsigned hdr[2] = {0, 0};
+  NGPU_CUDA(cudaMemcpyAsync(hdr, buf, sizeof(hdr), cudaMemcpyDeviceToHost, stream_));
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  return (long long)hdr[0];
+}
+
+int NeuronGPU::UnpackRemoteSpikes(int src_host, int n_steps, const unsigned *buf,
+                                  long long count) {
+  if (src_host < 0 || src_host >= n_hosts_) throw ngpu_exception("Invalid host index");
+  if (n_steps < 0 || n_steps > ring_R_ - 2)
+    throw ngpu_exception("the exchange interval must lie within the longest delay");
+  if (src_host == host_id_ || count <= 0 || src_host >= (int)d_image_lut_.size() ||
+      d_image_lut_[src_host] == nullptr)
+    return 0;
+  LaunchUnpackRemote(buf, count, d_image_lut_[src_host], image_lut_n_[src_host], d_ring_cnt_,
+                     d_ring_src_, d_ring_h_, ring_R_, ring_C_, d_ctx_, n_steps, stream_);
+  NGPU_CUDA(cudaGetLastError());
+  return 0;
+}
+
 int NeuronGPU::PushSpikesToNodes(int n, const int *nodes) {
   (void)n; (void)nodes;
   throw ngpu_exception("PushSpikesToNodes is only available for external-neuron co-simulation, which this build does not provide");
@@ -2506,8 +2846,8 @@ unsigned long long NeuronGPU::StageEvaluations() {
 
 unsigned long long NeuronGPU::DeliveredEvents() {
   if (!d_blk_events_) return 0;
-  std::vector<unsigned long long> v(deliver_blocks_);
-  NGPU_CUDA(cudaMemcpy(v.data(), d_blk_events_, sizeof(unsigned long long) * deliver_blocks_,
+  std::vector<unsigned long long> v(n_evt_blocks_);
+  NGPU_CUDA(cudaMemcpy(v.data(), d_blk_events_, sizeof(unsigned long long) * n_evt_blocks_,
                        cudaMemcpyDeviceToHost));
   unsigned long long tot = 0;
   for (auto x : v) tot += x;

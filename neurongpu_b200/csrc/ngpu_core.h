@@ -297,7 +297,39 @@ class NeuronGPU {
   int StartSimulation();
   int SimulationStep();
   int EndSimulation();
+  // n steps of a started simulation (graph chunks, as Simulate)
+  int SimulateSteps(long long n);
   int PushSpikesToNodes(int n, const int *nodes);
+
+  // A network partitioned over hosts (one GPU per host process), the
+  // reference's RemoteCreate / RemoteConnect (src/connect_rules.h:406-800,
+  // src/neurongpu.cu:1626-1642, 1820-1836) without MPI: every host runs the
+  // same script; a remote connection is made on its target host from image
+  // nodes of the remote sources (one per remote node, created by
+  // RemoteConnect), and its source host marks the source nodes as exported.
+  // The spikes of exported nodes are exchanged every RemoteExchangeSteps()
+  // steps (the shortest delay of a connection from an image node) by the
+  // caller's collective: PackRemoteSpikes after the steps, an all-gather of
+  // the packed lists, UnpackRemoteSpikes of every other host's list, which
+  // pushes each image node's spikes into the spike ring at the step the
+  // remote node emitted them, so they are delivered as the reference's
+  // per-step MPI exchange delivers them (src/neurongpu.cu:490-521).
+  int SetHost(int id, int n_hosts);
+  int HostId() const { return host_id_; }
+  int NHosts() const { return n_hosts_; }
+  // the group's first node on host i_host, -1 on the other hosts (their
+  // callers learn it from the owner by a broadcast)
+  int RemoteCreate(int i_host, const std::string &model, int n_node, int n_port);
+  int RemoteConnect(int i_source_host, const int *src_arr, int i_src0, int n_source,
+                    int i_target_host, const int *tgt_arr, int i_tgt0, int n_target,
+                    ConnSpec &cs, SynSpec &ss);
+  int RemoteExchangeSteps();
+  // spikes of exported nodes in the last n_steps steps into buf (device, u32:
+  // [count, overflow, 0, 0, then (step offset, node, height bits) per spike]);
+  // returns the count, which exceeds cap when only cap entries fitted
+  long long PackRemoteSpikes(int n_steps, unsigned *buf, long long cap);
+  // the packed list of host src_host (device buffer, count entries)
+  int UnpackRemoteSpikes(int src_host, int n_steps, const unsigned *buf, long long count);
 
   // statistics exposed through the extension entry points
   unsigned long long StageEvaluations();
@@ -479,6 +511,11 @@ class NeuronGPU {
   StepCtx *d_ctx_ = nullptr;
   long long *d_acc_ = nullptr;
   long long n_acc_ = 0;
+  // accumulator ring: 2 slots, or max delay + 2 for networks that can run
+  // several steps per launch; per slot the last step added into it
+  int acc_slots_ = 2;
+  static constexpr double kWindowAccBytes = 8e9;
+  long long *d_acc_stamp_ = nullptr;
   unsigned *d_ring_src_ = nullptr;
   float *d_ring_h_ = nullptr;
   int *d_ring_cnt_ = nullptr;
@@ -541,7 +578,7 @@ class NeuronGPU {
   double ktime_ms_[4] = {0, 0, 0, 0};
   long long klaunch_[4] = {0, 0, 0, 0};
   void KEvent(int step_in_chunk, int j);
-  void AccumulateKernelTiming(int n_steps);
+  void AccumulateKernelTiming(int k0, int n);
 
   // graphs
   bool use_graphs_ = true;
@@ -550,6 +587,28 @@ class NeuronGPU {
   void InvalidateGraphs();
   void LaunchSteps(int n_steps);
   void EnqueueStep(int step_in_chunk);
+  // several steps per launch (windows of W steps, W <= shortest delay + 1)
+  int WindowSteps();
+  void EnqueueWindow(int k0, int w);
+  void EnqueueWindowCatchUp();
+  int min_ring_delay_ = 0;      // shortest delay (steps) of a spiking source's connection
+  // partitioned networks: host of this instance, exported nodes, and per
+  // source host the image node of every remote node (host and device)
+  int host_id_ = 0, n_hosts_ = 1;
+  std::vector<unsigned char> exported_;
+  long long n_exported_ = 0;
+  std::vector<std::map<int, int>> image_of_;
+  unsigned char *d_exported_ = nullptr;
+  std::vector<int *> d_image_lut_;
+  std::vector<int> image_lut_n_;
+  int min_image_delay_ = 0;     // shortest delay of a connection from an image node
+  static const int kExchangeRingSteps = 32;   // spike-ring steps of an exporting host
+  bool has_images_ = false;
+  void BuildRemoteTables();
+  int window_w_ = 0;            // W of the captured graphs (0: one step per launch)
+  bool windowed_ = false;       // the last chunk ran in windows
+  int window_blocks_ = 0;       // grid of the window delivery (it runs alone)
+  int n_evt_blocks_ = 0;        // delivery event counters (max of both grids)
 
   // helpers
   NodeGroup *GroupOf(int i_node, int n, int &i_local);

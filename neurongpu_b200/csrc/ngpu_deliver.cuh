@@ -74,10 +74,10 @@ __device__ __forceinline__ void finish_step(const DeliverArgs &d, StepCtx *ctx, 
 // max delay + 2 slots).
 __device__ __forceinline__ void step_bookkeeping(int *ring_cnt, int ring_R, int ring_C,
                                                  StepCtx *ctx) {
-  const long long T = ctx->T0 + ctx->it + 1;
-  const int c = ring_cnt[(int)((T - 1) % ring_R)];
+  const int s = ctx->ring_slot;                 // slot of step T
+  const int c = ring_cnt[s > 0 ? s - 1 : ring_R - 1];
   ctx->n_spikes += (unsigned long long)(c < ring_C ? c : ring_C);
-  ring_cnt[(int)((T + 1) % ring_R)] = 0;
+  ring_cnt[s + 1 < ring_R ? s + 1 : 0] = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -85,6 +85,36 @@ __device__ __forceinline__ void step_bookkeeping(int *ring_cnt, int ring_R, int 
 // network has plastic synapses (the STDP pre rule runs on every edge); the
 // static instance does not carry that path's registers.
 // ---------------------------------------------------------------------------
+// Edges beg..end of one (spike, delay) group without plasticity, delivered
+// by a whole warp into the accumulators acc: eight edges per lane in flight;
+// edges are read once per spike, so they are loaded with the streaming
+// (evict-first) hint.
+__device__ __forceinline__ void deliver_static_edges(const DeliverArgs &d, long long *acc,
+                                                     unsigned long long beg,
+                                                     unsigned long long end, float height,
+                                                     int lane) {
+  for (unsigned long long e0 = beg + lane; e0 < end; e0 += 256) {
+    unsigned sl[8];
+    float wv[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const unsigned long long e = e0 + 32 * u;
+      if (e < end) {
+        sl[u] = __ldcs(d.e_slot + e);
+        wv[u] = __ldcs(d.e_w + e);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const unsigned long long e = e0 + 32 * u;
+      if (e < end) {
+        atomicAdd((unsigned long long *)(acc + sl[u]),
+                  (unsigned long long)ng_to_fixed(height * wv[u]));
+      }
+    }
+  }
+}
+
 // Delivery work of block blk of nblk delivery blocks (any block size that
 // is a multiple of 32, at most 256 threads): the whole grid of k_deliver, or
 // the first blocks of a fused RK5 update (k_rk5_update_deliver).
@@ -92,7 +122,12 @@ template <bool PLASTIC>
 __device__ __forceinline__ void deliver_blocks(const DeliverArgs &d, const SynGroupTable &syn,
                                                StepCtx *ctx, int blk, int nblk) {
   const long long T = ctx->T0 + ctx->it + 1;
-  long long *const acc = d.acc + ((T & 1) ? d.acc_par : 0);   // folded by the update of T + 1
+  // the slot the update of T + 1 folds, and the ring slot of step T
+  const int out_slot = ctx->acc_out_slot;
+  const int ring_T = ctx->ring_slot;
+  long long *const acc = d.acc + acc_slot_offset(out_slot, d.acc_slots, d.acc_par);
+  long long *const stamp =
+      d.acc_stamp != nullptr ? d.acc_stamp + (d.acc_slots > 1 ? out_slot : 0) : nullptr;
   if (d.step_book && blk == 0 && threadIdx.x == 0)
     step_bookkeeping(d.ring_cnt_w, d.ring_R, d.ring_C, ctx);
   const int lane = threadIdx.x & 31;
@@ -102,36 +137,12 @@ __device__ __forceinline__ void deliver_blocks(const DeliverArgs &d, const SynGr
   unsigned long long events = 0;
   // the edges of one (spike, delay) item: spike j of ring slot `slot` at
   // distinct-delay index di; called by whole warps
-  auto deliver_item = [&](int di, int slot, int j) {
-    const long long k = (long long)slot * d.ring_C + j;
-    const unsigned src = d.ring_src[k];
-    const float height = d.ring_h[k];
+  auto deliver_item = [&](int di, unsigned src, float height) {
     const unsigned long long gi = (unsigned long long)src * d.nd + di;
     const unsigned long long beg = d.grp_off[gi], end = d.grp_off[gi + 1];
     if (lane == 0) events += end - beg;
     if constexpr (!PLASTIC) {
-      // eight edges per lane in flight; edges are read once per spike, so
-      // they are loaded with the streaming (evict-first) hint
-      for (unsigned long long e0 = beg + lane; e0 < end; e0 += 256) {
-        unsigned sl[8];
-        float wv[8];
-#pragma unroll
-        for (int u = 0; u < 8; u++) {
-          const unsigned long long e = e0 + 32 * u;
-          if (e < end) {
-            sl[u] = __ldcs(d.e_slot + e);
-            wv[u] = __ldcs(d.e_w + e);
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < 8; u++) {
-          const unsigned long long e = e0 + 32 * u;
-          if (e < end) {
-            atomicAdd((unsigned long long *)(acc + sl[u]),
-                      (unsigned long long)ng_to_fixed(height * wv[u]));
-          }
-        }
-      }
+      deliver_static_edges(d, acc, beg, end, height, lane);
     } else {
       // plastic network: four edges per lane in flight, then the
       // post-synaptic last-spike gathers of all four, then the updates
@@ -178,7 +189,7 @@ __device__ __forceinline__ void deliver_blocks(const DeliverArgs &d, const SynGr
     int my_slot = 0, my_incl = 0, total;
     int c = 0;
     if (lane < d.nd) {
-      int slot = (int)((T - d.delays[lane]) % d.ring_R);
+      int slot = ring_T - d.delays[lane];       // delays are below ring_R
       if (slot < 0) slot += d.ring_R;
       my_slot = slot;
       c = d.ring_cnt[slot];
@@ -191,6 +202,10 @@ __device__ __forceinline__ void deliver_blocks(const DeliverArgs &d, const SynGr
       if (lane >= o) my_incl += v;
     }
     total = __shfl_sync(0xffffffffu, my_incl, 31);
+    // the slot may receive input this step: one store (see acc_stamp; a
+    // store per item, all to one word, held the grid's end for the L2 to
+    // serialise them)
+    if (warp == 0 && lane == 0 && total > 0 && stamp != nullptr) *stamp = T;
     for (int item = warp; item < total; item += n_warps) {
       // first delay whose inclusive prefix exceeds the item
       // (item < total, so some lane's inclusive prefix exceeds it)
@@ -198,7 +213,8 @@ __device__ __forceinline__ void deliver_blocks(const DeliverArgs &d, const SynGr
       const int di = __ffs(m) - 1;
       const int slot = __shfl_sync(0xffffffffu, my_slot, di);
       const int prev = __shfl_sync(0xffffffffu, my_incl, di > 0 ? di - 1 : 0);
-      deliver_item(di, slot, item - (di > 0 ? prev : 0));
+      const long long k = (long long)slot * d.ring_C + (item - (di > 0 ? prev : 0));
+      deliver_item(di, d.ring_src[k], d.ring_h[k]);
     }
   } else {
     // more than 32 distinct delays: every delay has a fixed set of G warps,
@@ -209,11 +225,28 @@ __device__ __forceinline__ void deliver_blocks(const DeliverArgs &d, const SynGr
     const int G = per_delay ? n_warps / d.nd : 1;
     if (!per_delay || warp < G * d.nd) {
       for (int di = per_delay ? warp % d.nd : warp; di < d.nd; di += per_delay ? d.nd : n_warps) {
-        int slot = (int)((T - d.delays[di]) % d.ring_R);
+        int slot = ring_T - d.delays[di];
         if (slot < 0) slot += d.ring_R;
+        // the warp's first ring entry is loaded together with the slot's
+        // spike count, not after it (one dependent load less per item; an
+        // entry past the count is within the slot and is not used)
+        const int j0 = per_delay ? warp / d.nd : 0;
+        const long long k0 = (long long)slot * d.ring_C + j0;
+        unsigned src0 = 0u;
+        float h0 = 0.0f;
+        if (j0 < d.ring_C) {
+          src0 = d.ring_src[k0];
+          h0 = d.ring_h[k0];
+        }
         int c = d.ring_cnt[slot];
         c = c < d.ring_C ? c : d.ring_C;
-        for (int j = per_delay ? warp / d.nd : 0; j < c; j += G) deliver_item(di, slot, j);
+        // one stamp store per delay with spikes (the delay's first warp)
+        if (j0 == 0 && c > 0 && lane == 0 && stamp != nullptr) *stamp = T;
+        if (j0 < c) deliver_item(di, src0, h0);
+        for (int j = j0 + G; j < c; j += G) {
+          const long long k = (long long)slot * d.ring_C + j;
+          deliver_item(di, d.ring_src[k], d.ring_h[k]);
+        }
       }
     }
   }
@@ -223,6 +256,82 @@ __device__ __forceinline__ void deliver_blocks(const DeliverArgs &d, const SynGr
     if (lane == 0 && events != 0) atomicAdd(d.blk_events + blk, events);
   }
   finish_step(d, ctx, nblk);
+}
+
+// Delivery after a window of integrated steps (networks without plastic
+// synapses, k_rk5_window): every spike emitted in the steps
+// T_b + first_off ... T_b + first_off + n - 1 (their ring slots) is
+// delivered at each of its delays D at once, into the accumulator slot of
+// step T_s + D, the slot the update of step T_s + D + 1 folds: the slot, and
+// the step, that the delivery of step T_s + D would use. Valid because a
+// window is no longer than the shortest delay + 1 steps, so no spike of a
+// window arrives inside it. Arrivals before step arrive_min are skipped
+// (made already by one-step deliveries, when steps switch to windows), and
+// so are the delays below min_delay, the shortest delay of a connection
+// whose source spikes (the others belong to Poisson generators, which reach
+// their targets by direct connections): such a group holds no edge, and its
+// slot stamp would name a step W + 1 or more before the slots this delivery
+// fills, i.e. a slot one of them shares, overwriting that slot's stamp.
+// Warps take (step, delay) groups in turn, several warps per group.
+__device__ __forceinline__ void deliver_window_blocks(const DeliverArgs &d, const StepCtx *ctx,
+                                                      long long first_off, int n,
+                                                      long long arrive_off, int min_delay,
+                                                      int blk, int nblk) {
+  const long long T_b = ctx->T0 + ctx->it + 1;
+  const int ring_b = ctx->ring_slot, acc_b = ctx->acc_out_slot;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blk * (int)blockDim.x + (int)threadIdx.x) >> 5;
+  const int n_warps = (nblk * (int)blockDim.x) >> 5;
+  const int NG = n * d.nd;
+  const bool per_group = n_warps >= NG;
+  const int G = per_group ? n_warps / NG : 1;
+  unsigned long long events = 0;
+  if (!per_group || warp < G * NG) {
+    for (int gi = per_group ? warp % NG : warp; gi < NG; gi += per_group ? NG : n_warps) {
+      const int k = gi / d.nd, di = gi % d.nd;
+      const long long rel = first_off + k;           // T_s = T_b + rel
+      const int D = d.delays[di];
+      const long long rel_v = rel + D;               // the step whose slot receives it
+      // before the first step, made already, or a delay no spiking source has
+      if (T_b + rel < 0 || rel_v < arrive_off || D < min_delay) continue;
+      const long long V = T_b + rel_v;
+      const int slot = ring_add(ring_b, rel, d.ring_R);
+      // the warp's first entry is loaded together with the spike count
+      const int j0 = per_group ? warp / NG : 0;
+      const long long k0 = (long long)slot * d.ring_C + j0;
+      unsigned src0 = 0u;
+      float h0 = 0.0f;
+      if (j0 < d.ring_C) {
+        src0 = d.ring_src[k0];
+        h0 = d.ring_h[k0];
+      }
+      int c = d.ring_cnt[slot];
+      c = c < d.ring_C ? c : d.ring_C;
+      const int v_slot = ring_add(acc_b, rel_v, d.acc_slots);
+      long long *acc = d.acc + acc_slot_offset(v_slot, d.acc_slots, d.acc_par);
+      long long *stamp = d.acc_stamp != nullptr ? d.acc_stamp + v_slot : nullptr;
+      // one stamp store per (step, delay) group with spikes
+      if (j0 == 0 && c > 0 && lane == 0 && stamp != nullptr) *stamp = V;
+      for (int j = j0; j < c; j += G) {
+        unsigned src = src0;
+        float height = h0;
+        if (j != j0) {
+          const long long kk = (long long)slot * d.ring_C + j;
+          src = d.ring_src[kk];
+          height = d.ring_h[kk];
+        }
+        const unsigned long long e_i = (unsigned long long)src * d.nd + di;
+        const unsigned long long beg = d.grp_off[e_i], end = d.grp_off[e_i + 1];
+        if (lane == 0) events += end - beg;
+        deliver_static_edges(d, acc, beg, end, height, lane);
+      }
+    }
+  }
+  if (d.blk_events != nullptr) {
+    // per warp, a reduction whose result is not waited for (see block_add_u64)
+    for (int o = 16; o > 0; o >>= 1) events += __shfl_down_sync(0xffffffffu, events, o);
+    if (lane == 0 && events != 0) atomicAdd(d.blk_events + blk, events);
+  }
 }
 
 }  // namespace ngpu

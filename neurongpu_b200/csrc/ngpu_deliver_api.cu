@@ -43,6 +43,9 @@ __global__ void k_prepare_batch(StepCtx *ctx, int *delays, int *ring_cnt, int nd
     ctx->T0 = nd;          // T = T0 + it + 1 = nd + 1
     ctx->t0 = 0.0;
     ctx->err = 0;
+    ctx->acc_slots = 0;    // one accumulator buffer
+    ctx->ring_R = nd + 1;
+    ctx_set_slots(*ctx);
   }
   for (int k = t; k < nd; k += blockDim.x) delays[k] = k + 1;
   for (int k = t; k < nd + 1; k += blockDim.x) ring_cnt[k] = 0;

@@ -39,7 +39,9 @@ unsigned char *g_scratch_addr[64] = {nullptr};
 
 // Device address of the scratch array on the current device. The host-side
 // name g_noalloc_scratch is only a stand-in: kernels must be given this
-// address, which is looked up once per device with that device current.
+// address, which is looked up once per device with that device current and
+// kept for the life of the process (a cudaDeviceReset ends the context it
+// belongs to; the entry point is documented as not usable after one).
 unsigned char *scratch_on_current_device() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;

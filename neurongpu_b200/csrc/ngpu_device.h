@@ -47,7 +47,7 @@ enum DeviceError : unsigned {
 };
 
 // Bits of GroupArgs::wait_test (test hook, 0 in normal runs): the marked
-// bounded waits make a single non-blocking test instead of waiting, so that
+// bounded waits give up at once, as if their limit had run out, so that
 // their time-out paths can be exercised without a fault or a hang.
 enum WaitTest : int {
   WAIT_TEST_FIRST = 1,          // the tile prefetch wait; the first MMA wait of a proposal round
@@ -86,7 +86,29 @@ struct StepCtx {
   unsigned err;                 // DeviceError bits
   long long rec_row;            // next row of the recording buffer
   unsigned long long n_spikes;  // spikes pushed (all time)
+  // ring sizes and the slots of this step, formed when the step index is
+  // set (ctx_set_slots): kernels index the rings without a 64-bit division
+  int acc_slots;                // accumulator ring (0 or 1: one buffer)
+  int ring_R;                   // spike ring
+  int acc_in_slot;              // accumulator slot of step T - 1 (folded by this step)
+  int acc_out_slot;             // accumulator slot of step T (this step's delivery)
+  int ring_slot;                // spike-ring slot of step T
 };
+
+// the slots of the step T = T0 + it + 1 of c
+NGPU_HD void ctx_set_slots(StepCtx &c) {
+  const long long T = c.T0 + c.it + 1;
+  c.acc_in_slot = c.acc_slots > 1 ? (int)((T - 1) % c.acc_slots) : 0;
+  c.acc_out_slot = c.acc_slots > 1 ? (int)(T % c.acc_slots) : 0;
+  c.ring_slot = c.ring_R > 0 ? (int)(T % c.ring_R) : 0;
+}
+
+// (slot + k) mod n for a ring of n slots and a small offset k (|k| < 2^30)
+NGPU_HD int ring_add(int slot, long long k, int n) {
+  if (n <= 1) return 0;
+  int r = (int)((slot + k) % n);
+  return r < 0 ? r + n : r;
+}
 
 // Where a node's spike goes and what bookkeeping it updates.
 struct PushArgs {
@@ -109,15 +131,27 @@ struct PushArgs {
   int rev_R, rev_C;
 };
 
+// Offset of accumulator slot `slot` in a ring of `slots` slots of `stride`
+// accumulators each (the slot of step T: the delivery of step T adds into
+// it and the update of step T + 1 folds and clears it; 0 for one buffer).
+NGPU_HD long long acc_slot_offset(int slot, int slots, long long stride) {
+  return slots > 1 ? (long long)slot * stride : 0;
+}
+
 // Per-group input folding: acc (+ Poisson direct connections) into state.
 struct InputArgs {
   long long *acc;               // global accumulator array
   long long acc_base;           // this group's first slot
-  // accumulators per parity half (0: one buffer). Deliveries of step T add
-  // into half T & 1 and the update of step T + 1 folds and clears that half,
+  // accumulators per slot (0: one buffer). Deliveries of step T add into
+  // slot T mod acc_slots and the update of step T + 1 folds and clears it,
   // so the update of a step and the delivery of the same step touch
-  // different halves and may run concurrently.
+  // different slots and may run concurrently.
   long long acc_par;
+  int acc_slots;                // 2, or max delay + 2 where steps run in windows
+  // per slot, the last step whose delivery (or large-rate Poisson pre-pass)
+  // added into it, or null: a slot stamped with another step holds zeros,
+  // and its loads are skipped
+  long long *acc_stamp;
   int np;                       // receptor ports
   int in_var;                   // var column of port-0 input
   int in_step;                  // column stride between ports
@@ -269,7 +303,9 @@ struct DeliverArgs {
   int *e_stamp;                        // arrival step of last pre spike
   const unsigned *e_post;              // target node id (plastic networks)
   long long *acc;
-  long long acc_par;                   // accumulators per parity half (0: one buffer)
+  long long acc_par;                   // accumulators per slot (0: one buffer)
+  int acc_slots;                       // slots of the accumulator ring (see InputArgs)
+  long long *acc_stamp;                // per slot, the last step added into it, or null
   const unsigned *ring_src;
   const float *ring_h;
   const int *ring_cnt;

@@ -51,6 +51,20 @@ bool LaunchRk5Update(int model, int np, const GroupArgs &g,
   }
 }
 
+bool LaunchRk5Window(int model, int np, const GroupArgs &g, const InputArgs &in,
+                     const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s) {
+  if (g.n <= 0) return true;
+  switch (model) {
+    case RK5_AEIF_COND_BETA: return LaunchRk5WindowAeifCondBeta(np, g, in, pa, ctxs, W, s);
+    case RK5_AEIF_COND_ALPHA: return LaunchRk5WindowAeifCondAlpha(np, g, in, pa, ctxs, W, s);
+    case RK5_AEIF_PSC_ALPHA:
+    case RK5_AEIF_PSC_EXP:
+    case RK5_AEIF_PSC_DELTA: return LaunchRk5WindowAeifPsc(model, np, g, in, pa, ctxs, W, s);
+    case RK5_IZHIKEVICH_COND_BETA: return LaunchRk5WindowIzhCondBeta(np, g, in, pa, ctxs, W, s);
+    default: return false;
+  }
+}
+
 // floats of a straggler record for the kernel instance LaunchRk5Update picks
 template <template <int> class MT>
 static int rk5_nvar(int np) {
@@ -94,7 +108,8 @@ __device__ __forceinline__ void iaf_psc_exp_node(const GroupArgs &g, const Input
   float I_ex = var[i], I_in = var[n_pad + i];
   float V = var[2 * n_pad + i], refr = var[3 * n_pad + i];
   long long s[2];
-  input_sum<2, false>(in, i, n_pad, 2, it, t0, g.dt, ctx->poisson_pending, T0, s);
+  input_sum<2, false>(in, i, n_pad, 2, it, t0, g.dt, ctx->poisson_pending, T0,
+               ctx->acc_in_slot, s);
   if (s[0] != 0) I_ex = fold_value(I_ex, s[0], 1.0f);
   if (s[1] != 0) I_in = fold_value(I_in, s[1], 1.0f);
   const float I_e = gparam(g, 3, i), Theta = gparam(g, 4, i);
@@ -150,7 +165,8 @@ __device__ __forceinline__ void iaf_psc_exp_g_node(const GroupArgs &g, const Inp
   float *var = g.var;
   float I_syn = var[i], V = var[n_pad + i], refr = var[2 * n_pad + i];
   long long s[1];
-  input_sum<1, false>(in, i, n_pad, 1, it, t0, g.dt, ctx->poisson_pending, T0, s);
+  input_sum<1, false>(in, i, n_pad, 1, it, t0, g.dt, ctx->poisson_pending, T0,
+               ctx->acc_in_slot, s);
   if (s[0] != 0) I_syn = fold_value(I_syn, s[0], 1.0f);
   const float I_e = gparam(g, 0, i);
   if (refr > 0.0f) {
@@ -187,7 +203,8 @@ __device__ __forceinline__ void izhikevich_node(const GroupArgs &g, const InputA
   float I_syn = var[i], V = var[n_pad + i], u = var[2 * n_pad + i];
   float refr = var[3 * n_pad + i];
   long long s[1];
-  input_sum<1, false>(in, i, n_pad, 1, it, t0, g.dt, ctx->poisson_pending, T0, s);
+  input_sum<1, false>(in, i, n_pad, 1, it, t0, g.dt, ctx->poisson_pending, T0,
+               ctx->acc_in_slot, s);
   if (s[0] != 0) I_syn = fold_value(I_syn, s[0], 1.0f);
   const float I_e = gparam(g, 0, i);
   const float h = g.gc[6], a = g.gc[1], b = g.gc[2];
@@ -231,7 +248,8 @@ __device__ __forceinline__ void izh_psc_exp_node(const GroupArgs &g, const Input
   float I_syn = var[i], V = var[n_pad + i], u = var[2 * n_pad + i];
   float refr = var[3 * n_pad + i];
   long long s[1];
-  input_sum<1, false>(in, i, n_pad, 1, it, t0, g.dt, ctx->poisson_pending, T0, s);
+  input_sum<1, false>(in, i, n_pad, 1, it, t0, g.dt, ctx->poisson_pending, T0,
+               ctx->acc_in_slot, s);
   if (s[0] != 0) I_syn = fold_value(I_syn, s[0], 1.0f);
   const float I_e = gparam(g, 0, i);
   const float h = g.gc[6], a = g.gc[1], b = g.gc[2], C_syn = g.gc[7];
@@ -346,7 +364,8 @@ __global__ void k_parrot(GroupArgs g, InputArgs in, PushArgs pa,
   const int n_pad = g.n_pad;
   float *var = g.var;
   long long s[2];
-  input_sum<2, false>(in, i, n_pad, 2, it, t0, g.dt, ctx->poisson_pending, T0, s);
+  input_sum<2, false>(in, i, n_pad, 2, it, t0, g.dt, ctx->poisson_pending, T0,
+               ctx->acc_in_slot, s);
   float sh = var[i];
   if (s[0] != 0) sh = fold_value(sh, s[0], 1.0f);
   if (s[1] != 0) var[n_pad + i] = fold_value(var[n_pad + i], s[1], 0.0f);
@@ -380,7 +399,7 @@ __global__ void k_spike_detector(GroupArgs g, InputArgs in, StepCtx *ctx) {
   float *var = g.var;
   long long s[1];
   input_sum<1>(in, i, n_pad, 1, ctx->it, ctx->t0, g.dt, ctx->poisson_pending,
-               ctx->T0, s);
+               ctx->T0, ctx->acc_in_slot, s);
   float sh = var[i];
   if (s[0] != 0) sh = fold_value(sh, s[0], 1.0f);
   if (sh != 0.0f) {
@@ -441,7 +460,7 @@ __global__ void k_fold_input(GroupArgs g, InputArgs in, StepCtx *ctx) {
   long long s[4];
   const int np = in.np < 4 ? in.np : 4;
   input_sum<4>(in, i, g.n_pad, np, ctx->it, ctx->t0, g.dt, ctx->poisson_pending,
-               ctx->T0, s);
+               ctx->T0, ctx->acc_in_slot, s);
   for (int q = 0; q < np; q++) {
     if (s[q] == 0) continue;
     float w;
@@ -455,7 +474,7 @@ __global__ void k_fold_input(GroupArgs g, InputArgs in, StepCtx *ctx) {
   }
   // ports beyond 4 (RK5 groups with many receptors)
   for (int q = 4; q < in.np; q++) {
-    long long *a = acc_in(in, ctx->T0, ctx->it) + (long long)q * g.n_pad + i;
+    long long *a = acc_in(in, ctx->acc_in_slot) + (long long)q * g.n_pad + i;
     long long sv = *a;
     if (sv == 0) continue;
     *a = 0;
@@ -468,7 +487,7 @@ __global__ void k_fold_input(GroupArgs g, InputArgs in, StepCtx *ctx) {
 
 // Poisson direct connections of NGPU_POISSON_INV_MAX or more expected spikes
 // per step into a group of RK5 neurons, simple-model neurons or parrots:
-// drawn here, before the group's update, and added into the accumulator half
+// drawn here, before the group's update, and added into the accumulator slot
 // that the update folds (those update kernels leave these connections out). The draws are the ones the update would make
 // and the accumulators hold fixed-point integers, so the folded input is the
 // same bit for bit. One thread per node, the only writer of its slots at
@@ -478,7 +497,11 @@ __global__ void k_poisson_large(GroupArgs g, InputArgs in, StepCtx *ctx) {
   if (i >= g.n || !ctx->poisson_pending) return;
   const long long it = ctx->it, T0 = ctx->T0;
   const double t = ctx->t0 + (double)g.dt * (double)it;
-  long long *acc = acc_in(in, T0, it) + i;
+  long long *acc = acc_in(in, ctx->acc_in_slot) + i;
+  // the slot may now hold input: stamp it for the update (one store; a
+  // stamp on a slot that stays zero only costs the update its loads)
+  if (i == 0 && in.acc_stamp != nullptr)
+    in.acc_stamp[in.acc_slots > 1 ? ctx->acc_in_slot : 0] = T0 + it;
   if (in.ud) {
     const unsigned n = direct_count<false, true>(
         t - (double)in.ud_origin - (double)in.ud_delay, in.ud_start, in.ud_stop, in.ud_lambda,
@@ -520,6 +543,55 @@ template <bool PLASTIC>
 __global__ void __launch_bounds__(256)
 k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
   deliver_blocks<PLASTIC>(d, syn, ctx, blockIdx.x, gridDim.x);
+}
+
+// Delivery after a window of integrated steps: the spikes of the steps
+// T_b + first_off ... T_b + first_off + n - 1, T_b the step of ctx (the
+// window's first step), delivered at all their delays at once.
+__global__ void __launch_bounds__(256)
+k_deliver_window(DeliverArgs d, const StepCtx *ctx, long long first_off, int n,
+                 long long arrive_off, int min_delay) {
+  deliver_window_blocks(d, ctx, first_off, n, arrive_off, min_delay, blockIdx.x, gridDim.x);
+}
+
+// Spike bookkeeping of a window (one block): the spikes of the steps
+// T_b + c_lo ... T_b + c_hi - 1 are counted into ctx->n_spikes, and the ring
+// slots of the steps T_b + first_off ... T_b + first_off + n - 1 are
+// emptied for reuse (their spikes have been delivered at every delay).
+__global__ void k_window_book(int *ring_cnt, int ring_R, int ring_C, StepCtx *ctx,
+                              long long first_off, int n, long long c_lo, long long c_hi) {
+  __shared__ unsigned long long s_cnt[256];
+  const long long T_b = ctx->T0 + ctx->it + 1;
+  unsigned long long cnt = 0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const long long rel = first_off + k;
+    const long long Ts = T_b + rel;
+    if (Ts < 0) continue;
+    const int slot = ring_add(ctx->ring_slot, rel, ring_R);
+    if (rel >= c_lo && rel < c_hi) {
+      const int c = ring_cnt[slot];
+      cnt += (unsigned long long)(c < ring_C ? c : ring_C);
+    }
+    ring_cnt[slot] = 0;
+  }
+  s_cnt[threadIdx.x] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int j = 1; j < (int)blockDim.x; j++) cnt += s_cnt[j];
+    ctx->n_spikes += cnt;
+  }
+}
+
+void LaunchDeliverWindow(const DeliverArgs &d, const StepCtx *ctx, long long first_off, int n,
+                         long long arrive_off, int min_delay, int n_blocks, cudaStream_t s) {
+  // no connection from a spiking source (min_delay 0): nothing to deliver
+  if (d.nd <= 0 || n <= 0 || min_delay <= 0) return;
+  k_deliver_window<<<n_blocks, 256, 0, s>>>(d, ctx, first_off, n, arrive_off, min_delay);
+}
+
+void LaunchWindowBook(int *ring_cnt, int ring_R, int ring_C, StepCtx *ctx, long long first_off,
+                      int n, long long c_lo, long long c_hi, cudaStream_t s) {
+  k_window_book<<<1, 256, 0, s>>>(ring_cnt, ring_R, ring_C, ctx, first_off, n, c_lo, c_hi);
 }
 
 // Resident delivery blocks per SM, at most 3: the delivery runs beside the
@@ -615,7 +687,7 @@ void LaunchRevArrive(const DeliverArgs &d, StepCtx *ctx, cudaStream_t s) {
 __global__ void __launch_bounds__(256)
 k_stdp_post(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
   const long long T = ctx->T0 + ctx->it + 1;
-  const int slot = (int)(T % d.ring_R);
+  const int slot = ctx->ring_slot;
   int cnt = d.ring_cnt[slot];
   cnt = cnt < d.ring_C ? cnt : d.ring_C;
   // one block per node: spikes of this step without dendritic delay
@@ -702,6 +774,7 @@ __global__ void k_step_prologue(const StepCtx *base, StepCtx *copies, int n, int
     c.rec_row = base->rec_row + (rec ? k : 0);
     c.err = 0u;
     c.n_spikes = 0ull;
+    ctx_set_slots(c);
     copies[k] = c;
   }
 }
@@ -728,6 +801,7 @@ __global__ void k_step_epilogue(StepCtx *base, const StepCtx *copies, int n, int
     base->n_spikes += sp;
     base->err |= err;
     base->it += n;
+    ctx_set_slots(*base);
     if (n > 0) base->poisson_pending = 1;
     if (rec) base->rec_row += n;
   }

@@ -36,6 +36,19 @@ bool LaunchRk5AeifPsc(int model, int np, const GroupArgs &g, const InputArgs &in
                       int n_del);
 bool LaunchRk5IzhCondBeta(int np, const GroupArgs &g, const InputArgs &in, const PushArgs &pa,
                           StepCtx *ctx, cudaStream_t s, const DeliverArgs *del, int n_del);
+// several steps per launch: one RK5 group through the W steps whose step
+// contexts are ctxs[0 .. W-1] (plain controller, 1-4 ports; false if the
+// model or port count has no window kernel)
+bool LaunchRk5Window(int model, int np, const GroupArgs &g, const InputArgs &in,
+                     const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s);
+bool LaunchRk5WindowAeifCondBeta(int np, const GroupArgs &g, const InputArgs &in,
+                                 const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s);
+bool LaunchRk5WindowAeifCondAlpha(int np, const GroupArgs &g, const InputArgs &in,
+                                  const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s);
+bool LaunchRk5WindowAeifPsc(int model, int np, const GroupArgs &g, const InputArgs &in,
+                            const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s);
+bool LaunchRk5WindowIzhCondBeta(int np, const GroupArgs &g, const InputArgs &in,
+                                const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s);
 // whether the variant's update grid can carry the delivery blocks (the
 // register-capped one-block-per-tile variants; not the persistent ones)
 inline bool Rk5FusesDelivery(int variant) {
@@ -57,6 +70,7 @@ struct Rk5Batch {
   const int *blk_seg;
   unsigned long long *blk_evals;  // [n_blocks] or null
   Rk5Queue q;                     // straggler queue of the launch (cap 0: off)
+  GroupArgs first;                // the first segment's arguments (proposer weights, margin)
 };
 bool Rk5BatchSupported(int model, int np);
 void LaunchRk5Batch(const Rk5Batch &b, StepCtx *ctx, cudaStream_t s);
@@ -96,6 +110,24 @@ void LaunchPoissonLarge(const GroupArgs &g, const InputArgs &in, StepCtx *ctx,
 // synaptic delivery and plasticity
 void LaunchDeliver(const DeliverArgs &d, const SynGroupTable &syn,
                    StepCtx *ctx, int n_blocks, cudaStream_t s);
+// after a window: the spikes of the steps T_b + first_off ...
+// T_b + first_off + n - 1 (T_b: the step of ctx) delivered at all their
+// delays of min_delay or more (the shortest delay of a spiking source's
+// connection), arrivals from step T_b + arrive_off on
+void LaunchDeliverWindow(const DeliverArgs &d, const StepCtx *ctx, long long first_off, int n,
+                         long long arrive_off, int min_delay, int n_blocks, cudaStream_t s);
+// spike count of the steps T_b + c_lo ... T_b + c_hi - 1 into ctx, and the
+// ring slots of the steps T_b + first_off ... + n - 1 emptied
+void LaunchWindowBook(int *ring_cnt, int ring_R, int ring_C, StepCtx *ctx, long long first_off,
+                      int n, long long c_lo, long long c_hi, cudaStream_t s);
+// spike exchange of partitioned networks (ngpu_remote.cu)
+void LaunchPackRemote(const int *ring_cnt, const unsigned *ring_src, const float *ring_h,
+                      int ring_R, int ring_C, const StepCtx *ctx, int n_steps,
+                      const unsigned char *exported, unsigned *out, long long cap,
+                      cudaStream_t s);
+void LaunchUnpackRemote(const unsigned *in, long long count, const int *lut, int lut_n,
+                        int *ring_cnt, unsigned *ring_src, float *ring_h, int ring_R, int ring_C,
+                        StepCtx *ctx, int n_steps, cudaStream_t s);
 // resident 256-thread delivery blocks per SM (grid = SMs x this)
 int DeliverBlocksPerSM();
 int DeliverOccupancy();

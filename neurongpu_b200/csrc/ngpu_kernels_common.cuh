@@ -75,7 +75,9 @@ __device__ __forceinline__ void push_spike(const PushArgs &pa, StepCtx *ctx,
                                            int node, int local, float height,
                                            long long T, double t_now,
                                            int den_delay_steps) {
-  int slot = (int)(T % pa.ring_R);
+  // the ring slot of step T, the step of ctx (every caller pushes the
+  // spikes of its context's step)
+  const int slot = ctx->ring_slot;
   int pos = atomicAdd(&pa.ring_cnt[slot], 1);
   if (pos < pa.ring_C) {
     long long k = (long long)slot * pa.ring_C + pos;
@@ -111,10 +113,18 @@ __device__ __forceinline__ void push_spike(const PushArgs &pa, StepCtx *ctx,
   }
 }
 
-// This group's accumulators that the update following step T0 + it + 1's
-// predecessor folds: the parity half written by the delivery of step T0 + it.
-__device__ __forceinline__ long long *acc_in(const InputArgs &in, long long T0, long long it) {
-  return in.acc + (((T0 + it) & 1) ? in.acc_par : 0) + in.acc_base;
+// This group's accumulators that the update of step T0 + it + 1 folds: the
+// slot written by the delivery of step T0 + it (StepCtx::acc_in_slot).
+__device__ __forceinline__ long long *acc_in(const InputArgs &in, int slot) {
+  return in.acc + acc_slot_offset(slot, in.acc_slots, in.acc_par) + in.acc_base;
+}
+
+// whether that slot may hold input: no stamps, or stamped by a delivery of
+// step T0 + it (one load that every thread of the block shares)
+__device__ __forceinline__ bool acc_live(const InputArgs &in, int slot, long long T0,
+                                         long long it) {
+  if (in.acc_stamp == nullptr) return true;
+  return __ldcg(in.acc_stamp + (in.acc_slots > 1 ? slot : 0)) == T0 + it;
 }
 
 // Poisson count of one direct connection for the step T_prev (the
@@ -166,14 +176,15 @@ template <int NP, bool LARGE = true>
 __device__ __forceinline__ void input_sum(const InputArgs &in, int i,
                                           int n_pad, int np, long long it,
                                           double t0, float dt, int pending,
-                                          long long T0, long long *s,
+                                          long long T0, int acc_slot, long long *s,
                                           bool dry = false,
                                           const long long *pre_acc = nullptr) {
+  const bool live = pre_acc != nullptr || acc_live(in, acc_slot, T0, it);
 #pragma unroll
   for (int q = 0; q < NP; q++) {
     s[q] = 0;
-    if (q < np) {
-      long long *a = acc_in(in, T0, it) + (long long)q * n_pad + i;
+    if (q < np && live) {
+      long long *a = acc_in(in, acc_slot) + (long long)q * n_pad + i;
       long long v = pre_acc ? pre_acc[q] : *a;
       if (v != 0 && !(in.dry || dry)) *a = 0;
       s[q] = v;
@@ -643,11 +654,9 @@ __device__ __forceinline__ void rk5_queue_reset(const Rk5Queue &qu) {
 // parameters are loaded per neuron and q is formed in registers.
 // MODE STEP_PLAIN: the reference's controller; STEP_LOG: the same, and every
 // sub-step that starts with a controller guess shorter than the rest of the
-// time step is logged for training the proposer; STEP_LEARNED: that guess is
-// replaced by the learned proposer's (the error test still accepts or
-// rejects). STEP_LEARNED is called by every thread of the CTA, in lock-step
-// rounds of one accepted sub-step, because each proposal round is one
-// CTA-wide tensor-core MMA; threads past the group end only take part.
+// time step is logged for training the proposer. (The learned proposer runs
+// in the straggler queue's finishing launch, k_rk5_finish_learned, after a
+// STEP_PLAIN update with the queue on.)
 // With a straggler queue (STEP_PLAIN), a neuron still inside the step after
 // its first sub-step is handed over to the queue (segment seg). pre_col /
 // pre_acc: the neuron's state columns (M::NVAR state variables, refractory
@@ -661,7 +670,7 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
                                            int seg = 0, const float *pre_col = nullptr,
                                            const long long *pre_acc = nullptr, int tile = -1) {
   using Tr = ModelTraits<M>;
-  const bool active = (MODE != STEP_LEARNED) || (i < g.n);
+  const bool active = true;
   const bool dry = g.dry || dry_run;
   // the launchers pick the template port count NP = np for 2..4 ports (1
   // serves 0 and 1), so there the count is a compile-time constant
@@ -676,7 +685,8 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
   constexpr int NPI = (M::NPV == 0) ? 1 : NP;
   long long s[NPI];
   if (active)
-    input_sum<NPI, false>(in, i, n_pad, np, it, t0, g.dt, pending, T0, s, dry, pre_acc);
+    input_sum<NPI, false>(in, i, n_pad, np, it, t0, g.dt, pending, T0, ctx->acc_in_slot, s, dry,
+                          pre_acc);
   float y[M::NVAR];
 #pragma unroll
   for (int j = 0; j < M::NVAR; j++) {
@@ -716,48 +726,7 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
   bool end_step = !active;
   int guard = 0;
   float h_acc, err_acc;
-  if constexpr (MODE == STEP_LEARNED) {
-    bool staged = false, failed = false;
-    proposer_alloc(*ps);
-    while (__syncthreads_or(!end_step)) {
-      const float hmax = active ? (float)(x1 - x) : 0.0f;
-      const bool want = !end_step && !failed && h < hmax;
-      if (__syncthreads_or(want)) {
-        if (!staged) {
-          proposer_stage_weights(*ps, g.mlp);
-          staged = true;
-        }
-        float f[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-        if (want) ProposerFeatures<M>::get(y, p, h, g.dt, f);
-        float o = 0.0f;
-        if (proposer_round(*ps, want, f, o, &ctx->err, g.wait_test)) {
-          if (want) {
-            // the proposal may shrink the controller's guess by at most 4x
-            // (after a low-error step it then still grows, >= 1.25x) and
-            // enlarge it by at most 16x: a network queried outside its
-            // training distribution cannot stall or blow up the integration
-            const float hp = g.dt * exp2f(o - g.mlp_margin);
-            h = fminf(fmaxf(fminf(fmaxf(hp, 0.25f * h), 16.0f * h), h_min), hmax);
-          }
-        } else {
-          failed = true;
-        }
-      }
-      if (!end_step) {
-        rk5_step<M, NP>(x, y, h, h_min, g.h_min_thr, hmax, p, q, refr, np, inv_eps, evals, h_acc,
-                        err_acc);
-        end_step = (x >= x1 - (double)h_min);
-        if (M::external(y, p, refr, end_step, g.dt)) {
-          if (!dry) push_spike(pa, ctx, g.i_node_0 + i, i, 1.0f, T, x1, den);
-        }
-        if (++guard > g.max_substeps) {
-          atomicOr(&ctx->err, (unsigned)DERR_RK5_STUCK);
-          end_step = true;
-        }
-      }
-    }
-    proposer_teardown(*ps, failed);
-  } else if constexpr (MODE == STEP_LOG) {
+  if constexpr (MODE == STEP_LOG) {
     while (!end_step) {
       const float hmax = (float)(x1 - x);
       float f[6];
@@ -808,14 +777,91 @@ k_rk5_update(const __grid_constant__ GroupArgs g, const __grid_constant__ InputA
   pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned evals = 0;
-  if constexpr (MODE == STEP_LEARNED) {
-    __shared__ ProposerSmem ps;
-    rk5_neuron<M, NP, UNI, MODE>(g, in, pa, ctx, i, g.puni, g.pinv, evals, false, &ps);
-  } else {
-    const bool queued = (MODE == STEP_PLAIN) && g.q.cap > 0;
-    if (i < g.n) rk5_neuron<M, NP, UNI, MODE>(g, in, pa, ctx, i, g.puni, g.pinv, evals, false,
-                                              nullptr, queued ? &g.q : nullptr, 0);
+  const bool queued = (MODE == STEP_PLAIN) && g.q.cap > 0;
+  if (i < g.n) rk5_neuron<M, NP, UNI, MODE>(g, in, pa, ctx, i, g.puni, g.pinv, evals, false,
+                                            nullptr, queued ? &g.q : nullptr, 0);
+  if (g.blk_evals != nullptr) block_add_u64(evals, g.blk_evals);
+}
+
+// Integrates neuron i through the W consecutive steps of a window (plain
+// controller), its state in registers from the first step to the last: each
+// step reads its own step context (ctxs[k]), folds that step's pending input
+// (its accumulator slot, filled before the window by earlier deliveries, and
+// its Poisson draws) and integrates the step with rk5_neuron's sub-step
+// sequence; the time offset is rounded to float between steps, as
+// rk5_neuron stores it, so the result is the one-step path's, bit for bit.
+// Spikes go to each step's ring slot.
+template <class M, int NP, bool UNI>
+__device__ __forceinline__ void rk5_window_neuron(const GroupArgs &g, const InputArgs &in,
+                                                  const PushArgs &pa, StepCtx *ctxs, int W,
+                                                  int i, const float *p_uni,
+                                                  const float *q_uni, unsigned &evals) {
+  using Tr = ModelTraits<M>;
+  const int np = (NP >= 2 && NP <= 4) ? NP : in.np;
+  const int n_pad = g.n_pad;
+  constexpr int NPI = (M::NPV == 0) ? 1 : NP;
+  float y[M::NVAR];
+#pragma unroll
+  for (int j = 0; j < M::NVAR; j++)
+    y[j] = ((NP >= 2 && NP <= 4) || j < g.nvar) ? g.var[(long long)j * n_pad + i] : 0.0f;
+  float p_loc[UNI ? 1 : M::NPARAM];
+  float q_loc[UNI ? 1 : M::NPARAM];
+  rk5_load_params<M, UNI>(g, i, true, p_loc, q_loc);
+  const float *p = UNI ? p_uni : p_loc;
+  const float *q = UNI ? q_uni : q_loc;
+  float refr = g.param[(long long)Tr::refr * n_pad + i];
+  const float refr0 = refr;
+  float h = g.h[i];
+  float dxf = g.dx[i];
+  const int den = (UNI && g.den_delay_col == Tr::den) ? g.den_steps
+                                                       : (int)roundf(p[Tr::den] / g.dt);
+  for (int k = 0; k < W; k++) {
+    StepCtx *ctx = ctxs + k;
+    const long long it = ctx->it;
+    const long long T0 = ctx->T0;
+    const double t0 = ctx->t0;
+    long long s[NPI];
+    input_sum<NPI, false>(in, i, n_pad, np, it, t0, g.dt, ctx->poisson_pending, T0,
+                          ctx->acc_in_slot, s);
+#pragma unroll
+    for (int qq = 0; qq < NPI; qq++) {
+      if (qq < np && s[qq] != 0) {
+        const int vi = Tr::in_base + qq * Tr::in_step;
+        const float w = (Tr::w_base >= 0) ? p[Tr::w_base + qq * Tr::w_step] : 1.0f;
+        y[vi] = fold_value(y[vi], s[qq], w);
+      }
+    }
+    const double x1 = t0 + (double)g.dt * (double)(it + 1);
+    double x = t0 + (double)g.dt * (double)it + (double)dxf;
+    const long long T = T0 + it + 1;
+    int guard = 0;
+    bool end_step = false;
+    while (!end_step) {
+      end_step = rk5_plain_substep<M, NP>(g, pa, ctx, i, y, x, h, refr, guard, p, q, np,
+                                          g.inv_eps, x1, T, den, false, evals);
+    }
+    dxf = (float)(x - x1);
   }
+#pragma unroll
+  for (int j = 0; j < M::NVAR; j++) {
+    if ((NP >= 2 && NP <= 4) || j < g.nvar) g.var[(long long)j * n_pad + i] = y[j];
+  }
+  g.h[i] = h;
+  g.dx[i] = dxf;
+  if (refr != refr0) g.param[(long long)Tr::refr * n_pad + i] = refr;
+}
+
+// One RK5 group through a window of W steps (several steps per launch);
+// MINB: the register cap of the single-step variant the autotuner chose.
+template <class M, int NP, bool UNI, int MINB>
+__global__ void __launch_bounds__(NGPU_BLOCK, MINB)
+k_rk5_window(const __grid_constant__ GroupArgs g, const __grid_constant__ InputArgs in,
+             const __grid_constant__ PushArgs pa, StepCtx *ctxs, int W) {
+  pdl_wait();
+  pdl_trigger();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned evals = 0;
+  if (i < g.n) rk5_window_neuron<M, NP, UNI>(g, in, pa, ctxs, W, i, g.puni, g.pinv, evals);
   if (g.blk_evals != nullptr) block_add_u64(evals, g.blk_evals);
 }
 
@@ -883,7 +929,7 @@ k_rk5_update_tiles(const __grid_constant__ GroupArgs g, const __grid_constant__ 
   }
   __syncthreads();
   // this step's input half (thread 0 issues every copy)
-  const long long *acc = threadIdx.x == 0 ? acc_in(in, ctx->T0, ctx->it) : nullptr;
+  const long long *acc = threadIdx.x == 0 ? acc_in(in, ctx->acc_in_slot) : nullptr;
   if (threadIdx.x == 0) {
     if ((int)blockIdx.x < n_tiles) rk5_issue_tile<M, NP>(s_st[0], &s_bar[0], g, acc, n_acc, blockIdx.x);
     if ((int)blockIdx.x + G < n_tiles)
@@ -973,15 +1019,10 @@ k_rk5_update_seg(const SegArgs *__restrict__ segs, const int *__restrict__ blk_s
   }
   const int i = (blockIdx.x - S.blk0) * blockDim.x + threadIdx.x;
   unsigned evals = 0;
-  if constexpr (MODE == STEP_LEARNED) {
-    __shared__ ProposerSmem ps;
-    rk5_neuron<M, NP, UNI, MODE>(S.g, S.in, S.pa, ctx, i, s_p, s_q, evals, dry != 0, &ps);
-  } else {
-    const bool queued = (MODE == STEP_PLAIN) && qu.cap > 0;
-    if (i < S.g.n)
-      rk5_neuron<M, NP, UNI, MODE>(S.g, S.in, S.pa, ctx, i, s_p, s_q, evals, dry != 0, nullptr,
-                                   queued ? &qu : nullptr, seg, nullptr, nullptr, blockIdx.x);
-  }
+  const bool queued = (MODE == STEP_PLAIN) && qu.cap > 0;
+  if (i < S.g.n)
+    rk5_neuron<M, NP, UNI, MODE>(S.g, S.in, S.pa, ctx, i, s_p, s_q, evals, dry != 0, nullptr,
+                                 queued ? &qu : nullptr, seg, nullptr, nullptr, blockIdx.x);
   if (blk_evals != nullptr) block_add_u64(evals, blk_evals);
 }
 
@@ -1005,6 +1046,96 @@ k_rk5_finish_seg(const SegArgs *__restrict__ segs, unsigned long long *blk_evals
     rk5_resume<M, NP, UNI>(R.g, R.pa, ctx, R.g.puni, R.g.pinv, R.in.np, r, evals,
                            R.g.dry || dry != 0);
   }
+  if (blk_evals != nullptr) block_add_u64(evals, blk_evals);
+  rk5_queue_reset(qu);
+}
+
+// Finishing launch of an update with the learned step proposer: the update
+// is the plain kernel with the straggler queue on, so a neuron whose first
+// sub-step (the controller's guess) completes the time step, the common
+// case, never waits for a tensor-core round; the records of the others are
+// taken 128 per CTA, which integrates them in lock-step rounds of one
+// sub-step: each round in which a record's next step is shorter than the
+// rest of the time step is one CTA-wide MMA of the proposer network
+// (src/rk5.h:57-162 for the sub-step; the proposal replaces the
+// controller's guess, the error test still accepts or rejects). SEG: records
+// of a batched launch (the record's segment gives its arguments; g0 is the
+// first segment's, for the proposer's weights and margin).
+template <class M, int NP, bool UNI, bool SEG>
+__global__ void __launch_bounds__(NGPU_BLOCK, 1)
+k_rk5_finish_learned(const __grid_constant__ GroupArgs g0, const __grid_constant__ PushArgs pa0,
+                     int np0, const SegArgs *__restrict__ segs, unsigned long long *blk_evals,
+                     int dry, StepCtx *ctx, const __grid_constant__ Rk5Queue qu) {
+  using Tr = ModelTraits<M>;
+  pdl_trigger();
+  pdl_wait();
+  __shared__ unsigned s_pref[NGPU_QLANES + 1];
+  const unsigned n = rk5_queue_prefix(qu, s_pref);
+  if (n == 0) return;             // the same for every block: nothing to reset
+  __shared__ ProposerSmem ps;
+  proposer_alloc(ps);
+  bool staged = false, failed = false;
+  unsigned evals = 0;
+  const long long it = ctx->it;
+  const long long T = ctx->T0 + it + 1;
+  for (unsigned base = blockIdx.x * NGPU_BLOCK; base < n; base += gridDim.x * NGPU_BLOCK) {
+    const unsigned k = base + threadIdx.x;
+    const bool act = k < n;
+    const float *r = act ? rk5_queue_record(qu, s_pref, k) : nullptr;
+    const int seg = (SEG && act) ? __float_as_int(r[1]) : 0;
+    const GroupArgs &g = SEG ? segs[seg].g : g0;
+    const PushArgs &pa = SEG ? segs[seg].pa : pa0;
+    const int np = (NP >= 2 && NP <= 4) ? NP : (SEG ? segs[seg].in.np : np0);
+    const int i = act ? __float_as_int(r[0]) : 0;
+    int guard = act ? __float_as_int(r[2]) : 0;
+    float h = act ? r[3] : 0.0f;
+    float refr = act ? r[4] : 0.0f;
+    double x = act ? *reinterpret_cast<const double *>(r + 6) : 0.0;
+    float y[M::NVAR];
+#pragma unroll
+    for (int j = 0; j < M::NVAR; j++) y[j] = act ? r[8 + j] : 0.0f;
+    float p_loc[UNI ? 1 : M::NPARAM];
+    float q_loc[UNI ? 1 : M::NPARAM];
+    rk5_load_params<M, UNI>(g, i, act, p_loc, q_loc);
+    const float *p = UNI ? g.puni : p_loc;
+    const float *q = UNI ? g.pinv : q_loc;
+    const double x1 = ctx->t0 + (double)g.dt * (double)(it + 1);
+    const int den = (UNI && g.den_delay_col == Tr::den) ? g.den_steps
+                                                         : (int)roundf(p[Tr::den] / g.dt);
+    const bool dry_g = dry != 0 || g.dry != 0;
+    bool end = !act;
+    while (__syncthreads_or(!end)) {
+      const float hmax = !end ? (float)(x1 - x) : 0.0f;
+      const bool want = !end && !failed && h < hmax;
+      if (__syncthreads_or(want)) {
+        if (!staged) {
+          proposer_stage_weights(ps, g0.mlp);
+          staged = true;
+        }
+        float f[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        if (want) ProposerFeatures<M>::get(y, p, h, g.dt, f);
+        float o = 0.0f;
+        if (proposer_round(ps, want, f, o, &ctx->err, g0.wait_test)) {
+          if (want) {
+            // the proposal may shrink the controller's guess by at most 4x
+            // (after a low-error step it then still grows, >= 1.25x) and
+            // enlarge it by at most 16x: a network queried outside its
+            // training distribution cannot stall or blow up the integration
+            const float hp = g.dt * exp2f(o - g0.mlp_margin);
+            h = fminf(fmaxf(fminf(fmaxf(hp, 0.25f * h), 16.0f * h), g.h_min), hmax);
+          }
+        } else {
+          failed = true;
+        }
+      }
+      if (!end) {
+        end = rk5_plain_substep<M, NP>(g, pa, ctx, i, y, x, h, refr, guard, p, q, np, g.inv_eps,
+                                       x1, T, den, dry_g, evals);
+      }
+    }
+    if (act && !dry_g) rk5_store<M, NP>(g, i, y, h, x, x1, refr, true);
+  }
+  proposer_teardown(ps, failed);
   if (blk_evals != nullptr) block_add_u64(evals, blk_evals);
   rk5_queue_reset(qu);
 }

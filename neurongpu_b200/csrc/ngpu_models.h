@@ -40,7 +40,10 @@ enum ModelKind {
   MK_POISSON_NODES,       // CreatePoissonGenerator: nodes that push spike counts
   MK_IAF_PSC_EXP_G,       // iaf_psc_exp_g / iaf_psc_exp_hc: one port, group parameters
   MK_IZHIKEVICH,          // Euler Izhikevich, input added to V_m
-  MK_IZH_PSC_EXP          // Euler Izhikevich with an exponential current, n_sub Euler steps
+  MK_IZH_PSC_EXP,         // Euler Izhikevich with an exponential current, n_sub Euler steps
+  MK_IMAGE                // image of a node of another host (remote connections): no
+                          // dynamics, its spikes are the remote node's, received by
+                          // the host's spike exchange
 };
 
 enum Rk5Model {
@@ -289,6 +292,17 @@ inline const std::vector<ModelInfo> &ModelCatalogue() {
     m.rk5_model = -1; m.fixed_n_port = 0;
     m.scal_param = {"rate", "origin", "start", "stop"};
     m.scal_param_def = {0.0f, 0.0f, 0.0f, 1.0e30f};
+    m.in_var = -1; m.in_step = 0; m.w_param = false; m.w_param_idx = -1;
+    m.refr_param = -1; m.den_delay_param = -1;
+    cat.push_back(m);
+  }
+  {
+    // the reference's remote nodes (src/neurongpu.cu:1626-1642, a base
+    // neuron group created at calibration): created by RemoteConnect on the
+    // target host, one per remote source node
+    ModelInfo m;
+    m.name = "remote_image"; m.kind = MK_IMAGE;
+    m.rk5_model = -1; m.fixed_n_port = 0;
     m.in_var = -1; m.in_step = 0; m.w_param = false; m.w_param_idx = -1;
     m.refr_param = -1; m.den_delay_param = -1;
     cat.push_back(m);

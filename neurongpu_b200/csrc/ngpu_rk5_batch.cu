@@ -2,6 +2,8 @@
 // launch through a device segment table (k_rk5_update_seg), e.g. the
 // independent networks of a parameter sweep. Kept in its own translation unit
 // so that its template instances compile in parallel with ngpu_kernels.cu.
+#include <cstring>
+
 #include "ngpu_kernels_common.cuh"
 
 namespace ngpu {
@@ -9,18 +11,18 @@ namespace ngpu {
 template <class M, int NP>
 static void launch_rk5_seg(const Rk5Batch &b, StepCtx *ctx, cudaStream_t s) {
   dim3 grid(b.n_blocks), block(NGPU_BLOCK);
-  if (b.mode != STEP_PLAIN) {
-    if constexpr (ProposerFeatures<M>::supported && NP <= 2) {
-      if (b.mode == STEP_LOG) {
-        if (b.uni) k_rk5_update_seg<M, NP, true, 1, STEP_LOG><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q);
-        else k_rk5_update_seg<M, NP, false, 1, STEP_LOG><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q);
-      } else {
-        if (b.uni) k_rk5_update_seg<M, NP, true, 4, STEP_LEARNED><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q);
-        else k_rk5_update_seg<M, NP, false, 4, STEP_LEARNED><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q);
-      }
+  constexpr bool kProposer = ProposerFeatures<M>::supported && NP <= 2;
+  if (b.mode == STEP_LOG) {
+    if constexpr (kProposer) {
+      if (b.uni) k_rk5_update_seg<M, NP, true, 1, STEP_LOG><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q);
+      else k_rk5_update_seg<M, NP, false, 1, STEP_LOG><<<grid, block, 0, s>>>(b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q);
     }
     return;
   }
+  // the learned proposer: the plain update of the chosen variant with the
+  // straggler queue, the proposer in the queue's finishing launch
+  const bool learned = b.mode == STEP_LEARNED;
+  if (learned && !kProposer) return;
   if constexpr (NP <= 4) {
     if (b.uni) {
       switch (b.variant) {
@@ -32,7 +34,14 @@ static void launch_rk5_seg(const Rk5Batch &b, StepCtx *ctx, cudaStream_t s) {
     } else {
       launch_pdl(k_rk5_update_seg<M, NP, false, 1, STEP_PLAIN>, grid, block, s, b.segs, b.blk_seg, b.blk_evals, b.dry, ctx, b.q);
     }
-    if (b.q.cap > 0) {
+    if (b.q.cap > 0 && learned) {
+      if constexpr (kProposer) {
+        PushArgs no_pa;
+        memset(&no_pa, 0, sizeof(no_pa));
+        if (b.uni) launch_pdl(k_rk5_finish_learned<M, NP, true, true>, dim3(b.q.fin_blocks), block, s, b.first, no_pa, 0, b.segs, b.blk_evals, b.dry, ctx, b.q);
+        else launch_pdl(k_rk5_finish_learned<M, NP, false, true>, dim3(b.q.fin_blocks), block, s, b.first, no_pa, 0, b.segs, b.blk_evals, b.dry, ctx, b.q);
+      }
+    } else if (b.q.cap > 0) {
       if (b.uni) launch_pdl(k_rk5_finish_seg<M, NP, true>, dim3(b.q.fin_blocks), block, s, b.segs, b.blk_evals, b.dry, ctx, b.q);
       else launch_pdl(k_rk5_finish_seg<M, NP, false>, dim3(b.q.fin_blocks), block, s, b.segs, b.blk_evals, b.dry, ctx, b.q);
     }

@@ -4,6 +4,8 @@
 // family (ngpu_rk5_<model>.cu), so that their template instances compile in
 // parallel.
 #pragma once
+#include <type_traits>
+
 #include "ngpu_kernels_common.cuh"
 #include "ngpu_deliver.cuh"
 
@@ -70,19 +72,32 @@ static bool launch_rk5(const GroupArgs &g, const InputArgs &in, const PushArgs &
                        StepCtx *ctx, cudaStream_t s, const DeliverArgs *del = nullptr,
                        int n_del = 0) {
   dim3 grid((g.n + NGPU_BLOCK - 1) / NGPU_BLOCK), block(NGPU_BLOCK);
-  if (g.step_mode != STEP_PLAIN) {
-    // step logging and the learned proposer: conductance AdEx, <= 2 ports
-    if constexpr (ProposerFeatures<M>::supported && NP <= 2) {
-      if (g.step_mode == STEP_LOG) {
-        if (g.all_uniform) k_rk5_update<M, NP, true, 1, STEP_LOG><<<grid, block, 0, s>>>(g, in, pa, ctx);
-        else k_rk5_update<M, NP, false, 1, STEP_LOG><<<grid, block, 0, s>>>(g, in, pa, ctx);
-      } else {
-        if (g.all_uniform) k_rk5_update<M, NP, true, 4, STEP_LEARNED><<<grid, block, 0, s>>>(g, in, pa, ctx);
-        else k_rk5_update<M, NP, false, 4, STEP_LEARNED><<<grid, block, 0, s>>>(g, in, pa, ctx);
-      }
+  constexpr bool kProposer = ProposerFeatures<M>::supported && NP <= 2;
+  if (g.step_mode == STEP_LOG) {
+    // step logging: conductance AdEx, <= 2 ports
+    if constexpr (kProposer) {
+      if (g.all_uniform) k_rk5_update<M, NP, true, 1, STEP_LOG><<<grid, block, 0, s>>>(g, in, pa, ctx);
+      else k_rk5_update<M, NP, false, 1, STEP_LOG><<<grid, block, 0, s>>>(g, in, pa, ctx);
     }
     return false;
   }
+  // the learned proposer: the plain update of the chosen variant with the
+  // straggler queue, the proposer in the queue's finishing launch
+  const bool learned = g.step_mode == STEP_LEARNED;
+  if (learned && !kProposer) return false;
+  auto finish = [&](auto uni) {
+    constexpr bool U = decltype(uni)::value;
+    if (g.q.cap <= 0) return;
+    if (learned) {
+      if constexpr (kProposer) {
+        const SegArgs *no_segs = nullptr;
+        launch_pdl(k_rk5_finish_learned<M, NP, U, false>, dim3(g.q.fin_blocks), block, s, g, pa,
+                   in.np, no_segs, g.blk_evals, g.dry, ctx, g.q);
+      }
+    } else {
+      launch_pdl(k_rk5_finish<M, NP, U>, dim3(g.q.fin_blocks), block, s, g, in, pa, ctx);
+    }
+  };
   if (g.all_uniform) {
     if constexpr (NP <= 4) {
       // occupancy variants chosen by the autotuner (register cap per thread)
@@ -98,7 +113,7 @@ static bool launch_rk5(const GroupArgs &g, const InputArgs &in, const PushArgs &
           case 6: launch_pdl(k_rk5_update_deliver<M, NP, 4>, fgrid, block, s, g, in, pa, ctx, *del, n_del); break;
           default: launch_pdl(k_rk5_update_deliver<M, NP, 1>, fgrid, block, s, g, in, pa, ctx, *del, n_del); break;
         }
-        if (g.q.cap > 0) launch_pdl(k_rk5_finish<M, NP, true>, dim3(g.q.fin_blocks), block, s, g, in, pa, ctx);
+        finish(std::true_type());
         return true;
       }
       switch (variant) {
@@ -123,12 +138,49 @@ static bool launch_rk5(const GroupArgs &g, const InputArgs &in, const PushArgs &
     } else {
       launch_pdl(k_rk5_update<M, NP, true, 1, STEP_PLAIN>, grid, block, s, g, in, pa, ctx);
     }
-    if (g.q.cap > 0) launch_pdl(k_rk5_finish<M, NP, true>, dim3(g.q.fin_blocks), block, s, g, in, pa, ctx);
+    finish(std::true_type());
   } else {
     launch_pdl(k_rk5_update<M, NP, false, 1, STEP_PLAIN>, grid, block, s, g, in, pa, ctx);
-    if (g.q.cap > 0) launch_pdl(k_rk5_finish<M, NP, false>, dim3(g.q.fin_blocks), block, s, g, in, pa, ctx);
+    finish(std::false_type());
   }
   return false;
+}
+
+// The window kernel (several steps per launch) with the register cap of the
+// group's chosen single-step variant.
+template <class M, int NP>
+static void launch_rk5_window(const GroupArgs &g, const InputArgs &in, const PushArgs &pa,
+                              StepCtx *ctxs, int W, cudaStream_t s) {
+  const dim3 grid((g.n + NGPU_BLOCK - 1) / NGPU_BLOCK), block(NGPU_BLOCK);
+  if (!g.all_uniform) {
+    launch_pdl(k_rk5_window<M, NP, false, 1>, grid, block, s, g, in, pa, ctxs, W);
+    return;
+  }
+  // the register cap for 6 blocks per SM was the fastest window kernel on
+  // the 1e6-neuron network whatever the single-step variant (4.19 bio-s per
+  // wall-s against 4.00-4.01 for 5 and 8 blocks and 3.60 for 4); variant 0
+  // (no cap) and the 4-block variants keep their own
+  switch (g.variant) {
+    case 0: launch_pdl(k_rk5_window<M, NP, true, 1>, grid, block, s, g, in, pa, ctxs, W); break;
+    case 6:
+    case 7:
+    case 8: launch_pdl(k_rk5_window<M, NP, true, 4>, grid, block, s, g, in, pa, ctxs, W); break;
+    default: launch_pdl(k_rk5_window<M, NP, true, 6>, grid, block, s, g, in, pa, ctxs, W); break;
+  }
+}
+
+// windows: 1-4 ports (the group kinds that WindowSteps admits)
+template <template <int> class MT>
+static bool launch_rk5_window_model(int np, const GroupArgs &g, const InputArgs &in,
+                                    const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s) {
+  switch (np) {
+    case 0:
+    case 1: launch_rk5_window<MT<1>, 1>(g, in, pa, ctxs, W, s); return true;
+    case 2: launch_rk5_window<MT<2>, 2>(g, in, pa, ctxs, W, s); return true;
+    case 3: launch_rk5_window<MT<3>, 3>(g, in, pa, ctxs, W, s); return true;
+    case 4: launch_rk5_window<MT<4>, 4>(g, in, pa, ctxs, W, s); return true;
+    default: return false;
+  }
 }
 
 template <template <int> class MT>

@@ -123,24 +123,15 @@ __device__ __forceinline__ void mbar_init(uint64_t *mbar, uint32_t count) {
   asm volatile("fence.mbarrier_init.release.cluster;" : : : "memory");
 }
 
-// bounded wait for the phase with the given parity; false on time-out
 // Bounded wait for the completion of the barrier phase with the given
-// parity; false if it did not complete within max_iter tries. test_once: a
-// single non-blocking test instead (the wait-test hook of GroupArgs).
+// parity; false if it did not complete within max_iter tries. give_up: the
+// wait's limit is reached at once (the wait-test hook of GroupArgs), with the
+// operation it waits for still in flight, so that the time-out path runs
+// deterministically (a single test could see a fast operation complete).
 __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, int max_iter,
-                                          bool test_once = false) {
+                                          bool give_up = false) {
   const uint32_t a = smem_u32(mbar);
-  if (test_once) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    return done != 0;
-  }
+  if (give_up) return false;
   for (int k = 0; k < max_iter; k++) {
     uint32_t done;
     asm volatile(

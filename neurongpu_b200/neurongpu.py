@@ -269,6 +269,13 @@ _EXT_SIG = {
                                     ctypes.POINTER(ctypes.c_longlong))),
     "NGB200_GetRk5Tuning": (_I, (_I, ctypes.POINTER(ctypes.c_int),
                                  ctypes.POINTER(ctypes.c_float))),
+    "NGB200_SetInstance": (_I, (_I,)),
+    "NGB200_GetInstance": (_I, ()),
+    "NGB200_SetHost": (_I, (_I, _I)),
+    "NGB200_SimulateSteps": (_I, (ctypes.c_longlong,)),
+    "NGB200_RemoteExchangeSteps": (_I, ()),
+    "NGB200_PackRemoteSpikes": (ctypes.c_longlong, (_I, c_void_p, ctypes.c_longlong)),
+    "NGB200_UnpackRemoteSpikes": (_I, (_I, _I, c_void_p, ctypes.c_longlong)),
 }
 
 
@@ -299,6 +306,9 @@ class Binding(object):
                 self._c[name] = f
         # errors are returned as codes and raised here as ValueError
         self._c["SetOnException"](1)
+        # collective of a network partitioned over hosts (ConnectMpiInit)
+        self._comm = None
+        self._xbuf = None
 
     # -- errors ----------------------------------------------------------
     def GetErrorMessage(self):
@@ -456,6 +466,10 @@ class Binding(object):
             return rg
         i_node = self._call("RemoteCreate", ctypes.c_int(i_host), _cstr(model_name),
                             ctypes.c_int(n_node), ctypes.c_int(n_ports))
+        # the group's first node is known on its own host only: the other
+        # hosts receive it (the reference broadcasts it over MPI)
+        if self._comm is not None and self._comm.size > 1:
+            i_node = self._comm.broadcast_int(i_node, i_host)
         return RemoteNodeSeq(i_host, NodeSeq(i_node, n_node))
 
     def _nodes_arr(self, nodes):
@@ -817,7 +831,59 @@ class Binding(object):
     def Simulate(self, sim_time=1000.0):
         "Simulate neural activity"
         self.SetSimTime(sim_time)
+        if self._comm is not None and self._comm.size > 1:
+            return self._simulate_partitioned(sim_time)
         return self._call("Simulate")
+
+    def _simulate_partitioned(self, sim_time):
+        """Simulate on every host of a partitioned network: runs of E steps
+        (the shortest delay of a remote connection, the same on every host),
+        each followed by the spike exchange, so a remote spike reaches its
+        image before any delivery of it is due (the reference exchanges
+        every step, src/neurongpu.cu:490-521)."""
+        self._call("StartSimulation")
+        n_total = int(round(sim_time / self.GetTimeResolution()))
+        e = self._call("NGB200_RemoteExchangeSteps")
+        e = self._comm.min_int(e if e > 0 else 1 << 30)
+        e = max(1, min(e, 1000))
+        done = 0
+        while done < n_total:
+            k = min(e, n_total - done)
+            self._call("NGB200_SimulateSteps", ctypes.c_longlong(k))
+            self._exchange_spikes(k)
+            done += k
+        return self._call("EndSimulation")
+
+    def _exchange_spikes(self, n_steps):
+        """Packs this host's exported spikes of the last n_steps steps,
+        all-gathers the lists over the hosts and pushes the other hosts'
+        spikes into the images here."""
+        comm = self._comm
+        if self._xbuf is None:
+            self._xbuf = comm.empty_u32(4 + 3 * 4096)
+        cap = (self._xbuf.numel() - 4) // 3
+        count = self.PackRemoteSpikes(n_steps, self._xbuf.data_ptr(), cap)
+        if count > cap:
+            self._xbuf = comm.empty_u32(4 + 3 * (2 * count))
+            cap = (self._xbuf.numel() - 4) // 3
+            count = self.PackRemoteSpikes(n_steps, self._xbuf.data_ptr(), cap)
+        counts = comm.allgather_int(count)
+        m = max(counts)
+        if m == 0:
+            return
+        if self._xbuf.numel() < 4 + 3 * m:
+            # every host sends the longest list's length: keep this host's
+            # packed spikes in a buffer that long
+            grown = comm.empty_u32(4 + 3 * (2 * m))
+            grown[:self._xbuf.numel()] = self._xbuf
+            self._xbuf = grown
+        rows = comm.allgather_rows(self._xbuf, 4 + 3 * m)
+        for h, c in enumerate(counts):
+            if h != comm.rank and c > 0:
+                self.UnpackRemoteSpikes(h, n_steps, comm.row_ptr(rows, h), c)
+        # the unpacks read the gathered rows on the simulation stream: wait
+        # for them before the rows' memory can be reused
+        comm.sync()
 
     def StartSimulation(self):
         return self._call("StartSimulation")
@@ -828,10 +894,20 @@ class Binding(object):
     def EndSimulation(self):
         return self._call("EndSimulation")
 
-    def ConnectMpiInit(self):
-        "Initialize MPI connections"
+    def ConnectMpiInit(self, comm=None):
+        """Initialize the hosts of a network partitioned over GPUs, one
+        process per GPU (the reference's MPI initialisation): the host index
+        and count come from the job launcher (torchrun, mpirun); the spike
+        exchange uses torch.distributed (NCCL over NVLink), or comm, an
+        object with the methods of HostComm"""
         argv = (ctypes.c_char_p * 1)(b"python")
-        return self._call("ConnectMpiInit", ctypes.c_int(1), ctypes.cast(argv, c_void_p))
+        ret = self._call("ConnectMpiInit", ctypes.c_int(1), ctypes.cast(argv, c_void_p))
+        if comm is None and self.MpiNp() > 1:
+            comm = HostComm()
+        if comm is not None:
+            self._call("NGB200_SetHost", ctypes.c_int(comm.rank), ctypes.c_int(comm.size))
+        self._comm = comm
+        return ret
 
     def MpiId(self):
         return self._call("MpiId")
@@ -977,6 +1053,17 @@ class Binding(object):
 
     def Connect(self, source, target, conn_dict, syn_dict):
         "Connect two node groups"
+        return self._connect("Connect", lambda sa, sn, ta, tn: (sa, sn, ta, tn),
+                             source, target, conn_dict, syn_dict)
+
+    def _connect(self, prefix, args, source, target, conn_dict, syn_dict):
+        """Sets the connection and synapse specifications, then calls
+        <prefix>SeqSeq / SeqGroup / GroupSeq / GroupGroup with the arguments
+        args(source, n_source, target, n_target) forms."""
+        if isinstance(source, RemoteNodeSeq):
+            source = source.node_seq
+        if isinstance(target, RemoteNodeSeq):
+            target = target.node_seq
         if not _is_seq(source):
             raise ValueError("Unknown source type")
         if not _is_seq(target):
@@ -1012,24 +1099,29 @@ class Binding(object):
                 else:
                     raise ValueError("Unknown synapse parameter")
             if isinstance(source, NodeSeq) and isinstance(target, NodeSeq):
-                return self._call("ConnectSeqSeq", source.i0, source.n, target.i0, target.n)
+                return self._call(prefix + "SeqSeq", *args(source.i0, source.n, target.i0, target.n))
             if not isinstance(source, NodeSeq):
                 sa, sp = self._nodes_arr(source)
             if not isinstance(target, NodeSeq):
                 ta, tp = self._nodes_arr(target)
             if isinstance(source, NodeSeq):
-                return self._call("ConnectSeqGroup", source.i0, source.n, tp, len(target))
+                return self._call(prefix + "SeqGroup", *args(source.i0, source.n, tp, len(target)))
             if isinstance(target, NodeSeq):
-                return self._call("ConnectGroupSeq", sp, len(source), target.i0, target.n)
-            return self._call("ConnectGroupGroup", sp, len(source), tp, len(target))
+                return self._call(prefix + "GroupSeq", *args(sp, len(source), target.i0, target.n))
+            return self._call(prefix + "GroupGroup", *args(sp, len(source), tp, len(target)))
         finally:
             self._keep = []
             gc.enable()
 
     def RemoteConnect(self, i_source_host, source, i_target_host, target, conn_dict,
                       syn_dict):
-        "Connect two node groups of different hosts"
-        raise ValueError("MPI is not available in this build (single-GPU core)")
+        """Connect two node groups of different hosts (every host runs the
+        same call): the target host connects image nodes of the remote
+        sources to its targets with the rule, the source host marks the
+        sources as exported"""
+        return self._connect("RemoteConnect",
+                             lambda sa, sn, ta, tn: (i_source_host, sa, sn, i_target_host, ta, tn),
+                             source, target, conn_dict, syn_dict)
 
     def GetConnections(self, source=None, target=None, syn_group=-1):
         "Get connections between two node groups"
@@ -1363,6 +1455,97 @@ class Binding(object):
         ms = (ctypes.c_float * 9)()
         self._call("NGB200_GetRk5Tuning", ctypes.c_int(i_node), ctypes.byref(v), ms)
         return v.value, list(ms)
+
+    # -- networks partitioned over hosts ---------------------------------
+    def SetInstance(self, k):
+        "Select simulation instance k (0..15) for every later call"
+        if self._call("NGB200_SetInstance", ctypes.c_int(k)) != 0:
+            raise ValueError("instance index out of range")
+        return 0
+
+    def GetInstance(self):
+        return self._call("NGB200_GetInstance")
+
+    def SetHost(self, i_host, n_hosts):
+        "Host index and host count of this instance (partitioned networks)"
+        return self._call("NGB200_SetHost", ctypes.c_int(i_host), ctypes.c_int(n_hosts))
+
+    def SimulateSteps(self, n_steps):
+        "Run n_steps steps of a started simulation"
+        return self._call("NGB200_SimulateSteps", ctypes.c_longlong(n_steps))
+
+    def RemoteExchangeSteps(self):
+        "Shortest delay (steps) of a connection from an image node (0: none)"
+        return self._call("NGB200_RemoteExchangeSteps")
+
+    def PackRemoteSpikes(self, n_steps, buf_ptr, cap):
+        """Spikes of this host's exported nodes in the last n_steps steps into
+        the device buffer at buf_ptr (4 + 3 cap int32 words); returns the
+        count, which may exceed cap (then pack again into a larger buffer)"""
+        return self._call("NGB200_PackRemoteSpikes", ctypes.c_int(n_steps),
+                          ctypes.c_void_p(buf_ptr), ctypes.c_longlong(cap))
+
+    def UnpackRemoteSpikes(self, src_host, n_steps, buf_ptr, count):
+        "Push host src_host's packed spikes (device buffer) into the images here"
+        return self._call("NGB200_UnpackRemoteSpikes", ctypes.c_int(src_host),
+                          ctypes.c_int(n_steps), ctypes.c_void_p(buf_ptr),
+                          ctypes.c_longlong(count))
+
+
+class HostComm(object):
+    """Collectives of the hosts of a partitioned network over
+    torch.distributed: NCCL (device tensors over NVLink) when the process
+    group uses it, gloo otherwise. The default process group is created
+    from the launcher's environment (RANK, WORLD_SIZE, MASTER_ADDR,
+    MASTER_PORT) if none exists."""
+
+    def __init__(self):
+        import torch
+        import torch.distributed as dist
+        self._torch, self._dist = torch, dist
+        if not dist.is_initialized():
+            dist.init_process_group(backend="nccl" if torch.cuda.is_available() else "gloo")
+        self.rank = dist.get_rank()
+        self.size = dist.get_world_size()
+        if dist.get_backend() == "nccl":
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        else:
+            self.device = torch.device("cpu")
+
+    def _t(self, vals):
+        return self._torch.tensor(vals, dtype=self._torch.int64, device=self.device)
+
+    def broadcast_int(self, v, src):
+        t = self._t([int(v)])
+        self._dist.broadcast(t, src)
+        return int(t.item())
+
+    def min_int(self, v):
+        t = self._t([int(v)])
+        self._dist.all_reduce(t, op=self._dist.ReduceOp.MIN)
+        return int(t.item())
+
+    def allgather_int(self, v):
+        parts = [self._t([0]) for _ in range(self.size)]
+        self._dist.all_gather(parts, self._t([int(v)]))
+        return [int(p.item()) for p in parts]
+
+    def empty_u32(self, n):
+        return self._torch.zeros(n, dtype=self._torch.int32, device=self.device)
+
+    def allgather_rows(self, buf, n):
+        parts = [self.empty_u32(n) for _ in range(self.size)]
+        self._dist.all_gather(parts, buf[:n].contiguous())
+        if self.device.type == "cuda":
+            self._torch.cuda.current_stream().synchronize()
+        return parts
+
+    def row_ptr(self, rows, h):
+        return rows[h].data_ptr()
+
+    def sync(self):
+        if self.device.type == "cuda":
+            self._torch.cuda.synchronize()
 
 
 _default = None

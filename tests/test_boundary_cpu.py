@@ -77,8 +77,12 @@ def test_kernel_params_and_error_convention_without_gpu():
         with pytest.raises(ValueError):
             api.Create("aeif_cond_beta", 10, 2)
         assert b.GetErrorCode() == 2
+    # hosts of a partitioned network: without a launcher, host 0 of 1; an
+    # invalid host index is an error with the reference's code
+    assert api.MpiId() == 0 and api.MpiNp() == 1 and api.ProcMaster() == 1
     with pytest.raises(ValueError):
-        api.MpiId()
+        b.SetHost(2, 2)
+    assert b.GetErrorCode() == 2
 
 
 def test_graft_build_entry_exists():

@@ -57,8 +57,10 @@ def test_rk5_substep_limit_is_reported(ngpu):
 
 
 def test_tile_prefetch_timeout_is_reported(ngpu, monkeypatch):
-    # the persistent variant with shared-memory prefetch (uniform parameters)
+    # the persistent variant with shared-memory prefetch (uniform parameters),
+    # a kernel of one step per launch
     monkeypatch.setenv("NGB200_RK5_VARIANT", "7")
+    monkeypatch.setenv("NGB200_WINDOW", "0")
     nrn = ngpu.Create("aeif_cond_beta", 20000, 2)
     ngpu.Simulate(0.5)
     assert ngpu.GetRk5Tuning(nrn.i0)[0] == 7
@@ -82,6 +84,9 @@ def _proposer_net(ngpu):
     ngpu.SetStatus(pg, "rate", 20000.0)
     nrn = ngpu.Create("aeif_cond_beta", 4096, 2)
     ngpu.SetNeuronGroupParam(nrn, "rk5_eps", 1e-3)
+    # a strong constant current: the neurons spike from the first
+    # milliseconds, so steps of several sub-steps (the proposer's) occur
+    ngpu.SetStatus(nrn, {"I_e": 1000.0})
     ngpu.Connect(pg, nrn, {"rule": "all_to_all"}, {"weight": 0.6, "delay": 0.1, "receptor": 0})
     ngpu.SetStepProposerParams(P)
     ngpu.SetStepProposer(nrn, True)
@@ -93,11 +98,14 @@ def test_proposer_wait_timeout_is_reported(ngpu, mask):
     """mask 1: the first tensor-core wait of a proposal round gives up;
     mask 2: the second one (layer 2 still in flight when the round fails,
     so the teardown must wait for that completion before it frees the
-    tensor memory). The CTA falls back to the plain controller."""
+    tensor memory). The CTA falls back to the plain controller. The
+    proposer runs for neurons that need more than one sub-step in a step
+    (the straggler queue's records): 20 ms lets the driven neurons reach
+    their first spikes."""
     nrn = _proposer_net(ngpu)
     ngpu.SetWaitTest(mask)
     with pytest.raises(ValueError, match="step proposer timed out"):
-        ngpu.Simulate(2.0)
+        ngpu.Simulate(20.0)
     ngpu.SetWaitTest(0)
     ngpu.Simulate(2.0)
     v = np.asarray(ngpu.GetNeuronVar(nrn.i0, nrn.n, "V_m"), dtype=np.float64)

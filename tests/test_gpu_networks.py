@@ -224,18 +224,28 @@ def test_stdp_network_full_scale(ngpu):
     assert ngpu.TotalSpikes() > 0
 
 
-# delivery modes: in the update's grid (default), on a forked stream, serial
-DELIVERY_ENV = {"fused": {}, "fork": {"NGB200_FUSE_DELIVERY": "0"},
-                "serial": {"NGB200_FUSE_DELIVERY": "0", "NGB200_FORK_DELIVERY": "0"}}
+# step modes: several steps per launch (windows, the default where the
+# delays allow), and one step per launch with the delivery in the update's
+# grid, on a forked stream, or serial
+DELIVERY_ENV = {"window": {}, "fused": {"NGB200_WINDOW": "0"},
+                "fork": {"NGB200_WINDOW": "0", "NGB200_FUSE_DELIVERY": "0"},
+                "serial": {"NGB200_WINDOW": "0", "NGB200_FUSE_DELIVERY": "0",
+                           "NGB200_FORK_DELIVERY": "0"}}
 
 
 def _chunk_run(ngpu, chunk, mode):
+    """mode: one step mode, or one per Simulate call (the mode switches
+    between the calls)."""
     import os
-    keys = ("NGB200_FUSE_DELIVERY", "NGB200_FORK_DELIVERY")
+    keys = ("NGB200_FUSE_DELIVERY", "NGB200_FORK_DELIVERY", "NGB200_WINDOW")
+    modes = [mode] * 3 if isinstance(mode, str) else list(mode)
     old = {k: os.environ.get(k) for k in keys}
-    for k in keys:
-        os.environ.pop(k, None)
-    os.environ.update(DELIVERY_ENV[mode])
+
+    def set_mode(m):
+        for k in keys:
+            os.environ.pop(k, None)
+        os.environ.update(DELIVERY_ENV[m])
+    set_mode(modes[0])
     try:
         b = ngpu.default_binding()
         b.Reset()
@@ -255,7 +265,8 @@ def _chunk_run(ngpu, chunk, mode):
         ngpu.ActivateSpikeCount(nrn)
         b.SetGraphChunk(chunk)
         totals = []
-        for t in (33.3, 50.0, 16.7):
+        for t, m in zip((33.3, 50.0, 16.7), modes):
+            set_mode(m)
             ngpu.Simulate(t)
             totals.append(b.TotalSpikes())
         counts = ngpu.GetNeuronIntVarArray(nrn.i0, nrn.n, "spike_count")
@@ -272,8 +283,11 @@ def _chunk_run(ngpu, chunk, mode):
 def test_step_chunks_and_spike_totals(ngpu):
     """Each step of a captured chunk reads its own copy of the step context
     and the delivery does the step bookkeeping: graphs of 100, 7 and 1 steps,
-    no graph at all, and the delivery in the update's grid, on a forked
-    stream or serial give bit-identical state, and the running spike total
+    no graph at all, windows of several steps per launch (5 steps in chunks
+    of 100 at the 0.7 ms shortest delay, 7 in chunks of 7), and one step per
+    launch with the delivery in the update's grid, on a forked stream or
+    serial, and switches between windows and one step per launch between
+    Simulate calls, give bit-identical state, and the running spike total
     equals the sum of the per-neuron spike counts after every Simulate
     call."""
     ref = _chunk_run(ngpu, 100, "fused")
@@ -281,8 +295,43 @@ def test_step_chunks_and_spike_totals(ngpu):
     assert ref[0][-1] == int(ref[1].sum())
     assert ref[0][0] < ref[0][1] < ref[0][2]
     for chunk, mode in ((7, "fused"), (1, "fused"), (0, "fused"), (100, "fork"), (7, "fork"),
-                        (100, "serial")):
+                        (100, "serial"), (100, "window"), (7, "window"), (1, "window"),
+                        (100, ("window", "fused", "window")),
+                        (7, ("fork", "window", "serial"))):
         totals, counts, v = _chunk_run(ngpu, chunk, mode)
         assert totals == ref[0], (chunk, mode)
         assert np.array_equal(counts, ref[1]), (chunk, mode)
         assert np.array_equal(v.view(np.int32), ref[2].view(np.int32)), (chunk, mode)
+
+
+def test_window_spike_totals_with_generator_connections_only(ngpu):
+    """Windows of up to 16 steps where no connection goes through the spike
+    ring (Poisson generators only: their 0.1 ms delay does not bound the
+    window): every step of a window keeps its own ring slot, so the running
+    spike total equals the per-neuron counts and the one-step run's."""
+    import os
+    out = []
+    for window in ("16", "0"):
+        os.environ["NGB200_WINDOW"] = window
+        try:
+            b = ngpu.default_binding()
+            b.Reset()
+            b.SetVerbosityLevel(0)
+            ngpu.SetKernelStatus("rnd_seed", 5)
+            pg = ngpu.Create("poisson_generator")
+            ngpu.SetStatus(pg, "rate", 20000.0)
+            nrn = ngpu.Create("aeif_cond_beta", 4096, 2)
+            ngpu.SetStatus(nrn, {"I_e": 1000.0})
+            ngpu.Connect(pg, nrn, {"rule": "all_to_all"}, {"weight": 0.6, "delay": 0.1,
+                                                           "receptor": 0})
+            ngpu.ActivateSpikeCount(nrn)
+            ngpu.Simulate(20.0)
+            counts = ngpu.GetNeuronIntVarArray(nrn.i0, nrn.n, "spike_count")
+            out.append((b.TotalSpikes(), counts, b.KernelsPerStep()))
+        finally:
+            os.environ.pop("NGB200_WINDOW", None)
+    (tw, cw, kw), (ts, cs, ks) = out
+    assert kw < 0.5 < ks                        # the first run used windows
+    assert cw.sum() > 10000
+    assert np.array_equal(cw, cs)
+    assert tw == int(cw.sum()) == ts

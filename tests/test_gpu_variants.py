@@ -6,8 +6,9 @@ persistent kernel with shared-memory prefetch at 3-6 blocks per SM); with
 the straggler queue on or off, and the delivery in the update's grid or on
 its own stream. The arithmetic is written with explicit rounding (paired
 FP32x2 intrinsics, ex2/lg2/rcp of the special-function unit), so every
-choice must give the same state bit for bit: two runs on two machines
-agree whatever the timings made the tuner choose.
+choice, and the kernels that integrate several steps per launch, must give
+the same state bit for bit: two runs on two machines agree whatever the
+timings made the tuner choose.
 """
 import os
 
@@ -20,7 +21,7 @@ N_VARIANTS = 9
 
 
 def _run(ngpu, env):
-    keys = ("NGB200_RK5_VARIANT", "NGB200_RK5_QUEUE", "NGB200_FUSE_DELIVERY")
+    keys = ("NGB200_RK5_VARIANT", "NGB200_RK5_QUEUE", "NGB200_FUSE_DELIVERY", "NGB200_WINDOW")
     old = {k: os.environ.get(k) for k in keys}
     for k in keys:
         os.environ.pop(k, None)
@@ -58,12 +59,15 @@ def _run(ngpu, env):
 
 
 def test_rk5_variants_bit_identical(ngpu):
-    ref_v, ref_state, ref_counts = _run(ngpu, {"NGB200_RK5_VARIANT": "0"})
+    ref_v, ref_state, ref_counts = _run(ngpu, {"NGB200_RK5_VARIANT": "0", "NGB200_WINDOW": "0"})
     assert ref_v == 0
     assert ref_counts.sum() > 1000          # the network fires: stragglers exist
-    runs = [{"NGB200_RK5_VARIANT": str(v)} for v in range(1, N_VARIANTS)]
-    runs += [{"NGB200_RK5_VARIANT": "2", "NGB200_RK5_QUEUE": "0"},
-             {"NGB200_RK5_VARIANT": "2", "NGB200_FUSE_DELIVERY": "0"}]
+    runs = [{"NGB200_RK5_VARIANT": str(v), "NGB200_WINDOW": "0"} for v in range(1, N_VARIANTS)]
+    runs += [{"NGB200_RK5_VARIANT": "2", "NGB200_RK5_QUEUE": "0", "NGB200_WINDOW": "0"},
+             {"NGB200_RK5_VARIANT": "2", "NGB200_FUSE_DELIVERY": "0", "NGB200_WINDOW": "0"}]
+    # several steps per launch (windows of up to 11 steps at 1 ms delays),
+    # with the window kernel's register caps
+    runs += [{"NGB200_RK5_VARIANT": v} for v in ("0", "1", "2", "3", "6")]
     for env in runs:
         v, state, counts = _run(ngpu, env)
         assert v == int(env["NGB200_RK5_VARIANT"]), env
