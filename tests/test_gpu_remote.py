@@ -135,3 +135,99 @@ def test_partitioned_network_matches_single_host(ngpu):
             b.SetInstance(inst)
             b.Reset()
         b.SetInstance(0)
+
+
+def _brunel_host(ngpu, b, host):
+    """One host of the reference's two-host Brunel test
+    (python/test/test_brunel_mpi.py): 400 excitatory and 100 inhibitory
+    aeif_cond_beta per host, local and remote connections with fixed
+    in-degrees, normal-clipped delays, a Poisson drive of 20 kHz at 0.37 nS."""
+    b.Reset()
+    b.SetVerbosityLevel(0)
+    b.SetHost(host, 2)
+    ngpu.SetKernelStatus("rnd_seed", 1234)
+    NE, NI, CE, CI = 400, 100, 800, 200
+    pg = ngpu.Create("poisson_generator")
+    ngpu.SetStatus(pg, "rate", 20000.0)
+    neuron = ngpu.Create("aeif_cond_beta", NE + NI, 2)
+    exc, inh = neuron[0:NE], neuron[NE:NE + NI]
+    ngpu.SetStatus(neuron, {"E_rev": [0.0, -85.0], "tau_decay": [1.0, 1.0],
+                            "tau_rise": [1.0, 1.0]})
+    delay = {"distribution": "normal_clipped", "mu": 0.5, "low": 0.1, "high": 0.5 + 3 * 0.25,
+             "sigma": 0.25}
+    exc_syn = {"weight": 0.05, "delay": delay, "receptor": 0}
+    inh_syn = {"weight": 0.35, "delay": delay, "receptor": 1}
+    ngpu.Connect(exc, neuron, {"rule": "fixed_indegree", "indegree": CE // 2}, exc_syn)
+    ngpu.Connect(inh, exc, {"rule": "fixed_indegree", "indegree": CI // 2}, inh_syn)
+    ngpu.Connect(inh, inh, {"rule": "fixed_indegree", "indegree": CI // 2}, inh_syn)
+    ngpu.Connect(pg, neuron, {"rule": "all_to_all"},
+                 {"weight": 0.37, "delay": 0.2, "receptor": 0})
+    for src_host, tgt_host in ((0, 1), (1, 0)):
+        ngpu.RemoteConnect(src_host, exc, tgt_host, neuron,
+                           {"rule": "fixed_indegree", "indegree": CE // 2}, exc_syn)
+    for src_host, tgt_host in ((0, 1), (1, 0)):
+        ngpu.RemoteConnect(src_host, inh, tgt_host, neuron,
+                           {"rule": "fixed_indegree", "indegree": CI // 2}, inh_syn)
+    ngpu.ActivateSpikeCount(neuron)
+    return neuron
+
+
+def test_reference_two_host_brunel(ngpu):
+    """The reference's two-host test on two instances: every local neuron
+    connects to all NE + NI local neurons, every neuron receives
+    2 (NE + NI) + 1 connections (the remote ones from image nodes), and the
+    spike count of 100 sampled neurons per host over 1 s lies within the
+    reference's acceptance, 30.78 +- 3 sqrt(30.78)
+    (python/test/test_brunel_mpi.py:11,135-175). The exchange runs every step
+    (the shortest remote delay is 0.1 ms)."""
+    import math
+    import torch
+    b = ngpu.default_binding()
+    NE, NI = 400, 100
+    try:
+        nrn = {}
+        for inst, host in ((4, 0), (5, 1)):
+            b.SetInstance(inst)
+            nrn[host] = _brunel_host(ngpu, b, host)
+        e_steps = []
+        for inst in (4, 5):
+            b.SetInstance(inst)
+            b.SetSimTime(1000.0)
+            b.StartSimulation()
+            e_steps.append(b.RemoteExchangeSteps())
+            for i in range(NE + NI):
+                assert len(ngpu.GetConnections(i + 1)) == NE + NI
+            for i in (1, 137, 250, 412, 500):
+                assert len(ngpu.GetConnections(target=i)) == 2 * (NE + NI) + 1
+        E = min(e_steps)
+        assert E == 1
+        cap = (NE + NI) * E
+        bufs = [torch.zeros(4 + 3 * cap, dtype=torch.int32, device="cuda") for _ in range(2)]
+        for _ in range(10000 // E):
+            counts = []
+            for inst, host in ((4, 0), (5, 1)):
+                b.SetInstance(inst)
+                b.SimulateSteps(E)
+                counts.append(b.PackRemoteSpikes(E, bufs[host].data_ptr(), cap))
+            b.SetInstance(4)
+            b.UnpackRemoteSpikes(1, E, bufs[1].data_ptr(), counts[1])
+            b.SetInstance(5)
+            b.UnpackRemoteSpikes(0, E, bufs[0].data_ptr(), counts[0])
+            torch.cuda.synchronize()
+        rng = np.random.default_rng(7)
+        expected = 30.78
+        lo, hi = expected - 3.0 * math.sqrt(expected), expected + 3.0 * math.sqrt(expected)
+        for inst, host in ((4, 0), (5, 1)):
+            b.SetInstance(inst)
+            b.EndSimulation()
+            counts = ngpu.GetNeuronIntVarArray(nrn[host].i0, nrn[host].n, "spike_count")
+            sample = [0, NE + NI - 1] + list(rng.integers(0, NE + NI, 98))
+            s = counts[sample]
+            print("host", host, "mean rate %.2f Hz" % counts.mean(), "sample min", s.min(),
+                  "max", s.max())
+            assert lo <= s.min() and s.max() <= hi
+    finally:
+        for inst in (5, 4):
+            b.SetInstance(inst)
+            b.Reset()
+        b.SetInstance(0)
