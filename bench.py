@@ -659,6 +659,14 @@ def main():
         ev_launch = ar["events_instr"] / max(d_n, 1)
         d_avg = d_ms / max(d_n, 1)
         d_ach = BYTES_PER_EVENT * ev_launch / (d_avg / 1000.0) / 1e9 if d_avg > 0 else 0.0
+        # the delivery's own bound: its inner loop alone (8 B read and one
+        # 64-bit reduction per event into the network's accumulators),
+        # measured on this GPU
+        try:
+            probe = b.StreamingDeliveryRate(2 * acfg["n"], max(1, int(ev_launch)), 10)
+        except Exception:
+            probe = None
+        ev_rate = ev_launch / (d_avg / 1000.0) if d_avg > 0 else 0.0
         line["active"] = {
             "workload": "the same network with Poisson w %g nS" % acfg["w_pg"],
             "value": world * a_bio / (ar["dev_ms"] / 1000.0), "unit": "bio_s/wall_s",
@@ -673,7 +681,13 @@ def main():
                                  "traffic": TRAFFIC_DELIVER_PER_EVENT * ev_launch,
                                  "avg_launch_ms": d_avg,
                                  "timing": "delivery launch events of the instrumented run "
-                                           "(serial delivery)"},
+                                           "(serial delivery)",
+                                 "l2_atomics": None if not probe else {
+                                     "achieved": ev_rate, "peak": probe, "unit": "events/s",
+                                     "frac": ev_rate / probe,
+                                     "peak_source": "measured in this run: the delivery's inner "
+                                                    "loop alone on the same events and "
+                                                    "accumulators (NGB200_StreamingDeliveryRate)"}},
             "kernel_ms": {k: v[0] for k, v in ar["ktime"].items()},
             "rk5_tuning": ar["tuning"], "clocks": ar["clocks"]}
     if rank != 0:

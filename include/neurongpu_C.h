@@ -245,6 +245,14 @@ long long NGB200_PackRemoteSpikes(int n_steps, void *buf, long long cap);
  * they were emitted; n_steps as in the matching pack. Queued on the
  * simulation stream. */
 int NGB200_UnpackRemoteSpikes(int src_host, int n_steps, const void *buf, long long count);
+/* The rate (synaptic events per second) at which this GPU delivers events
+ * when nothing else limits the delivery: n_events edges (4-byte target slot,
+ * 4-byte weight) added as 64-bit fixed-point values into n_slots randomly
+ * addressed accumulators by the delivery kernel's inner loop, timed over
+ * reps launches. The bench uses it as the bound of the delivery (mostly the
+ * L2's 64-bit reductions). Allocates its own arrays; returns 0 on success. */
+int NGB200_StreamingDeliveryRate(long long n_slots, long long n_events, int reps,
+                                 double *events_per_s);
 /* Selects simulation instance k (0 <= k < 16; created on first use): every
  * later call of this interface acts on it. Instance 0 is the default. */
 int NGB200_SetInstance(int k);

@@ -1495,10 +1495,11 @@ void NeuronGPU::BuildDevice() {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
   }
+  n_sm_ = n_sm;
   deliver_blocks_ = n_sm * DeliverBlocksPerSM();
   // the delivery after a window runs alone: every resident block
-  window_blocks_ = n_sm * DeliverOccupancy();
-  n_evt_blocks_ = std::max(deliver_blocks_, window_blocks_);
+  solo_deliver_blocks_ = n_sm * DeliverOccupancy();
+  n_evt_blocks_ = std::max(deliver_blocks_, solo_deliver_blocks_);
   NGPU_CUDA(cudaMalloc(&d_done_, sizeof(unsigned)));
   NGPU_CUDA(cudaMemset(d_done_, 0, sizeof(unsigned)));
   NGPU_CUDA(cudaMalloc(&d_blk_events_, sizeof(unsigned long long) * n_evt_blocks_));
@@ -1858,11 +1859,14 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
   }
   if (fuse_g != nullptr) return;
   if (plastic_ && rev_R_ > 1) LaunchRevArrive(d, ctx, stream_);
-  LaunchDeliver(d, syn_table_, ctx, deliver_blocks_, stream_);
+  // the delivery runs alone here (plastic networks, no second stream, the
+  // instrumented run): every resident block (beside the updates it takes
+  // at most 3 per SM)
+  LaunchDeliver(d, syn_table_, ctx, solo_deliver_blocks_, stream_);
   if (ktime_) KEvent(step_in_chunk, 2);
   if (plastic_) {
     d.advance_flags = 1;        // the post rule's last block empties the dendritic slot
-    LaunchStdpPost(d, syn_table_, ctx, 148 * 2, stream_);
+    LaunchStdpPost(d, syn_table_, ctx, 2 * n_sm_, stream_);
   }
   if (ktime_) KEvent(step_in_chunk, 3);
   if (!has_delivery) LaunchAdvance(d_ring_cnt_, ring_R_, ring_C_, 1, ctx, stream_);
@@ -1924,7 +1928,7 @@ void NeuronGPU::EnqueueWindow(int k0, int w) {
   }
   if (ktime_) KEvent(k0, 1);
   const DeliverArgs d = MakeDeliverArgs();
-  LaunchDeliverWindow(d, ctxs, 0, w, 0, min_ring_delay_, window_blocks_, stream_);
+  LaunchDeliverWindow(d, ctxs, 0, w, 0, min_ring_delay_, solo_deliver_blocks_, stream_);
   if (ktime_) {
     KEvent(k0, 2);
     KEvent(k0, 3);
@@ -1944,7 +1948,7 @@ void NeuronGPU::EnqueueWindow(int k0, int w) {
 void NeuronGPU::EnqueueWindowCatchUp() {
   const int maxD = ring_R_ - 2;
   const DeliverArgs d = MakeDeliverArgs();
-  LaunchDeliverWindow(d, d_ctx_, -(long long)maxD, maxD, 0, min_ring_delay_, window_blocks_,
+  LaunchDeliverWindow(d, d_ctx_, -(long long)maxD, maxD, 0, min_ring_delay_, solo_deliver_blocks_,
                       stream_);
   LaunchWindowBook(d_ring_cnt_, ring_R_, ring_C_, d_ctx_, -(long long)(ring_R_ - 1), ring_R_,
                    -1, 0, stream_);

@@ -607,7 +607,8 @@ class NeuronGPU {
   void BuildRemoteTables();
   int window_w_ = 0;            // W of the captured graphs (0: one step per launch)
   bool windowed_ = false;       // the last chunk ran in windows
-  int window_blocks_ = 0;       // grid of the window delivery (it runs alone)
+  int solo_deliver_blocks_ = 0; // grid of a delivery that runs alone (windows, serial steps)
+  int n_sm_ = 148;              // multiprocessors of the device (queried at calibration)
   int n_evt_blocks_ = 0;        // delivery event counters (max of both grids)
 
   // helpers

@@ -11,6 +11,7 @@
 
 #include "ngpu_device.h"
 #include "ngpu_kernels.h"
+#include "ngpu_deliver.cuh"
 
 namespace ngpu {
 
@@ -141,5 +142,87 @@ extern "C" int NGB200_DeliverSpikes(const unsigned long long *grp_off, const uns
   cudaFree(delays);
   cudaFree(ctx);
   cudaFree(err);
+  return rc;
+}
+
+namespace ngpu {
+
+// event e's target slot and weight of the streaming-delivery probe: a
+// multiplicative hash of e spreads the targets over the whole slot array
+__global__ void k_probe_edges(unsigned *e_slot, float *e_w, long long n_events, long long n_slots) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n_events;
+       e += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long h = (unsigned long long)e * 0x9E3779B97F4A7C15ull;
+    e_slot[e] = (unsigned)((h >> 17) % (unsigned long long)n_slots);
+    e_w[e] = 0.05f;
+  }
+}
+
+// the delivery's inner loop (deliver_static_edges) over the whole edge
+// array in chunks of 256 edges per warp, without the ring and CSR lookups
+__global__ void __launch_bounds__(256) k_probe_deliver(DeliverArgs d, long long n_events) {
+  const int lane = threadIdx.x & 31;
+  const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long n_warps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long c = warp * 256; c < n_events; c += n_warps * 256) {
+    const unsigned long long end = (unsigned long long)(c + 256 < n_events ? c + 256 : n_events);
+    deliver_static_edges(d, d.acc, (unsigned long long)c, end, 1.0f, lane);
+  }
+}
+
+}  // namespace ngpu
+
+// The rate (events/s) at which this GPU delivers synaptic events when
+// nothing else limits the delivery: n_events edges (4-byte target slot and
+// 4-byte weight read once, evict-first) added as 64-bit fixed-point values
+// into n_slots accumulators by the delivery's inner loop with the grid of a
+// standalone delivery, timed over reps launches after one warm-up launch.
+// The bound of the simulator's delivery kernel when its events per step are
+// this many into this many accumulators (the ring and CSR lookups of the
+// real kernel add a chain of dependent loads per (spike, delay) item).
+// Allocates and frees its arrays; returns 0, 2 on an allocation failure.
+extern "C" int NGB200_StreamingDeliveryRate(long long n_slots, long long n_events, int reps,
+                                            double *events_per_s) {
+  using namespace ngpu;
+  if (n_slots <= 0 || n_events <= 0 || reps <= 0 || events_per_s == nullptr) return 1;
+  long long *acc = nullptr;
+  unsigned *e_slot = nullptr;
+  float *e_w = nullptr;
+  cudaStream_t s = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = 0;
+  if (cudaMalloc(&acc, sizeof(long long) * n_slots) != cudaSuccess ||
+      cudaMalloc(&e_slot, sizeof(unsigned) * n_events) != cudaSuccess ||
+      cudaMalloc(&e_w, sizeof(float) * n_events) != cudaSuccess ||
+      cudaStreamCreate(&s) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+      cudaEventCreate(&e1) != cudaSuccess) {
+    rc = 2;
+  } else {
+    cudaMemsetAsync(acc, 0, sizeof(long long) * n_slots, s);
+    k_probe_edges<<<1184, 256, 0, s>>>(e_slot, e_w, n_events, n_slots);
+    DeliverArgs d;
+    memset(&d, 0, sizeof(d));
+    d.e_slot = e_slot;
+    d.e_w = e_w;
+    d.acc = acc;
+    const int blocks = StandaloneDeliverBlocks();
+    k_probe_deliver<<<blocks, 256, 0, s>>>(d, n_events);
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < reps; r++) k_probe_deliver<<<blocks, 256, 0, s>>>(d, n_events);
+    cudaEventRecord(e1, s);
+    float ms = 0.0f;
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess ||
+        ms <= 0.0f) {
+      rc = 3;
+    } else {
+      *events_per_s = (double)n_events * reps / (ms * 1e-3);
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (s) cudaStreamDestroy(s);
+  cudaFree(acc);
+  cudaFree(e_slot);
+  cudaFree(e_w);
   return rc;
 }

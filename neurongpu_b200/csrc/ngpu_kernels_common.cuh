@@ -666,11 +666,10 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
                                            const PushArgs &pa, StepCtx *ctx, int i,
                                            const float *p_uni, const float *q_uni,
                                            unsigned &evals, bool dry_run,
-                                           ProposerSmem *ps, const Rk5Queue *qu = nullptr,
+                                           const Rk5Queue *qu = nullptr,
                                            int seg = 0, const float *pre_col = nullptr,
                                            const long long *pre_acc = nullptr, int tile = -1) {
   using Tr = ModelTraits<M>;
-  const bool active = true;
   const bool dry = g.dry || dry_run;
   // the launchers pick the template port count NP = np for 2..4 ports (1
   // serves 0 and 1), so there the count is a compile-time constant
@@ -684,46 +683,42 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
   // is not live across the Poisson draws (fewer registers and spills)
   constexpr int NPI = (M::NPV == 0) ? 1 : NP;
   long long s[NPI];
-  if (active)
-    input_sum<NPI, false>(in, i, n_pad, np, it, t0, g.dt, pending, T0, ctx->acc_in_slot, s, dry,
+  input_sum<NPI, false>(in, i, n_pad, np, it, t0, g.dt, pending, T0, ctx->acc_in_slot, s, dry,
                           pre_acc);
   float y[M::NVAR];
 #pragma unroll
   for (int j = 0; j < M::NVAR; j++) {
-    y[j] = (active && ((NP >= 2 && NP <= 4) || j < g.nvar))
+    y[j] = ((NP >= 2 && NP <= 4) || j < g.nvar)
                ? (pre_col ? pre_col[j] : g.var[(long long)j * n_pad + i])
                                   : 0.0f;
   }
   float p_loc[UNI ? 1 : M::NPARAM];
   float q_loc[UNI ? 1 : M::NPARAM];
-  rk5_load_params<M, UNI>(g, i, active, p_loc, q_loc);
+  rk5_load_params<M, UNI>(g, i, true, p_loc, q_loc);
   const float *p = UNI ? p_uni : p_loc;
   const float *q = UNI ? q_uni : q_loc;
-  float refr = active ? (pre_col ? pre_col[M::NVAR] : g.param[(long long)Tr::refr * n_pad + i])
-                      : 0.0f;
+  float refr = pre_col ? pre_col[M::NVAR] : g.param[(long long)Tr::refr * n_pad + i];
   // fold the previous step's input
-  if (active) {
 #pragma unroll
-    for (int qq = 0; qq < NPI; qq++) {
-      if (qq < np && s[qq] != 0) {
-        const int vi = Tr::in_base + qq * Tr::in_step;
-        const float w = (Tr::w_base >= 0) ? p[Tr::w_base + qq * Tr::w_step] : 1.0f;
-        y[vi] = fold_value(y[vi], s[qq], w);
-      }
+  for (int qq = 0; qq < NPI; qq++) {
+    if (qq < np && s[qq] != 0) {
+      const int vi = Tr::in_base + qq * Tr::in_step;
+      const float w = (Tr::w_base >= 0) ? p[Tr::w_base + qq * Tr::w_step] : 1.0f;
+      y[vi] = fold_value(y[vi], s[qq], w);
     }
   }
   const float refr0 = refr;
   const double x1 = t0 + (double)g.dt * (double)(it + 1);
   double x = t0 + (double)g.dt * (double)it +
-             (active ? (double)(pre_col ? pre_col[M::NVAR + 2] : g.dx[i]) : 0.0);
-  float h = active ? (pre_col ? pre_col[M::NVAR + 1] : g.h[i]) : 0.0f;
+             (double)(pre_col ? pre_col[M::NVAR + 2] : g.dx[i]);
+  float h = pre_col ? pre_col[M::NVAR + 1] : g.h[i];
   const float h_min = g.h_min;
   const float inv_eps = g.inv_eps;
   const long long T = T0 + it + 1;
   // group-wide dendritic delay: the steps formed on the host
   const int den = (UNI && g.den_delay_col == Tr::den) ? g.den_steps
                                                        : (int)roundf(p[Tr::den] / g.dt);
-  bool end_step = !active;
+  bool end_step = false;
   int guard = 0;
   float h_acc, err_acc;
   if constexpr (MODE == STEP_LOG) {
@@ -758,7 +753,6 @@ __device__ __forceinline__ void rk5_neuron(const GroupArgs &g, const InputArgs &
       }
     }
   }
-  if (!active) return;
   if (!dry) {
     rk5_store<M, NP>(g, i, y, h, x, x1, refr, refr != refr0);
   } else if (y[0] == 1.2345e30f) {
@@ -779,7 +773,7 @@ k_rk5_update(const __grid_constant__ GroupArgs g, const __grid_constant__ InputA
   unsigned evals = 0;
   const bool queued = (MODE == STEP_PLAIN) && g.q.cap > 0;
   if (i < g.n) rk5_neuron<M, NP, UNI, MODE>(g, in, pa, ctx, i, g.puni, g.pinv, evals, false,
-                                            nullptr, queued ? &g.q : nullptr, 0);
+                                            queued ? &g.q : nullptr, 0);
   if (g.blk_evals != nullptr) block_add_u64(evals, g.blk_evals);
 }
 
@@ -970,7 +964,7 @@ k_rk5_update_tiles(const __grid_constant__ GroupArgs g, const __grid_constant__ 
     }
     const int i = t * NGPU_BLOCK + threadIdx.x;
     if (i < g.n) rk5_neuron<M, NP, true, STEP_PLAIN>(g, in, pa, ctx, i, g.puni, g.pinv, evals,
-                                                     false, nullptr, qu, 0, pc, pq);
+                                                     false, qu, 0, pc, pq);
   }
   if (g.blk_evals != nullptr) block_add_u64(evals, g.blk_evals);
 }
@@ -1021,7 +1015,7 @@ k_rk5_update_seg(const SegArgs *__restrict__ segs, const int *__restrict__ blk_s
   unsigned evals = 0;
   const bool queued = (MODE == STEP_PLAIN) && qu.cap > 0;
   if (i < S.g.n)
-    rk5_neuron<M, NP, UNI, MODE>(S.g, S.in, S.pa, ctx, i, s_p, s_q, evals, dry != 0, nullptr,
+    rk5_neuron<M, NP, UNI, MODE>(S.g, S.in, S.pa, ctx, i, s_p, s_q, evals, dry != 0,
                                  queued ? &qu : nullptr, seg, nullptr, nullptr, blockIdx.x);
   if (blk_evals != nullptr) block_add_u64(evals, blk_evals);
 }

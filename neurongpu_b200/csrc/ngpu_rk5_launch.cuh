@@ -39,7 +39,7 @@ k_rk5_update_deliver(const __grid_constant__ GroupArgs g, const __grid_constant_
   unsigned evals = 0;
   const bool queued = g.q.cap > 0;
   if (i < g.n) rk5_neuron<M, NP, true, STEP_PLAIN>(g, in, pa, ctx, i, g.puni, g.pinv, evals, false,
-                                                   nullptr, queued ? &g.q : nullptr, 0);
+                                                   queued ? &g.q : nullptr, 0);
   if (g.blk_evals != nullptr) block_add_u64(evals, g.blk_evals, blk);
 }
 

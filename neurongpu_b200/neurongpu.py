@@ -269,6 +269,8 @@ _EXT_SIG = {
                                     ctypes.POINTER(ctypes.c_longlong))),
     "NGB200_GetRk5Tuning": (_I, (_I, ctypes.POINTER(ctypes.c_int),
                                  ctypes.POINTER(ctypes.c_float))),
+    "NGB200_StreamingDeliveryRate": (_I, (ctypes.c_longlong, ctypes.c_longlong, _I,
+                                          ctypes.POINTER(ctypes.c_double))),
     "NGB200_SetInstance": (_I, (_I,)),
     "NGB200_GetInstance": (_I, ()),
     "NGB200_SetHost": (_I, (_I, _I)),
@@ -1455,6 +1457,17 @@ class Binding(object):
         ms = (ctypes.c_float * 9)()
         self._call("NGB200_GetRk5Tuning", ctypes.c_int(i_node), ctypes.byref(v), ms)
         return v.value, list(ms)
+
+    def StreamingDeliveryRate(self, n_slots, n_events, reps=10):
+        """Events/s of the delivery's inner loop alone (n_events edges into
+        n_slots accumulators): the bound of the delivery kernel"""
+        r = ctypes.c_double(0.0)
+        rc = self._c["NGB200_StreamingDeliveryRate"](ctypes.c_longlong(n_slots),
+                                                     ctypes.c_longlong(n_events),
+                                                     ctypes.c_int(reps), ctypes.byref(r))
+        if rc != 0:
+            raise ValueError("streaming delivery probe failed (%d)" % rc)
+        return r.value
 
     # -- networks partitioned over hosts ---------------------------------
     def SetInstance(self, k):
