@@ -107,7 +107,9 @@ void NeuronGPU::FreeDevice() {
   kev_.clear();
   if (ev_start_) cudaEventDestroy(ev_start_);
   if (ev_stop_) cudaEventDestroy(ev_stop_);
-  ev_start_ = ev_stop_ = nullptr;
+  if (ev_c0_) cudaEventDestroy(ev_c0_);
+  if (ev_c1_) cudaEventDestroy(ev_c1_);
+  ev_start_ = ev_stop_ = ev_c0_ = ev_c1_ = nullptr;
   d_ctx_ = nullptr;
   if (ev_fork_) cudaEventDestroy(ev_fork_);
   if (ev_join_) cudaEventDestroy(ev_join_);
@@ -1766,7 +1768,8 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
   // (k_rk5_update_deliver): no second stream, no join, and consecutive
   // steps' updates keep their programmatic launch overlap.
   NodeGroup *fuse_g = (has_delivery && !plastic_ && !ktime_) ? FusedDeliveryGroup() : nullptr;
-  const bool fork = has_delivery && !plastic_ && !ktime_ && dstream_ != nullptr && fuse_g == nullptr;
+  const bool fork = has_delivery && !plastic_ && !ktime_ && dstream_ != nullptr &&
+                    fuse_g == nullptr && !serial_delivery_;
   if (fuse_g != nullptr) d.advance_flags = 0;
   if (fork) {
     NGPU_CUDA(cudaEventRecord(ev_fork_, stream_));
@@ -1992,7 +1995,7 @@ void NeuronGPU::LaunchSteps(int n_steps) {
   if (!use_graphs_) {
     enqueue_chunk();
   } else {
-    auto it = graphs_.find(n_steps);
+    auto it = graphs_.find(GraphKey(n_steps));
     if (it == graphs_.end()) {
       cudaGraph_t graph;
       NGPU_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
@@ -2020,7 +2023,7 @@ void NeuronGPU::LaunchSteps(int n_steps) {
       cudaGraphExec_t exec;
       NGPU_CUDA(cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority));
       cudaGraphDestroy(graph);
-      it = graphs_.emplace(n_steps, exec).first;
+      it = graphs_.emplace(GraphKey(n_steps), exec).first;
     }
     NGPU_CUDA(cudaGraphLaunch(it->second, stream_));
   }
@@ -2223,13 +2226,25 @@ void NeuronGPU::TuneRk5(NodeGroup *g) {
 // it. Both give the same results.
 void NeuronGPU::RecheckDeliveryMode() {
   const long long ds = steps_total_ - deliver_checked_;
-  if (ds < kQueueRecheckSteps || d_blk_events_ == nullptr) return;
+  // during the first kQueueRecheckSteps steps after every chunk, so that a
+  // busy network leaves the quiet network's modes (windows, the delivery in
+  // the update's grid) early; then every kQueueRecheckSteps steps
+  const long long interval = steps_total_ <= kQueueRecheckSteps
+                                 ? std::min<long long>(graph_chunk_, kQueueRecheckSteps)
+                                 : kQueueRecheckSteps;
+  if (ds < interval || d_blk_events_ == nullptr) return;
   const unsigned long long e = DeliveredEvents();
   const double per_step = (double)(e - events_mark_) / (double)ds;
   const bool busy = delivery_busy_ ? per_step > 0.5 * kFusedDeliveryMaxEvents
                                    : per_step > kFusedDeliveryMaxEvents;
   if (busy != delivery_busy_) {
     delivery_busy_ = busy;
+    // a network that turns busy times its two delivery modes
+    serial_delivery_ = false;
+    delivery_trial_ = busy ? 1 : 0;
+    trial_chunk_ = 0;
+    trial_ms_[0] = trial_ms_[1] = 0.0;
+    trial_steps_[0] = trial_steps_[1] = 0;
     InvalidateGraphs();
   }
   events_mark_ = e;
@@ -2633,7 +2648,7 @@ int NeuronGPU::Simulate() {
       printf("%.3lf\n", neur_t0_ + (double)time_resolution_ * (double)done);
     long long n = std::min<long long>(graph_chunk_, Nt_ - done);
     if (verbosity_level_ >= 2) n = std::min<long long>(n, 100 - done % 100);
-    LaunchSteps((int)n);
+    LaunchStepsTimed((int)n);
     done += n;
     it_ = done;
     input_pending_ = true;
@@ -2653,13 +2668,50 @@ int NeuronGPU::Simulate() {
   return 0;
 }
 
+// LaunchSteps; while a delivery-mode trial runs, chunks alternate between the
+// modes and are timed on the device
+void NeuronGPU::LaunchStepsTimed(int n_steps) {
+  if (delivery_trial_ == 1 && steps_total_ >= kQueueRecheckSteps) delivery_trial_ = 2;
+  if (delivery_trial_ != 2 || ktime_) {
+    LaunchSteps(n_steps);
+    return;
+  }
+  if (!ev_c0_) {
+    NGPU_CUDA(cudaEventCreate(&ev_c0_));
+    NGPU_CUDA(cudaEventCreate(&ev_c1_));
+  }
+  const int mode = (int)(trial_chunk_++ & 1);     // 0 forked, 1 serial
+  serial_delivery_ = mode == 1;
+  // a chunk that captures its graph is not timed (the device waits for the
+  // host meanwhile)
+  const bool timed = graphs_.find(GraphKey(n_steps)) != graphs_.end();
+  NGPU_CUDA(cudaEventRecord(ev_c0_, stream_));
+  LaunchSteps(n_steps);
+  NGPU_CUDA(cudaEventRecord(ev_c1_, stream_));
+  if (timed) {
+    NGPU_CUDA(cudaEventSynchronize(ev_c1_));
+    float ms = 0.0f;
+    NGPU_CUDA(cudaEventElapsedTime(&ms, ev_c0_, ev_c1_));
+    trial_ms_[mode] += ms;
+    trial_steps_[mode] += n_steps;
+  }
+  if (trial_steps_[0] >= kDeliveryTrialSteps && trial_steps_[1] >= kDeliveryTrialSteps) {
+    const double f = trial_ms_[0] / (double)trial_steps_[0];
+    const double sr = trial_ms_[1] / (double)trial_steps_[1];
+    serial_delivery_ = sr < f;
+    delivery_trial_ = 0;
+    if (verbosity_level_ >= 2)
+      printf("delivery: %.2f us per step forked, %.2f serial\n", 1000.0 * f, 1000.0 * sr);
+  }
+}
+
 int NeuronGPU::SimulateSteps(long long n) {
   if (n < 0) throw ngpu_exception("the number of steps must be >= 0");
   if (first_simulation_flag_) StartSimulation();
   long long done = 0;
   while (done < n) {
     const long long k = std::min<long long>(graph_chunk_, n - done);
-    LaunchSteps((int)k);
+    LaunchStepsTimed((int)k);
     done += k;
     it_ += k;
     steps_total_ += k;

@@ -370,6 +370,21 @@ class NeuronGPU {
   static constexpr double kFusedDeliveryMaxEvents = 65536.0;
   void RecheckDeliveryMode();
   bool delivery_busy_ = false;
+  // a busy network's delivery runs on its own stream beside the updates or
+  // after them on every resident block, whichever a trial on the live
+  // network timed faster (both give the same results): from step
+  // kQueueRecheckSteps on (past the start's transient), chunks alternate
+  // between the two modes until each has kDeliveryTrialSteps timed steps
+  // (chunks that capture a graph are not timed), so a drift of the
+  // network's activity weighs on both alike
+  static const long long kDeliveryTrialSteps = 300;
+  bool serial_delivery_ = false;
+  int delivery_trial_ = 0;      // 0 none, 1 waiting for the trial's first step, 2 running
+  long long trial_chunk_ = 0;
+  double trial_ms_[2] = {0.0, 0.0};
+  long long trial_steps_[2] = {0, 0};
+  cudaEvent_t ev_c0_ = nullptr, ev_c1_ = nullptr;
+  void LaunchStepsTimed(int n_steps);
   long long deliver_checked_ = 0;
   unsigned long long events_mark_ = 0;
   // RK5 groups of one model and port count are integrated by one launch
@@ -583,7 +598,12 @@ class NeuronGPU {
   // graphs
   bool use_graphs_ = true;
   int graph_chunk_ = 100;
-  std::map<int, cudaGraphExec_t> graphs_;
+  // captured step graphs by (steps, delivery mode): a busy network can
+  // change its delivery mode without capturing again
+  std::map<long long, cudaGraphExec_t> graphs_;
+  long long GraphKey(int n_steps) const {
+    return (long long)n_steps | ((long long)(serial_delivery_ ? 1 : 0) << 32);
+  }
   void InvalidateGraphs();
   void LaunchSteps(int n_steps);
   void EnqueueStep(int step_in_chunk);

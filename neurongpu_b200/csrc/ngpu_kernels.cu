@@ -539,8 +539,11 @@ void LaunchClearPending(StepCtx *ctx, cudaStream_t s) {
   k_clear_pending<<<1, 1, 0, s>>>(ctx);
 }
 
+// register cap of the static delivery kernels: 4 blocks of 256 threads per
+// SM (64 registers, no spill; 6 and 8 blocks spill 80-230 bytes)
+#define NGPU_DELIVER_MINB 4
 template <bool PLASTIC>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, PLASTIC ? 1 : NGPU_DELIVER_MINB)
 k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
   deliver_blocks<PLASTIC>(d, syn, ctx, blockIdx.x, gridDim.x);
 }
@@ -548,7 +551,7 @@ k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
 // Delivery after a window of integrated steps: the spikes of the steps
 // T_b + first_off ... T_b + first_off + n - 1, T_b the step of ctx (the
 // window's first step), delivered at all their delays at once.
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, NGPU_DELIVER_MINB)
 k_deliver_window(DeliverArgs d, const StepCtx *ctx, long long first_off, int n,
                  long long arrive_off, int min_delay) {
   deliver_window_blocks(d, ctx, first_off, n, arrive_off, min_delay, blockIdx.x, gridDim.x);
