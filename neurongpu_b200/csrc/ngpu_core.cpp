@@ -1769,7 +1769,7 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
   // steps' updates keep their programmatic launch overlap.
   NodeGroup *fuse_g = (has_delivery && !plastic_ && !ktime_) ? FusedDeliveryGroup() : nullptr;
   const bool fork = has_delivery && !plastic_ && !ktime_ && dstream_ != nullptr &&
-                    fuse_g == nullptr && !serial_delivery_;
+                    fuse_g == nullptr && !(delivery_busy_ && busy_mode_ == BUSY_SERIAL);
   if (fuse_g != nullptr) d.advance_flags = 0;
   if (fork) {
     NGPU_CUDA(cudaEventRecord(ev_fork_, stream_));
@@ -1881,26 +1881,32 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
 // spike of a window of W steps arrives inside it, and one launch per RK5
 // group can integrate its neurons through all W steps before one delivery
 // of the window's spikes (k_rk5_window, k_deliver_window, k_window_book).
-// Windows need: every node group an RK5 group with its own launch and the
+// Windows need: every node group an RK5 group (batched or not) with the
 // plain controller, or a Poisson generator; no plastic synapse, multimeter
 // record or large-rate Poisson pre-pass; the accumulator ring of the
-// longest delay + 2 slots; and a quiet network (below kFusedDeliveryMaxEvents
-// delivered events per step, checked every kQueueRecheckSteps steps): the
-// delivery after a window adds into the slots of up to W + max delay later
-// steps at once, a working set that leaves L2 when many events arrive,
-// where one step's delivery adds into one slot. W is at most 16 and
-// preferably divides the graph chunk; NGB200_WINDOW caps it (0: one step
-// per launch). 0: no windows.
+// longest delay + 2 slots. A quiet network (below kFusedDeliveryMaxEvents
+// delivered events per step) runs in windows; a busy one only where its
+// mode trial timed them fastest (LaunchStepsTimed): the delivery after a
+// window adds into the slots of up to W + max delay later steps at once, a
+// working set that leaves L2 when many events arrive, where one step's
+// delivery adds into one slot. W is at most 16 and preferably divides the
+// graph chunk; NGB200_WINDOW caps it (0: one step per launch). 0: no
+// windows.
 int NeuronGPU::WindowSteps() {
+  if (delivery_busy_ && busy_mode_ != BUSY_WINDOW) return 0;
+  return WindowEligible();
+}
+
+int NeuronGPU::WindowEligible() {
   const char *env = getenv("NGB200_WINDOW");
   int cap = 16;
   if (env != nullptr) cap = std::max(0, std::min(16, atoi(env)));
   if (cap < 2 || acc_slots_ <= 2 || d_acc_stamp_ == nullptr || plastic_ || n_rec_cols_ > 0 ||
-      delivery_busy_ || n_exported_ > 0 || has_images_)
+      n_exported_ > 0 || has_images_)
     return 0;
   for (NodeGroup *g : groups_) {
     if (g->mi->kind == MK_POISSON_GENERATOR) continue;
-    if (g->mi->kind != MK_RK5 || g->batch >= 0 || g->step_mode != STEP_PLAIN || g->n_port > 4 ||
+    if (g->mi->kind != MK_RK5 || g->step_mode != STEP_PLAIN || g->n_port > 4 ||
         HasLargePoisson(g))
       return 0;
   }
@@ -1925,6 +1931,12 @@ void NeuronGPU::EnqueueWindow(int k0, int w) {
   if (ktime_) KEvent(k0, 0);
   for (NodeGroup *g : groups_) {
     if (g->mi->kind != MK_RK5) continue;
+    if (g->batch >= 0) {
+      // a batch is launched once, at its first group
+      const Rk5BatchHost &bh = batches_[g->batch];
+      if (bh.groups[0] == g) LaunchRk5BatchWindow(MakeRk5Batch(bh), ctxs, w, stream_);
+      continue;
+    }
     if (!LaunchRk5Window(g->mi->rk5_model, g->n_port, MakeGroupArgs(g), MakeInputArgs(g),
                          MakePushArgs(g), ctxs, w, stream_))
       throw ngpu_exception("internal error: no window kernel for this node group");
@@ -1975,10 +1987,7 @@ void NeuronGPU::LaunchSteps(int n_steps) {
   }
   const int rec = n_rec_cols_ > 0 ? 1 : 0;
   const int W = WindowSteps();
-  if (W != window_w_) {
-    InvalidateGraphs();
-    window_w_ = W;
-  }
+  window_w_ = W;
   // the hand-over to windows depends on the mode of the previous chunk, so
   // it runs before the chunk's graph, not in it
   if (W > 0 && !windowed_) EnqueueWindowCatchUp();
@@ -1995,7 +2004,7 @@ void NeuronGPU::LaunchSteps(int n_steps) {
   if (!use_graphs_) {
     enqueue_chunk();
   } else {
-    auto it = graphs_.find(GraphKey(n_steps));
+    auto it = graphs_.find(GraphKey(n_steps, W));
     if (it == graphs_.end()) {
       cudaGraph_t graph;
       NGPU_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
@@ -2023,7 +2032,7 @@ void NeuronGPU::LaunchSteps(int n_steps) {
       cudaGraphExec_t exec;
       NGPU_CUDA(cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority));
       cudaGraphDestroy(graph);
-      it = graphs_.emplace(GraphKey(n_steps), exec).first;
+      it = graphs_.emplace(GraphKey(n_steps, W), exec).first;
     }
     NGPU_CUDA(cudaGraphLaunch(it->second, stream_));
   }
@@ -2240,11 +2249,13 @@ void NeuronGPU::RecheckDeliveryMode() {
   if (busy != delivery_busy_) {
     delivery_busy_ = busy;
     // a network that turns busy times its two delivery modes
-    serial_delivery_ = false;
+    busy_mode_ = BUSY_FORK;
     delivery_trial_ = busy ? 1 : 0;
     trial_chunk_ = 0;
-    trial_ms_[0] = trial_ms_[1] = 0.0;
-    trial_steps_[0] = trial_steps_[1] = 0;
+    for (int m = 0; m < 3; m++) {
+      trial_ms_[m] = 0.0;
+      trial_steps_[m] = 0;
+    }
     InvalidateGraphs();
   }
   events_mark_ = e;
@@ -2668,11 +2679,11 @@ int NeuronGPU::Simulate() {
   return 0;
 }
 
-// LaunchSteps; while a delivery-mode trial runs, chunks alternate between the
-// modes and are timed on the device
+// LaunchSteps; while a busy network's mode trial runs, the candidate modes
+// take turns (two chunks each, the second timed on the device)
 void NeuronGPU::LaunchStepsTimed(int n_steps) {
   if (delivery_trial_ == 1 && steps_total_ >= kQueueRecheckSteps) delivery_trial_ = 2;
-  if (delivery_trial_ != 2 || ktime_) {
+  if (delivery_trial_ != 2 || ktime_ || !delivery_busy_) {
     LaunchSteps(n_steps);
     return;
   }
@@ -2680,11 +2691,11 @@ void NeuronGPU::LaunchStepsTimed(int n_steps) {
     NGPU_CUDA(cudaEventCreate(&ev_c0_));
     NGPU_CUDA(cudaEventCreate(&ev_c1_));
   }
-  const int mode = (int)(trial_chunk_++ & 1);     // 0 forked, 1 serial
-  serial_delivery_ = mode == 1;
-  // a chunk that captures its graph is not timed (the device waits for the
-  // host meanwhile)
-  const bool timed = graphs_.find(GraphKey(n_steps)) != graphs_.end();
+  const int n_modes = WindowEligible() > 0 ? 3 : 2;
+  const int mode = (int)((trial_chunk_ / 2) % n_modes);
+  const bool timed = (trial_chunk_ & 1) != 0;
+  trial_chunk_++;
+  busy_mode_ = mode;
   NGPU_CUDA(cudaEventRecord(ev_c0_, stream_));
   LaunchSteps(n_steps);
   NGPU_CUDA(cudaEventRecord(ev_c1_, stream_));
@@ -2695,13 +2706,22 @@ void NeuronGPU::LaunchStepsTimed(int n_steps) {
     trial_ms_[mode] += ms;
     trial_steps_[mode] += n_steps;
   }
-  if (trial_steps_[0] >= kDeliveryTrialSteps && trial_steps_[1] >= kDeliveryTrialSteps) {
-    const double f = trial_ms_[0] / (double)trial_steps_[0];
-    const double sr = trial_ms_[1] / (double)trial_steps_[1];
-    serial_delivery_ = sr < f;
+  bool done = true;
+  for (int m = 0; m < n_modes; m++) done = done && trial_steps_[m] >= kDeliveryTrialSteps;
+  if (done) {
+    int best = 0;
+    double best_t = 1e300;
+    for (int m = 0; m < n_modes; m++) {
+      const double t = trial_ms_[m] / (double)trial_steps_[m];
+      if (t < best_t) {
+        best_t = t;
+        best = m;
+      }
+      if (verbosity_level_ >= 2)
+        printf("busy mode %d: %.2f us per step\n", m, 1000.0 * t);
+    }
+    busy_mode_ = best;
     delivery_trial_ = 0;
-    if (verbosity_level_ >= 2)
-      printf("delivery: %.2f us per step forked, %.2f serial\n", 1000.0 * f, 1000.0 * sr);
   }
 }
 

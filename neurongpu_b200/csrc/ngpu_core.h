@@ -370,19 +370,24 @@ class NeuronGPU {
   static constexpr double kFusedDeliveryMaxEvents = 65536.0;
   void RecheckDeliveryMode();
   bool delivery_busy_ = false;
-  // a busy network's delivery runs on its own stream beside the updates or
-  // after them on every resident block, whichever a trial on the live
-  // network timed faster (both give the same results): from step
-  // kQueueRecheckSteps on (past the start's transient), chunks alternate
-  // between the two modes until each has kDeliveryTrialSteps timed steps
-  // (chunks that capture a graph are not timed), so a drift of the
-  // network's activity weighs on both alike
+  // A busy network runs in the mode a trial on the live network timed
+  // fastest (every mode gives the same results): one step per launch with
+  // the delivery on its own stream beside the updates (BUSY_FORK) or after
+  // them on every resident block (BUSY_SERIAL), or windows of steps
+  // (BUSY_WINDOW, where the network can run them). From step
+  // kQueueRecheckSteps on (past the start's transient) the candidates take
+  // turns, two chunks each, of which the second is timed (the first
+  // captures the mode's graph and makes the hand-over to windows), until
+  // each has kDeliveryTrialSteps timed steps, so that a drift of the
+  // network's activity weighs on all alike.
+  enum BusyMode { BUSY_FORK = 0, BUSY_SERIAL = 1, BUSY_WINDOW = 2 };
   static const long long kDeliveryTrialSteps = 300;
-  bool serial_delivery_ = false;
+  int busy_mode_ = BUSY_FORK;
   int delivery_trial_ = 0;      // 0 none, 1 waiting for the trial's first step, 2 running
   long long trial_chunk_ = 0;
-  double trial_ms_[2] = {0.0, 0.0};
-  long long trial_steps_[2] = {0, 0};
+  double trial_ms_[3] = {0.0, 0.0, 0.0};
+  long long trial_steps_[3] = {0, 0, 0};
+  int WindowEligible();         // W of the network's structure, ignoring its activity
   cudaEvent_t ev_c0_ = nullptr, ev_c1_ = nullptr;
   void LaunchStepsTimed(int n_steps);
   long long deliver_checked_ = 0;
@@ -598,11 +603,12 @@ class NeuronGPU {
   // graphs
   bool use_graphs_ = true;
   int graph_chunk_ = 100;
-  // captured step graphs by (steps, delivery mode): a busy network can
-  // change its delivery mode without capturing again
+  // captured step graphs by (steps, busy mode, steps per window): a network
+  // can change its mode without capturing again
   std::map<long long, cudaGraphExec_t> graphs_;
-  long long GraphKey(int n_steps) const {
-    return (long long)n_steps | ((long long)(serial_delivery_ ? 1 : 0) << 32);
+  long long GraphKey(int n_steps, int W) const {
+    return (long long)n_steps | ((long long)(delivery_busy_ ? busy_mode_ + 1 : 0) << 32) |
+           ((long long)W << 40);
   }
   void InvalidateGraphs();
   void LaunchSteps(int n_steps);
@@ -625,7 +631,7 @@ class NeuronGPU {
   static const int kExchangeRingSteps = 32;   // spike-ring steps of an exporting host
   bool has_images_ = false;
   void BuildRemoteTables();
-  int window_w_ = 0;            // W of the captured graphs (0: one step per launch)
+  int window_w_ = 0;            // W of the last chunk (0: one step per launch)
   bool windowed_ = false;       // the last chunk ran in windows
   int solo_deliver_blocks_ = 0; // grid of a delivery that runs alone (windows, serial steps)
   int n_sm_ = 148;              // multiprocessors of the device (queried at calibration)

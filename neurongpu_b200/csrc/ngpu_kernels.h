@@ -74,6 +74,8 @@ struct Rk5Batch {
 };
 bool Rk5BatchSupported(int model, int np);
 void LaunchRk5Batch(const Rk5Batch &b, StepCtx *ctx, cudaStream_t s);
+// a batch through the W steps of a window (plain controller)
+void LaunchRk5BatchWindow(const Rk5Batch &b, StepCtx *ctxs, int W, cudaStream_t s);
 // step logging / learned proposer available for this model and port count
 bool StepProposerSupported(int model, int np);
 void LaunchIafPscExpUpdate(const GroupArgs &g, const InputArgs &in,

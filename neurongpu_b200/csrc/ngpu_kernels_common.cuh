@@ -859,6 +859,32 @@ k_rk5_window(const __grid_constant__ GroupArgs g, const __grid_constant__ InputA
   if (g.blk_evals != nullptr) block_add_u64(evals, g.blk_evals);
 }
 
+// Many RK5 groups of one model through a window of W steps in one launch
+// (the batched form of k_rk5_window): block b integrates its 128 neurons of
+// segment blk_seg[b]; the segment's uniform parameters are staged in shared
+// memory.
+template <class M, int NP, bool UNI, int MINB>
+__global__ void __launch_bounds__(NGPU_BLOCK, MINB)
+k_rk5_window_seg(const SegArgs *__restrict__ segs, const int *__restrict__ blk_seg,
+                 unsigned long long *blk_evals, StepCtx *ctxs, int W) {
+  pdl_wait();
+  pdl_trigger();
+  __shared__ float s_p[M::NPARAM], s_q[M::NPARAM];
+  const int seg = blk_seg[blockIdx.x];
+  const SegArgs &S = segs[seg];
+  if (UNI) {
+    for (int j = threadIdx.x; j < M::NPARAM; j += blockDim.x) {
+      s_p[j] = S.g.puni[j];
+      s_q[j] = S.g.pinv[j];
+    }
+    __syncthreads();
+  }
+  const int i = (blockIdx.x - S.blk0) * blockDim.x + threadIdx.x;
+  unsigned evals = 0;
+  if (i < S.g.n) rk5_window_neuron<M, NP, UNI>(S.g, S.in, S.pa, ctxs, W, i, s_p, s_q, evals);
+  if (blk_evals != nullptr) block_add_u64(evals, blk_evals);
+}
+
 // ---------------------------------------------------------------------------
 // Persistent RK5 update with TMA prefetch of the neuron state. Each block
 // walks the 128-neuron tiles blockIdx.x, blockIdx.x + gridDim.x, ...; the

@@ -48,6 +48,37 @@ static void launch_rk5_seg(const Rk5Batch &b, StepCtx *ctx, cudaStream_t s) {
   }
 }
 
+// windows of W steps: the window kernel with the register cap for 5 blocks
+// per SM (the batched kernel's segment arguments raise its register need:
+// at 6 blocks it spills 112 bytes) unless the batch's variant is 0 (no
+// cap); per-neuron parameters without a cap
+template <class M, int NP>
+static void launch_rk5_window_seg(const Rk5Batch &b, StepCtx *ctxs, int W, cudaStream_t s) {
+  const dim3 grid(b.n_blocks), block(NGPU_BLOCK);
+  if (!b.uni) {
+    launch_pdl(k_rk5_window_seg<M, NP, false, 1>, grid, block, s, b.segs, b.blk_seg, b.blk_evals,
+               ctxs, W);
+  } else if (b.variant == 0) {
+    launch_pdl(k_rk5_window_seg<M, NP, true, 1>, grid, block, s, b.segs, b.blk_seg, b.blk_evals,
+               ctxs, W);
+  } else {
+    launch_pdl(k_rk5_window_seg<M, NP, true, 5>, grid, block, s, b.segs, b.blk_seg, b.blk_evals,
+               ctxs, W);
+  }
+}
+
+template <template <int> class MT>
+static void launch_rk5_window_seg_model(const Rk5Batch &b, StepCtx *ctxs, int W, cudaStream_t s) {
+  switch (b.np) {
+    case 0:
+    case 1: launch_rk5_window_seg<MT<1>, 1>(b, ctxs, W, s); break;
+    case 2: launch_rk5_window_seg<MT<2>, 2>(b, ctxs, W, s); break;
+    case 3: launch_rk5_window_seg<MT<3>, 3>(b, ctxs, W, s); break;
+    case 4: launch_rk5_window_seg<MT<4>, 4>(b, ctxs, W, s); break;
+    default: break;
+  }
+}
+
 template <template <int> class MT>
 static void launch_rk5_seg_model(const Rk5Batch &b, StepCtx *ctx, cudaStream_t s) {
   switch (b.np) {
@@ -77,6 +108,19 @@ void LaunchRk5Batch(const Rk5Batch &b, StepCtx *ctx, cudaStream_t s) {
     case RK5_AEIF_PSC_EXP: launch_rk5_seg_model<AeifPscExp>(b, ctx, s); break;
     case RK5_AEIF_PSC_DELTA: launch_rk5_seg<AeifPscDelta<1>, 1>(b, ctx, s); break;
     case RK5_IZHIKEVICH_COND_BETA: launch_rk5_seg_model<IzhCondBeta>(b, ctx, s); break;
+    default: break;
+  }
+}
+
+void LaunchRk5BatchWindow(const Rk5Batch &b, StepCtx *ctxs, int W, cudaStream_t s) {
+  if (b.n_blocks <= 0) return;
+  switch (b.model) {
+    case RK5_AEIF_COND_BETA: launch_rk5_window_seg_model<AeifCondBeta>(b, ctxs, W, s); break;
+    case RK5_AEIF_COND_ALPHA: launch_rk5_window_seg_model<AeifCondAlpha>(b, ctxs, W, s); break;
+    case RK5_AEIF_PSC_ALPHA: launch_rk5_window_seg_model<AeifPscAlpha>(b, ctxs, W, s); break;
+    case RK5_AEIF_PSC_EXP: launch_rk5_window_seg_model<AeifPscExp>(b, ctxs, W, s); break;
+    case RK5_AEIF_PSC_DELTA: launch_rk5_window_seg<AeifPscDelta<1>, 1>(b, ctxs, W, s); break;
+    case RK5_IZHIKEVICH_COND_BETA: launch_rk5_window_seg_model<IzhCondBeta>(b, ctxs, W, s); break;
     default: break;
   }
 }

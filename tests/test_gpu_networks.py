@@ -335,3 +335,68 @@ def test_window_spike_totals_with_generator_connections_only(ngpu):
     assert cw.sum() > 10000
     assert np.array_equal(cw, cs)
     assert tw == int(cw.sum()) == ts
+
+
+def _mixed_window_net(ngpu, window):
+    import os
+    os.environ["NGB200_WINDOW"] = window
+    try:
+        b = ngpu.default_binding()
+        b.Reset()
+        b.SetVerbosityLevel(0)
+        ngpu.SetKernelStatus("rnd_seed", 2024)
+        pg1 = ngpu.Create("poisson_generator")
+        ngpu.SetStatus(pg1, "rate", 12000.0)
+        pg2 = ngpu.Create("poisson_generator")
+        ngpu.SetStatus(pg2, "rate", 30000.0)
+        a = ngpu.Create("aeif_cond_alpha", 1000, 2)
+        c = ngpu.Create("aeif_cond_beta", 1500, 2)
+        ngpu.SetStatus(c, {"E_rev": [0.0, -85.0], "tau_rise": [0.2, 0.5],
+                           "tau_decay": [2.0, 8.0]})
+        p = ngpu.Create("aeif_psc_exp", 800, 2)
+        groups = (a, c, p)
+        for g in groups:
+            # per-neuron draws from two generators (the per-connection path
+            # of the Poisson input, not the uniform drive)
+            ngpu.Connect(pg1, g, {"rule": "all_to_all"}, {"weight": 0.4, "delay": 0.1,
+                                                          "receptor": 0})
+            ngpu.Connect(pg2, g[0:g.n // 2], {"rule": "all_to_all"},
+                         {"weight": 0.2, "delay": 0.3, "receptor": 0})
+        delay = {"distribution": "uniform", "low": 1.0, "high": 2.0}
+        for src in groups:
+            for tgt in groups:
+                ngpu.Connect(src, tgt, {"rule": "fixed_indegree", "indegree": 30},
+                             {"weight": 0.05 if tgt is not p else 5.0, "delay": delay,
+                              "receptor": 0})
+        ngpu.Connect(p[0:200], c, {"rule": "fixed_indegree", "indegree": 10},
+                     {"weight": 0.3, "delay": 1.4, "receptor": 1})
+        for g in groups:
+            ngpu.ActivateRecSpikeTimes(g, 200)
+        ngpu.Simulate(40.0)
+        ngpu.Simulate(23.7)
+        kps = b.KernelsPerStep()
+        out = []
+        for g in groups:
+            v = np.asarray(ngpu.GetNeuronVar(g.i0, g.n, "V_m"), dtype=np.float32).view(np.int32)
+            times = [np.asarray(ngpu.GetRecSpikeTimes(g[i]), dtype=np.float32)
+                     for i in range(0, g.n, 7)]
+            out.append((v, times))
+        return out, b.TotalSpikes(), kps
+    finally:
+        os.environ.pop("NGB200_WINDOW", None)
+
+
+def test_windows_mixed_models_per_connection_poisson(ngpu):
+    """Windows (10 steps at the 1.0 ms shortest delay) against one step per
+    launch on three RK5 models with per-neuron Poisson inputs from two
+    generators, a uniformly distributed delay and recorded spike times:
+    every membrane potential, every recorded spike time and the spike total
+    agree bit for bit."""
+    w, tw, kw = _mixed_window_net(ngpu, "16")
+    s, ts, ks = _mixed_window_net(ngpu, "0")
+    assert kw < 0.6 < ks
+    assert ts == tw and ts > 1000
+    for (vw, timew), (vs, times) in zip(w, s):
+        assert np.array_equal(vw, vs)
+        for a, b in zip(timew, times):
+            assert np.array_equal(a, b)
