@@ -1656,10 +1656,11 @@ void NeuronGPU::KEvent(int step_in_chunk, int j) {
 
 // class times of the event groups k0 ... k0 + n - 1 (one group per step, or
 // one per window at the window's first step)
-void NeuronGPU::AccumulateKernelTiming(int k0, int n) {
+void NeuronGPU::AccumulateKernelTiming(int k0, int n, unsigned kinds) {
   NGPU_CUDA(cudaStreamSynchronize(stream_));
   for (int k = k0; k < k0 + n; k++) {
     for (int j = 0; j < 4; j++) {
+      if (!(kinds & (1u << j))) continue;       // no launch between these events
       float ms = 0.0f;
       NGPU_CUDA(cudaEventElapsedTime(&ms, kev_[(size_t)k * 5 + j], kev_[(size_t)k * 5 + j + 1]));
       ktime_ms_[j] += ms;
@@ -1943,13 +1944,13 @@ void NeuronGPU::EnqueueWindow(int k0, int w) {
   }
   if (ktime_) KEvent(k0, 1);
   const DeliverArgs d = MakeDeliverArgs();
-  LaunchDeliverWindow(d, ctxs, 0, w, 0, min_ring_delay_, solo_deliver_blocks_, stream_);
+  LaunchDeliverWindow(d, ctxs, 0, w, 0, min_ring_delay_, 0, w, 0, w, solo_deliver_blocks_,
+                      stream_);
   if (ktime_) {
     KEvent(k0, 2);
     KEvent(k0, 3);
+    KEvent(k0, 4);
   }
-  LaunchWindowBook(d_ring_cnt_, ring_R_, ring_C_, ctxs, 0, w, 0, w, stream_);
-  if (ktime_) KEvent(k0, 4);
 }
 
 // Hand-over from one step per launch to windows, before the first window
@@ -1963,10 +1964,8 @@ void NeuronGPU::EnqueueWindow(int k0, int w) {
 void NeuronGPU::EnqueueWindowCatchUp() {
   const int maxD = ring_R_ - 2;
   const DeliverArgs d = MakeDeliverArgs();
-  LaunchDeliverWindow(d, d_ctx_, -(long long)maxD, maxD, 0, min_ring_delay_, solo_deliver_blocks_,
-                      stream_);
-  LaunchWindowBook(d_ring_cnt_, ring_R_, ring_C_, d_ctx_, -(long long)(ring_R_ - 1), ring_R_,
-                   -1, 0, stream_);
+  LaunchDeliverWindow(d, d_ctx_, -(long long)maxD, maxD, 0, min_ring_delay_,
+                      -(long long)(ring_R_ - 1), ring_R_, -1, 0, solo_deliver_blocks_, stream_);
 }
 
 void NeuronGPU::LaunchSteps(int n_steps) {
@@ -2040,9 +2039,11 @@ void NeuronGPU::LaunchSteps(int n_steps) {
   NGPU_CUDA(cudaGetLastError());
   if (ktime_) {
     if (W > 0) {
-      for (int k = 0; k < n_steps; k += W) AccumulateKernelTiming(k, 1);
+      // a window: its update launches and one delivery (with the bookkeeping)
+      for (int k = 0; k < n_steps; k += W) AccumulateKernelTiming(k, 1, 1u | 2u);
     } else {
-      AccumulateKernelTiming(0, n_steps);
+      const bool has_delivery = MakeDeliverArgs().nd > 0;
+      AccumulateKernelTiming(0, n_steps, 1u | (has_delivery ? 2u : 8u) | (plastic_ ? 4u : 0u));
     }
   }
 }

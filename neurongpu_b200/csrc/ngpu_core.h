@@ -598,7 +598,9 @@ class NeuronGPU {
   double ktime_ms_[4] = {0, 0, 0, 0};
   long long klaunch_[4] = {0, 0, 0, 0};
   void KEvent(int step_in_chunk, int j);
-  void AccumulateKernelTiming(int k0, int n);
+  // kinds: bit j set where the interval between the events j and j + 1 of
+  // a step holds a launch (update, delivery, post rule, bookkeeping)
+  void AccumulateKernelTiming(int k0, int n, unsigned kinds);
 
   // graphs
   bool use_graphs_ = true;

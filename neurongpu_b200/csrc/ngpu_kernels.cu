@@ -548,30 +548,27 @@ k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
   deliver_blocks<PLASTIC>(d, syn, ctx, blockIdx.x, gridDim.x);
 }
 
-// Delivery after a window of integrated steps: the spikes of the steps
-// T_b + first_off ... T_b + first_off + n - 1, T_b the step of ctx (the
-// window's first step), delivered at all their delays at once.
-__global__ void __launch_bounds__(256, NGPU_DELIVER_MINB)
-k_deliver_window(DeliverArgs d, const StepCtx *ctx, long long first_off, int n,
-                 long long arrive_off, int min_delay) {
-  deliver_window_blocks(d, ctx, first_off, n, arrive_off, min_delay, blockIdx.x, gridDim.x);
-}
+// Spike bookkeeping of a window, by the threads of one block: the spikes of
+// the steps T_b + c_lo ... T_b + c_hi - 1 (T_b the step of ctx) are counted
+// into ctx->n_spikes, and the ring slots of the steps T_b + bk.first_off ...
+// T_b + bk.first_off + bk.n - 1 are emptied for reuse (their spikes have
+// been delivered at every delay).
+struct WindowBook {
+  long long first_off;
+  int n;
+  long long c_lo, c_hi;
+};
 
-// Spike bookkeeping of a window (one block): the spikes of the steps
-// T_b + c_lo ... T_b + c_hi - 1 are counted into ctx->n_spikes, and the ring
-// slots of the steps T_b + first_off ... T_b + first_off + n - 1 are
-// emptied for reuse (their spikes have been delivered at every delay).
-__global__ void k_window_book(int *ring_cnt, int ring_R, int ring_C, StepCtx *ctx,
-                              long long first_off, int n, long long c_lo, long long c_hi) {
+__device__ __forceinline__ void window_book_block(int *ring_cnt, int ring_R, int ring_C,
+                                                  StepCtx *ctx, const WindowBook &bk) {
   __shared__ unsigned long long s_cnt[256];
   const long long T_b = ctx->T0 + ctx->it + 1;
   unsigned long long cnt = 0;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    const long long rel = first_off + k;
-    const long long Ts = T_b + rel;
-    if (Ts < 0) continue;
+  for (int k = threadIdx.x; k < bk.n; k += blockDim.x) {
+    const long long rel = bk.first_off + k;
+    if (T_b + rel < 0) continue;
     const int slot = ring_add(ctx->ring_slot, rel, ring_R);
-    if (rel >= c_lo && rel < c_hi) {
+    if (rel >= bk.c_lo && rel < bk.c_hi) {
       const int c = ring_cnt[slot];
       cnt += (unsigned long long)(c < ring_C ? c : ring_C);
     }
@@ -585,16 +582,44 @@ __global__ void k_window_book(int *ring_cnt, int ring_R, int ring_C, StepCtx *ct
   }
 }
 
-void LaunchDeliverWindow(const DeliverArgs &d, const StepCtx *ctx, long long first_off, int n,
-                         long long arrive_off, int min_delay, int n_blocks, cudaStream_t s) {
-  // no connection from a spiking source (min_delay 0): nothing to deliver
-  if (d.nd <= 0 || n <= 0 || min_delay <= 0) return;
-  k_deliver_window<<<n_blocks, 256, 0, s>>>(d, ctx, first_off, n, arrive_off, min_delay);
+// Delivery after a window of integrated steps: the spikes of the steps
+// T_b + first_off ... T_b + first_off + n - 1, T_b the step of ctx (the
+// window's first step), delivered at all their delays at once; the last
+// block to finish (every block has then read the ring) does the window's
+// bookkeeping (one launch less per window).
+__global__ void __launch_bounds__(256, NGPU_DELIVER_MINB)
+k_deliver_window(DeliverArgs d, StepCtx *ctx, long long first_off, int n, long long arrive_off,
+                 int min_delay, WindowBook bk) {
+  deliver_window_blocks(d, ctx, first_off, n, arrive_off, min_delay, blockIdx.x, gridDim.x);
+  __shared__ bool s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(d.done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  window_book_block(d.ring_cnt_w, d.ring_R, d.ring_C, ctx, bk);
+  if (threadIdx.x == 0) *d.done = 0u;
 }
 
-void LaunchWindowBook(int *ring_cnt, int ring_R, int ring_C, StepCtx *ctx, long long first_off,
-                      int n, long long c_lo, long long c_hi, cudaStream_t s) {
-  k_window_book<<<1, 256, 0, s>>>(ring_cnt, ring_R, ring_C, ctx, first_off, n, c_lo, c_hi);
+// the bookkeeping alone (a window with nothing to deliver)
+__global__ void k_window_book(int *ring_cnt, int ring_R, int ring_C, StepCtx *ctx, WindowBook bk) {
+  window_book_block(ring_cnt, ring_R, ring_C, ctx, bk);
+}
+
+void LaunchDeliverWindow(const DeliverArgs &d, StepCtx *ctx, long long first_off, int n,
+                         long long arrive_off, int min_delay, long long book_first_off,
+                         int book_n, long long c_lo, long long c_hi, int n_blocks,
+                         cudaStream_t s) {
+  const WindowBook bk = {book_first_off, book_n, c_lo, c_hi};
+  // no connection from a spiking source (min_delay 0): nothing to deliver
+  if (d.nd <= 0 || n <= 0 || min_delay <= 0) {
+    k_window_book<<<1, 256, 0, s>>>(d.ring_cnt_w, d.ring_R, d.ring_C, ctx, bk);
+    return;
+  }
+  k_deliver_window<<<n_blocks, 256, 0, s>>>(d, ctx, first_off, n, arrive_off, min_delay, bk);
 }
 
 // Resident delivery blocks per SM, at most 3: the delivery runs beside the

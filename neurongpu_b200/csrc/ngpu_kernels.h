@@ -115,13 +115,14 @@ void LaunchDeliver(const DeliverArgs &d, const SynGroupTable &syn,
 // after a window: the spikes of the steps T_b + first_off ...
 // T_b + first_off + n - 1 (T_b: the step of ctx) delivered at all their
 // delays of min_delay or more (the shortest delay of a spiking source's
-// connection), arrivals from step T_b + arrive_off on
-void LaunchDeliverWindow(const DeliverArgs &d, const StepCtx *ctx, long long first_off, int n,
-                         long long arrive_off, int min_delay, int n_blocks, cudaStream_t s);
-// spike count of the steps T_b + c_lo ... T_b + c_hi - 1 into ctx, and the
-// ring slots of the steps T_b + first_off ... + n - 1 emptied
-void LaunchWindowBook(int *ring_cnt, int ring_R, int ring_C, StepCtx *ctx, long long first_off,
-                      int n, long long c_lo, long long c_hi, cudaStream_t s);
+// connection), arrivals from step T_b + arrive_off on; then, in the same
+// launch, the spike count of the steps T_b + c_lo ... T_b + c_hi - 1 into
+// ctx and the ring slots of the steps T_b + book_first_off ... + book_n - 1
+// emptied
+void LaunchDeliverWindow(const DeliverArgs &d, StepCtx *ctx, long long first_off, int n,
+                         long long arrive_off, int min_delay, long long book_first_off,
+                         int book_n, long long c_lo, long long c_hi, int n_blocks,
+                         cudaStream_t s);
 // spike exchange of partitioned networks (ngpu_remote.cu)
 void LaunchPackRemote(const int *ring_cnt, const unsigned *ring_src, const float *ring_h,
                       int ring_R, int ring_C, const StepCtx *ctx, int n_steps,
