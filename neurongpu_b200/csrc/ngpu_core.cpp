@@ -92,7 +92,7 @@ void NeuronGPU::FreeDevice() {
   F(d_grp_off_); F(d_e_slot_); F(d_e_w_); F(d_e_syn_); F(d_e_stamp_); F(d_c_port_);
   d_grp_off_ = nullptr; d_e_slot_ = nullptr; d_e_w_ = nullptr; d_e_syn_ = nullptr;
   d_e_stamp_ = nullptr; d_c_port_ = nullptr;
-  F(d_e_post_); F(d_rev_off_); F(d_rev_edge_); F(d_delays_);
+  F(d_e_post_); F(d_rev_off_); F(d_rev_edge_); F(d_delays_); F(d_delay_di_);
   F(d_rev_src_); F(d_rev_cnt_);
   d_rev_src_ = nullptr;
   d_rev_cnt_ = nullptr;
@@ -1126,6 +1126,7 @@ DeliverArgs NeuronGPU::MakeDeliverArgs() {
   d.ring_C = ring_C_;
   d.nd = (int)delays_.size();
   d.delays = d_delays_;
+  d.delay_di = d_delay_di_;
   d.last_rev_T = d_last_rev_T_;
   d.last_post_T = d_last_post_T_;
   d.rev_off = d_rev_off_;
@@ -1321,6 +1322,12 @@ void NeuronGPU::BuildDevice() {
   std::vector<int> dl(delays_.begin(), delays_.end());
   NGPU_CUDA(cudaMalloc(&d_delays_, sizeof(int) * (nd > 0 ? nd : 1)));
   if (nd > 0) NGPU_CUDA(cudaMemcpy(d_delays_, dl.data(), sizeof(int) * nd, cudaMemcpyHostToDevice));
+  if (nd > 0) {
+    const int dmax = delays_.back();
+    NGPU_CUDA(cudaMalloc(&d_delay_di_, sizeof(int) * (dmax + 1)));
+    NGPU_CUDA(cudaMemcpy(d_delay_di_, delay_index_.data(), sizeof(int) * (dmax + 1),
+                         cudaMemcpyHostToDevice));
+  }
   if (nd > NGPU_MAX_DELAYS) throw ngpu_exception("Too many distinct delays");
   // STDP structures: stamps and per-target incoming plastic lists (the CSR
   // targets d_e_post_ and groups d_e_syn_ are shared with the queries)
@@ -2249,9 +2256,19 @@ void NeuronGPU::RecheckDeliveryMode() {
                                    : per_step > kFusedDeliveryMaxEvents;
   if (busy != delivery_busy_) {
     delivery_busy_ = busy;
-    // a network that turns busy times its two delivery modes
+    // a network that turns busy times its delivery modes, unless
+    // NGB200_BUSY_MODE names one (0: forked, 1: serial, 2: windows where
+    // the network can run them, else forked)
     busy_mode_ = BUSY_FORK;
     delivery_trial_ = busy ? 1 : 0;
+    const char *force = getenv("NGB200_BUSY_MODE");
+    if (force != nullptr) {
+      const int m = atoi(force);
+      if (m < BUSY_FORK || m > BUSY_WINDOW)
+        throw ngpu_exception("NGB200_BUSY_MODE must be 0, 1 or 2");
+      busy_mode_ = (m == BUSY_WINDOW && WindowEligible() == 0) ? (int)BUSY_FORK : m;
+      delivery_trial_ = 0;
+    }
     trial_chunk_ = 0;
     for (int m = 0; m < 3; m++) {
       trial_ms_[m] = 0.0;

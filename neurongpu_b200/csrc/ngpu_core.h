@@ -556,6 +556,7 @@ class NeuronGPU {
   unsigned long long *d_rev_off_ = nullptr;
   unsigned *d_rev_edge_ = nullptr;
   int *d_delays_ = nullptr;
+  int *d_delay_di_ = nullptr;         // delay in steps -> index in delays_, or -1
   bool plastic_ = false;
   std::vector<unsigned char> has_out_;
   // Poisson direct connections (global arrays, CSR by target node)

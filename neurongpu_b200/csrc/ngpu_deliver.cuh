@@ -258,6 +258,82 @@ __device__ __forceinline__ void deliver_blocks(const DeliverArgs &d, const SynGr
   finish_step(d, ctx, nblk);
 }
 
+// The window delivery's items in arrival order (see deliver_window_blocks):
+// lane k holds the spike count of step T_b + first_off + k; the (arrival,
+// emission) pairs are taken 32 at a time, a lane each, and a scan of their
+// spike counts gives every pair's first item, so each warp knows its own
+// items of the 32 pairs without looking at the others' items.
+__device__ __forceinline__ void deliver_window_ordered(const DeliverArgs &d, long long T_b,
+                                                       int ring_b, int acc_b, long long first_off,
+                                                       int n, long long arrive_off, int min_delay,
+                                                       int lane, int warp, int n_warps, int blk) {
+  const unsigned full = 0xffffffffu;
+  int my_c = 0, my_slot = 0;
+  if (lane < n && T_b + first_off + lane >= 0) {
+    my_slot = ring_add(ring_b, first_off + lane, d.ring_R);
+    const int c = d.ring_cnt[my_slot];
+    my_c = c < d.ring_C ? c : d.ring_C;
+  }
+  if (!__any_sync(full, my_c > 0)) return;
+  const int D_hi = d.delays[d.nd - 1];
+  const int D_lo = min_delay > d.delays[0] ? min_delay : d.delays[0];
+  if (D_lo > D_hi) return;
+  // pair p: arrival index u = p / n (the step T_b + first_off + D_lo + u
+  // receives it), emission step k = p % n, delay D = D_lo + u - k
+  const int P = (D_hi - D_lo + n) * n;
+  int base = 0;                       // items before this round, modulo n_warps
+  unsigned long long events = 0;
+  for (int p0 = 0; p0 < P; p0 += 32) {
+    const int p = p0 + lane;
+    const int u = p / n, k = p - u * n;
+    const int D = D_lo + u - k;
+    const int ck = __shfl_sync(full, my_c, k);
+    int di = -1;
+    if (p < P && D >= D_lo && D <= D_hi) di = d.delay_di[D];
+    const long long rel_v = first_off + k + D;
+    const int c = (di >= 0 && rel_v >= arrive_off) ? ck : 0;
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(full, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(full, incl, 31);
+    // this warp's first item of the pair: item j of the pair is item
+    // base + (incl - c) + j of the order
+    int j = warp - (base + incl - c) % n_warps;
+    if (j < 0) j += n_warps;
+    unsigned m = __ballot_sync(full, j < c);
+    while (m) {
+      const int l = __ffs(m) - 1;
+      m &= m - 1;
+      const int jl = __shfl_sync(full, j, l), cl = __shfl_sync(full, c, l);
+      const int kl = __shfl_sync(full, k, l), dil = __shfl_sync(full, di, l);
+      const int Dl = __shfl_sync(full, D, l);
+      const int slot = __shfl_sync(full, my_slot, kl);
+      const long long rv = first_off + kl + Dl;
+      const int v_slot = ring_add(acc_b, rv, d.acc_slots);
+      long long *acc = d.acc + acc_slot_offset(v_slot, d.acc_slots, d.acc_par);
+      // one stamp store per (step, delay) pair with spikes: by the warp of its first item
+      if (jl == 0 && lane == 0 && d.acc_stamp != nullptr) d.acc_stamp[v_slot] = T_b + rv;
+      for (int jj = jl; jj < cl; jj += n_warps) {
+        const long long kk = (long long)slot * d.ring_C + jj;
+        const unsigned src = d.ring_src[kk];
+        const float height = d.ring_h[kk];
+        const unsigned long long e_i = (unsigned long long)src * d.nd + dil;
+        const unsigned long long beg = d.grp_off[e_i], end = d.grp_off[e_i + 1];
+        if (lane == 0) events += end - beg;
+        deliver_static_edges(d, acc, beg, end, height, lane);
+      }
+    }
+    base = (base + total) % n_warps;
+  }
+  if (d.blk_events != nullptr) {
+    for (int o = 16; o > 0; o >>= 1) events += __shfl_down_sync(full, events, o);
+    if (lane == 0 && events != 0) atomicAdd(d.blk_events + blk, events);
+  }
+}
+
 // Delivery after a window of integrated steps (networks without plastic
 // synapses, k_rk5_window): every spike emitted in the steps
 // T_b + first_off ... T_b + first_off + n - 1 (their ring slots) is
@@ -272,7 +348,16 @@ __device__ __forceinline__ void deliver_blocks(const DeliverArgs &d, const SynGr
 // their targets by direct connections): such a group holds no edge, and its
 // slot stamp would name a step W + 1 or more before the slots this delivery
 // fills, i.e. a slot one of them shares, overwriting that slot's stamp.
-// Warps take (step, delay) groups in turn, several warps per group.
+//
+// Up to 32 steps (a window): the items, one per (spike, delay), are ordered
+// by the step whose slot receives them, then by the step that emitted them,
+// and warp w takes the items w, w + n_warps, w + 2 n_warps, ... of that
+// order. The warps advance through it together, so the accumulator slots in
+// use at any time are one or two, and stay in L2, where (step, delay) groups
+// taken all at once would add into up to W + max delay slots together (on a
+// network with 2.6e6 events per step and 16 MB slots, 50 slots: the atomics
+// then went to HBM at a tenth of the rate). More steps (the hand-over to
+// windows): warps take (step, delay) groups in turn, several warps per group.
 __device__ __forceinline__ void deliver_window_blocks(const DeliverArgs &d, const StepCtx *ctx,
                                                       long long first_off, int n,
                                                       long long arrive_off, int min_delay,
@@ -282,6 +367,12 @@ __device__ __forceinline__ void deliver_window_blocks(const DeliverArgs &d, cons
   const int lane = threadIdx.x & 31;
   const int warp = (blk * (int)blockDim.x + (int)threadIdx.x) >> 5;
   const int n_warps = (nblk * (int)blockDim.x) >> 5;
+  // (the scan of 32 pairs' spike counts stays within int below 2^26 spikes per step)
+  if (n <= 32 && d.delay_di != nullptr && d.ring_C < (1 << 26)) {
+    deliver_window_ordered(d, T_b, ring_b, acc_b, first_off, n, arrive_off, min_delay, lane,
+                           warp, n_warps, blk);
+    return;
+  }
   const int NG = n * d.nd;
   const bool per_group = n_warps >= NG;
   const int G = per_group ? n_warps / NG : 1;

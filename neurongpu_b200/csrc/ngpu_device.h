@@ -311,7 +311,8 @@ struct DeliverArgs {
   const int *ring_cnt;
   int ring_R, ring_C;
   int nd;
-  const int *delays;                   // [nd] distinct delays in steps
+  const int *delays;                   // [nd] distinct delays in steps, ascending
+  const int *delay_di;                 // [delays[nd-1] + 1] delay -> its index, or -1
   int *last_rev_T;
   int *last_post_T;
   const unsigned *rev_src;             // dendritic-delay ring (see PushArgs)
