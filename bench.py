@@ -138,6 +138,9 @@ def measured_peaks():
 # active network at 400,000 neurons (profiles/deliver_active_400k.md).
 TRAFFIC_RK5_PER_NEURON_STEP = 6.2        # bytes (the state stays L2-resident)
 TRAFFIC_DELIVER_PER_EVENT = 11.3         # bytes
+# the delivery before a window (k_deliver_window) on the active network at
+# 400,000 neurons in windows of 10 steps (profiles/deliver_window_400k.md)
+TRAFFIC_DELIVER_WINDOW_PER_EVENT = 20.7  # bytes
 INST_RK5_PER_WARP_STEP = 821.9           # warp instructions per 32 neuron-steps
 # the window kernel (several steps per launch; register cap for 6 blocks per
 # SM), 200,000 neurons of the silent network, windows of 10 steps
@@ -656,6 +659,7 @@ def main():
         a_bio = a_steps * step_ms / 1000.0
         a_nst = int(round(a_steps * step_ms / 0.1))
         d_ms, d_n = ar["ktime"]["deliver"]
+        a_window = a_nst / max(ar["ktime"]["update"][1], 1) > 1.5
         ev_launch = ar["events_instr"] / max(d_n, 1)
         d_avg = d_ms / max(d_n, 1)
         d_ach = BYTES_PER_EVENT * ev_launch / (d_avg / 1000.0) / 1e9 if d_avg > 0 else 0.0
@@ -678,10 +682,13 @@ def main():
             "deliver_roofline": {"kernel": "deliver", "bound": "hbm", "achieved": d_ach,
                                  "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
                                  "frac": d_ach / peak, "events_per_launch": ev_launch,
-                                 "traffic": TRAFFIC_DELIVER_PER_EVENT * ev_launch,
+                                 "traffic": (TRAFFIC_DELIVER_WINDOW_PER_EVENT if a_window
+                                             else TRAFFIC_DELIVER_PER_EVENT) * ev_launch,
                                  "avg_launch_ms": d_avg,
                                  "timing": "delivery launch events of the instrumented run "
-                                           "(serial delivery)",
+                                           + ("(one delivery before each window of steps, "
+                                              "one more per chunk)" if a_window
+                                              else "(serial delivery)"),
                                  "l2_atomics": None if not probe else {
                                      "achieved": ev_rate, "peak": probe, "unit": "events/s",
                                      "frac": ev_rate / probe,

@@ -1260,17 +1260,18 @@ void NeuronGPU::BuildDevice() {
   if (n_acc_ > 0xFFFFFFFFLL) throw ngpu_exception("Too many (node, port) input slots");
   // accumulator ring (InputArgs::acc_par, acc_slots): two slots, or, for a
   // network that can run several steps per launch (RK5 neurons and Poisson
-  // generators only, no plastic synapse), one slot per step up to the
-  // longest delay + 2, so that the delivery after a window can fill the
-  // slots of every later step at once; at most kWindowAccBytes
+  // generators only, no plastic synapse), one slot per step of the longest
+  // window + 1 (the delivery before a window fills the slots of all its
+  // steps), and no more than the longest delay + 2; at most kWindowAccBytes
   {
     int maxD_acc = 1;
     for (int dly : delays_) maxD_acc = std::max(maxD_acc, dly);
     bool capable = !any_plastic_;
     for (NodeGroup *g : groups_)
       if (g->mi->kind != MK_RK5 && g->mi->kind != MK_POISSON_GENERATOR) capable = false;
-    const double bytes = (double)(maxD_acc + 2) * 8.0 * (double)(n_acc_ > 0 ? n_acc_ : 1);
-    acc_slots_ = (capable && bytes <= kWindowAccBytes) ? maxD_acc + 2 : 2;
+    const int slots = std::min(maxD_acc + 2, kWindowMaxSteps + 1);
+    const double bytes = (double)slots * 8.0 * (double)(n_acc_ > 0 ? n_acc_ : 1);
+    acc_slots_ = (capable && bytes <= kWindowAccBytes) ? slots : 2;
   }
   const size_t acc_bytes = (size_t)acc_slots_ * sizeof(long long) * (n_acc_ > 0 ? n_acc_ : 1);
   NGPU_CUDA(cudaMalloc(&d_acc_, acc_bytes));
@@ -1508,7 +1509,8 @@ void NeuronGPU::BuildDevice() {
   deliver_blocks_ = n_sm * DeliverBlocksPerSM();
   // the delivery after a window runs alone: every resident block
   solo_deliver_blocks_ = n_sm * DeliverOccupancy();
-  n_evt_blocks_ = std::max(deliver_blocks_, solo_deliver_blocks_);
+  window_deliver_blocks_ = n_sm * DeliverWindowOccupancy();
+  n_evt_blocks_ = std::max(std::max(deliver_blocks_, solo_deliver_blocks_), window_deliver_blocks_);
   NGPU_CUDA(cudaMalloc(&d_done_, sizeof(unsigned)));
   NGPU_CUDA(cudaMemset(d_done_, 0, sizeof(unsigned)));
   NGPU_CUDA(cudaMalloc(&d_blk_events_, sizeof(unsigned long long) * n_evt_blocks_));
@@ -1663,6 +1665,20 @@ void NeuronGPU::KEvent(int step_in_chunk, int j) {
 
 // class times of the event groups k0 ... k0 + n - 1 (one group per step, or
 // one per window at the window's first step)
+// a window: its delivery (events 0 -> 1), its update launches (1 -> 2) and,
+// after the chunk's last window, the delivery into the last step's slot
+// (2 -> 3)
+void NeuronGPU::AccumulateWindowTiming(int k0, bool last) {
+  NGPU_CUDA(cudaStreamSynchronize(stream_));
+  const int kind[3] = {1, 0, 1};
+  for (int j = 0; j < (last ? 3 : 2); j++) {
+    float ms = 0.0f;
+    NGPU_CUDA(cudaEventElapsedTime(&ms, kev_[(size_t)k0 * 5 + j], kev_[(size_t)k0 * 5 + j + 1]));
+    ktime_ms_[kind[j]] += ms;
+    klaunch_[kind[j]] += 1;
+  }
+}
+
 void NeuronGPU::AccumulateKernelTiming(int k0, int n, unsigned kinds) {
   NGPU_CUDA(cudaStreamSynchronize(stream_));
   for (int k = k0; k < k0 + n; k++) {
@@ -1886,20 +1902,17 @@ void NeuronGPU::EnqueueStep(int step_in_chunk) {
 
 // Steps per launch. A spike emitted in step s with a delay of D steps is
 // folded by the update of step s + D + 1, so with W <= shortest delay + 1 no
-// spike of a window of W steps arrives inside it, and one launch per RK5
-// group can integrate its neurons through all W steps before one delivery
-// of the window's spikes (k_rk5_window, k_deliver_window, k_window_book).
-// Windows need: every node group an RK5 group (batched or not) with the
-// plain controller, or a Poisson generator; no plastic synapse, multimeter
-// record or large-rate Poisson pre-pass; the accumulator ring of the
-// longest delay + 2 slots. A quiet network (below kFusedDeliveryMaxEvents
-// delivered events per step) runs in windows; a busy one only where its
-// mode trial timed them fastest (LaunchStepsTimed): the delivery after a
-// window adds into the slots of up to W + max delay later steps at once, a
-// working set that leaves L2 when many events arrive, where one step's
-// delivery adds into one slot. W is at most 16 and preferably divides the
-// graph chunk; NGB200_WINDOW caps it (0: one step per launch). 0: no
-// windows.
+// spike of a window of W steps arrives inside it: one delivery before the
+// window fills the accumulator slots its W steps fold (k_deliver_window),
+// then one launch per RK5 group integrates its neurons through all W steps
+// (k_rk5_window). Windows need: every node group an RK5 group (batched or
+// not) with the plain controller, or a Poisson generator; no plastic
+// synapse, multimeter record or large-rate Poisson pre-pass; the
+// accumulator ring of the longest delay + 2 slots. A quiet network (below
+// kFusedDeliveryMaxEvents delivered events per step) runs in windows; a
+// busy one where its mode trial timed them fastest (LaunchStepsTimed). W
+// is at most 16 and preferably divides the graph chunk; NGB200_WINDOW caps
+// it (0: one step per launch). 0: no windows.
 int NeuronGPU::WindowSteps() {
   if (delivery_busy_ && busy_mode_ != BUSY_WINDOW) return 0;
   return WindowEligible();
@@ -1907,10 +1920,11 @@ int NeuronGPU::WindowSteps() {
 
 int NeuronGPU::WindowEligible() {
   const char *env = getenv("NGB200_WINDOW");
-  int cap = 16;
-  if (env != nullptr) cap = std::max(0, std::min(16, atoi(env)));
+  int cap = kWindowMaxSteps;
+  if (env != nullptr) cap = std::max(0, std::min(kWindowMaxSteps, atoi(env)));
+  // (the delivery's scan of 32 slots' spike counts stays within int)
   if (cap < 2 || acc_slots_ <= 2 || d_acc_stamp_ == nullptr || plastic_ || n_rec_cols_ > 0 ||
-      n_exported_ > 0 || has_images_)
+      n_exported_ > 0 || has_images_ || ring_C_ >= (1 << 26))
     return 0;
   for (NodeGroup *g : groups_) {
     if (g->mi->kind == MK_POISSON_GENERATOR) continue;
@@ -1921,6 +1935,8 @@ int NeuronGPU::WindowEligible() {
   // no connection through the spike ring: any W; every step of a window
   // has its own ring slot
   const int minD = min_ring_delay_ > 0 ? min_ring_delay_ : 15;
+  // (the accumulator ring, min(max delay + 2, 17) slots, then holds the
+  // slots of every step of a window: W <= min(shortest delay + 1, 16))
   int W = std::min(std::min(cap, minD + 1), ring_R_ - 1);
   if (W < 2) return 0;
   // prefer a divisor of the chunk (equal windows in every chunk) if one of
@@ -1931,12 +1947,31 @@ int NeuronGPU::WindowEligible() {
   return W;
 }
 
-// The steps k0 ... k0 + w - 1 of the chunk as one window: each RK5 group's
-// window launch, the delivery of the window's spikes at all their delays,
-// the window's spike count and the emptying of its ring slots.
-void NeuronGPU::EnqueueWindow(int k0, int w) {
+// The steps k0 ... k0 + w - 1 of a chunk of n_steps steps in windows of W
+// steps: the delivery into the accumulator slots the window's steps fold
+// (from the slot of the step before the window on; the chunk's first
+// window starts at its own first step, as the step before filled its slot
+// itself), with the spike count of the previous window's steps (the
+// chunk's first window: of the step before it) and the emptying of the
+// ring slots the window writes; then each RK5 group's window launch. After
+// the chunk's last window, the delivery into the slot of its last step, the
+// count of the window's other steps and the emptying of the next step's
+// ring slot: a chunk ends as a chunk of one step per launch does (the slot
+// of its last step filled, the spikes of the steps before that step
+// counted, the next step's ring slot empty), so either kind may follow.
+void NeuronGPU::EnqueueWindow(int k0, int w, int W, int n_steps) {
   StepCtx *ctxs = d_ctxs_ + k0;
+  const DeliverArgs d = MakeDeliverArgs();
+  // the first delay of a spiking source (the others are Poisson
+  // generators', which reach their targets by direct connections)
+  const int di0 = min_ring_delay_ > 0 ? delay_index_[min_ring_delay_] : d.nd;
+  const int D_lo = min_ring_delay_, D_hi = d.nd > 0 ? delays_.back() : 0;
+  const int v_lo = k0 == 0 ? 0 : -1;
+  const long long c_lo = k0 == 0 ? -1 : -(long long)W;
   if (ktime_) KEvent(k0, 0);
+  LaunchDeliverWindow(d, ctxs, v_lo, w - 1 - v_lo, di0, D_lo, D_hi, 0, w, c_lo, 0,
+                      window_deliver_blocks_, stream_);
+  if (ktime_) KEvent(k0, 1);
   for (NodeGroup *g : groups_) {
     if (g->mi->kind != MK_RK5) continue;
     if (g->batch >= 0) {
@@ -1949,30 +1984,14 @@ void NeuronGPU::EnqueueWindow(int k0, int w) {
                          MakePushArgs(g), ctxs, w, stream_))
       throw ngpu_exception("internal error: no window kernel for this node group");
   }
-  if (ktime_) KEvent(k0, 1);
-  const DeliverArgs d = MakeDeliverArgs();
-  LaunchDeliverWindow(d, ctxs, 0, w, 0, min_ring_delay_, 0, w, 0, w, solo_deliver_blocks_,
-                      stream_);
+  if (ktime_) KEvent(k0, 2);
+  if (k0 + w == n_steps)
+    LaunchDeliverWindow(d, ctxs, w - 1, 1, di0, D_lo, D_hi, w, 1, 0, w - 1,
+                        window_deliver_blocks_, stream_);
   if (ktime_) {
-    KEvent(k0, 2);
     KEvent(k0, 3);
     KEvent(k0, 4);
   }
-}
-
-// Hand-over from one step per launch to windows, before the first window
-// (T_b = its first step): the spikes of the last max-delay steps are
-// delivered for their arrivals from T_b on (the one-step deliveries made
-// the earlier ones), the spikes of step T_b - 1 (which the next step's
-// bookkeeping would count) are counted, and every ring slot is emptied, as
-// the windows expect. From windows back to one step per launch needs
-// nothing: every window leaves its ring slots empty and its spikes
-// delivered.
-void NeuronGPU::EnqueueWindowCatchUp() {
-  const int maxD = ring_R_ - 2;
-  const DeliverArgs d = MakeDeliverArgs();
-  LaunchDeliverWindow(d, d_ctx_, -(long long)maxD, maxD, 0, min_ring_delay_,
-                      -(long long)(ring_R_ - 1), ring_R_, -1, 0, solo_deliver_blocks_, stream_);
 }
 
 void NeuronGPU::LaunchSteps(int n_steps) {
@@ -1994,14 +2013,10 @@ void NeuronGPU::LaunchSteps(int n_steps) {
   const int rec = n_rec_cols_ > 0 ? 1 : 0;
   const int W = WindowSteps();
   window_w_ = W;
-  // the hand-over to windows depends on the mode of the previous chunk, so
-  // it runs before the chunk's graph, not in it
-  if (W > 0 && !windowed_) EnqueueWindowCatchUp();
-  windowed_ = W > 0;
   auto enqueue_chunk = [&]() {
     LaunchStepPrologue(d_ctx_, d_ctxs_, n_steps, rec, stream_);
     if (W > 0) {
-      for (int k = 0; k < n_steps; k += W) EnqueueWindow(k, std::min(W, n_steps - k));
+      for (int k = 0; k < n_steps; k += W) EnqueueWindow(k, std::min(W, n_steps - k), W, n_steps);
     } else {
       for (int k = 0; k < n_steps; k++) EnqueueStep(k);
     }
@@ -2046,8 +2061,7 @@ void NeuronGPU::LaunchSteps(int n_steps) {
   NGPU_CUDA(cudaGetLastError());
   if (ktime_) {
     if (W > 0) {
-      // a window: its update launches and one delivery (with the bookkeeping)
-      for (int k = 0; k < n_steps; k += W) AccumulateKernelTiming(k, 1, 1u | 2u);
+      for (int k = 0; k < n_steps; k += W) AccumulateWindowTiming(k, k + W >= n_steps);
     } else {
       const bool has_delivery = MakeDeliverArgs().nd > 0;
       AccumulateKernelTiming(0, n_steps, 1u | (has_delivery ? 2u : 8u) | (plastic_ ? 4u : 0u));

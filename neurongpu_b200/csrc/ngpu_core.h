@@ -535,6 +535,7 @@ class NeuronGPU {
   // several steps per launch; per slot the last step added into it
   int acc_slots_ = 2;
   static constexpr double kWindowAccBytes = 8e9;
+  static constexpr int kWindowMaxSteps = 16;    // steps per window at most
   long long *d_acc_stamp_ = nullptr;
   unsigned *d_ring_src_ = nullptr;
   float *d_ring_h_ = nullptr;
@@ -602,6 +603,7 @@ class NeuronGPU {
   // kinds: bit j set where the interval between the events j and j + 1 of
   // a step holds a launch (update, delivery, post rule, bookkeeping)
   void AccumulateKernelTiming(int k0, int n, unsigned kinds);
+  void AccumulateWindowTiming(int k0, bool last);
 
   // graphs
   bool use_graphs_ = true;
@@ -618,8 +620,7 @@ class NeuronGPU {
   void EnqueueStep(int step_in_chunk);
   // several steps per launch (windows of W steps, W <= shortest delay + 1)
   int WindowSteps();
-  void EnqueueWindow(int k0, int w);
-  void EnqueueWindowCatchUp();
+  void EnqueueWindow(int k0, int w, int W, int n_steps);
   int min_ring_delay_ = 0;      // shortest delay (steps) of a spiking source's connection
   // partitioned networks: host of this instance, exported nodes, and per
   // source host the image node of every remote node (host and device)
@@ -635,8 +636,8 @@ class NeuronGPU {
   bool has_images_ = false;
   void BuildRemoteTables();
   int window_w_ = 0;            // W of the last chunk (0: one step per launch)
-  bool windowed_ = false;       // the last chunk ran in windows
-  int solo_deliver_blocks_ = 0; // grid of a delivery that runs alone (windows, serial steps)
+  int solo_deliver_blocks_ = 0; // grid of a delivery that runs alone (serial steps)
+  int window_deliver_blocks_ = 0;   // grid of the delivery after a window (all resident)
   int n_sm_ = 148;              // multiprocessors of the device (queried at calibration)
   int n_evt_blocks_ = 0;        // delivery event counters (max of both grids)
 

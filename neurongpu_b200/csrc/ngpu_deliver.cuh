@@ -258,169 +258,158 @@ __device__ __forceinline__ void deliver_blocks(const DeliverArgs &d, const SynGr
   finish_step(d, ctx, nblk);
 }
 
-// The window delivery's items in arrival order (see deliver_window_blocks):
-// lane k holds the spike count of step T_b + first_off + k; the (arrival,
-// emission) pairs are taken 32 at a time, a lane each, and a scan of their
-// spike counts gives every pair's first item, so each warp knows its own
-// items of the 32 pairs without looking at the others' items.
-__device__ __forceinline__ void deliver_window_ordered(const DeliverArgs &d, long long T_b,
-                                                       int ring_b, int acc_b, long long first_off,
-                                                       int n, long long arrive_off, int min_delay,
-                                                       int lane, int warp, int n_warps, int blk) {
-  const unsigned full = 0xffffffffu;
-  int my_c = 0, my_slot = 0;
-  if (lane < n && T_b + first_off + lane >= 0) {
-    my_slot = ring_add(ring_b, first_off + lane, d.ring_R);
-    const int c = d.ring_cnt[my_slot];
-    my_c = c < d.ring_C ? c : d.ring_C;
-  }
-  if (!__any_sync(full, my_c > 0)) return;
-  const int D_hi = d.delays[d.nd - 1];
-  const int D_lo = min_delay > d.delays[0] ? min_delay : d.delays[0];
-  if (D_lo > D_hi) return;
-  // pair p: arrival index u = p / n (the step T_b + first_off + D_lo + u
-  // receives it), emission step k = p % n, delay D = D_lo + u - k
-  const int P = (D_hi - D_lo + n) * n;
-  int base = 0;                       // items before this round, modulo n_warps
-  unsigned long long events = 0;
-  for (int p0 = 0; p0 < P; p0 += 32) {
-    const int p = p0 + lane;
-    const int u = p / n, k = p - u * n;
-    const int D = D_lo + u - k;
-    const int ck = __shfl_sync(full, my_c, k);
-    int di = -1;
-    if (p < P && D >= D_lo && D <= D_hi) di = d.delay_di[D];
-    const long long rel_v = first_off + k + D;
-    const int c = (di >= 0 && rel_v >= arrive_off) ? ck : 0;
-    int incl = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int v = __shfl_up_sync(full, incl, o);
-      if (lane >= o) incl += v;
-    }
-    const int total = __shfl_sync(full, incl, 31);
-    // this warp's first item of the pair: item j of the pair is item
-    // base + (incl - c) + j of the order
-    int j = warp - (base + incl - c) % n_warps;
-    if (j < 0) j += n_warps;
-    unsigned m = __ballot_sync(full, j < c);
-    while (m) {
-      const int l = __ffs(m) - 1;
-      m &= m - 1;
-      const int jl = __shfl_sync(full, j, l), cl = __shfl_sync(full, c, l);
-      const int kl = __shfl_sync(full, k, l), dil = __shfl_sync(full, di, l);
-      const int Dl = __shfl_sync(full, D, l);
-      const int slot = __shfl_sync(full, my_slot, kl);
-      const long long rv = first_off + kl + Dl;
-      const int v_slot = ring_add(acc_b, rv, d.acc_slots);
-      long long *acc = d.acc + acc_slot_offset(v_slot, d.acc_slots, d.acc_par);
-      // one stamp store per (step, delay) pair with spikes: by the warp of its first item
-      if (jl == 0 && lane == 0 && d.acc_stamp != nullptr) d.acc_stamp[v_slot] = T_b + rv;
-      for (int jj = jl; jj < cl; jj += n_warps) {
-        const long long kk = (long long)slot * d.ring_C + jj;
-        const unsigned src = d.ring_src[kk];
-        const float height = d.ring_h[kk];
-        const unsigned long long e_i = (unsigned long long)src * d.nd + dil;
-        const unsigned long long beg = d.grp_off[e_i], end = d.grp_off[e_i + 1];
-        if (lane == 0) events += end - beg;
-        deliver_static_edges(d, acc, beg, end, height, lane);
-      }
-    }
-    base = (base + total) % n_warps;
-  }
-  if (d.blk_events != nullptr) {
-    for (int o = 16; o > 0; o >>= 1) events += __shfl_down_sync(full, events, o);
-    if (lane == 0 && events != 0) atomicAdd(d.blk_events + blk, events);
-  }
-}
-
-// Delivery after a window of integrated steps (networks without plastic
-// synapses, k_rk5_window): every spike emitted in the steps
-// T_b + first_off ... T_b + first_off + n - 1 (their ring slots) is
-// delivered at each of its delays D at once, into the accumulator slot of
-// step T_s + D, the slot the update of step T_s + D + 1 folds: the slot, and
-// the step, that the delivery of step T_s + D would use. Valid because a
-// window is no longer than the shortest delay + 1 steps, so no spike of a
-// window arrives inside it. Arrivals before step arrive_min are skipped
-// (made already by one-step deliveries, when steps switch to windows), and
-// so are the delays below min_delay, the shortest delay of a connection
-// whose source spikes (the others belong to Poisson generators, which reach
-// their targets by direct connections): such a group holds no edge, and its
-// slot stamp would name a step W + 1 or more before the slots this delivery
-// fills, i.e. a slot one of them shares, overwriting that slot's stamp.
+// Delivery before a window of integrated steps (networks without plastic
+// synapses, k_rk5_window): the accumulator slots of the steps
+// T_b + v_lo ... T_b + v_lo + v_n - 1 (T_b: the step of ctx, the window's
+// first step) receive every spike that arrives in them, at each delay D of
+// a spiking source (d.delays[di0 ...]): the spikes of step v - D, all
+// emitted before the window since a window is no longer than the shortest
+// such delay + 1 steps. The slot of step v is the one the update of step
+// v + 1 folds, filled as the one-step delivery of step v fills it, so each
+// slot gets all its input in one launch, where a delivery of the window's
+// own spikes at all their delays would add into every slot once per delay,
+// each time from HBM.
 //
-// Up to 32 steps (a window): the items, one per (spike, delay), are ordered
-// by the step whose slot receives them, then by the step that emitted them,
-// and warp w takes the items w, w + n_warps, w + 2 n_warps, ... of that
-// order. The warps advance through it together, so the accumulator slots in
-// use at any time are one or two, and stay in L2, where (step, delay) groups
-// taken all at once would add into up to W + max delay slots together (on a
-// network with 2.6e6 events per step and 16 MB slots, 50 slots: the atomics
-// then went to HBM at a tenth of the rate). More steps (the hand-over to
-// windows): warps take (step, delay) groups in turn, several warps per group.
+// The items (slot, delay, spike) are ordered by slot, then delay, and warp
+// w takes the items w, w + n_warps, w + 2 n_warps, ...: the warps go
+// through the order together, so one or two slots are written at a time
+// and stay in L2. The (slot, delay) pairs are taken 32 at a time, a lane
+// each, and a scan of their spike counts gives every pair's first item, so
+// a warp finds its own items without looking at the others'. A warp's
+// items are software-pipelined: an item's spike entry and edge range load
+// while the previous item's edges are in flight.
 __device__ __forceinline__ void deliver_window_blocks(const DeliverArgs &d, const StepCtx *ctx,
-                                                      long long first_off, int n,
-                                                      long long arrive_off, int min_delay,
-                                                      int blk, int nblk) {
+                                                      int v_lo, int v_n, int di0, int D_lo,
+                                                      int D_hi, int blk, int nblk) {
+  const unsigned full = 0xffffffffu;
   const long long T_b = ctx->T0 + ctx->it + 1;
   const int ring_b = ctx->ring_slot, acc_b = ctx->acc_out_slot;
   const int lane = threadIdx.x & 31;
   const int warp = (blk * (int)blockDim.x + (int)threadIdx.x) >> 5;
   const int n_warps = (nblk * (int)blockDim.x) >> 5;
-  // (the scan of 32 pairs' spike counts stays within int below 2^26 spikes per step)
-  if (n <= 32 && d.delay_di != nullptr && d.ring_C < (1 << 26)) {
-    deliver_window_ordered(d, T_b, ring_b, acc_b, first_off, n, arrive_off, min_delay, lane,
-                           warp, n_warps, blk);
-    return;
+  const int nd_s = d.nd - di0;                 // delays of spiking sources
+  const int P = v_n * nd_s;
+  // the delays in registers (lane i: delay di0 + i), where they fit
+  const int my_delay = (lane < nd_s) ? d.delays[di0 + lane] : 0;
+  // a quiet window: no spike in the emission steps T_b + v_lo - D_hi ...
+  // T_b + v_lo + v_n - 1 - D_lo, one round of independent loads
+  {
+    const int span = (v_n - 1) + (D_hi - D_lo) + 1;
+    int any = 0;
+    for (int i = lane; i < span; i += 32) {
+      const long long rel_s = (long long)v_lo - D_hi + i;
+      if (T_b + rel_s >= 0) any |= d.ring_cnt[ring_add(ring_b, rel_s, d.ring_R)];
+    }
+    if (!__any_sync(full, any != 0)) return;
   }
-  const int NG = n * d.nd;
-  const bool per_group = n_warps >= NG;
-  const int G = per_group ? n_warps / NG : 1;
+  // the round (32 pairs, a lane each): pair values, this warp's first item
+  // of each pair (r_j), the lanes with items left (m)
+  int p0 = -32, base = 0, total = 0;
+  int r_v = 0, r_di = 0, r_c = 0, r_j = 0, r_slot = 0;
+  unsigned m = 0u;
+  // the current pair's items: jj, jj + n_warps, ... below cl
+  bool in_pair = false;
+  int jj = 0, cl = 0, dil = 0, slot_l = 0, v_slot = 0;
+  // the previous item, its edge range loaded
+  bool has_prev = false;
+  unsigned long long pbeg = 0, pend = 0;
+  float ph = 0.0f;
+  long long *pacc = nullptr;
   unsigned long long events = 0;
-  if (!per_group || warp < G * NG) {
-    for (int gi = per_group ? warp % NG : warp; gi < NG; gi += per_group ? NG : n_warps) {
-      const int k = gi / d.nd, di = gi % d.nd;
-      const long long rel = first_off + k;           // T_s = T_b + rel
-      const int D = d.delays[di];
-      const long long rel_v = rel + D;               // the step whose slot receives it
-      // before the first step, made already, or a delay no spiking source has
-      if (T_b + rel < 0 || rel_v < arrive_off || D < min_delay) continue;
-      const long long V = T_b + rel_v;
-      const int slot = ring_add(ring_b, rel, d.ring_R);
-      // the warp's first entry is loaded together with the spike count
-      const int j0 = per_group ? warp / NG : 0;
-      const long long k0 = (long long)slot * d.ring_C + j0;
-      unsigned src0 = 0u;
-      float h0 = 0.0f;
-      if (j0 < d.ring_C) {
-        src0 = d.ring_src[k0];
-        h0 = d.ring_h[k0];
-      }
-      int c = d.ring_cnt[slot];
-      c = c < d.ring_C ? c : d.ring_C;
-      const int v_slot = ring_add(acc_b, rel_v, d.acc_slots);
-      long long *acc = d.acc + acc_slot_offset(v_slot, d.acc_slots, d.acc_par);
-      long long *stamp = d.acc_stamp != nullptr ? d.acc_stamp + v_slot : nullptr;
-      // one stamp store per (step, delay) group with spikes
-      if (j0 == 0 && c > 0 && lane == 0 && stamp != nullptr) *stamp = V;
-      for (int j = j0; j < c; j += G) {
-        unsigned src = src0;
-        float height = h0;
-        if (j != j0) {
-          const long long kk = (long long)slot * d.ring_C + j;
-          src = d.ring_src[kk];
-          height = d.ring_h[kk];
+  while (true) {
+    // the next item of this warp in the order (warp-uniform control flow)
+    bool got = false;
+    if (in_pair) {
+      jj += n_warps;
+      got = jj < cl;
+      in_pair = got;
+    }
+    while (!got) {
+      if (m == 0u) {
+        if (p0 >= 0) base = (base + total) % n_warps;
+        p0 += 32;
+        if (p0 >= P) break;
+        const int p = p0 + lane;
+        r_v = p / nd_s;
+        r_di = di0 + (p - r_v * nd_s);
+        r_c = 0;
+        r_slot = 0;
+        const int D = __shfl_sync(full, my_delay, (r_di - di0) & 31);
+        if (p < P) {
+          // emission step
+          const long long rel_s = (long long)v_lo + r_v - (nd_s <= 32 ? D : d.delays[r_di]);
+          if (T_b + rel_s >= 0) {
+            r_slot = ring_add(ring_b, rel_s, d.ring_R);
+            const int c = d.ring_cnt[r_slot];
+            r_c = c < d.ring_C ? c : d.ring_C;
+          }
         }
-        const unsigned long long e_i = (unsigned long long)src * d.nd + di;
-        const unsigned long long beg = d.grp_off[e_i], end = d.grp_off[e_i + 1];
-        if (lane == 0) events += end - beg;
-        deliver_static_edges(d, acc, beg, end, height, lane);
+        int incl = r_c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(full, incl, o);
+          if (lane >= o) incl += v;
+        }
+        total = __shfl_sync(full, incl, 31);
+        // item j of the pair is item base + (incl - r_c) + j of the order
+        r_j = warp - (base + incl - r_c) % n_warps;
+        if (r_j < 0) r_j += n_warps;
+        m = __ballot_sync(full, r_j < r_c);
+        continue;
+      }
+      const int l = __ffs(m) - 1;
+      m &= m - 1;
+      jj = __shfl_sync(full, r_j, l);
+      cl = __shfl_sync(full, r_c, l);
+      dil = __shfl_sync(full, r_di, l);
+      slot_l = __shfl_sync(full, r_slot, l);
+      const long long rv = (long long)v_lo + __shfl_sync(full, r_v, l);
+      v_slot = ring_add(acc_b, rv, d.acc_slots);
+      // one stamp store per (slot, delay) pair with spikes: by the warp of its first item
+      if (jj == 0 && lane == 0 && d.acc_stamp != nullptr) d.acc_stamp[v_slot] = T_b + rv;
+      in_pair = true;
+      got = true;
+    }
+    if (!got) break;
+    // this item's spike entry
+    const long long kk = (long long)slot_l * d.ring_C + jj;
+    const unsigned src = d.ring_src[kk];
+    const float height = d.ring_h[kk];
+    // the previous item's first 256 edges, loaded before this item's edge range
+    unsigned sl[8];
+    float wv[8];
+    const int n_mine = has_prev ? (int)(pend - pbeg < 256ull ? pend - pbeg : 256ull) - lane : 0;
+    {
+      const unsigned *ps = d.e_slot + pbeg + lane;
+      const float *pw = d.e_w + pbeg + lane;
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        if (32 * u < n_mine) {
+          sl[u] = __ldcs(ps + 32 * u);
+          wv[u] = __ldcs(pw + 32 * u);
+        }
       }
     }
+    const unsigned long long e_i = (unsigned long long)src * d.nd + dil;
+    const unsigned long long beg = d.grp_off[e_i], end = d.grp_off[e_i + 1];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      if (32 * u < n_mine)
+        atomicAdd((unsigned long long *)(pacc + sl[u]),
+                  (unsigned long long)ng_to_fixed(ph * wv[u]));
+    }
+    if (has_prev && pend > pbeg + 256) deliver_static_edges(d, pacc, pbeg + 256, pend, ph, lane);
+    if (lane == 0) events += end - beg;
+    pbeg = beg;
+    pend = end;
+    ph = height;
+    pacc = d.acc + acc_slot_offset(v_slot, d.acc_slots, d.acc_par);
+    has_prev = true;
   }
+  if (has_prev) deliver_static_edges(d, pacc, pbeg, pend, ph, lane);
   if (d.blk_events != nullptr) {
     // per warp, a reduction whose result is not waited for (see block_add_u64)
-    for (int o = 16; o > 0; o >>= 1) events += __shfl_down_sync(0xffffffffu, events, o);
+    for (int o = 16; o > 0; o >>= 1) events += __shfl_down_sync(full, events, o);
     if (lane == 0 && events != 0) atomicAdd(d.blk_events + blk, events);
   }
 }

@@ -23,6 +23,7 @@
 // its own device-resident copy of the step context (k_step_prologue).
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdlib.h>
 #include "ngpu_device.h"
 #include "ngpu_kernels.h"
 #include "ngpu_models.h"
@@ -548,11 +549,21 @@ k_deliver(DeliverArgs d, SynGroupTable syn, StepCtx *ctx) {
   deliver_blocks<PLASTIC>(d, syn, ctx, blockIdx.x, gridDim.x);
 }
 
+// the register cap of the window delivery (blocks per SM): 3, or 2 where
+// NGB200_WINDOW_DELIVER_BLOCKS says so
+static int WindowDeliverCap() {
+  static const int cap = [] {
+    const char *e = getenv("NGB200_WINDOW_DELIVER_BLOCKS");
+    return (e != nullptr && atoi(e) == 2) ? 2 : 3;
+  }();
+  return cap;
+}
+
 // Spike bookkeeping of a window, by the threads of one block: the spikes of
 // the steps T_b + c_lo ... T_b + c_hi - 1 (T_b the step of ctx) are counted
-// into ctx->n_spikes, and the ring slots of the steps T_b + bk.first_off ...
-// T_b + bk.first_off + bk.n - 1 are emptied for reuse (their spikes have
-// been delivered at every delay).
+// into ctx->n_spikes, then the ring slots of the steps T_b + first_off ...
+// T_b + first_off + n - 1 are emptied for the steps that will write them
+// (the two ranges may share ring slots: counted first).
 struct WindowBook {
   long long first_off;
   int n;
@@ -564,15 +575,10 @@ __device__ __forceinline__ void window_book_block(int *ring_cnt, int ring_R, int
   __shared__ unsigned long long s_cnt[256];
   const long long T_b = ctx->T0 + ctx->it + 1;
   unsigned long long cnt = 0;
-  for (int k = threadIdx.x; k < bk.n; k += blockDim.x) {
-    const long long rel = bk.first_off + k;
+  for (long long rel = bk.c_lo + threadIdx.x; rel < bk.c_hi; rel += blockDim.x) {
     if (T_b + rel < 0) continue;
-    const int slot = ring_add(ctx->ring_slot, rel, ring_R);
-    if (rel >= bk.c_lo && rel < bk.c_hi) {
-      const int c = ring_cnt[slot];
-      cnt += (unsigned long long)(c < ring_C ? c : ring_C);
-    }
-    ring_cnt[slot] = 0;
+    const int c = ring_cnt[ring_add(ctx->ring_slot, rel, ring_R)];
+    cnt += (unsigned long long)(c < ring_C ? c : ring_C);
   }
   s_cnt[threadIdx.x] = cnt;
   __syncthreads();
@@ -580,17 +586,26 @@ __device__ __forceinline__ void window_book_block(int *ring_cnt, int ring_R, int
     for (int j = 1; j < (int)blockDim.x; j++) cnt += s_cnt[j];
     ctx->n_spikes += cnt;
   }
+  for (int k = threadIdx.x; k < bk.n; k += blockDim.x) {
+    const long long rel = bk.first_off + k;
+    if (T_b + rel >= 0) ring_cnt[ring_add(ctx->ring_slot, rel, ring_R)] = 0;
+  }
 }
 
-// Delivery after a window of integrated steps: the spikes of the steps
-// T_b + first_off ... T_b + first_off + n - 1, T_b the step of ctx (the
-// window's first step), delivered at all their delays at once; the last
-// block to finish (every block has then read the ring) does the window's
-// bookkeeping (one launch less per window).
-__global__ void __launch_bounds__(256, NGPU_DELIVER_MINB)
-k_deliver_window(DeliverArgs d, StepCtx *ctx, long long first_off, int n, long long arrive_off,
-                 int min_delay, WindowBook bk) {
-  deliver_window_blocks(d, ctx, first_off, n, arrive_off, min_delay, blockIdx.x, gridDim.x);
+// Delivery before a window of integrated steps: the accumulator slots of
+// the steps T_b + v_lo ... T_b + v_lo + v_n - 1 (T_b: the step of ctx, the
+// window's first step) filled from the spike ring at the delays
+// d.delays[di0 ...]; the last block to finish (every block has then read
+// the ring) does the window's bookkeeping (one launch less per window).
+// MINB: resident blocks per SM the registers are capped for. The window
+// delivery keeps two items in flight per warp (105 registers uncapped): 3
+// blocks per SM spill a few words, 2 blocks do not;
+// NGB200_WINDOW_DELIVER_BLOCKS picks one (default 3).
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB)
+k_deliver_window(DeliverArgs d, StepCtx *ctx, int v_lo, int v_n, int di0, int D_lo, int D_hi,
+                 WindowBook bk) {
+  deliver_window_blocks(d, ctx, v_lo, v_n, di0, D_lo, D_hi, blockIdx.x, gridDim.x);
   __shared__ bool s_last;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -609,17 +624,20 @@ __global__ void k_window_book(int *ring_cnt, int ring_R, int ring_C, StepCtx *ct
   window_book_block(ring_cnt, ring_R, ring_C, ctx, bk);
 }
 
-void LaunchDeliverWindow(const DeliverArgs &d, StepCtx *ctx, long long first_off, int n,
-                         long long arrive_off, int min_delay, long long book_first_off,
-                         int book_n, long long c_lo, long long c_hi, int n_blocks,
-                         cudaStream_t s) {
+void LaunchDeliverWindow(const DeliverArgs &d, StepCtx *ctx, int v_lo, int v_n, int di0,
+                         int D_lo, int D_hi, long long book_first_off, int book_n,
+                         long long c_lo, long long c_hi, int n_blocks, cudaStream_t s) {
   const WindowBook bk = {book_first_off, book_n, c_lo, c_hi};
-  // no connection from a spiking source (min_delay 0): nothing to deliver
-  if (d.nd <= 0 || n <= 0 || min_delay <= 0) {
+  // no slot to fill, or no connection from a spiking source (di0 out of
+  // range): the bookkeeping alone
+  if (d.nd <= 0 || v_n <= 0 || di0 < 0 || di0 >= d.nd) {
     k_window_book<<<1, 256, 0, s>>>(d.ring_cnt_w, d.ring_R, d.ring_C, ctx, bk);
     return;
   }
-  k_deliver_window<<<n_blocks, 256, 0, s>>>(d, ctx, first_off, n, arrive_off, min_delay, bk);
+  if (WindowDeliverCap() == 2)
+    k_deliver_window<2><<<n_blocks, 256, 0, s>>>(d, ctx, v_lo, v_n, di0, D_lo, D_hi, bk);
+  else
+    k_deliver_window<3><<<n_blocks, 256, 0, s>>>(d, ctx, v_lo, v_n, di0, D_lo, D_hi, bk);
 }
 
 // Resident delivery blocks per SM, at most 3: the delivery runs beside the
@@ -637,6 +655,18 @@ int DeliverOccupancy() {
   int nb = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_deliver<false>, 256, 0) != cudaSuccess)
     return 8;
+  return nb > 0 ? nb : 1;
+}
+
+// Resident blocks per SM of the window delivery: its grid is resident at
+// once, so that its warps go through the items in order together.
+int DeliverWindowOccupancy() {
+  int nb = 0;
+  const cudaError_t e =
+      WindowDeliverCap() == 2
+          ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_deliver_window<2>, 256, 0)
+          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_deliver_window<3>, 256, 0);
+  if (e != cudaSuccess) return WindowDeliverCap();
   return nb > 0 ? nb : 1;
 }
 

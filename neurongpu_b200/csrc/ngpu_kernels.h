@@ -112,17 +112,16 @@ void LaunchPoissonLarge(const GroupArgs &g, const InputArgs &in, StepCtx *ctx,
 // synaptic delivery and plasticity
 void LaunchDeliver(const DeliverArgs &d, const SynGroupTable &syn,
                    StepCtx *ctx, int n_blocks, cudaStream_t s);
-// after a window: the spikes of the steps T_b + first_off ...
-// T_b + first_off + n - 1 (T_b: the step of ctx) delivered at all their
-// delays of min_delay or more (the shortest delay of a spiking source's
-// connection), arrivals from step T_b + arrive_off on; then, in the same
-// launch, the spike count of the steps T_b + c_lo ... T_b + c_hi - 1 into
-// ctx and the ring slots of the steps T_b + book_first_off ... + book_n - 1
-// emptied
-void LaunchDeliverWindow(const DeliverArgs &d, StepCtx *ctx, long long first_off, int n,
-                         long long arrive_off, int min_delay, long long book_first_off,
-                         int book_n, long long c_lo, long long c_hi, int n_blocks,
-                         cudaStream_t s);
+// around a window: the accumulator slots of the steps T_b + v_lo ...
+// T_b + v_lo + v_n - 1 (T_b: the step of ctx) filled from the spike ring at
+// the delays d.delays[di0 ...] (those of spiking sources, D_lo ... D_hi
+// steps); then, in the
+// same launch, the spike count of the steps T_b + c_lo ... T_b + c_hi - 1
+// into ctx and the ring slots of the steps T_b + book_first_off ...
+// + book_n - 1 emptied
+void LaunchDeliverWindow(const DeliverArgs &d, StepCtx *ctx, int v_lo, int v_n, int di0,
+                         int D_lo, int D_hi, long long book_first_off, int book_n,
+                         long long c_lo, long long c_hi, int n_blocks, cudaStream_t s);
 // spike exchange of partitioned networks (ngpu_remote.cu)
 void LaunchPackRemote(const int *ring_cnt, const unsigned *ring_src, const float *ring_h,
                       int ring_R, int ring_C, const StepCtx *ctx, int n_steps,
@@ -134,6 +133,7 @@ void LaunchUnpackRemote(const unsigned *in, long long count, const int *lut, int
 // resident 256-thread delivery blocks per SM (grid = SMs x this)
 int DeliverBlocksPerSM();
 int DeliverOccupancy();
+int DeliverWindowOccupancy();
 // dendritic-delay arrivals of this step (before the delivery kernel)
 void LaunchRevArrive(const DeliverArgs &d, StepCtx *ctx, cudaStream_t s);
 void LaunchStdpPost(const DeliverArgs &d, const SynGroupTable &syn,
