@@ -377,7 +377,7 @@ class NeuronGPU {
   // (BUSY_WINDOW, where the network can run them). From step
   // kQueueRecheckSteps on (past the start's transient) the candidates take
   // turns, two chunks each, of which the second is timed (the first
-  // captures the mode's graph and makes the hand-over to windows), until
+  // captures the mode's graph), until
   // each has kDeliveryTrialSteps timed steps, so that a drift of the
   // network's activity weighs on all alike.
   enum BusyMode { BUSY_FORK = 0, BUSY_SERIAL = 1, BUSY_WINDOW = 2 };
