@@ -1507,7 +1507,8 @@ void NeuronGPU::BuildDevice() {
   }
   n_sm_ = n_sm;
   deliver_blocks_ = n_sm * DeliverBlocksPerSM();
-  // the delivery after a window runs alone: every resident block
+  // a serial step's delivery runs alone: every resident block; so does the
+  // delivery before a window, with its own register cap
   solo_deliver_blocks_ = n_sm * DeliverOccupancy();
   window_deliver_blocks_ = n_sm * DeliverWindowOccupancy();
   n_evt_blocks_ = std::max(std::max(deliver_blocks_, solo_deliver_blocks_), window_deliver_blocks_);
@@ -1980,8 +1981,8 @@ void NeuronGPU::EnqueueWindow(int k0, int w, int W, int n_steps) {
       if (bh.groups[0] == g) LaunchRk5BatchWindow(MakeRk5Batch(bh), ctxs, w, stream_);
       continue;
     }
-    if (!LaunchRk5Window(g->mi->rk5_model, g->n_port, MakeGroupArgs(g), MakeInputArgs(g),
-                         MakePushArgs(g), ctxs, w, stream_))
+    if (!LaunchRk5Window(g->mi->rk5_model, g->n_port, delivery_busy_, MakeGroupArgs(g),
+                         MakeInputArgs(g), MakePushArgs(g), ctxs, w, stream_))
       throw ngpu_exception("internal error: no window kernel for this node group");
   }
   if (ktime_) KEvent(k0, 2);

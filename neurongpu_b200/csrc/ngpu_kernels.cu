@@ -52,16 +52,16 @@ bool LaunchRk5Update(int model, int np, const GroupArgs &g,
   }
 }
 
-bool LaunchRk5Window(int model, int np, const GroupArgs &g, const InputArgs &in,
+bool LaunchRk5Window(int model, int np, bool free_lanes, const GroupArgs &g, const InputArgs &in,
                      const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s) {
   if (g.n <= 0) return true;
   switch (model) {
-    case RK5_AEIF_COND_BETA: return LaunchRk5WindowAeifCondBeta(np, g, in, pa, ctxs, W, s);
-    case RK5_AEIF_COND_ALPHA: return LaunchRk5WindowAeifCondAlpha(np, g, in, pa, ctxs, W, s);
+    case RK5_AEIF_COND_BETA: return LaunchRk5WindowAeifCondBeta(np, free_lanes, g, in, pa, ctxs, W, s);
+    case RK5_AEIF_COND_ALPHA: return LaunchRk5WindowAeifCondAlpha(np, free_lanes, g, in, pa, ctxs, W, s);
     case RK5_AEIF_PSC_ALPHA:
     case RK5_AEIF_PSC_EXP:
-    case RK5_AEIF_PSC_DELTA: return LaunchRk5WindowAeifPsc(model, np, g, in, pa, ctxs, W, s);
-    case RK5_IZHIKEVICH_COND_BETA: return LaunchRk5WindowIzhCondBeta(np, g, in, pa, ctxs, W, s);
+    case RK5_AEIF_PSC_DELTA: return LaunchRk5WindowAeifPsc(model, np, free_lanes, g, in, pa, ctxs, W, s);
+    case RK5_IZHIKEVICH_COND_BETA: return LaunchRk5WindowIzhCondBeta(np, free_lanes, g, in, pa, ctxs, W, s);
     default: return false;
   }
 }

@@ -38,16 +38,20 @@ bool LaunchRk5IzhCondBeta(int np, const GroupArgs &g, const InputArgs &in, const
                           StepCtx *ctx, cudaStream_t s, const DeliverArgs *del, int n_del);
 // several steps per launch: one RK5 group through the W steps whose step
 // contexts are ctxs[0 .. W-1] (plain controller, 1-4 ports; false if the
-// model or port count has no window kernel)
-bool LaunchRk5Window(int model, int np, const GroupArgs &g, const InputArgs &in,
+// model or port count has no window kernel); free_lanes: a lane whose step
+// ended begins its next step while the others go on (busy networks)
+bool LaunchRk5Window(int model, int np, bool free_lanes, const GroupArgs &g, const InputArgs &in,
                      const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s);
-bool LaunchRk5WindowAeifCondBeta(int np, const GroupArgs &g, const InputArgs &in,
-                                 const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s);
-bool LaunchRk5WindowAeifCondAlpha(int np, const GroupArgs &g, const InputArgs &in,
-                                  const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s);
-bool LaunchRk5WindowAeifPsc(int model, int np, const GroupArgs &g, const InputArgs &in,
-                            const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s);
-bool LaunchRk5WindowIzhCondBeta(int np, const GroupArgs &g, const InputArgs &in,
+bool LaunchRk5WindowAeifCondBeta(int np, bool free_lanes, const GroupArgs &g,
+                                 const InputArgs &in, const PushArgs &pa, StepCtx *ctxs, int W,
+                                 cudaStream_t s);
+bool LaunchRk5WindowAeifCondAlpha(int np, bool free_lanes, const GroupArgs &g,
+                                  const InputArgs &in, const PushArgs &pa, StepCtx *ctxs, int W,
+                                  cudaStream_t s);
+bool LaunchRk5WindowAeifPsc(int model, int np, bool free_lanes, const GroupArgs &g,
+                            const InputArgs &in, const PushArgs &pa, StepCtx *ctxs, int W,
+                            cudaStream_t s);
+bool LaunchRk5WindowIzhCondBeta(int np, bool free_lanes, const GroupArgs &g, const InputArgs &in,
                                 const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s);
 // whether the variant's update grid can carry the delivery blocks (the
 // register-capped one-block-per-tile variants; not the persistent ones)

@@ -9,9 +9,9 @@ bool LaunchRk5AeifCondAlpha(int np, const GroupArgs &g, const InputArgs &in, con
   return launch_rk5_model<AeifCondAlpha>(np, g, in, pa, ctx, s, del, n_del);
 }
 
-bool LaunchRk5WindowAeifCondAlpha(int np, const GroupArgs &g, const InputArgs &in,
-                                  const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s) {
-  return launch_rk5_window_model<AeifCondAlpha>(np, g, in, pa, ctxs, W, s);
+bool LaunchRk5WindowAeifCondAlpha(int np, bool free_lanes, const GroupArgs &g, const InputArgs &in,
+                       const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s) {
+  return launch_rk5_window_model<AeifCondAlpha>(np, free_lanes, g, in, pa, ctxs, W, s);
 }
 
 }  // namespace ngpu

@@ -9,9 +9,9 @@ bool LaunchRk5AeifCondBeta(int np, const GroupArgs &g, const InputArgs &in, cons
   return launch_rk5_model<AeifCondBeta>(np, g, in, pa, ctx, s, del, n_del);
 }
 
-bool LaunchRk5WindowAeifCondBeta(int np, const GroupArgs &g, const InputArgs &in,
-                                 const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s) {
-  return launch_rk5_window_model<AeifCondBeta>(np, g, in, pa, ctxs, W, s);
+bool LaunchRk5WindowAeifCondBeta(int np, bool free_lanes, const GroupArgs &g, const InputArgs &in,
+                       const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s) {
+  return launch_rk5_window_model<AeifCondBeta>(np, free_lanes, g, in, pa, ctxs, W, s);
 }
 
 }  // namespace ngpu

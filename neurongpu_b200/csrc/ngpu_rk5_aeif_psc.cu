@@ -15,13 +15,16 @@ bool LaunchRk5AeifPsc(int model, int np, const GroupArgs &g, const InputArgs &in
   }
 }
 
-bool LaunchRk5WindowAeifPsc(int model, int np, const GroupArgs &g, const InputArgs &in,
-                            const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s) {
+bool LaunchRk5WindowAeifPsc(int model, int np, bool free_lanes, const GroupArgs &g,
+                            const InputArgs &in, const PushArgs &pa, StepCtx *ctxs, int W,
+                            cudaStream_t s) {
   switch (model) {
-    case RK5_AEIF_PSC_ALPHA: return launch_rk5_window_model<AeifPscAlpha>(np, g, in, pa, ctxs, W, s);
-    case RK5_AEIF_PSC_EXP: return launch_rk5_window_model<AeifPscExp>(np, g, in, pa, ctxs, W, s);
+    case RK5_AEIF_PSC_ALPHA:
+      return launch_rk5_window_model<AeifPscAlpha>(np, free_lanes, g, in, pa, ctxs, W, s);
+    case RK5_AEIF_PSC_EXP:
+      return launch_rk5_window_model<AeifPscExp>(np, free_lanes, g, in, pa, ctxs, W, s);
     case RK5_AEIF_PSC_DELTA:
-      launch_rk5_window<AeifPscDelta<1>, 1>(g, in, pa, ctxs, W, s);
+      launch_rk5_window<AeifPscDelta<1>, 1>(free_lanes, g, in, pa, ctxs, W, s);
       return true;
     default: return false;
   }

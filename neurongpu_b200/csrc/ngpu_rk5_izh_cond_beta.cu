@@ -9,9 +9,9 @@ bool LaunchRk5IzhCondBeta(int np, const GroupArgs &g, const InputArgs &in, const
   return launch_rk5_model<IzhCondBeta>(np, g, in, pa, ctx, s, del, n_del);
 }
 
-bool LaunchRk5WindowIzhCondBeta(int np, const GroupArgs &g, const InputArgs &in,
-                                const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s) {
-  return launch_rk5_window_model<IzhCondBeta>(np, g, in, pa, ctxs, W, s);
+bool LaunchRk5WindowIzhCondBeta(int np, bool free_lanes, const GroupArgs &g, const InputArgs &in,
+                       const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s) {
+  return launch_rk5_window_model<IzhCondBeta>(np, free_lanes, g, in, pa, ctxs, W, s);
 }
 
 }  // namespace ngpu

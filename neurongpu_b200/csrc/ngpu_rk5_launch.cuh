@@ -149,8 +149,8 @@ static bool launch_rk5(const GroupArgs &g, const InputArgs &in, const PushArgs &
 // The window kernel (several steps per launch) with the register cap of the
 // group's chosen single-step variant.
 template <class M, int NP>
-static void launch_rk5_window(const GroupArgs &g, const InputArgs &in, const PushArgs &pa,
-                              StepCtx *ctxs, int W, cudaStream_t s) {
+static void launch_rk5_window(bool free_lanes, const GroupArgs &g, const InputArgs &in,
+                              const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s) {
   const dim3 grid((g.n + NGPU_BLOCK - 1) / NGPU_BLOCK), block(NGPU_BLOCK);
   if (!g.all_uniform) {
     launch_pdl(k_rk5_window<M, NP, false, 1>, grid, block, s, g, in, pa, ctxs, W);
@@ -165,20 +165,27 @@ static void launch_rk5_window(const GroupArgs &g, const InputArgs &in, const Pus
     case 6:
     case 7:
     case 8: launch_pdl(k_rk5_window<M, NP, true, 4>, grid, block, s, g, in, pa, ctxs, W); break;
-    default: launch_pdl(k_rk5_window<M, NP, true, 6>, grid, block, s, g, in, pa, ctxs, W); break;
+    default:
+      // busy networks: lanes go through the window's steps at their own pace
+      if (free_lanes)
+        launch_pdl(k_rk5_window<M, NP, true, 6, true>, grid, block, s, g, in, pa, ctxs, W);
+      else
+        launch_pdl(k_rk5_window<M, NP, true, 6>, grid, block, s, g, in, pa, ctxs, W);
+      break;
   }
 }
 
 // windows: 1-4 ports (the group kinds that WindowSteps admits)
 template <template <int> class MT>
-static bool launch_rk5_window_model(int np, const GroupArgs &g, const InputArgs &in,
-                                    const PushArgs &pa, StepCtx *ctxs, int W, cudaStream_t s) {
+static bool launch_rk5_window_model(int np, bool free_lanes, const GroupArgs &g,
+                                    const InputArgs &in, const PushArgs &pa, StepCtx *ctxs,
+                                    int W, cudaStream_t s) {
   switch (np) {
     case 0:
-    case 1: launch_rk5_window<MT<1>, 1>(g, in, pa, ctxs, W, s); return true;
-    case 2: launch_rk5_window<MT<2>, 2>(g, in, pa, ctxs, W, s); return true;
-    case 3: launch_rk5_window<MT<3>, 3>(g, in, pa, ctxs, W, s); return true;
-    case 4: launch_rk5_window<MT<4>, 4>(g, in, pa, ctxs, W, s); return true;
+    case 1: launch_rk5_window<MT<1>, 1>(free_lanes, g, in, pa, ctxs, W, s); return true;
+    case 2: launch_rk5_window<MT<2>, 2>(free_lanes, g, in, pa, ctxs, W, s); return true;
+    case 3: launch_rk5_window<MT<3>, 3>(free_lanes, g, in, pa, ctxs, W, s); return true;
+    case 4: launch_rk5_window<MT<4>, 4>(free_lanes, g, in, pa, ctxs, W, s); return true;
     default: return false;
   }
 }

@@ -400,3 +400,60 @@ def test_windows_mixed_models_per_connection_poisson(ngpu):
         assert np.array_equal(vw, vs)
         for a, b in zip(timew, times):
             assert np.array_equal(a, b)
+
+
+def _busy_net(ngpu, env):
+    """40,000 aeif_cond_beta at about 25 Hz with in-degree 1000: about 1e5
+    delivered events per step, a busy network (the event rate is checked
+    after every chunk of the first 1000 steps)."""
+    import os
+    keys = ("NGB200_WINDOW", "NGB200_BUSY_MODE")
+    old = {k: os.environ.get(k) for k in keys}
+    for k in keys:
+        os.environ.pop(k, None)
+    os.environ.update(env)
+    try:
+        b = ngpu.default_binding()
+        b.Reset()
+        b.SetVerbosityLevel(0)
+        ngpu.SetKernelStatus("rnd_seed", 17)
+        n = 40000
+        pg = ngpu.Create("poisson_generator")
+        ngpu.SetStatus(pg, "rate", 20000.0)
+        nrn = ngpu.Create("aeif_cond_beta", n, 2)
+        ngpu.SetStatus(nrn, {"E_rev": [0.0, -85.0], "tau_rise": [1.0, 1.0],
+                             "tau_decay": [1.0, 1.0]})
+        ngpu.Connect(pg, nrn, {"rule": "all_to_all"}, {"weight": 0.5, "delay": 0.1,
+                                                       "receptor": 0})
+        ngpu.Connect(nrn[0:32000], nrn, {"rule": "fixed_indegree", "indegree": 800},
+                     {"weight": 0.05, "delay": 1.0, "receptor": 0})
+        ngpu.Connect(nrn[32000:n], nrn, {"rule": "fixed_indegree", "indegree": 200},
+                     {"weight": 0.35, "delay": 1.5, "receptor": 1})
+        ngpu.ActivateSpikeCount(nrn)
+        ngpu.Simulate(150.0)
+        ev0 = b.DeliveredEvents()
+        ngpu.Simulate(50.0)
+        ev_step = (b.DeliveredEvents() - ev0) / 500.0
+        counts = ngpu.GetNeuronIntVarArray(nrn.i0, nrn.n, "spike_count")
+        v = np.asarray(ngpu.GetNeuronVar(nrn.i0, nrn.n, "V_m"), dtype=np.float32).ravel()
+        return v, counts, b.TotalSpikes(), b.KernelsPerStep(), ev_step
+    finally:
+        for k in keys:
+            if old[k] is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = old[k]
+
+
+def test_busy_network_windows_match_one_step_per_launch(ngpu):
+    """A busy network in windows (its lanes going through a window's steps
+    each at its own pace, the delivery before each window) against one step
+    per launch: every membrane potential, every spike count and the spike
+    total agree bit for bit."""
+    vw, cw, tw, kw, ew = _busy_net(ngpu, {"NGB200_BUSY_MODE": "2"})
+    vs, cs, ts, ks, es = _busy_net(ngpu, {"NGB200_WINDOW": "0"})
+    assert ew > 65536 and es == ew          # busy, the same events
+    assert kw < 0.5 < ks                    # the first run used windows
+    assert tw == ts == int(cw.sum())
+    assert np.array_equal(cw, cs)
+    assert np.array_equal(vw.view(np.int32), vs.view(np.int32))
