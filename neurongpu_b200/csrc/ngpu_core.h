@@ -637,7 +637,7 @@ class NeuronGPU {
   void BuildRemoteTables();
   int window_w_ = 0;            // W of the last chunk (0: one step per launch)
   int solo_deliver_blocks_ = 0; // grid of a delivery that runs alone (serial steps)
-  int window_deliver_blocks_ = 0;   // grid of the delivery after a window (all resident)
+  int window_deliver_blocks_ = 0;   // grid of the delivery before a window (all resident)
   int n_sm_ = 148;              // multiprocessors of the device (queried at calibration)
   int n_evt_blocks_ = 0;        // delivery event counters (max of both grids)
 
