@@ -66,7 +66,9 @@ def build_network(ngpu, cfg, seed=1234, eps_param=True):
 
 
 class ClockSampler(object):
-    """nvidia-smi clock / throttle samples during the timed region."""
+    """nvidia-smi clock / throttle samples during the timed region: started
+    before it (nvidia-smi takes a moment to start), every 50 ms; only the
+    samples that arrive after mark() count."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -75,12 +77,16 @@ class ClockSampler(object):
         self.index = index
         self.proc = None
         self.lines = []
+        self.t_mark = 0.0
+
+    def mark(self):
+        self.t_mark = time.monotonic()
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -89,7 +95,7 @@ class ClockSampler(object):
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
     def stop(self):
         if self.proc is None:
@@ -101,7 +107,9 @@ class ClockSampler(object):
             self.proc.kill()
         sm, smax, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for t, ln in list(self.lines):
+            if t < self.t_mark:
+                continue
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 9:
                 continue
@@ -467,12 +475,13 @@ def run_network(ngpu, b, cfg, args, world, step_ms, steps, warmup):
     connect_s = time.perf_counter() - t_build
     ngpu.Calibrate()
     build_s = time.perf_counter() - t_build
+    sampler = ClockSampler(0)
+    sampler.start()
     for _ in range(warmup):
         ngpu.Simulate(step_ms)
     ev0, evals0, spikes0 = b.DeliveredEvents(), b.StageEvaluations(), b.TotalSpikes()
     barrier(world)
-    sampler = ClockSampler(0)
-    sampler.start()
+    sampler.mark()
     dev_ms = 0.0
     for _ in range(steps):
         ngpu.Simulate(step_ms)
